@@ -1,0 +1,360 @@
+"""Throughput benchmark of the wavefront path integrator (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C]
+
+Workload: configuration 1 by default (64 spheres + 2-triangle plane + 4 sphere emitters,
+1024x1024, 64 spp per frame, depth 8, NEE+MIS). One step = one progressive frame of the
+whole image. Metric: Mrays/s of canonical queries (camera + continuation closest hits +
+contributing shadow rays); Mpaths/s is reported beside it.
+
+  value   device time (CUDA events on the session's stream, summed over the K frames), the
+          scene already resident in HBM, L2 flushed between steps; N > 1: N independent
+          replicas (own seeds), max device time over ranks, rays summed over ranks.
+  e2e     through the C ABI with host buffers: camera upload, render, wait, readback of the
+          W x H x 3 FP32 radiance into pinned host memory, wall clock per step.
+  roofline  the extend (closest-hit) stage, timed live with events around its launches.
+  cpu_baseline  the oracle's restatement of the reference integrator (two traces per bounce,
+          linear primitive scan) on the host cores, on a bounded pixel sample.
+
+--impl reference runs that CPU restatement as the reference arm (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-pathed_b200"))
+
+WORKLOADS = {
+    0: dict(name="cornell-box-36tri", res=(512, 512), spp=16, depth=5),
+    1: dict(name="spheres-64+4-emitters-plane", res=(1024, 1024), spp=64, depth=8),
+    2: dict(name="icosphere-1310720tri-env2048x1024", res=(1920, 1080), spp=32, depth=6),
+    3: dict(name="slit-room-2002tri+icosphere-1310720tri", res=(1024, 1024), spp=16, depth=10),
+}
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        cmd = ["nvidia-smi", "-i", str(self.index),
+               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+               "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_run(cfg, seconds_target, threads=0, seed=0x5EED):
+    """Oracle restatement of the reference integrator (reference trace convention, linear scan)
+    on a bounded pixel sample. Returns (Mrays/s, Mpaths/s, sample description, threads)."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc  # CPU baseline leg only
+    import pathed
+
+    wl = WORKLOADS[cfg]
+    w, h = wl["res"]
+    s = pathed.Session(w, h)
+    s.load_config(cfg)
+    sc = s.export_scene()
+    s.close()
+    o = orc.Oracle()
+    osc = o.scene(sc)
+    nthreads = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(1)
+    # calibrate on a small sample, then size the run to about `seconds_target`
+    spp = wl["spp"]
+    npx = 64
+    t0 = time.perf_counter()
+    pix = np.sort(rng.choice(w * h, npx, replace=False)).astype(np.int32)
+    o.render(osc, sc["camera"], w, h, pix, spp, wl["depth"], nee=True, seed=seed, trace_once=False,
+             threads=nthreads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    npx = int(min(w * h, max(64, npx * seconds_target / dt)))
+    pix = np.sort(rng.choice(w * h, npx, replace=False)).astype(np.int32)
+    t0 = time.perf_counter()
+    _, _, counts = o.render(osc, sc["camera"], w, h, pix, spp, wl["depth"], nee=True, seed=seed, trace_once=False,
+                            threads=nthreads)
+    dt = time.perf_counter() - t0
+    rays = float(counts[0] + counts[1])
+    paths = float(npx * spp)
+    sample = f"{npx} seeded pixels x {spp} spp of the {w}x{h} frame ({paths:.0f} paths, {rays:.0f} canonical rays)"
+    return rays / dt / 1e6, paths / dt / 1e6, sample, nthreads, dt
+
+
+def run_reference(args):
+    world, rank, _ = _dist_init()
+    if rank != 0:
+        return 0
+    wl = WORKLOADS[args.config]
+    vals = []
+    for _ in range(args.warmup):
+        cpu_reference_run(args.config, 1.0)
+    per = []
+    for _ in range(args.steps):
+        mr, mp, sample, thr, dt = cpu_reference_run(args.config, 8.0)
+        vals.append(mr)
+        per.append((mp, dt))
+    v = sum(vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": "Mrays/s", "value": v, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(p[1] for p in per) / len(per),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "mpaths_per_s": sum(p[0] for p in per) / len(per),
+        "config": {"workload": wl["name"], "resolution": list(wl["res"]), "spp": wl["spp"], "max_depth": wl["depth"],
+                   "nee": True, "parallelism": "cpu-threads"},
+        "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import pathed
+
+    world, rank, local = _dist_init()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    wl = WORKLOADS[args.config]
+    w, h = wl["res"]
+    spp = args.spp or wl["spp"]
+    s = pathed.Session(w, h)
+    s.set_device(local)  # the library's CUDA runtime keeps its own current device
+    s.load_config(args.config)
+    s.set_seed(0x5EED + 7919 * rank)
+    if args.wave_paths:
+        s.set_launch(wave_paths=args.wave_paths)
+    counts = s.counts()
+
+    # one untimed frame with work counters for the algorithmic-bytes accounting
+    s.set_profiling(stage_timing=True, work_counters=True)
+    s.render(spp)
+    prof_count = s.profile()
+    st_count = s.stats()
+    s.set_profiling(stage_timing=True, work_counters=False)
+    for _ in range(args.warmup):
+        s.render(spp)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    dev_ms = 0.0
+    rays = paths = 0
+    stage_ms = {k: 0.0 for k in pathed.STAGES}
+    stage_launches = {k: 0 for k in pathed.STAGES}
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between steps (outside the frame's events)
+        torch.cuda.synchronize()
+        ms = s.render(spp)
+        dev_ms += ms
+        st = s.stats()
+        rays += st["rays_extend"] + st["rays_shadow"]
+        paths += st["rays_camera"]
+        p = s.profile()
+        for k in pathed.STAGES:
+            stage_ms[k] += p["stage_ms"][k]
+            stage_launches[k] += p["stage_launches"][k]
+    barrier()
+    clk = clocks.stop()
+    t_max = dev_ms
+    rays_all, paths_all = float(rays), float(paths)
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        rr = torch.tensor([rays_all, paths_all], dtype=torch.float64, device="cuda")
+        dist.all_reduce(rr, op=dist.ReduceOp.SUM)
+        rays_all, paths_all = float(rr[0].item()), float(rr[1].item())
+    value = rays_all / (t_max / 1e3) / 1e6
+
+    # ---- end to end through the C ABI with host buffers
+    cam = s.export_scene()["camera"]
+    host = torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
+    cam_host = torch.from_numpy(cam.copy()).pin_memory().numpy()
+    barrier()
+    e2e_rays = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.set_camera(cam_host[0:3], cam_host[3:6], cam_host[6:9], float(cam_host[9]), bool(cam_host[10]))
+        s.render(spp)
+        s.readback(out=host)
+        st = s.stats()
+        e2e_rays += st["rays_extend"] + st["rays_shadow"]
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+        rr = torch.tensor([float(e2e_rays)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(rr, op=dist.ReduceOp.SUM)
+        e2e_rays = float(rr.item())
+    e2e_value = e2e_rays / e2e_s / 1e6
+
+    # ---- roofline of the extend stage (closest hit): algorithmic bytes per launch
+    hbm, peak_kind = _peaks()
+    ext_launches = max(1, prof_count["stage_launches"]["extend"])
+    nodes = prof_count["extend_nodes"]
+    prims = prof_count["extend_prims"]
+    roof = None
+    if rank == 0:
+        # algorithmic bytes of the counted frame: nodes x node size + leaf entries x 48 B +
+        # queue traffic (ray 32 B read + hit 16 B written per closest-hit query)
+        q_ext = st_count["rays_extend"]
+        algo_bytes_frame = nodes * prof_count["node_bytes"] + prims * prof_count["prim_bytes"] + q_ext * 48
+        per_launch_bytes = algo_bytes_frame / ext_launches
+        ext_ms = stage_ms["extend"] / max(1, stage_launches["extend"])
+        achieved = per_launch_bytes / (ext_ms / 1e3) / 1e9
+        roof = {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": _ncu_traffic(),
+                "peak_source": peak_kind + " hbm_gbs (burst copy)",
+                "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": ext_ms,
+                "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+                "stage_share": {k: v / max(1e-9, sum(stage_ms.values())) for k, v in stage_ms.items()},
+                "nodes_per_query": nodes / max(1, q_ext),
+                "prims_per_query": prims / max(1, q_ext)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        mr, mp, sample, thr, _ = cpu_reference_run(args.config, args.cpu_seconds)
+        cpu = {"value": mr, "unit": "Mrays/s", "cores": thr, "kind": "port", "sample": sample,
+               "mpaths_per_s": mp, "algorithm": "reference integrator restated (two traces per bounce, linear scan)"}
+
+    gpu_launches = sum(stage_launches.values())
+    if rank == 0:
+        line = {
+            "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "mpaths_per_s": paths_all / (t_max / 1e3) / 1e6,
+            "config": {"workload": wl["name"], "resolution": [w, h], "spp": spp, "max_depth": wl["depth"],
+                       "nee": True, "triangles": counts.num_triangles, "spheres": counts.num_spheres,
+                       "bvh_width": counts.bvh_width, "parallelism": f"replicas{world}",
+                       "l2": "flushed between steps (256 MiB write)"},
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 44,
+                    "d2h_bytes_per_step": w * h * 3 * 4},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": gpu_launches,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _ncu_traffic():
+    """DRAM bytes per extend launch from the committed ncu summary, when present."""
+    p = os.path.join(ROOT, "profiles", "extend_traffic.json")
+    if os.path.exists(p):
+        try:
+            with open(p) as f:
+                return json.load(f).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3])
+    ap.add_argument("--spp", type=int, default=0)
+    ap.add_argument("--wave-paths", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

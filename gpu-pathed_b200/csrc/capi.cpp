@@ -1,0 +1,256 @@
+// extern "C" entry points of libpathed.so (declared in include/pathed.h).
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/pathed.h"
+#include "session.h"
+
+struct pt_session {
+    pt::Session impl;
+    pt_session(int w, int h) : impl(w, h) {}
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(pt_session* s, F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return s ? s->impl.fail(PT_ERR_CUDA, "host allocation failed") : PT_ERR_CUDA;
+    } catch (const std::exception& e) {
+        return s ? s->impl.fail(PT_ERR_ARG, e.what()) : PT_ERR_ARG;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* pt_version(void) { return "pathed-b200 0.1 (sm_100a)"; }
+
+int pt_create(int width, int height, pt_session** out) {
+    if (!out) return PT_ERR_ARG;
+    *out = nullptr;
+    if (width <= 0 || height <= 0 || (long long)width * height > (1LL << 28)) {
+        g_create_error = "resolution must be positive and at most 2^28 pixels";
+        return PT_ERR_ARG;
+    }
+    try {
+        *out = new pt_session(width, height);
+    } catch (...) {
+        g_create_error = "host allocation failed";
+        return PT_ERR_CUDA;
+    }
+    return PT_OK;
+}
+
+int pt_destroy(pt_session* s) {
+    delete s;
+    return PT_OK;
+}
+
+const char* pt_last_error(const pt_session* s) {
+    return s ? s->impl.error().c_str() : g_create_error.c_str();
+}
+
+int pt_set_device(pt_session* s, int device) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.set_device(device);
+}
+
+int pt_load_config(pt_session* s, int config, uint64_t seed) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.load_config(config, seed, -1); });
+}
+
+int pt_load_config_level(pt_session* s, int config, uint64_t seed, int level) {
+    if (!s) return PT_ERR_ARG;
+    if (level < 0 || level > 9) return s->impl.fail(PT_ERR_ARG, "icosphere level must be in [0, 9]");
+    return guarded(s, [&] { return s->impl.load_config(config, seed, level); });
+}
+
+int pt_load_arrays(pt_session* s, const pt_scene_desc* d) {
+    if (!s) return PT_ERR_ARG;
+    if (!d) return s->impl.fail(PT_ERR_ARG, "null scene description");
+    return guarded(s, [&]() -> int {
+        pt::HostScene sc;
+        if (d->num_triangles < 0 || d->num_spheres < 0 || d->num_materials <= 0)
+            return s->impl.fail(PT_ERR_ARG, "negative counts or no materials");
+        if (d->num_triangles > 0 && (!d->tri_vertices || !d->tri_materials))
+            return s->impl.fail(PT_ERR_ARG, "triangle arrays missing");
+        if (d->num_spheres > 0 && (!d->spheres || !d->sphere_materials))
+            return s->impl.fail(PT_ERR_ARG, "sphere arrays missing");
+        if (!d->material_types) return s->impl.fail(PT_ERR_ARG, "material types missing");
+        const size_t nt = (size_t)d->num_triangles;
+        sc.tri_p.assign(d->tri_vertices, d->tri_vertices + nt * 9);
+        if (d->tri_normals) {
+            sc.tri_n.assign(d->tri_normals, d->tri_normals + nt * 9);
+        } else {
+            sc.tri_n.resize(nt * 9);
+            for (size_t i = 0; i < nt; i++) {
+                const float* p = &sc.tri_p[i * 9];
+                const float e1[3] = {p[3] - p[0], p[4] - p[1], p[5] - p[2]};
+                const float e2[3] = {p[6] - p[0], p[7] - p[1], p[8] - p[2]};
+                float n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                              e1[0] * e2[1] - e1[1] * e2[0]};
+                const float l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                for (int k = 0; k < 3; k++) n[k] = l > 0 ? n[k] / l : 0.f;
+                for (int v = 0; v < 3; v++)
+                    for (int k = 0; k < 3; k++) sc.tri_n[i * 9 + v * 3 + k] = n[k];
+            }
+        }
+        sc.tri_mat.assign(d->tri_materials, d->tri_materials + nt);
+        const size_t ns = (size_t)d->num_spheres;
+        if (ns) {
+            sc.sph.assign(d->spheres, d->spheres + ns * 4);
+            sc.sph_mat.assign(d->sphere_materials, d->sphere_materials + ns);
+        }
+        sc.mats.resize(d->num_materials);
+        for (int i = 0; i < d->num_materials; i++) {
+            pt::Material& m = sc.mats[i];
+            std::memset(&m, 0, sizeof(m));
+            m.type = d->material_types[i];
+            for (int k = 0; k < 3; k++) {
+                m.albedo[k] = d->material_albedo ? d->material_albedo[3 * i + k] : 0.f;
+                m.emit[k] = d->material_emit ? d->material_emit[3 * i + k] : 0.f;
+            }
+            m.ior = d->material_ior ? d->material_ior[i] : 1.f;
+            m.alpha = d->material_alpha ? d->material_alpha[i] : 0.1f;
+        }
+        if (d->env_rgba) {
+            if (d->env_width <= 0 || d->env_height <= 0)
+                return s->impl.fail(PT_ERR_ARG, "environment map size must be positive");
+            sc.env_w = d->env_width;
+            sc.env_h = d->env_height;
+            sc.env_rgba.assign(d->env_rgba, d->env_rgba + (size_t)d->env_width * d->env_height * 4);
+        }
+        sc.name = "arrays";
+        return s->impl.load_scene(std::move(sc));
+    });
+}
+
+int pt_scene_counts_get(const pt_session* s, pt_scene_counts* out) {
+    if (!s || !out) return PT_ERR_ARG;
+    return s->impl.counts(out);
+}
+
+int pt_export_scene(const pt_session* s, pt_scene_export* out) {
+    if (!s || !out) return PT_ERR_ARG;
+    return s->impl.export_scene(out);
+}
+
+int pt_set_bvh(pt_session* s, int width, int max_leaf) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.set_bvh(width, max_leaf); });
+}
+
+int pt_check_bvh(const pt_session* s) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.check_bvh();
+}
+
+int pt_set_camera(pt_session* s, const float origin[3], const float target[3], const float up[3], float vfov,
+                  int flip) {
+    if (!s || !origin || !target || !up) return PT_ERR_ARG;
+    pt::CameraSpec c;
+    for (int k = 0; k < 3; k++) {
+        c.origin[k] = origin[k];
+        c.target[k] = target[k];
+        c.up[k] = up[k];
+    }
+    c.vfov = vfov;
+    c.flip = flip != 0;
+    if (!(vfov > 0.f && vfov < 3.14159f)) return s->impl.fail(PT_ERR_ARG, "vertical field of view out of range");
+    return s->impl.set_camera(c);
+}
+
+int pt_set_material(pt_session* s, int id, int type, const float albedo[3], const float emit[3], float ior,
+                    float alpha) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.set_material(id, type, albedo, emit, ior, alpha);
+}
+
+int pt_set_max_depth(pt_session* s, int d) { return s ? s->impl.set_max_depth(d) : PT_ERR_ARG; }
+int pt_set_nee(pt_session* s, int on) { return s ? s->impl.set_nee(on) : PT_ERR_ARG; }
+int pt_set_seed(pt_session* s, uint64_t seed) {
+    if (!s) return PT_ERR_ARG;
+    s->impl.set_seed(seed);
+    return PT_OK;
+}
+int pt_set_guiding(pt_session* s, int enabled) {
+    if (!s) return PT_ERR_ARG;
+    if (enabled) return s->impl.fail(PT_ERR_ARG, "path guiding is not available in this build");
+    return PT_OK;
+}
+int pt_reset(pt_session* s) {
+    if (!s) return PT_ERR_ARG;
+    s->impl.reset();
+    return PT_OK;
+}
+int pt_set_launch(pt_session* s, const pt_launch_config* c) {
+    if (!s || !c) return PT_ERR_ARG;
+    return s->impl.set_launch(c);
+}
+int pt_get_launch(const pt_session* s, pt_launch_config* c) {
+    if (!s || !c) return PT_ERR_ARG;
+    s->impl.get_launch(c);
+    return PT_OK;
+}
+
+int pt_render_async(pt_session* s, int spp) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.render_async(spp); });
+}
+int pt_poll(pt_session* s, int* done, float* ms) { return s ? s->impl.poll(done, ms) : PT_ERR_ARG; }
+int pt_wait(pt_session* s, float* ms) { return s ? s->impl.wait(ms) : PT_ERR_ARG; }
+int pt_get_spp(const pt_session* s, int* spp) {
+    if (!s || !spp) return PT_ERR_ARG;
+    *spp = s->impl.spp();
+    return PT_OK;
+}
+int pt_get_stats(const pt_session* s, pt_stats* out) {
+    if (!s || !out) return PT_ERR_ARG;
+    return s->impl.stats(out);
+}
+
+int pt_set_profiling(pt_session* s, int stage_timing, int work_counters) {
+    return s ? s->impl.set_profiling(stage_timing, work_counters) : PT_ERR_ARG;
+}
+int pt_get_profile(const pt_session* s, pt_profile* out) {
+    if (!s || !out) return PT_ERR_ARG;
+    return s->impl.profile(out);
+}
+
+int pt_readback(pt_session* s, float* rgb, size_t n) { return s ? s->impl.readback(rgb, n, false) : PT_ERR_ARG; }
+int pt_readback_pass(pt_session* s, float* rgb, size_t n) { return s ? s->impl.readback(rgb, n, true) : PT_ERR_ARG; }
+int pt_readback_rgba8(pt_session* s, uint8_t* rgba, size_t n) {
+    return s ? s->impl.readback_rgba8(rgba, n) : PT_ERR_ARG;
+}
+
+int pt_hit_test(pt_session* s, int x, int y, int* material_id) {
+    if (!s || !material_id) return PT_ERR_ARG;
+    return s->impl.hit_test(x, y, material_id);
+}
+
+int pt_trace_rays(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax, int n,
+                  int* prim_type, int* prim_id, int* mat_id, float* t, float* bary) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.trace_rays(o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary, false); });
+}
+
+int pt_trace_rays_device(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax, int n,
+                         int* prim_type, int* prim_id, int* mat_id, float* t, float* bary) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.trace_rays(o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary, true);
+}
+
+int pt_occluded(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax, int n,
+                int* occluded) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.occluded(o, d, tmin, tmax, n, occluded); });
+}
+
+}  // extern "C"

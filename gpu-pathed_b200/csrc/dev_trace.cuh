@@ -1,0 +1,326 @@
+// Ray queries against the wide BVH: closest hit and any hit.
+//
+// Primitive tests restate the reference's arithmetic with uncontracted IEEE single
+// operations (__fmul_rn/__fadd_rn/__fsub_rn/__fdiv_rn/__fsqrt_rn):
+//   Triangle::hit  src/primitives/triangle.cu:7-48   (Moller-Trumbore form, inclusive bounds)
+//   Sphere::hit    src/primitives/sphere.cu:7-43     (near root, then far root, strict bounds)
+// and World::hit's selection rule (src/world.cu:5-41): a linear scan of all triangles in index
+// order accepting t <= tNear (so on an exact tie the higher triangle index wins), then all
+// spheres accepting only t < tNear (so triangles win ties against spheres and, among spheres,
+// the lower index wins). Here the same outcome is computed as the minimum of a total order
+// (t, then the tie rank), which does not depend on the order the BVH visits leaves in.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dev_math.cuh"
+#include "pt_types.h"
+
+namespace pt {
+
+constexpr int kMissPrim = 0x7fffffff;  // no hit
+// Relative slack applied to box-interval ends: boxes are visited when they might contain a
+// hit the primitive test would accept (never culls what the linear scan reports).
+constexpr float kBoxSlack = 1.00006103515625f;  // 1 + 2^-14
+
+struct Hit {
+    float t, b1, b2;
+    int prim;  // >= 0 triangle id, < 0 ~sphere id, kMissPrim: none
+};
+
+__device__ __forceinline__ float xdot(V a, V b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ V xcross(V a, V b) {
+    return V{__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+             -__fsub_rn(__fmul_rn(a.x, b.z), __fmul_rn(a.z, b.x)),
+             __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ V xsub(V a, V b) {
+    return V{__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)};
+}
+
+// Triangle::hit arithmetic. e1 = p1 - p0 and e2 = p2 - p0 arrive precomputed (same FP32
+// subtractions). Returns false on a miss; otherwise t, b1, b2. tmax is inclusive.
+__device__ __forceinline__ bool tri_test(V p0, V e1, V e2, V o, V d, float tmin, float tmax,
+                                         float& t, float& b1, float& b2) {
+    const V s1 = xcross(d, e2);
+    const float divisor = xdot(s1, e1);
+    if (divisor == 0.f) return false;
+    const float inv = __fdiv_rn(1.f, divisor);
+    const V s = xsub(o, p0);
+    b1 = __fmul_rn(xdot(s, s1), inv);
+    if (b1 < 0.f || b1 > 1.f) return false;
+    const V s2 = xcross(s, e1);
+    b2 = __fmul_rn(xdot(d, s2), inv);
+    if (b2 < 0.f || __fadd_rn(b1, b2) > 1.f) return false;
+    t = __fmul_rn(xdot(e2, s2), inv);
+    if (t < tmin || t > tmax) return false;
+    return true;
+}
+
+// Sphere::hit root selection: the near root when it lies above tmin, else the far root.
+// Returns false when neither root is above tmin (the caller applies the strict upper bound).
+__device__ __forceinline__ bool sphere_candidate(V c, float r, V o, V d, float tmin, float& t) {
+    const V oc = xsub(o, c);
+    const float a = xdot(d, d);
+    const float b = xdot(oc, d);
+    const float cc = __fsub_rn(xdot(oc, oc), __fmul_rn(r, r));
+    const float disc = __fsub_rn(__fmul_rn(b, b), __fmul_rn(a, cc));
+    if (!(disc > 0.f)) return false;
+    const float sq = __fsqrt_rn(disc);
+    const float nb = -b;
+    float tt = __fdiv_rn(__fsub_rn(nb, sq), a);
+    if (tt > tmin) { t = tt; return true; }
+    tt = __fdiv_rn(__fadd_rn(nb, sq), a);
+    if (tt > tmin) { t = tt; return true; }
+    return false;
+}
+
+struct RayPre {
+    V o, d;
+    float ix, iy, iz, ox, oy, oz;
+};
+__device__ __forceinline__ RayPre make_raypre(V o, V d) {
+    RayPre r;
+    r.o = o;
+    r.d = d;
+    const float dx = fabsf(d.x) < 1e-20f ? copysignf(1e-20f, d.x) : d.x;
+    const float dy = fabsf(d.y) < 1e-20f ? copysignf(1e-20f, d.y) : d.y;
+    const float dz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
+    r.ix = 1.f / dx;
+    r.iy = 1.f / dy;
+    r.iz = 1.f / dz;
+    r.ox = o.x * r.ix;
+    r.oy = o.y * r.iy;
+    r.oz = o.z * r.iz;
+    return r;
+}
+
+// Slab test; returns the entry distance or +inf when the interval is empty.
+__device__ __forceinline__ float box_entry(const RayPre& r, float lx, float hx, float ly, float hy,
+                                           float lz, float hz, float tmin, float tlim) {
+    const float t0x = fmaf(lx, r.ix, -r.ox), t1x = fmaf(hx, r.ix, -r.ox);
+    const float t0y = fmaf(ly, r.iy, -r.oy), t1y = fmaf(hy, r.iy, -r.oy);
+    const float t0z = fmaf(lz, r.iz, -r.oz), t1z = fmaf(hz, r.iz, -r.oz);
+    const float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), tmin));
+    const float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tlim));
+    return (tn <= tf * kBoxSlack) ? tn : __int_as_float(0x7f800000);
+}
+
+// Closest-hit acceptance for one leaf entry (tie rules above). `tcur` is best.t or tmax.
+__device__ __forceinline__ void leaf_entry(const float4* __restrict__ prims, int e, const RayPre& r,
+                                           float tmin, float tmax, Hit& best) {
+    const float4 a = __ldg(prims + 3 * e);
+    const int id = __float_as_int(a.w);
+    const float tcur = best.prim == kMissPrim ? tmax : best.t;
+    if (id >= 0) {
+        const float4 b = __ldg(prims + 3 * e + 1);
+        const float4 c = __ldg(prims + 3 * e + 2);
+        float t, b1, b2;
+        if (tri_test(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tcur, t, b1, b2)) {
+            // equal t: the higher triangle index wins; a triangle beats a sphere
+            if (t == tcur && best.prim != kMissPrim && best.prim >= 0 && id < best.prim) return;
+            best.t = t;
+            best.b1 = b1;
+            best.b2 = b2;
+            best.prim = id;
+        }
+    } else {
+        const float4 b = __ldg(prims + 3 * e + 1);
+        float t;
+        if (sphere_candidate(mkv(a), b.x, r.o, r.d, tmin, t)) {
+            const bool better = t < tcur ||
+                                (t == tcur && best.prim != kMissPrim && best.prim < 0 && id > best.prim);
+            // id = ~k: a larger id is a lower sphere index k
+            if (better) {
+                best.t = t;
+                best.b1 = 0.f;
+                best.b2 = 0.f;
+                best.prim = id;
+            }
+        }
+    }
+}
+
+// Any-hit acceptance for one leaf entry: true if the entry blocks [tmin, tmax].
+__device__ __forceinline__ bool leaf_entry_any(const float4* __restrict__ prims, int e, const RayPre& r,
+                                               float tmin, float tmax) {
+    const float4 a = __ldg(prims + 3 * e);
+    const int id = __float_as_int(a.w);
+    if (id >= 0) {
+        const float4 b = __ldg(prims + 3 * e + 1);
+        const float4 c = __ldg(prims + 3 * e + 2);
+        float t, b1, b2;
+        return tri_test(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tmax, t, b1, b2);
+    }
+    const float4 b = __ldg(prims + 3 * e + 1);
+    float t;
+    return sphere_candidate(mkv(a), b.x, r.o, r.d, tmin, t) && t < tmax;
+}
+
+template <int W>
+struct NodeView {
+    float lo_x[W], hi_x[W], lo_y[W], hi_y[W], lo_z[W], hi_z[W];
+    int child[W];
+};
+
+template <int W>
+__device__ __forceinline__ void load_node(const float4* __restrict__ p, NodeView<W>& nv) {
+    constexpr int kUsed = (7 * W + 3) / 4;  // float4s that hold bounds + children
+    float4 raw[kUsed];
+#pragma unroll
+    for (int i = 0; i < kUsed; i++) raw[i] = __ldg(p + i);
+    const float* f = reinterpret_cast<const float*>(raw);
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        nv.lo_x[k] = f[0 * W + k];
+        nv.hi_x[k] = f[1 * W + k];
+        nv.lo_y[k] = f[2 * W + k];
+        nv.hi_y[k] = f[3 * W + k];
+        nv.lo_z[k] = f[4 * W + k];
+        nv.hi_z[k] = f[5 * W + k];
+        nv.child[k] = __float_as_int(f[6 * W + k]);
+    }
+}
+
+// Per-query work counters (only maintained when the CNT template flag is set).
+struct TraceWork {
+    unsigned nodes = 0;  // wide nodes loaded
+    unsigned prims = 0;  // leaf entries tested
+};
+
+// Stack entry: x = node index, y = (remaining count << 24) | 3-bit child slots, nearest first.
+// The stack holds at most one entry per tree level.
+template <int W, bool ANY, bool CNT = false>
+__device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r, float tmin, float tmax,
+                                         int2* __restrict__ stk, int stride, int max_depth, Hit& best,
+                                         int& overflow, TraceWork* work = nullptr) {
+    constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
+    const float4* __restrict__ nodes = sc.nodes;
+    const float4* __restrict__ prims = sc.prims;
+    best.prim = kMissPrim;
+    best.t = tmax;
+    int sp = 0;
+    int node = sc.root;
+    for (;;) {
+        // ---- visit an internal node
+        NodeView<W> nv;
+        load_node<W>(nodes + (size_t)node * kNF4, nv);
+        if (CNT) work->nodes++;
+        const float tcur = best.prim == kMissPrim ? tmax : best.t;
+        const float tlim = tcur * kBoxSlack;
+        float key[W];
+        int slot[W];
+        int nhit = 0;
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+            float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k],
+                                 tmin, tlim);
+            if (nv.child[k] == kEmptyChild) te = __int_as_float(0x7f800000);
+            key[k] = te;
+            slot[k] = k;
+            nhit += te != __int_as_float(0x7f800000) ? 1 : 0;
+        }
+        if (!ANY) {
+            // odd-even transposition sort of (key, slot), W <= 8
+#pragma unroll
+            for (int pass = 0; pass < W; pass++) {
+#pragma unroll
+                for (int k = (pass & 1); k + 1 < W; k += 2) {
+                    if (key[k + 1] < key[k]) {
+                        const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
+                        const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
+                    }
+                }
+            }
+        } else {
+            // any order; compact hits to the front
+#pragma unroll
+            for (int pass = 0; pass < W; pass++) {
+#pragma unroll
+                for (int k = (pass & 1); k + 1 < W; k += 2) {
+                    const bool inf_k = key[k] == __int_as_float(0x7f800000);
+                    const bool inf_k1 = key[k + 1] == __int_as_float(0x7f800000);
+                    if (inf_k && !inf_k1) {
+                        const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
+                        const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
+                    }
+                }
+            }
+        }
+        int next_child = kEmptyChild;
+        if (nhit > 0) {
+            if (nhit > 1) {
+                uint32_t list = 0;
+#pragma unroll
+                for (int k = W - 1; k >= 1; k--) {
+                    if (k < nhit) list = (list << 3) | (uint32_t)slot[k];
+                }
+                if (sp >= max_depth) {
+                    overflow = 1;
+                    return best.prim != kMissPrim;
+                }
+                stk[sp * stride] = make_int2(node, (int)(((uint32_t)(nhit - 1) << 24) | list));
+                sp++;
+            }
+            int sel = slot[0];
+            int c = kEmptyChild;
+#pragma unroll
+            for (int k = 0; k < W; k++)
+                if (k == sel) c = nv.child[k];
+            next_child = c;
+        }
+        // ---- descend / process leaves / pop
+        for (;;) {
+            if (next_child != kEmptyChild) {
+                const int c = next_child;
+                next_child = kEmptyChild;
+                if (!child_is_leaf(c)) {
+                    node = c;
+                    break;
+                }
+                const int first = leaf_first(c), cnt = leaf_count(c);
+                if (CNT) work->prims += cnt;
+                if (ANY) {
+                    for (int e = first; e < first + cnt; e++) {
+                        if (leaf_entry_any(prims, e, r, tmin, tmax)) {
+                            best.prim = 0;
+                            return true;
+                        }
+                    }
+                } else {
+                    for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
+                }
+            }
+            if (sp == 0) return best.prim != kMissPrim;
+            int2 ent = stk[(sp - 1) * stride];
+            const int parent = ent.x;
+            const uint32_t packed = (uint32_t)ent.y;
+            const int cnt = (int)(packed >> 24);
+            const uint32_t list = packed & 0xFFFFFFu;
+            const int sl = (int)(list & 7u);
+            if (cnt > 1) {
+                stk[(sp - 1) * stride] = make_int2(parent, (int)(((uint32_t)(cnt - 1) << 24) | (list >> 3)));
+            } else {
+                sp--;
+            }
+            const float* pf = reinterpret_cast<const float*>(nodes + (size_t)parent * kNF4);
+            if (!ANY) {
+                // re-test against the shrunken interval; siblings behind it are farther
+                const float tc = best.prim == kMissPrim ? tmax : best.t;
+                const float te = box_entry(r, __ldg(pf + 0 * W + sl), __ldg(pf + 1 * W + sl), __ldg(pf + 2 * W + sl),
+                                           __ldg(pf + 3 * W + sl), __ldg(pf + 4 * W + sl), __ldg(pf + 5 * W + sl),
+                                           tmin, tc * kBoxSlack);
+                if (te == __int_as_float(0x7f800000)) {
+                    if (cnt > 1) sp--;
+                    continue;
+                }
+            }
+            next_child = __float_as_int(__ldg(pf + 6 * W + sl));
+        }
+    }
+}
+
+}  // namespace pt

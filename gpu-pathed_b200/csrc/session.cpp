@@ -1,0 +1,703 @@
+#include "session.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "../../include/pathed.h"
+
+namespace pt {
+
+namespace {
+constexpr int kMaxStackBytesDefault = 48 * 1024;
+}
+
+Session::Session(int w, int h) : w_(w), h_(h) {
+    // Reference default camera of scene 0 (src/scene.cu:176-184).
+    camspec_ = {{0.f, 1.f, 6.8f}, {0.f, 1.f, 0.f}, {0.f, 1.f, 0.f}, (float)(19.5f / 180.f * M_PI), false};
+}
+
+Session::~Session() {
+    if (dev_ready_) {
+        cudaSetDevice(device_);
+        if (stream_) cudaStreamSynchronize(stream_);
+        if (ev_begin_) cudaEventDestroy(ev_begin_);
+        if (ev_end_) cudaEventDestroy(ev_end_);
+        for (cudaEvent_t e : mark_events_) cudaEventDestroy(e);
+        if (stream_) cudaStreamDestroy(stream_);
+        if (h_stats_) cudaFreeHost(h_stats_);
+    }
+}
+
+int Session::check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return PT_OK;
+    cudaGetLastError();
+    return fail(PT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int Session::set_device(int dev) {
+    if (dev_ready_) return fail(PT_ERR_STATE, "device already selected for this session");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || dev < 0 || dev >= n) {
+        cudaGetLastError();
+        return fail(PT_ERR_ARG, "no CUDA device with index " + std::to_string(dev));
+    }
+    device_ = dev;
+    return PT_OK;
+}
+
+int Session::ensure_device() {
+    if (dev_ready_) return check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(PT_ERR_CUDA, "no CUDA device available (the CUDA path has no CPU fallback)");
+    }
+    if (device_ < 0) {
+        if (cudaGetDevice(&device_) != cudaSuccess) device_ = 0;
+    }
+    int r;
+    if ((r = check_cuda(cudaSetDevice(device_), "cudaSetDevice"))) return r;
+    cudaDeviceProp prop;
+    if ((r = check_cuda(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties"))) return r;
+    num_sms_ = prop.multiProcessorCount;
+    max_smem_ = prop.sharedMemPerBlockOptin;
+    if ((r = check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return r;
+    if ((r = check_cuda(cudaEventCreate(&ev_begin_), "cudaEventCreate"))) return r;
+    if ((r = check_cuda(cudaEventCreate(&ev_end_), "cudaEventCreate"))) return r;
+    if ((r = check_cuda(cudaMallocHost((void**)&h_stats_, sizeof(FrameStats)), "cudaMallocHost"))) return r;
+    std::memset(h_stats_, 0, sizeof(FrameStats));
+    if ((r = check_cuda(d_counters_.alloc(sizeof(WaveCounters)), "counters"))) return r;
+    if ((r = check_cuda(d_stats_.alloc(sizeof(FrameStats)), "stats"))) return r;
+    dev_ready_ = true;
+    return PT_OK;
+}
+
+int Session::load_config(int config, uint64_t seed, int level) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    HostScene s;
+    std::string err;
+    if (!generate_config(config, seed, s, err, level)) return fail(PT_ERR_ARG, err);
+    const CameraSpec cam = s.camera;
+    const int depth = s.default_depth;
+    const int nee = s.default_nee ? 1 : 0;
+    int r = load_scene(std::move(s));
+    if (r) return r;
+    camspec_ = cam;
+    max_depth_ = depth;
+    nee_ = nee;
+    return PT_OK;
+}
+
+int Session::load_scene(HostScene&& s) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    std::string err;
+    finalize_materials(s);
+    if (!validate_scene(s, err)) return fail(PT_ERR_SCENE, err);
+    BvhBuild b;
+    if (!build_bvh(s, bvh_width_, bvh_leaf_, b, err)) return fail(PT_ERR_SCENE, err);
+    scene_ = std::move(s);
+    bvh_ = std::move(b);
+    lights_ = build_light_list(scene_);
+    env_cdf_ = EnvCdf();
+    if (scene_.env_w > 0) build_env_cdf(scene_.env_rgba.data(), scene_.env_w, scene_.env_h, env_cdf_);
+    have_scene_ = true;
+    scene_dirty_ = true;
+    mats_dirty_ = true;
+    reset();
+    return PT_OK;
+}
+
+int Session::set_bvh(int width, int max_leaf) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    if (width != 2 && width != 4 && width != 8) return fail(PT_ERR_ARG, "BVH width must be 2, 4 or 8");
+    if (max_leaf < 1 || max_leaf > kMaxLeafPrims) return fail(PT_ERR_ARG, "leaf size must be in [1, 16]");
+    bvh_width_ = width;
+    bvh_leaf_ = max_leaf;
+    if (!have_scene_) return PT_OK;
+    BvhBuild b;
+    std::string err;
+    if (!build_bvh(scene_, bvh_width_, bvh_leaf_, b, err)) return fail(PT_ERR_SCENE, err);
+    bvh_ = std::move(b);
+    scene_dirty_ = true;
+    return PT_OK;
+}
+
+int Session::check_bvh() const {
+    if (!have_scene_) return PT_ERR_STATE;
+    std::string err;
+    return pt::check_bvh(scene_, bvh_, err) ? PT_OK : PT_ERR_SCENE;
+}
+
+int Session::counts(pt_scene_counts* out) const {
+    if (!have_scene_) return PT_ERR_STATE;
+    std::memset(out, 0, sizeof(*out));
+    out->num_triangles = scene_.num_tri();
+    out->num_spheres = scene_.num_sph();
+    out->num_materials = (int)scene_.mats.size();
+    out->num_lights = (int)lights_.size();
+    out->env_width = scene_.env_w;
+    out->env_height = scene_.env_h;
+    out->bvh_width = bvh_.width;
+    out->bvh_nodes = bvh_.num_nodes;
+    out->bvh_depth = bvh_.depth;
+    out->bvh_max_leaf = bvh_.max_leaf;
+    out->res_x = scene_.res_x;
+    out->res_y = scene_.res_y;
+    out->default_spp = scene_.default_spp;
+    out->default_depth = scene_.default_depth;
+    out->default_nee = scene_.default_nee ? 1 : 0;
+    out->bvh_build_ms = bvh_.build_ms;
+    return PT_OK;
+}
+
+int Session::export_scene(pt_scene_export* o) const {
+    if (!have_scene_) return PT_ERR_STATE;
+    const HostScene& s = scene_;
+    if (o->tri_vertices) std::memcpy(o->tri_vertices, s.tri_p.data(), s.tri_p.size() * 4);
+    if (o->tri_normals) std::memcpy(o->tri_normals, s.tri_n.data(), s.tri_n.size() * 4);
+    if (o->tri_materials) std::memcpy(o->tri_materials, s.tri_mat.data(), s.tri_mat.size() * 4);
+    if (o->spheres) std::memcpy(o->spheres, s.sph.data(), s.sph.size() * 4);
+    if (o->sphere_materials) std::memcpy(o->sphere_materials, s.sph_mat.data(), s.sph_mat.size() * 4);
+    for (size_t i = 0; i < s.mats.size(); i++) {
+        const Material& m = s.mats[i];
+        if (o->material_types) o->material_types[i] = m.type;
+        for (int k = 0; k < 3; k++) {
+            if (o->material_albedo) o->material_albedo[3 * i + k] = m.albedo[k];
+            if (o->material_emit) o->material_emit[3 * i + k] = m.emit[k];
+        }
+        if (o->material_ior) o->material_ior[i] = m.ior;
+        if (o->material_alpha) o->material_alpha[i] = m.alpha;
+    }
+    for (size_t i = 0; i < lights_.size(); i++) {
+        if (o->light_types) o->light_types[i] = lights_[i].type;
+        if (o->light_indices) o->light_indices[i] = lights_[i].index;
+    }
+    if (o->env_rgba && !s.env_rgba.empty()) std::memcpy(o->env_rgba, s.env_rgba.data(), s.env_rgba.size() * 4);
+    if (o->camera) {
+        for (int k = 0; k < 3; k++) {
+            o->camera[k] = camspec_.origin[k];
+            o->camera[3 + k] = camspec_.target[k];
+            o->camera[6 + k] = camspec_.up[k];
+        }
+        o->camera[9] = camspec_.vfov;
+        o->camera[10] = camspec_.flip ? 1.f : 0.f;
+    }
+    return PT_OK;
+}
+
+int Session::set_camera(const CameraSpec& c) {
+    CameraParams tmp;
+    std::string err;
+    if (!make_camera(c, w_, h_, tmp, err)) return fail(PT_ERR_ARG, err);
+    camspec_ = c;
+    reset();
+    return PT_OK;
+}
+
+int Session::set_material(int id, int type, const float* albedo, const float* emit, float ior, float alpha) {
+    if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (id < 0 || id >= (int)scene_.mats.size()) return fail(PT_ERR_ARG, "material id out of range");
+    if (type < kLambertian || type > kMicrofacet) return fail(PT_ERR_ARG, "unknown material type");
+    Material& m = scene_.mats[id];
+    if (m.type != type) {
+        // Scene::setMaterialType defaults (include/scene.h:36-61)
+        Material n{};
+        n.type = type;
+        if (type == kGlass) n.ior = 1.4f;
+        if (type == kMicrofacet) n.alpha = 0.1f;
+        m = n;
+    } else {
+        // the type's own parameters only (MaterialParams setters, include/materials/params.h)
+        if (type == kLambertian) {
+            for (int k = 0; k < 3; k++) {
+                if (albedo) m.albedo[k] = albedo[k];
+                if (emit) m.emit[k] = emit[k];
+            }
+        } else if (type == kGlass) {
+            m.ior = ior;
+        } else if (type == kMicrofacet) {
+            m.alpha = alpha;
+        }
+    }
+    finalize_materials(scene_);
+    lights_ = build_light_list(scene_);
+    mats_dirty_ = true;
+    reset();
+    return PT_OK;
+}
+
+int Session::set_max_depth(int d) {
+    if (d < 0 || d > kMaxDepthLimit) return fail(PT_ERR_ARG, "max depth must be in [0, 64]");
+    max_depth_ = d;
+    reset();
+    return PT_OK;
+}
+
+int Session::set_nee(int on) {
+    nee_ = on ? 1 : 0;
+    reset();
+    return PT_OK;
+}
+
+int Session::set_launch(const pt_launch_config* c) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    auto ok_block = [](int b) { return b == 0 || (b >= 32 && b <= 1024 && b % 32 == 0); };
+    if (!ok_block(c->block_extend) || !ok_block(c->block_shade) || !ok_block(c->block_shadow))
+        return fail(PT_ERR_ARG, "block sizes must be multiples of 32 in [32, 1024]");
+    if (c->wave_paths < 0 || c->blocks_per_sm < 0 || c->blocks_per_sm > 64)
+        return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
+    if (c->wave_paths) wave_paths_ = c->wave_paths;
+    if (c->block_extend) shape_.block_extend = c->block_extend;
+    if (c->block_shade) shape_.block_shade = c->block_shade;
+    if (c->block_shadow) shape_.block_shadow = c->block_shadow;
+    if (c->blocks_per_sm) shape_.blocks_per_sm = c->blocks_per_sm;
+    if (c->sort_materials) shape_.sort_materials = c->sort_materials == 1 ? 1 : 0;
+    if (c->use_graph) use_graph_ = c->use_graph == 1 ? 1 : 0;
+    return PT_OK;
+}
+
+void Session::get_launch(pt_launch_config* c) const {
+    c->wave_paths = wave_paths_;
+    c->block_extend = shape_.block_extend;
+    c->block_shade = shape_.block_shade;
+    c->block_shadow = shape_.block_shadow;
+    c->blocks_per_sm = shape_.blocks_per_sm;
+    c->sort_materials = shape_.sort_materials ? 1 : 2;
+    c->use_graph = use_graph_ ? 1 : 2;
+}
+
+template <class T>
+static cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    cudaError_t e = b.alloc(v.size() * sizeof(T));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+int Session::upload_materials() {
+    int r;
+    if ((r = check_cuda(upload(d_mats_, scene_.mats, stream_), "upload materials"))) return r;
+    if ((r = check_cuda(upload(d_lights_, lights_, stream_), "upload lights"))) return r;
+    if ((r = check_cuda(cudaStreamSynchronize(stream_), "upload materials"))) return r;
+    mats_dirty_ = false;
+    return PT_OK;
+}
+
+int Session::upload_scene() {
+    int r;
+    const int nt = scene_.num_tri();
+    std::vector<float> tp((size_t)nt * 12, 0.f), tn((size_t)nt * 12, 0.f);
+    for (int i = 0; i < nt; i++)
+        for (int v = 0; v < 3; v++)
+            for (int k = 0; k < 3; k++) {
+                tp[(size_t)i * 12 + v * 4 + k] = scene_.tri_p[(size_t)i * 9 + v * 3 + k];
+                tn[(size_t)i * 12 + v * 4 + k] = scene_.tri_n[(size_t)i * 9 + v * 3 + k];
+            }
+    if ((r = check_cuda(upload(d_nodes_, bvh_.nodes, stream_), "upload BVH nodes"))) return r;
+    if ((r = check_cuda(upload(d_prims_, bvh_.prims, stream_), "upload BVH primitives"))) return r;
+    if ((r = check_cuda(upload(d_tri_p_, tp, stream_), "upload triangles"))) return r;
+    if ((r = check_cuda(upload(d_tri_n_, tn, stream_), "upload normals"))) return r;
+    if ((r = check_cuda(upload(d_tri_mat_, scene_.tri_mat, stream_), "upload triangle materials"))) return r;
+    if ((r = check_cuda(upload(d_sph_, scene_.sph, stream_), "upload spheres"))) return r;
+    if ((r = check_cuda(upload(d_sph_mat_, scene_.sph_mat, stream_), "upload sphere materials"))) return r;
+    if (scene_.env_w > 0) {
+        if ((r = check_cuda(upload(d_env_rgba_, scene_.env_rgba, stream_), "upload environment"))) return r;
+        if ((r = check_cuda(upload(d_env_marg_, env_cdf_.marg, stream_), "upload environment CDF"))) return r;
+        if ((r = check_cuda(upload(d_env_cond_, env_cdf_.cond, stream_), "upload environment CDF"))) return r;
+        if ((r = check_cuda(upload(d_env_row_, env_cdf_.row_mass, stream_), "upload environment CDF"))) return r;
+    }
+    // host vectors above must outlive the async copies
+    if ((r = check_cuda(cudaStreamSynchronize(stream_), "scene upload"))) return r;
+    scene_dirty_ = false;
+    return upload_materials();
+}
+
+SceneDevice Session::scene_view() const {
+    SceneDevice v{};
+    v.nodes = d_nodes_.as<float4>();
+    v.prims = d_prims_.as<float4>();
+    v.tri_p = d_tri_p_.as<float4>();
+    v.tri_n = d_tri_n_.as<float4>();
+    v.tri_mat = d_tri_mat_.as<int>();
+    v.sph = d_sph_.as<float4>();
+    v.sph_mat = d_sph_mat_.as<int>();
+    v.mats = d_mats_.as<Material>();
+    v.lights = d_lights_.as<LightRef>();
+    v.num_tri = scene_.num_tri();
+    v.num_sph = scene_.num_sph();
+    v.num_mat = (int)scene_.mats.size();
+    v.num_lights = (int)lights_.size();
+    v.bvh_width = bvh_.width;
+    v.root = bvh_.root;
+    if (scene_.env_w > 0) {
+        v.env.rgba = d_env_rgba_.as<float>();
+        v.env.marg_cdf = d_env_marg_.as<float>();
+        v.env.cond_cdf = d_env_cond_.as<float>();
+        v.env.row_mass = d_env_row_.as<float>();
+        v.env.width = scene_.env_w;
+        v.env.height = scene_.env_h;
+        v.env.total_mass = env_cdf_.total;
+        v.env.present = 1;
+    }
+    return v;
+}
+
+int Session::ensure_frame_buffers(int spp) {
+    int r;
+    const size_t np = (size_t)w_ * h_;
+    if ((r = check_cuda(d_pass_.alloc(np * 3 * 4), "frame buffer"))) return r;
+    if ((r = check_cuda(d_accum_.alloc(np * 3 * 4), "frame buffer"))) return r;
+    if ((r = check_cuda(d_rgba8_.alloc(np * 4), "frame buffer"))) return r;
+    const int wave_pixels = std::max(1, std::min((int)np, wave_paths_ / spp));
+    const size_t cap = (size_t)wave_pixels * spp;
+    const size_t f4 = cap * sizeof(float4);
+    for (int k = 0; k < 2; k++) {
+        for (int a = 0; a < 6; a++) {
+            const size_t bytes = a == 3 ? cap * sizeof(uint2) : a == 5 ? cap * sizeof(int) : f4;
+            if ((r = check_cuda(d_q_[k][a].alloc(bytes), "ray queue"))) return r;
+        }
+    }
+    for (int a = 0; a < 3; a++)
+        if ((r = check_cuda(d_sq_[a].alloc(f4), "shadow queue"))) return r;
+    if ((r = check_cuda(d_L_.alloc(f4), "path radiance"))) return r;
+    if ((r = check_cuda(d_sort_.alloc(cap * sizeof(int)), "sort index"))) return r;
+    queue_cap_ = (int)cap;
+    return PT_OK;
+}
+
+int Session::render_async(int spp) {
+    if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is already in flight");
+    if (spp < 1) return fail(PT_ERR_ARG, "spp must be >= 1");
+    int r;
+    if ((r = ensure_device())) return r;
+    if (scene_dirty_ && (r = upload_scene())) return r;
+    if (mats_dirty_ && (r = upload_materials())) return r;
+    if ((r = ensure_frame_buffers(spp))) return r;
+    std::string err;
+    if (!make_camera(camspec_, w_, h_, cam_, err)) return fail(PT_ERR_ARG, err);
+    const int stack_depth = bvh_.depth + 1;
+    const int maxb = std::max(shape_.block_extend, shape_.block_shadow);
+    const size_t smem = stack_bytes(stack_depth, maxb);
+    if (smem > max_smem_) return fail(PT_ERR_SCENE, "BVH too deep for the traversal stack in shared memory");
+    if (smem > smem_configured_) {
+        if ((r = check_cuda(configure_traversal_smem(smem), "shared memory configuration"))) return r;
+        smem_configured_ = smem;
+    }
+    if (reset_pending_) {  // PathTracer::renderAsync resets m_currentSamples (path_tracer.cu:306-309)
+        total_spp_ = 0;
+        reset_pending_ = false;
+    }
+    FrameParams p{};
+    p.sc = scene_view();
+    p.cam = cam_;
+    for (int k = 0; k < 2; k++) {
+        p.q[k].o = d_q_[k][0].as<float4>();
+        p.q[k].d = d_q_[k][1].as<float4>();
+        p.q[k].beta = d_q_[k][2].as<float4>();
+        p.q[k].rng = d_q_[k][3].as<uint2>();
+        p.q[k].hit = d_q_[k][4].as<float4>();
+        p.q[k].key = d_q_[k][5].as<int>();
+    }
+    p.sq.o = d_sq_[0].as<float4>();
+    p.sq.d = d_sq_[1].as<float4>();
+    p.sq.c = d_sq_[2].as<float4>();
+    p.L = d_L_.as<float4>();
+    p.sort_index = d_sort_.as<int>();
+    p.counters = d_counters_.as<WaveCounters>();
+    p.stats = d_stats_.as<FrameStats>();
+    p.pass_rgb = d_pass_.as<float>();
+    p.accum_rgb = d_accum_.as<float>();
+    p.rgba8 = d_rgba8_.as<uchar4>();
+    p.width = w_;
+    p.height = h_;
+    p.spp = spp;
+    p.prev_spp = total_spp_;
+    p.max_depth = max_depth_;
+    p.nee = nee_;
+    p.seed = seed_;
+    p.sample_base = (uint64_t)total_spp_;
+    p.wave_pixels = queue_cap_ / spp;
+    p.stack_depth = stack_depth;
+    p.num_sms = num_sms_;
+    p.count_work = work_counters_;
+    p.shape = shape_;
+    last_wave_paths_ = p.wave_pixels * spp;
+    StageMarks* mk = nullptr;
+    marks_active_ = false;
+    if (stage_timing_) {
+        const int waves = (w_ * h_ + p.wave_pixels - 1) / p.wave_pixels;
+        const size_t need = (size_t)waves * (max_depth_ * 4 + 3) + 8;
+        while (mark_events_.size() < need) {
+            cudaEvent_t e;
+            if ((r = check_cuda(cudaEventCreate(&e), "cudaEventCreate"))) return r;
+            mark_events_.push_back(e);
+        }
+        mark_stage_.assign(mark_events_.size(), -1);
+        marks_.events = mark_events_.data();
+        marks_.stage = mark_stage_.data();
+        marks_.capacity = (int)mark_events_.size();
+        marks_.used = 0;
+        mk = &marks_;
+        marks_active_ = true;
+    }
+    if ((r = check_cuda(cudaMemsetAsync(d_stats_.p, 0, sizeof(FrameStats), stream_), "stats reset"))) return r;
+    if ((r = check_cuda(cudaEventRecord(ev_begin_, stream_), "cudaEventRecord"))) return r;
+    if ((r = check_cuda(enqueue_frame(p, stream_, mk), "frame launch"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(h_stats_, d_stats_.p, sizeof(FrameStats), cudaMemcpyDeviceToHost, stream_),
+                        "stats readback")))
+        return r;
+    if ((r = check_cuda(cudaEventRecord(ev_end_, stream_), "cudaEventRecord"))) return r;
+    in_flight_ = true;
+    inflight_spp_ = spp;
+    return PT_OK;
+}
+
+int Session::finish_frame(float* ms) {
+    int r;
+    float t = 0.f;
+    if ((r = check_cuda(cudaEventElapsedTime(&t, ev_begin_, ev_end_), "cudaEventElapsedTime"))) return r;
+    in_flight_ = false;
+    last_ms_ = t;
+    last_spp_ = inflight_spp_;
+    total_spp_ += inflight_spp_;  // PathTracer::pollRender (path_tracer.cu:354)
+    frames_++;
+    last_stats_ = *h_stats_;
+    if (ms) *ms = t;
+    if (marks_active_) {
+        for (int k = 0; k < kNumStages; k++) {
+            stage_ms_[k] = 0.f;
+            stage_launches_[k] = 0;
+        }
+        for (int i = 1; i < marks_.used; i++) {
+            const int st = marks_.stage[i];
+            if (st < 0) continue;
+            float dt = 0.f;
+            if ((r = check_cuda(cudaEventElapsedTime(&dt, marks_.events[i - 1], marks_.events[i]), "stage timing")))
+                return r;
+            stage_ms_[st] += dt;
+            stage_launches_[st]++;
+        }
+        marks_active_ = false;
+    }
+    if (last_stats_.error & 1) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");
+    return PT_OK;
+}
+
+int Session::poll(int* done, float* ms) {
+    if (!in_flight_) {
+        if (done) *done = 1;
+        if (ms) *ms = last_ms_;
+        return PT_OK;
+    }
+    cudaError_t e = cudaEventQuery(ev_end_);
+    if (e == cudaErrorNotReady) {
+        cudaGetLastError();
+        if (done) *done = 0;
+        return PT_OK;
+    }
+    if (e != cudaSuccess) {
+        in_flight_ = false;
+        return check_cuda(e, "frame execution");
+    }
+    if (done) *done = 1;
+    return finish_frame(ms);
+}
+
+int Session::wait(float* ms) {
+    if (!in_flight_) {
+        if (ms) *ms = last_ms_;
+        return PT_OK;
+    }
+    cudaError_t e = cudaEventSynchronize(ev_end_);
+    if (e != cudaSuccess) {
+        in_flight_ = false;
+        return check_cuda(e, "frame execution");
+    }
+    return finish_frame(ms);
+}
+
+int Session::stats(pt_stats* out) const {
+    std::memset(out, 0, sizeof(*out));
+    out->rays_camera = last_stats_.rays_camera;
+    out->rays_extend = last_stats_.rays_extend;
+    out->rays_shadow = last_stats_.rays_shadow;
+    out->last_frame_ms = last_ms_;
+    out->last_frame_spp = last_spp_;
+    out->total_spp = total_spp_;
+    out->frames = frames_;
+    return PT_OK;
+}
+
+int Session::set_profiling(int stage_timing, int work_counters) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    stage_timing_ = stage_timing ? 1 : 0;
+    work_counters_ = work_counters ? 1 : 0;
+    return PT_OK;
+}
+
+int Session::profile(pt_profile* out) const {
+    std::memset(out, 0, sizeof(*out));
+    for (int k = 0; k < kNumStages && k < PT_NUM_STAGES; k++) {
+        out->stage_ms[k] = stage_ms_[k];
+        out->stage_launches[k] = stage_launches_[k];
+    }
+    out->extend_nodes = last_stats_.extend_nodes;
+    out->extend_prims = last_stats_.extend_prims;
+    out->shadow_nodes = last_stats_.shadow_nodes;
+    out->shadow_prims = last_stats_.shadow_prims;
+    out->bvh_width = bvh_.width;
+    out->node_bytes = bvh_.width == 2 ? 64 : bvh_.width == 4 ? 128 : 256;
+    out->prim_bytes = 48;
+    out->wave_paths = last_wave_paths_;
+    return PT_OK;
+}
+
+int Session::readback(float* rgb, size_t n, bool pass) {
+    const size_t need = (size_t)w_ * h_ * 3;
+    if (!rgb || n < need) return fail(PT_ERR_ARG, "readback buffer too small");
+    if (!dev_ready_ || frames_ == 0) return fail(PT_ERR_STATE, "nothing rendered yet");
+    int r;
+    if ((r = wait(nullptr))) return r;
+    DevBuf& src = pass ? d_pass_ : d_accum_;
+    if ((r = check_cuda(cudaMemcpyAsync(rgb, src.p, need * 4, cudaMemcpyDeviceToHost, stream_), "readback"))) return r;
+    return check_cuda(cudaStreamSynchronize(stream_), "readback");
+}
+
+int Session::readback_rgba8(uint8_t* out, size_t n) {
+    const size_t need = (size_t)w_ * h_ * 4;
+    if (!out || n < need) return fail(PT_ERR_ARG, "readback buffer too small");
+    if (!dev_ready_ || frames_ == 0) return fail(PT_ERR_STATE, "nothing rendered yet");
+    int r;
+    if ((r = wait(nullptr))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(out, d_rgba8_.p, need, cudaMemcpyDeviceToHost, stream_), "readback"))) return r;
+    return check_cuda(cudaStreamSynchronize(stream_), "readback");
+}
+
+int Session::hit_test(int x, int y, int* mat) {
+    if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (x < 0 || y < 0 || x >= w_ || y >= h_) {
+        // the reference's kernel matches no thread and reports no hit
+        *mat = -1;
+        return PT_OK;
+    }
+    int r;
+    if ((r = ensure_device())) return r;
+    if (in_flight_ && (r = wait(nullptr))) return r;
+    if (scene_dirty_ && (r = upload_scene())) return r;
+    if (mats_dirty_ && (r = upload_materials())) return r;
+    std::string err;
+    if (!make_camera(camspec_, w_, h_, cam_, err)) return fail(PT_ERR_ARG, err);
+    if ((r = check_cuda(d_scratch_.alloc(64), "scratch"))) return r;
+    int* dm = d_scratch_.as<int>();
+    if ((r = check_cuda(cudaMemsetAsync(dm, 0, 8, stream_), "memset"))) return r;
+    if ((r = check_cuda(enqueue_hit_test(scene_view(), cam_, bvh_.depth + 1, x, y, dm, dm + 1, stream_), "hit test")))
+        return r;
+    int res[2];
+    if ((r = check_cuda(cudaMemcpyAsync(res, dm, 8, cudaMemcpyDeviceToHost, stream_), "hit test readback"))) return r;
+    if ((r = check_cuda(cudaStreamSynchronize(stream_), "hit test"))) return r;
+    if (res[1]) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");
+    *mat = res[0];
+    return PT_OK;
+}
+
+int Session::trace_rays(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pty,
+                        int* pid, int* mid, float* t, float* bary, bool device_ptrs) {
+    if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (n < 0) return fail(PT_ERR_ARG, "negative ray count");
+    if (n == 0) return PT_OK;
+    if (!o || !d || !tmin || !tmax || !pty || !pid || !mid || !t) return fail(PT_ERR_ARG, "null array");
+    int r;
+    if ((r = ensure_device())) return r;
+    if (in_flight_ && (r = wait(nullptr))) return r;
+    if (scene_dirty_ && (r = upload_scene())) return r;
+    if (mats_dirty_ && (r = upload_materials())) return r;
+    const int sd = bvh_.depth + 1;
+    if (stack_bytes(sd, 128) > (size_t)kMaxStackBytesDefault)
+        return fail(PT_ERR_SCENE, "BVH too deep for the traversal stack in shared memory");
+    if (device_ptrs) {
+        if ((r = check_cuda(d_scratch_.alloc(64), "scratch"))) return r;
+        int* of = d_scratch_.as<int>();
+        if ((r = check_cuda(cudaMemsetAsync(of, 0, 4, stream_), "memset"))) return r;
+        if ((r = check_cuda(enqueue_trace_rays(scene_view(), sd, o, d, tmin, tmax, n, pty, pid, mid, t, bary, of, stream_),
+                            "trace rays")))
+            return r;
+        int hof = 0;
+        if ((r = check_cuda(cudaMemcpyAsync(&hof, of, 4, cudaMemcpyDeviceToHost, stream_), "readback"))) return r;
+        if ((r = check_cuda(cudaStreamSynchronize(stream_), "trace rays"))) return r;
+        if (hof) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");
+        return PT_OK;
+    }
+    // inputs 3+3+1+1 floats, outputs 3 ints + t + 2 bary, plus the overflow flag
+    const size_t N = (size_t)n;
+    const size_t bytes = N * 4 * (8 + 6) + 256;
+    if ((r = check_cuda(d_scratch_.alloc(bytes), "scratch"))) return r;
+    char* base = d_scratch_.as<char>();
+    float* dO = (float*)base;
+    float* dD = dO + 3 * N;
+    float* dTmin = dD + 3 * N;
+    float* dTmax = dTmin + N;
+    int* dPt = (int*)(dTmax + N);
+    int* dPid = dPt + N;
+    int* dMid = dPid + N;
+    float* dT = (float*)(dMid + N);
+    float* dB = dT + N;
+    int* dOf = (int*)(dB + 2 * N);
+    cudaStream_t st = stream_;
+    if ((r = check_cuda(cudaMemcpyAsync(dO, o, 12 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dD, d, 12 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dTmin, tmin, 4 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dTmax, tmax, 4 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(dOf, 0, 4, st), "memset"))) return r;
+    if ((r = check_cuda(enqueue_trace_rays(scene_view(), sd, dO, dD, dTmin, dTmax, n, dPt, dPid, dMid, dT,
+                                           bary ? dB : nullptr, dOf, st),
+                        "trace rays")))
+        return r;
+    if ((r = check_cuda(cudaMemcpyAsync(pty, dPt, 4 * N, cudaMemcpyDeviceToHost, st), "copy hits"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(pid, dPid, 4 * N, cudaMemcpyDeviceToHost, st), "copy hits"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(mid, dMid, 4 * N, cudaMemcpyDeviceToHost, st), "copy hits"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(t, dT, 4 * N, cudaMemcpyDeviceToHost, st), "copy hits"))) return r;
+    if (bary && (r = check_cuda(cudaMemcpyAsync(bary, dB, 8 * N, cudaMemcpyDeviceToHost, st), "copy hits"))) return r;
+    int hof = 0;
+    if ((r = check_cuda(cudaMemcpyAsync(&hof, dOf, 4, cudaMemcpyDeviceToHost, st), "copy flag"))) return r;
+    if ((r = check_cuda(cudaStreamSynchronize(st), "trace rays"))) return r;
+    if (hof) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");
+    return PT_OK;
+}
+
+int Session::occluded(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* occ) {
+    if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (n < 0) return fail(PT_ERR_ARG, "negative ray count");
+    if (n == 0) return PT_OK;
+    if (!o || !d || !tmin || !tmax || !occ) return fail(PT_ERR_ARG, "null array");
+    int r;
+    if ((r = ensure_device())) return r;
+    if (in_flight_ && (r = wait(nullptr))) return r;
+    if (scene_dirty_ && (r = upload_scene())) return r;
+    if (mats_dirty_ && (r = upload_materials())) return r;
+    const int sd = bvh_.depth + 1;
+    const size_t N = (size_t)n;
+    if ((r = check_cuda(d_scratch_.alloc(N * 4 * 9 + 256), "scratch"))) return r;
+    float* dO = d_scratch_.as<float>();
+    float* dD = dO + 3 * N;
+    float* dTmin = dD + 3 * N;
+    float* dTmax = dTmin + N;
+    int* dOcc = (int*)(dTmax + N);
+    int* dOf = dOcc + N;
+    cudaStream_t st = stream_;
+    if ((r = check_cuda(cudaMemcpyAsync(dO, o, 12 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dD, d, 12 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dTmin, tmin, 4 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dTmax, tmax, 4 * N, cudaMemcpyHostToDevice, st), "copy rays"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(dOf, 0, 4, st), "memset"))) return r;
+    if ((r = check_cuda(enqueue_occluded(scene_view(), sd, dO, dD, dTmin, dTmax, n, dOcc, dOf, st), "occluded"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(occ, dOcc, 4 * N, cudaMemcpyDeviceToHost, st), "copy"))) return r;
+    int hof = 0;
+    if ((r = check_cuda(cudaMemcpyAsync(&hof, dOf, 4, cudaMemcpyDeviceToHost, st), "copy flag"))) return r;
+    if ((r = check_cuda(cudaStreamSynchronize(st), "occluded"))) return r;
+    if (hof) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");
+    return PT_OK;
+}
+
+}  // namespace pt

@@ -1,0 +1,160 @@
+// Render session: owns the host scene, its BVH, every device buffer and the frame loop.
+// The C ABI (capi.cpp) is a thin shell over this class.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/pathed.h"
+#include "bvh_build.h"
+#include "host_scene.h"
+#include "host_util.h"
+#include "wavefront.h"
+
+namespace pt {
+
+// Owning device allocation.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        else p = nullptr;
+        return e;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+class Session {
+public:
+    Session(int w, int h);
+    ~Session();
+
+    int width() const { return w_; }
+    int height() const { return h_; }
+    const std::string& error() const { return err_; }
+    int fail(int code, const std::string& msg) {
+        err_ = msg;
+        return code;
+    }
+
+    int set_device(int dev);
+    int load_config(int config, uint64_t seed, int level);
+    int load_scene(HostScene&& s);
+    int set_bvh(int width, int max_leaf);
+    int check_bvh() const;
+    int counts(::pt_scene_counts* out) const;
+    int export_scene(::pt_scene_export* out) const;
+
+    int set_camera(const CameraSpec& c);
+    int set_material(int id, int type, const float* albedo, const float* emit, float ior, float alpha);
+    int set_max_depth(int d);
+    int set_nee(int on);
+    void set_seed(uint64_t s) { seed_ = s; reset(); }
+    void reset() { reset_pending_ = true; }
+    int set_launch(const ::pt_launch_config* c);
+    void get_launch(::pt_launch_config* c) const;
+
+    int render_async(int spp);
+    int poll(int* done, float* ms);
+    int wait(float* ms);
+    int spp() const { return total_spp_; }
+    int stats(::pt_stats* out) const;
+    int set_profiling(int stage_timing, int work_counters);
+    int profile(::pt_profile* out) const;
+
+    int readback(float* rgb, size_t n, bool pass);
+    int readback_rgba8(uint8_t* out, size_t n);
+    int hit_test(int x, int y, int* mat);
+    int trace_rays(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pt,
+                   int* pid, int* mid, float* t, float* bary, bool device_ptrs);
+    int occluded(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* occ);
+
+    const HostScene& scene() const { return scene_; }
+    const CameraSpec& camera_spec() const { return camspec_; }
+    int max_depth() const { return max_depth_; }
+    int nee() const { return nee_; }
+
+private:
+    int ensure_device();
+    int upload_scene();
+    int upload_materials();
+    int ensure_frame_buffers(int spp);
+    int check_cuda(cudaError_t e, const char* what);
+    int finish_frame(float* ms);
+    SceneDevice scene_view() const;
+
+    int w_, h_;
+    std::string err_;
+    // host scene
+    HostScene scene_;
+    bool have_scene_ = false;
+    BvhBuild bvh_;
+    int bvh_width_ = 4, bvh_leaf_ = 4;
+    EnvCdf env_cdf_;
+    std::vector<LightRef> lights_;
+    CameraSpec camspec_{};
+    CameraParams cam_{};
+    int max_depth_ = 3;  // include/scene.h:12
+    int nee_ = 1;        // include/scene.h:28
+    uint64_t seed_ = 0x5EEDULL;
+    // device
+    int device_ = -1;
+    bool dev_ready_ = false;
+    bool scene_dirty_ = true;
+    bool mats_dirty_ = true;
+    cudaStream_t stream_ = nullptr;
+    int num_sms_ = 0;
+    size_t max_smem_ = 0;
+    DevBuf d_nodes_, d_prims_, d_tri_p_, d_tri_n_, d_tri_mat_, d_sph_, d_sph_mat_, d_mats_, d_lights_;
+    DevBuf d_env_rgba_, d_env_marg_, d_env_cond_, d_env_row_;
+    // frame state
+    DevBuf d_pass_, d_accum_, d_rgba8_;
+    DevBuf d_q_[2][6];
+    DevBuf d_sq_[3];
+    DevBuf d_L_, d_sort_, d_counters_, d_stats_, d_scratch_;
+    int queue_cap_ = 0;
+    LaunchShape shape_;
+    int wave_paths_ = 1 << 21;
+    int use_graph_ = 0;
+    int total_spp_ = 0;
+    bool reset_pending_ = true;
+    bool in_flight_ = false;
+    int inflight_spp_ = 0;
+    cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
+    float last_ms_ = 0.f;
+    int last_spp_ = 0;
+    int frames_ = 0;
+    FrameStats last_stats_{};
+    FrameStats* h_stats_ = nullptr;  // pinned
+    // profiling
+    int stage_timing_ = 0;
+    int work_counters_ = 0;
+    std::vector<cudaEvent_t> mark_events_;
+    std::vector<int> mark_stage_;
+    StageMarks marks_{};
+    bool marks_active_ = false;
+    float stage_ms_[kNumStages] = {};
+    int stage_launches_[kNumStages] = {};
+    int last_wave_paths_ = 0;
+    size_t smem_configured_ = 48 * 1024;
+};
+
+}  // namespace pt

@@ -1,0 +1,573 @@
+// Wavefront path integrator: the reference's per-pixel megakernel
+// (src/renderers/path_tracer.cu:142-264) split into stages over SoA ray queues.
+//
+//   camera   one thread per path of the wave: PCG stream, generateRay, queue slot
+//   extend   persistent: closest hit for every queued ray (BVH, shared-memory stack)
+//   sort     optional: bucket the queue by material class (miss, Lambert, mirror, glass,
+//            Beckmann) so each warp of the shade stage runs one BSDF
+//   shade    persistent: emission with MIS, BSDF sample, emitter sample (NEE) -> shadow
+//            queue, continuation ray -> next queue (warp ballot/popc compaction)
+//   shadow   persistent: any-hit for every shadow ray; unoccluded ones add their
+//            contribution to the path radiance
+//   accumulate  per pixel: mean over the frame's samples and the running mean across frames
+//            (src/framebuffer.cu:7-41)
+//
+// Per bounce the reference traces the BSDF direction twice (path_tracer.cu:51 with tMin 1e-4
+// for the MIS emission term and :177 with 1e-3 for the continuation); here it is traced once
+// with tMin 1e-3 and the hit serves both.
+#include "wavefront.h"
+
+#include <cfloat>
+
+#include "dev_math.cuh"
+#include "dev_shade.cuh"
+#include "dev_trace.cuh"
+
+namespace pt {
+
+namespace {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated append: every lane of the full warp calls this; lanes with `want` get a
+// slot index, computed from one atomic per warp.
+__device__ __forceinline__ int warp_append(int* counter, bool want) {
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    if (mask == 0) return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return want ? base + __popc(mask & lanemask_lt()) : -1;
+}
+
+// Persistent work fetch: one atomic per warp for 32 consecutive items.
+__device__ __forceinline__ int warp_fetch(int* cursor) {
+    int base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(cursor, 32);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
+__global__ void k_camera(FrameParams p, long long wave_first, int n) {
+    const PathQueue q = p.q[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const long long gp = wave_first + i;
+        const int pixel = (int)(gp / p.spp);
+        const int s = (int)(gp - (long long)pixel * p.spp);
+        const int row = pixel / p.width;
+        const int col = pixel - row * p.width;
+        const uint64_t inc = pcg_inc((uint32_t)pixel);
+        uint64_t st = pcg_seed(p.seed, p.sample_base + (uint64_t)s, (uint32_t)pixel);
+        const float xi1 = pcg_uniform(st, inc);
+        const float xi2 = pcg_uniform(st, inc);
+        V o, d;
+        camera_ray(p.cam, row, col, xi1, xi2, o, d);
+        q.o[i] = make_float4(o.x, o.y, o.z, __int_as_float(i));
+        q.d[i] = make_float4(d.x, d.y, d.z, 0.f);
+        q.beta[i] = make_float4(1.f, 1.f, 1.f, __int_as_float(1));  // camera ray: no MIS
+        q.rng[i] = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
+        p.L[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        p.counters->ray_count[0] = n;
+        atomicAdd(&p.stats->rays_camera, (unsigned long long)n);
+    }
+}
+
+__device__ __forceinline__ int material_class(const SceneDevice& sc, int prim) {
+    if (prim == kMissPrim) return 0;
+    const int mat = prim >= 0 ? __ldg(sc.tri_mat + prim) : __ldg(sc.sph_mat + ~prim);
+    return sc.mats[mat].type + 1;
+}
+
+// Warp-sum of per-thread work counters, one 64-bit atomic per warp.
+__device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long long* nodes, unsigned long long* prims) {
+    unsigned n = w.nodes, m = w.prims;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+        m += __shfl_xor_sync(0xffffffffu, m, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(nodes, (unsigned long long)n);
+        atomicAdd(prims, (unsigned long long)m);
+    }
+}
+
+template <int W, bool CNT>
+__global__ void k_extend(FrameParams p, int depth) {
+    extern __shared__ int2 stk[];
+    const int count = p.counters->ray_count[depth];
+    const PathQueue q = p.q[depth & 1];
+    const float tmin = depth == 0 ? kCameraTMin : kBounceTMin;
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_extend, (unsigned long long)count);
+    TraceWork work;
+    for (;;) {
+        const int base = warp_fetch(&p.counters->work_extend[depth]);
+        if (base >= count) break;
+        const int i = base + lane;
+        int key = -1;
+        if (i < count) {
+            const float4 o = q.o[i];
+            const float4 d = q.d[i];
+            const RayPre r = make_raypre(mkv(o), mkv(d));
+            Hit h;
+            int of = 0;
+            traverse<W, false, CNT>(p.sc, r, tmin, FLT_MAX, stk + threadIdx.x, blockDim.x, p.stack_depth, h, of,
+                                    &work);
+            if (of) atomicOr(&p.stats->error, 1);
+            q.hit[i] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
+            if (p.shape.sort_materials) {
+                key = material_class(p.sc, h.prim);
+                q.key[i] = key;
+            }
+        }
+        if (p.shape.sort_materials) {
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                const unsigned m = __ballot_sync(0xffffffffu, key == c);
+                if (lane == 0 && m) atomicAdd(&p.counters->sort_count[depth][c], __popc(m));
+            }
+        }
+    }
+    if (CNT) flush_work(work, &p.stats->extend_nodes, &p.stats->extend_prims);
+}
+
+__global__ void k_sort(FrameParams p, int depth) {
+    const int count = p.counters->ray_count[depth];
+    const PathQueue q = p.q[depth & 1];
+    int off[5];
+    int acc = 0;
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        off[c] = acc;
+        acc += p.counters->sort_count[depth][c];
+    }
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < count; base += stride) {
+        const int i = base + threadIdx.x;
+        const bool valid = i < count;
+        const int key = valid ? q.key[i] : 7;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        int b = 0;
+        if (valid && lane == leader) b = atomicAdd(&p.counters->sort_fill[depth][key], __popc(peers));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (valid) {
+            int ko = 0;
+#pragma unroll
+            for (int c = 0; c < 5; c++)
+                if (c == key) ko = off[c];
+            p.sort_index[ko + b + __popc(peers & lanemask_lt())] = i;
+        }
+    }
+}
+
+__global__ void k_shade(FrameParams p, int depth, long long wave_first) {
+    const int count = p.counters->ray_count[depth];
+    const PathQueue q = p.q[depth & 1];
+    const PathQueue qn = p.q[(depth + 1) & 1];
+    const bool last = depth >= p.max_depth - 1;
+    const int n_choice = p.sc.num_lights + (p.sc.env.present ? 1 : 0);
+    const bool do_nee = p.nee && n_choice > 0;
+    for (;;) {
+        const int base = warp_fetch(&p.counters->work_shade[depth]);
+        if (base >= count) break;
+        const int i = base + (threadIdx.x & 31);
+        bool cont = false, shadow = false;
+        float4 co, cd, cb, so, sd, sc4;
+        uint2 crng;
+        if (i < count) {
+            const int slot = p.shape.sort_materials ? p.sort_index[i] : i;
+            const float4 o4 = q.o[slot];
+            const float4 d4 = q.d[slot];
+            const float4 b4 = q.beta[slot];
+            const float4 h4 = q.hit[slot];
+            const int path = __float_as_int(o4.w);
+            const int flags = __float_as_int(b4.w);
+            const V o = mkv(o4), dir = mkv(d4), beta = mkv(b4);
+            const int prim = __float_as_int(h4.w);
+            const bool nomis = (flags & 1) || !p.nee;
+            V Ladd = mkv(0.f);
+            if (prim == kMissPrim) {
+                // escaped: environment radiance (path_tracer.cu:68-79, :162, :206, :228)
+                const V Le = env_emit(p.sc.env, dir);
+                if (!is_zero(Le)) {
+                    const float w = nomis ? 1.f : balance(d4.w, pdf_env_light(p.sc, dir));
+                    Ladd = beta * Le * w;
+                }
+            } else {
+                V point, n;
+                int mat;
+                if (prim >= 0) {
+                    // Triangle::hit's hit point and interpolated (unnormalised) shading normal
+                    const float b1 = h4.y, b2 = h4.z;
+                    const float w0 = 1.f - b1 - b2;
+                    const V p0 = mkv(__ldg(p.sc.tri_p + 3 * prim + 0));
+                    const V p1 = mkv(__ldg(p.sc.tri_p + 3 * prim + 1));
+                    const V p2 = mkv(__ldg(p.sc.tri_p + 3 * prim + 2));
+                    const V n0 = mkv(__ldg(p.sc.tri_n + 3 * prim + 0));
+                    const V n1 = mkv(__ldg(p.sc.tri_n + 3 * prim + 1));
+                    const V n2 = mkv(__ldg(p.sc.tri_n + 3 * prim + 2));
+                    point = p0 * w0 + p1 * b1 + p2 * b2;
+                    n = w0 * n0 + b1 * n1 + b2 * n2;
+                    mat = __ldg(p.sc.tri_mat + prim);
+                } else {
+                    const float4 s = __ldg(p.sc.sph + ~prim);
+                    point = o + h4.x * dir;
+                    n = normalized((point - mkv(s.x, s.y, s.z)) / s.w);
+                    mat = __ldg(p.sc.sph_mat + ~prim);
+                }
+                const Frame fr = make_frame(n);
+                const V wo = normalized(to_local(fr, -dir));
+                const Material m = p.sc.mats[mat];
+                if (m.emitting && wo.z >= 0.f) {  // front-face emission (lambertian.cu:5-11)
+                    const float w = nomis ? 1.f : balance(d4.w, pdf_scene_light(p.sc, o, point, n, prim));
+                    Ladd = beta * mkv(m.emit[0], m.emit[1], m.emit[2]) * w;
+                }
+                if (!last) {
+                    const long long gp = wave_first + path;
+                    const uint32_t pixel = (uint32_t)(gp / p.spp);
+                    const uint64_t inc = pcg_inc(pixel);
+                    uint64_t st = ((uint64_t)q.rng[slot].y << 32) | q.rng[slot].x;
+                    BsdfSample bs;
+                    switch (m.type) {
+                        case kLambertian: {
+                            const float x1 = pcg_uniform(st, inc);
+                            const float x2 = pcg_uniform(st, inc);
+                            bs = lambert_sample(m, wo, x1, x2);
+                            break;
+                        }
+                        case kMirror: bs = mirror_sample(wo); break;
+                        case kGlass: bs = glass_sample(m, wo, pcg_uniform(st, inc)); break;
+                        default: {
+                            const float x1 = pcg_uniform(st, inc);
+                            const float x2 = pcg_uniform(st, inc);
+                            bs = mf_sample(m.alpha, wo, x1, x2);
+                        }
+                    }
+                    if (do_nee && !bs.delta) {
+                        // directSampleLights (path_tracer.cu:83-126)
+                        const float x1 = pcg_uniform(st, inc);
+                        const float x2 = pcg_uniform(st, inc);
+                        const float x3 = pcg_uniform(st, inc);
+                        const LightSample ls = sample_lights(p.sc, point, x1, x2, x3);
+                        if (dot(ls.normal, ls.wi) < 0.f && ls.pdf > 0.f) {
+                            const V wil = to_local(fr, ls.wi);
+                            const float bpdf = bsdf_pdf(m, wo, wil);
+                            const float wl = balance(ls.pdf, bpdf);
+                            const V f = bsdf_f(m, wo, wil);
+                            const V contrib = beta * (ls.emitted * wl * f * fabsf(dot(n, ls.wi)) / ls.pdf);
+                            if (!is_zero(contrib)) {
+                                shadow = true;
+                                so = make_float4(point.x, point.y, point.z, ls.distance - 2e-4f);
+                                sd = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, __int_as_float(path));
+                                sc4 = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+                            }
+                        }
+                    }
+                    // beta *= f * |cos| / pdf (path_tracer.cu:171-173)
+                    if (bs.pdf > 0.f) {
+                        const V nb = beta * (bs.f * fabsf(bs.wi.z) / bs.pdf);
+                        if (!is_zero(nb) && isfinite(nb.x + nb.y + nb.z)) {
+                            const V wd = to_world(fr, bs.wi);
+                            cont = true;
+                            co = make_float4(point.x, point.y, point.z, __int_as_float(path));
+                            cd = make_float4(wd.x, wd.y, wd.z, bs.pdf);
+                            cb = make_float4(nb.x, nb.y, nb.z, __int_as_float(bs.delta ? 1 : 0));
+                            crng = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
+                        }
+                    }
+                }
+            }
+            if (!is_zero(Ladd)) {
+                float4 l = p.L[path];
+                l.x += Ladd.x;
+                l.y += Ladd.y;
+                l.z += Ladd.z;
+                p.L[path] = l;
+            }
+        }
+        const int cslot = warp_append(&p.counters->ray_count[depth + 1], cont);
+        if (cont) {
+            qn.o[cslot] = co;
+            qn.d[cslot] = cd;
+            qn.beta[cslot] = cb;
+            qn.rng[cslot] = crng;
+        }
+        const int sslot = warp_append(&p.counters->shadow_count[depth], shadow);
+        if (shadow) {
+            p.sq.o[sslot] = so;
+            p.sq.d[sslot] = sd;
+            p.sq.c[sslot] = sc4;
+        }
+    }
+}
+
+template <int W, bool CNT>
+__global__ void k_shadow(FrameParams p, int depth) {
+    extern __shared__ int2 stk[];
+    const int count = p.counters->shadow_count[depth];
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_shadow, (unsigned long long)count);
+    TraceWork work;
+    for (;;) {
+        const int base = warp_fetch(&p.counters->work_shadow[depth]);
+        if (base >= count) break;
+        const int i = base + lane;
+        if (i < count) {
+            const float4 o = p.sq.o[i];
+            const float4 d = p.sq.d[i];
+            const RayPre r = make_raypre(mkv(o), mkv(d));
+            Hit h;
+            int of = 0;
+            const bool occ = traverse<W, true, CNT>(p.sc, r, kShadowTMin, o.w, stk + threadIdx.x, blockDim.x,
+                                                    p.stack_depth, h, of, &work);
+            if (of) atomicOr(&p.stats->error, 1);
+            if (!occ) {
+                const float4 c = p.sq.c[i];
+                const int path = __float_as_int(d.w);
+                float4 l = p.L[path];
+                l.x += c.x;
+                l.y += c.y;
+                l.z += c.z;
+                p.L[path] = l;
+            }
+        }
+    }
+    if (CNT) flush_work(work, &p.stats->shadow_nodes, &p.stats->shadow_prims);
+}
+
+__global__ void k_accumulate(FrameParams p, int first_pixel, int npix) {
+    const int pi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pi >= npix) return;
+    const int pixel = first_pixel + pi;
+    float r = 0.f, g = 0.f, b = 0.f;
+    const float inv_spp = (float)p.spp;
+    for (int s = 0; s < p.spp; s++) {  // passRadiances += Li / spp (path_tracer.cu:258-262)
+        const float4 l = p.L[(size_t)pi * p.spp + s];
+        r += l.x / inv_spp;
+        g += l.y / inv_spp;
+        b += l.z / inv_spp;
+    }
+    p.pass_rgb[3 * (size_t)pixel + 0] = r;
+    p.pass_rgb[3 * (size_t)pixel + 1] = g;
+    p.pass_rgb[3 * (size_t)pixel + 2] = b;
+    float nr = r, ng = g, nb = b;
+    if (p.prev_spp > 0) {  // running mean (framebuffer.cu:23-33)
+        const float prev = (float)p.prev_spp;
+        const float total = (float)(p.prev_spp + p.spp);
+        const float wpass = 1.f * p.spp / total;
+        nr = p.accum_rgb[3 * (size_t)pixel + 0] * prev / total + r * wpass;
+        ng = p.accum_rgb[3 * (size_t)pixel + 1] * prev / total + g * wpass;
+        nb = p.accum_rgb[3 * (size_t)pixel + 2] * prev / total + b * wpass;
+    }
+    p.accum_rgb[3 * (size_t)pixel + 0] = nr;
+    p.accum_rgb[3 * (size_t)pixel + 1] = ng;
+    p.accum_rgb[3 * (size_t)pixel + 2] = nb;
+    uchar4 c;
+    c.x = (unsigned char)(fmaxf(0.f, fminf(1.f, to_srgb(nr))) * 255);
+    c.y = (unsigned char)(fmaxf(0.f, fminf(1.f, to_srgb(ng))) * 255);
+    c.z = (unsigned char)(fmaxf(0.f, fminf(1.f, to_srgb(nb))) * 255);
+    c.w = 255;
+    p.rgba8[pixel] = c;
+}
+
+struct Marker {
+    StageMarks* m;
+    cudaStream_t s;
+    cudaError_t err = cudaSuccess;
+    void operator()(int stage) {
+        if (!m || err != cudaSuccess) return;
+        if (m->used >= m->capacity) { err = cudaErrorInvalidValue; return; }
+        m->stage[m->used] = stage;
+        err = cudaEventRecord(m->events[m->used++], s);
+    }
+};
+
+template <int W, bool CNT>
+cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
+    const int npixels = p.width * p.height;
+    const int grid_e = p.num_sms * p.shape.blocks_per_sm;
+    const size_t smem_e = stack_bytes(p.stack_depth, p.shape.block_extend);
+    const size_t smem_s = stack_bytes(p.stack_depth, p.shape.block_shadow);
+    Marker mark{marks, stream};
+    for (int first = 0; first < npixels; first += p.wave_pixels) {
+        const int npix = npixels - first < p.wave_pixels ? npixels - first : p.wave_pixels;
+        const int n = npix * p.spp;
+        const long long wave_first = (long long)first * p.spp;
+        cudaError_t e = cudaMemsetAsync(p.counters, 0, sizeof(WaveCounters), stream);
+        if (e != cudaSuccess) return e;
+        mark(-1);
+        k_camera<<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
+        mark(kStageCamera);
+        for (int d = 0; d < p.max_depth; d++) {
+            k_extend<W, CNT><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+            mark(kStageExtend);
+            if (p.shape.sort_materials) {
+                k_sort<<<(n + 255) / 256, 256, 0, stream>>>(p, d);
+                mark(kStageSort);
+            }
+            k_shade<<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
+            mark(kStageShade);
+            if (p.nee && d < p.max_depth - 1) {
+                k_shadow<W, CNT><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d);
+                mark(kStageShadow);
+            }
+        }
+        k_accumulate<<<(npix + 127) / 128, 128, 0, stream>>>(p, first, npix);
+        mark(kStageAccum);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (mark.err != cudaSuccess) return mark.err;
+    }
+    return cudaSuccess;
+}
+
+template <int W>
+cudaError_t set_smem_w(size_t bytes) {
+    const int b = (int)bytes;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    return cudaSuccess;
+}
+
+template <int W>
+__global__ void k_trace_rays(SceneDevice sc, int stack_depth, const float* __restrict__ o,
+                             const float* __restrict__ d, const float* __restrict__ tmin,
+                             const float* __restrict__ tmax, int n, int* prim_type, int* prim_id, int* mat_id,
+                             float* t, float* bary, int* overflow) {
+    extern __shared__ int2 stk[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const RayPre r = make_raypre(mkv(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mkv(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
+    Hit h;
+    int of = 0;
+    traverse<W, false>(sc, r, tmin[i], tmax[i], stk + threadIdx.x, blockDim.x, stack_depth, h, of);
+    if (of) atomicOr(overflow, 1);
+    if (h.prim == kMissPrim) {
+        prim_type[i] = -1;
+        prim_id[i] = -1;
+        mat_id[i] = -1;
+        t[i] = 0.f;
+        if (bary) { bary[2 * i] = 0.f; bary[2 * i + 1] = 0.f; }
+    } else if (h.prim >= 0) {
+        prim_type[i] = kTriangle;
+        prim_id[i] = h.prim;
+        mat_id[i] = sc.tri_mat[h.prim];
+        t[i] = h.t;
+        if (bary) { bary[2 * i] = h.b1; bary[2 * i + 1] = h.b2; }
+    } else {
+        prim_type[i] = kSphere;
+        prim_id[i] = ~h.prim;
+        mat_id[i] = sc.sph_mat[~h.prim];
+        t[i] = h.t;
+        if (bary) { bary[2 * i] = 0.f; bary[2 * i + 1] = 0.f; }
+    }
+}
+
+template <int W>
+__global__ void k_occluded(SceneDevice sc, int stack_depth, const float* __restrict__ o,
+                           const float* __restrict__ d, const float* __restrict__ tmin,
+                           const float* __restrict__ tmax, int n, int* occluded, int* overflow) {
+    extern __shared__ int2 stk[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const RayPre r = make_raypre(mkv(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mkv(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
+    Hit h;
+    int of = 0;
+    occluded[i] = traverse<W, true>(sc, r, tmin[i], tmax[i], stk + threadIdx.x, blockDim.x, stack_depth, h, of) ? 1 : 0;
+    if (of) atomicOr(overflow, 1);
+}
+
+template <int W>
+__global__ void k_hit_test(SceneDevice sc, CameraParams cam, int stack_depth, int x, int y, int* out, int* overflow) {
+    extern __shared__ int2 stk[];
+    if (threadIdx.x != 0) return;
+    V o, d;
+    camera_ray(cam, y, x, 0.5f, 0.5f, o, d);
+    const RayPre r = make_raypre(o, d);
+    Hit h;
+    int of = 0;
+    traverse<W, false>(sc, r, 0.f, FLT_MAX, stk, 1, stack_depth, h, of);
+    if (of) atomicOr(overflow, 1);
+    if (h.prim == kMissPrim) *out = -1;
+    else if (h.prim >= 0) *out = sc.tri_mat[h.prim];
+    else *out = sc.sph_mat[~h.prim];
+}
+
+}  // namespace
+
+cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
+    if (p.max_depth < 0 || p.max_depth > kMaxDepthLimit) return cudaErrorInvalidValue;
+    const bool cnt = p.count_work != 0;
+    switch (p.sc.bvh_width) {
+        case 2: return cnt ? enqueue_frame_w<2, true>(p, stream, marks) : enqueue_frame_w<2, false>(p, stream, marks);
+        case 4: return cnt ? enqueue_frame_w<4, true>(p, stream, marks) : enqueue_frame_w<4, false>(p, stream, marks);
+        case 8: return cnt ? enqueue_frame_w<8, true>(p, stream, marks) : enqueue_frame_w<8, false>(p, stream, marks);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t configure_traversal_smem(size_t bytes) {
+    cudaError_t e;
+    if ((e = set_smem_w<2>(bytes))) return e;
+    if ((e = set_smem_w<4>(bytes))) return e;
+    return set_smem_w<8>(bytes);
+}
+
+cudaError_t enqueue_trace_rays(const SceneDevice& sc, int stack_depth, const float* o, const float* d,
+                               const float* tmin, const float* tmax, int n, int* prim_type, int* prim_id,
+                               int* mat_id, float* t, float* bary, int* overflow, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const int bs = 128;
+    const size_t smem = stack_bytes(stack_depth, bs);
+    const int grid = (n + bs - 1) / bs;
+    switch (sc.bvh_width) {
+        case 2: k_trace_rays<2><<<grid, bs, smem, stream>>>(sc, stack_depth, o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary, overflow); break;
+        case 4: k_trace_rays<4><<<grid, bs, smem, stream>>>(sc, stack_depth, o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary, overflow); break;
+        case 8: k_trace_rays<8><<<grid, bs, smem, stream>>>(sc, stack_depth, o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary, overflow); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_occluded(const SceneDevice& sc, int stack_depth, const float* o, const float* d,
+                             const float* tmin, const float* tmax, int n, int* occluded, int* overflow,
+                             cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const int bs = 128;
+    const size_t smem = stack_bytes(stack_depth, bs);
+    const int grid = (n + bs - 1) / bs;
+    switch (sc.bvh_width) {
+        case 2: k_occluded<2><<<grid, bs, smem, stream>>>(sc, stack_depth, o, d, tmin, tmax, n, occluded, overflow); break;
+        case 4: k_occluded<4><<<grid, bs, smem, stream>>>(sc, stack_depth, o, d, tmin, tmax, n, occluded, overflow); break;
+        case 8: k_occluded<8><<<grid, bs, smem, stream>>>(sc, stack_depth, o, d, tmin, tmax, n, occluded, overflow); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_hit_test(const SceneDevice& sc, const CameraParams& cam, int stack_depth, int x, int y,
+                             int* out_material, int* overflow, cudaStream_t stream) {
+    const size_t smem = stack_bytes(stack_depth, 1);
+    switch (sc.bvh_width) {
+        case 2: k_hit_test<2><<<1, 32, smem, stream>>>(sc, cam, stack_depth, x, y, out_material, overflow); break;
+        case 4: k_hit_test<4><<<1, 32, smem, stream>>>(sc, cam, stack_depth, x, y, out_material, overflow); break;
+        case 8: k_hit_test<8><<<1, 32, smem, stream>>>(sc, cam, stack_depth, x, y, out_material, overflow); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pt

@@ -1,0 +1,123 @@
+// Host-visible launch interface of the wavefront integrator kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pt_types.h"
+
+namespace pt {
+
+// Per-slot path state of a ray queue (structure of arrays, 16-byte elements).
+struct PathQueue {
+    float4* o;     // origin.xyz, wave-local path index (int bits)
+    float4* d;     // direction.xyz, pdf of the BSDF sample that produced the ray
+    float4* beta;  // throughput.xyz, flags (int bits): bit 0 = no MIS on the next emission
+    uint2* rng;    // PCG32 state
+    float4* hit;   // t, b1, b2, primitive (int bits); written by the extend stage
+    int* key;      // material-sort key of the hit (shade stage order), optional
+};
+
+struct ShadowQueue {
+    float4* o;  // origin.xyz, tmax
+    float4* d;  // direction.xyz, wave-local path index (int bits)
+    float4* c;  // contribution (beta * f * cos * Le * w / pdf).xyz, unused
+};
+
+constexpr int kMaxDepthLimit = 64;
+
+// Device counters of one wave (zeroed at wave start).
+struct WaveCounters {
+    int ray_count[kMaxDepthLimit + 1];     // rays in the queue consumed at depth d
+    int shadow_count[kMaxDepthLimit + 1];  // shadow rays produced at depth d
+    int work_extend[kMaxDepthLimit + 1];   // persistent work-fetch cursors
+    int work_shade[kMaxDepthLimit + 1];
+    int work_shadow[kMaxDepthLimit + 1];
+    int sort_count[kMaxDepthLimit + 1][8]; // per material class hit counts (sorted shading)
+    int sort_fill[kMaxDepthLimit + 1][8];
+};
+
+// Frame-wide device statistics (not reset per wave).
+struct FrameStats {
+    unsigned long long rays_camera;
+    unsigned long long rays_extend;   // closest-hit queries (camera + continuation)
+    unsigned long long rays_shadow;   // any-hit queries
+    unsigned long long extend_nodes;  // wide nodes loaded by closest-hit queries (work-count frames)
+    unsigned long long extend_prims;  // leaf entries tested by closest-hit queries
+    unsigned long long shadow_nodes;
+    unsigned long long shadow_prims;
+    int error;                        // bit 0: traversal stack overflow
+    int pad;
+};
+
+// Stages of a frame, for per-stage device timing.
+enum Stage : int { kStageCamera = 0, kStageExtend, kStageSort, kStageShade, kStageShadow, kStageAccum, kNumStages };
+
+// Host-side recorder of stage boundaries: an event is recorded after every launch.
+struct StageMarks {
+    cudaEvent_t* events = nullptr;  // pool
+    int capacity = 0;
+    int used = 0;
+    int* stage = nullptr;           // stage of the launch that ends at events[i] (-1: wave start)
+};
+
+struct LaunchShape {
+    int block_extend = 128;
+    int block_shade = 128;
+    int block_shadow = 128;
+    int blocks_per_sm = 8;    // persistent grid = SMs * blocks_per_sm
+    int sort_materials = 1;   // material-sorted shading
+};
+
+struct FrameParams {
+    SceneDevice sc;
+    CameraParams cam;
+    PathQueue q[2];
+    ShadowQueue sq;
+    float4* L;               // wave-local path radiance
+    int* sort_index;         // material-sorted slot order
+    WaveCounters* counters;
+    FrameStats* stats;
+    float* pass_rgb;         // W*H*3: this frame's per-pixel mean (passRadiances)
+    float* accum_rgb;        // W*H*3: running mean across frames (radiances)
+    uchar4* rgba8;           // W*H display buffer
+    int width, height;
+    int spp;                 // samples per pixel of this frame
+    int prev_spp;            // samples accumulated before this frame
+    int max_depth;
+    int nee;
+    uint64_t seed;
+    uint64_t sample_base;    // samples per pixel rendered before this frame (RNG offset)
+    int wave_pixels;         // pixels per wave
+    int stack_depth;         // traversal stack entries per thread
+    int num_sms;
+    int count_work;          // 1: traversal kernels count nodes and leaf entries (slower)
+    LaunchShape shape;
+};
+
+// Enqueue one frame (all waves) on `stream`. Grid sizes do not depend on queue lengths,
+// so the sequence can be captured into a CUDA graph. With `marks`, an event is recorded
+// after every launch (per-stage timing; not capturable).
+cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks* marks = nullptr);
+
+// Raise the dynamic shared-memory limit of the traversal kernels to `bytes`.
+cudaError_t configure_traversal_smem(size_t bytes);
+
+// Closest-hit queries for caller-provided rays (parity entry). Arrays are device pointers.
+cudaError_t enqueue_trace_rays(const SceneDevice& sc, int stack_depth, const float* o, const float* d,
+                               const float* tmin, const float* tmax, int n, int* prim_type, int* prim_id,
+                               int* mat_id, float* t, float* bary, int* overflow, cudaStream_t stream);
+
+// Any-hit queries for caller-provided rays: occluded[i] = 1 if something lies in [tmin, tmax].
+cudaError_t enqueue_occluded(const SceneDevice& sc, int stack_depth, const float* o, const float* d,
+                             const float* tmin, const float* tmax, int n, int* occluded, int* overflow,
+                             cudaStream_t stream);
+
+// One camera ray through the centre of pixel (x = col, y = row) (src/hit_test.cu:25-47).
+cudaError_t enqueue_hit_test(const SceneDevice& sc, const CameraParams& cam, int stack_depth, int x, int y,
+                             int* out_material, int* overflow, cudaStream_t stream);
+
+// Size in bytes of the traversal stack per block for `threads` threads.
+inline size_t stack_bytes(int stack_depth, int threads) { return (size_t)stack_depth * threads * sizeof(int2); }
+
+}  // namespace pt

@@ -1,0 +1,373 @@
+"""ctypes binding of libpathed.so (the C ABI declared in include/pathed.h).
+
+This is the call path tests and benchmarks use: every call goes through the C ABI into the
+sm_100a kernels; there is no Python or CPU fallback. Importing this module loads the
+in-tree libpathed.so and raises if it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpathed.so")
+
+PT_OK = 0
+PT_ERR_ARG = -1
+PT_ERR_STATE = -2
+PT_ERR_CUDA = -3
+PT_ERR_SCENE = -4
+PT_ERR_DEVICE = -5
+
+LAMBERTIAN, MIRROR, GLASS, MICROFACET = 0, 1, 2, 3
+
+# every symbol declared in include/pathed.h
+EXPORTED = [
+    "pt_create", "pt_destroy", "pt_last_error", "pt_set_device", "pt_load_config", "pt_load_config_level",
+    "pt_load_arrays", "pt_scene_counts_get", "pt_export_scene", "pt_set_bvh", "pt_check_bvh", "pt_set_camera",
+    "pt_set_material", "pt_set_max_depth", "pt_set_nee", "pt_set_seed", "pt_set_guiding", "pt_reset",
+    "pt_set_launch", "pt_get_launch", "pt_render_async", "pt_poll", "pt_wait", "pt_get_spp", "pt_get_stats",
+    "pt_readback", "pt_readback_pass", "pt_readback_rgba8", "pt_hit_test", "pt_trace_rays",
+    "pt_trace_rays_device", "pt_occluded", "pt_version", "pt_set_profiling", "pt_get_profile",
+]
+
+STAGES = ("camera", "extend", "sort", "shade", "shadow", "accumulate")
+
+
+class PathedError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pathed error {code}: {msg}")
+        self.code = code
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("num_triangles", C.c_int), ("tri_vertices", C.c_void_p), ("tri_normals", C.c_void_p),
+        ("tri_materials", C.c_void_p), ("num_spheres", C.c_int), ("spheres", C.c_void_p),
+        ("sphere_materials", C.c_void_p), ("num_materials", C.c_int), ("material_types", C.c_void_p),
+        ("material_albedo", C.c_void_p), ("material_emit", C.c_void_p), ("material_ior", C.c_void_p),
+        ("material_alpha", C.c_void_p), ("env_width", C.c_int), ("env_height", C.c_int),
+        ("env_rgba", C.c_void_p),
+    ]
+
+
+class SceneCounts(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "num_triangles", "num_spheres", "num_materials", "num_lights", "env_width", "env_height",
+        "bvh_width", "bvh_nodes", "bvh_depth", "bvh_max_leaf", "res_x", "res_y", "default_spp",
+        "default_depth", "default_nee")] + [("bvh_build_ms", C.c_double)]
+
+
+class SceneExport(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in (
+        "tri_vertices", "tri_normals", "tri_materials", "spheres", "sphere_materials", "material_types",
+        "material_albedo", "material_emit", "material_ior", "material_alpha", "light_types",
+        "light_indices", "env_rgba", "camera")]
+
+
+class LaunchConfig(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "wave_paths", "block_extend", "block_shade", "block_shadow", "blocks_per_sm", "sort_materials",
+        "use_graph")]
+
+
+class Stats(C.Structure):
+    _fields_ = [("rays_camera", C.c_ulonglong), ("rays_extend", C.c_ulonglong), ("rays_shadow", C.c_ulonglong),
+                ("last_frame_ms", C.c_float), ("last_frame_spp", C.c_int), ("total_spp", C.c_int),
+                ("frames", C.c_int)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("stage_ms", C.c_float * 6), ("stage_launches", C.c_int * 6), ("extend_nodes", C.c_ulonglong),
+                ("extend_prims", C.c_ulonglong), ("shadow_nodes", C.c_ulonglong), ("shadow_prims", C.c_ulonglong),
+                ("bvh_width", C.c_int), ("node_bytes", C.c_int), ("prim_bytes", C.c_int), ("wave_paths", C.c_int)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libpathed.so not built ({LIB_PATH}); run gpu-pathed_b200/build.py")
+    lib = C.CDLL(LIB_PATH)
+    lib.pt_last_error.restype = C.c_char_p
+    lib.pt_last_error.argtypes = [C.c_void_p]
+    lib.pt_version.restype = C.c_char_p
+    lib.pt_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    lib.pt_destroy.argtypes = [C.c_void_p]
+    lib.pt_load_config.argtypes = [C.c_void_p, C.c_int, C.c_uint64]
+    lib.pt_load_config_level.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_int]
+    lib.pt_set_seed.argtypes = [C.c_void_p, C.c_uint64]
+    lib.pt_set_camera.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int]
+    lib.pt_set_material.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float]
+    lib.pt_poll.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    lib.pt_wait.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+    lib.pt_readback.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.pt_readback_pass.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.pt_readback_rgba8.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.pt_trace_rays.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
+    lib.pt_trace_rays_device.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
+    lib.pt_occluded.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
+    lib.pt_hit_test.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
+    for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async"):
+        getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
+    lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.pt_set_profiling.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.pt_get_profile.argtypes = [C.c_void_p, C.c_void_p]
+    for name in ("pt_reset", "pt_check_bvh"):
+        getattr(lib, name).argtypes = [C.c_void_p]
+    for name in ("pt_scene_counts_get", "pt_export_scene", "pt_set_launch", "pt_get_launch", "pt_get_stats",
+                 "pt_load_arrays", "pt_get_spp"):
+        getattr(lib, name).argtypes = [C.c_void_p, C.c_void_p]
+    return lib
+
+
+lib = _load()
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+def _f32(a, n=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} floats, got {a.size}")
+    return a
+
+
+class Session:
+    """One render session (RenderSession + its PathTracer) on the current CUDA device."""
+
+    def __init__(self, width: int, height: int):
+        h = C.c_void_p()
+        rc = lib.pt_create(width, height, C.byref(h))
+        if rc != PT_OK:
+            raise PathedError(rc, lib.pt_last_error(None).decode())
+        self._h = h
+        self.width, self.height = width, height
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.pt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != PT_OK:
+            raise PathedError(rc, lib.pt_last_error(self._h).decode())
+        return rc
+
+    # ---- scene
+    def load_config(self, config: int, seed: int = 0x5EED, level: int | None = None):
+        if level is None:
+            self._check(lib.pt_load_config(self._h, config, seed))
+        else:
+            self._check(lib.pt_load_config_level(self._h, config, seed, level))
+
+    def load_arrays(self, tri_vertices=None, tri_normals=None, tri_materials=None, spheres=None,
+                    sphere_materials=None, material_types=None, material_albedo=None, material_emit=None,
+                    material_ior=None, material_alpha=None, env_rgba=None):
+        keep = []
+
+        def f(a, dt=np.float32):
+            if a is None:
+                return None, None
+            arr = np.ascontiguousarray(np.asarray(a, dtype=dt))
+            keep.append(arr)
+            return arr, arr.ctypes.data
+
+        tv, tvp = f(tri_vertices)
+        _, tnp = f(tri_normals)
+        _, tmp = f(tri_materials, np.int32)
+        sp, spp = f(spheres)
+        _, smp = f(sphere_materials, np.int32)
+        mt, mtp = f(material_types, np.int32)
+        d = SceneDesc()
+        d.num_triangles = 0 if tv is None else tv.size // 9
+        d.tri_vertices, d.tri_normals, d.tri_materials = tvp, tnp, tmp
+        d.num_spheres = 0 if sp is None else sp.size // 4
+        d.spheres, d.sphere_materials = spp, smp
+        d.num_materials = 0 if mt is None else mt.size
+        d.material_types = mtp
+        d.material_albedo = f(material_albedo)[1]
+        d.material_emit = f(material_emit)[1]
+        d.material_ior = f(material_ior)[1]
+        d.material_alpha = f(material_alpha)[1]
+        if env_rgba is not None:
+            e, ep = f(env_rgba)
+            d.env_height, d.env_width = e.shape[0], e.shape[1]
+            d.env_rgba = ep
+        self._check(lib.pt_load_arrays(self._h, C.byref(d)))
+
+    def counts(self) -> SceneCounts:
+        c = SceneCounts()
+        self._check(lib.pt_scene_counts_get(self._h, C.byref(c)))
+        return c
+
+    def export_scene(self) -> dict:
+        c = self.counts()
+        out = {
+            "tri_vertices": np.zeros((c.num_triangles, 9), np.float32),
+            "tri_normals": np.zeros((c.num_triangles, 9), np.float32),
+            "tri_materials": np.zeros(c.num_triangles, np.int32),
+            "spheres": np.zeros((c.num_spheres, 4), np.float32),
+            "sphere_materials": np.zeros(c.num_spheres, np.int32),
+            "material_types": np.zeros(c.num_materials, np.int32),
+            "material_albedo": np.zeros((c.num_materials, 3), np.float32),
+            "material_emit": np.zeros((c.num_materials, 3), np.float32),
+            "material_ior": np.zeros(c.num_materials, np.float32),
+            "material_alpha": np.zeros(c.num_materials, np.float32),
+            "light_types": np.zeros(c.num_lights, np.int32),
+            "light_indices": np.zeros(c.num_lights, np.int32),
+            "env_rgba": np.zeros((c.env_height, c.env_width, 4), np.float32) if c.env_width else None,
+            "camera": np.zeros(11, np.float32),
+        }
+        e = SceneExport()
+        for k, v in out.items():
+            setattr(e, k, _ptr(v) if v is not None and v.size else None)
+        self._check(lib.pt_export_scene(self._h, C.byref(e)))
+        out["counts"] = c
+        return out
+
+    def set_bvh(self, width: int, max_leaf: int = 4):
+        self._check(lib.pt_set_bvh(self._h, width, max_leaf))
+
+    def check_bvh(self) -> int:
+        return lib.pt_check_bvh(self._h)
+
+    # ---- model edits
+    def set_camera(self, origin, target, up, vfov_radians: float, flip: bool = False):
+        o, t, u = _f32(origin, 3), _f32(target, 3), _f32(up, 3)
+        self._check(lib.pt_set_camera(self._h, o.ctypes.data, t.ctypes.data, u.ctypes.data, vfov_radians, int(flip)))
+
+    def set_material(self, material_id, mtype, albedo=(0, 0, 0), emit=(0, 0, 0), ior=1.0, alpha=0.1):
+        a, e = _f32(albedo, 3), _f32(emit, 3)
+        self._check(lib.pt_set_material(self._h, material_id, mtype, a.ctypes.data, e.ctypes.data, ior, alpha))
+
+    def set_max_depth(self, d: int):
+        self._check(lib.pt_set_max_depth(self._h, d))
+
+    def set_nee(self, on: bool):
+        self._check(lib.pt_set_nee(self._h, int(bool(on))))
+
+    def set_seed(self, seed: int):
+        self._check(lib.pt_set_seed(self._h, seed))
+
+    def set_guiding(self, on: bool):
+        self._check(lib.pt_set_guiding(self._h, int(bool(on))))
+
+    def reset(self):
+        self._check(lib.pt_reset(self._h))
+
+    def set_launch(self, **kw):
+        c = LaunchConfig()
+        for k, v in kw.items():
+            setattr(c, k, int(v))
+        self._check(lib.pt_set_launch(self._h, C.byref(c)))
+
+    def get_launch(self) -> dict:
+        c = LaunchConfig()
+        self._check(lib.pt_get_launch(self._h, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in LaunchConfig._fields_}
+
+    # ---- rendering
+    def render_async(self, spp: int):
+        self._check(lib.pt_render_async(self._h, spp))
+
+    def poll(self):
+        done, ms = C.c_int(), C.c_float()
+        self._check(lib.pt_poll(self._h, C.byref(done), C.byref(ms)))
+        return bool(done.value), ms.value
+
+    def wait(self) -> float:
+        ms = C.c_float()
+        self._check(lib.pt_wait(self._h, C.byref(ms)))
+        return ms.value
+
+    def render(self, spp: int) -> float:
+        self.render_async(spp)
+        return self.wait()
+
+    def spp(self) -> int:
+        v = C.c_int()
+        self._check(lib.pt_get_spp(self._h, C.byref(v)))
+        return v.value
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(lib.pt_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def set_profiling(self, stage_timing: bool = True, work_counters: bool = False):
+        self._check(lib.pt_set_profiling(self._h, int(bool(stage_timing)), int(bool(work_counters))))
+
+    def profile(self) -> dict:
+        p = Profile()
+        self._check(lib.pt_get_profile(self._h, C.byref(p)))
+        d = {k: getattr(p, k) for k, _ in Profile._fields_ if k not in ("stage_ms", "stage_launches")}
+        d["stage_ms"] = dict(zip(STAGES, list(p.stage_ms)))
+        d["stage_launches"] = dict(zip(STAGES, list(p.stage_launches)))
+        return d
+
+    def readback(self, out: np.ndarray | None = None, pass_only: bool = False) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.height, self.width, 3), np.float32)
+        fn = lib.pt_readback_pass if pass_only else lib.pt_readback
+        self._check(fn(self._h, out.ctypes.data, out.size))
+        return out
+
+    def readback_rgba8(self) -> np.ndarray:
+        out = np.empty((self.height, self.width, 4), np.uint8)
+        self._check(lib.pt_readback_rgba8(self._h, out.ctypes.data, out.size))
+        return out
+
+    # ---- queries
+    def hit_test(self, x: int, y: int) -> int:
+        m = C.c_int()
+        self._check(lib.pt_hit_test(self._h, x, y, C.byref(m)))
+        return m.value
+
+    def trace_rays(self, o, d, tmin, tmax, with_bary=False):
+        o = _f32(o).reshape(-1, 3)
+        d = _f32(d).reshape(-1, 3)
+        n = o.shape[0]
+        tmin = _f32(np.broadcast_to(np.asarray(tmin, np.float32), (n,)))
+        tmax = _f32(np.broadcast_to(np.asarray(tmax, np.float32), (n,)))
+        pt_ = np.empty(n, np.int32)
+        pid = np.empty(n, np.int32)
+        mid = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        bary = np.empty((n, 2), np.float32) if with_bary else None
+        self._check(lib.pt_trace_rays(self._h, o.ctypes.data, d.ctypes.data, tmin.ctypes.data, tmax.ctypes.data,
+                                      n, pt_.ctypes.data, pid.ctypes.data, mid.ctypes.data, t.ctypes.data,
+                                      _ptr(bary)))
+        res = {"prim_type": pt_, "prim_id": pid, "mat_id": mid, "t": t}
+        if with_bary:
+            res["bary"] = bary
+        return res
+
+    def occluded(self, o, d, tmin, tmax):
+        o = _f32(o).reshape(-1, 3)
+        d = _f32(d).reshape(-1, 3)
+        n = o.shape[0]
+        tmin = _f32(np.broadcast_to(np.asarray(tmin, np.float32), (n,)))
+        tmax = _f32(np.broadcast_to(np.asarray(tmax, np.float32), (n,)))
+        occ = np.empty(n, np.int32)
+        self._check(lib.pt_occluded(self._h, o.ctypes.data, d.ctypes.data, tmin.ctypes.data, tmax.ctypes.data, n,
+                                    occ.ctypes.data))
+        return occ
+
+
+def version() -> str:
+    return lib.pt_version().decode()

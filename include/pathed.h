@@ -1,0 +1,234 @@
+/*
+ * pathed.h - C ABI of the B200 path-tracing core (libpathed.so).
+ *
+ * This is the drop-in boundary for the reference's vanilla CUDA backend. Each entry point
+ * names the reference interface it replaces (paths are inside chellmuth/gpu-pathed):
+ *
+ *   RenderSession          include/render_session.h:41-134, src/render_session.cu:55-136
+ *   Renderer / PathTracer  include/renderers/renderer.h:14-35, src/renderers/path_tracer.cu:266-361
+ *   SceneModel setters     include/scene_model.h:34-99, src/scene_model.cu:41-347
+ *   hit test               src/hit_test.cu:49-82
+ *   World::hit             src/world.cu:5-41 (parity entry pt_trace_rays)
+ *
+ * Conventions: every function returns PT_OK (0) or a negative PT_ERR_* code; on error
+ * pt_last_error() holds a message. No function calls exit() or traps the device (the
+ * reference exits through gpuAssert, include/macro_helper.h:10-19). Caller-owned host arrays
+ * are copied; the session owns all device memory and frees it in pt_destroy. A session is
+ * not thread-safe (one thread per session, like the reference's GUI thread).
+ *
+ * Device work runs on the session's own CUDA stream. Rendering is asynchronous:
+ * pt_render_async enqueues one progressive frame, pt_poll reports completion.
+ */
+#ifndef PATHED_H
+#define PATHED_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PT_OK 0
+#define PT_ERR_ARG (-1)      /* invalid argument */
+#define PT_ERR_STATE (-2)    /* call not valid in the current state (no scene, frame in flight) */
+#define PT_ERR_CUDA (-3)     /* CUDA runtime error (no device, out of memory, launch failure) */
+#define PT_ERR_SCENE (-4)    /* scene rejected (validation, BVH build) */
+#define PT_ERR_DEVICE (-5)   /* a kernel reported an error flag (e.g. traversal stack overflow) */
+
+/* Material types: same values as the reference enum (include/materials/types.h:5-11). */
+#define PT_LAMBERTIAN 0
+#define PT_MIRROR 1
+#define PT_GLASS 2
+#define PT_MICROFACET 3
+
+/* Renderer types (include/scene_model.h:16-20). Only PT_RENDERER_CUDA is built. */
+#define PT_RENDERER_CUDA 0
+#define PT_RENDERER_OPTIX 1
+#define PT_RENDERER_NORMALS 2
+
+typedef struct pt_session pt_session;
+
+/* Scene arrays handed over by a caller (replaces SceneData, include/scene_data.h:19-41,
+ * which the reference fills from OBJ/PLY parsers). Triangles keep the reference's record:
+ * three vertices, three shading normals (interpolated, not renormalised), a material id.
+ * tri_normals may be NULL: each vertex then takes the normalised geometric normal of its
+ * triangle (cross(p1 - p0, p2 - p0)). env_rgba may be NULL (no environment light). */
+typedef struct pt_scene_desc {
+    int num_triangles;
+    const float* tri_vertices;   /* 9 floats per triangle: p0, p1, p2 */
+    const float* tri_normals;    /* 9 floats per triangle: n0, n1, n2, or NULL */
+    const int* tri_materials;
+    int num_spheres;
+    const float* spheres;        /* 4 floats per sphere: cx, cy, cz, radius */
+    const int* sphere_materials;
+    int num_materials;
+    const int* material_types;   /* PT_LAMBERTIAN .. PT_MICROFACET */
+    const float* material_albedo;/* 3 per material (Lambertian) */
+    const float* material_emit;  /* 3 per material (Lambertian emitters) */
+    const float* material_ior;   /* 1 per material (glass) */
+    const float* material_alpha; /* 1 per material (Beckmann microfacet) */
+    int env_width, env_height;
+    const float* env_rgba;       /* env_width * env_height * 4 floats, row 0 = +y, or NULL */
+} pt_scene_desc;
+
+/* Sizes of the loaded scene, for pt_export_scene. */
+typedef struct pt_scene_counts {
+    int num_triangles, num_spheres, num_materials, num_lights;
+    int env_width, env_height;
+    int bvh_width, bvh_nodes, bvh_depth, bvh_max_leaf;
+    int res_x, res_y;          /* preferred resolution of a generated configuration */
+    int default_spp, default_depth, default_nee;
+    double bvh_build_ms;
+} pt_scene_counts;
+
+/* Caller-allocated destination for pt_export_scene (any pointer may be NULL). */
+typedef struct pt_scene_export {
+    float* tri_vertices;   /* 9 * num_triangles */
+    float* tri_normals;    /* 9 * num_triangles */
+    int* tri_materials;
+    float* spheres;        /* 4 * num_spheres */
+    int* sphere_materials;
+    int* material_types;
+    float* material_albedo;/* 3 * num_materials */
+    float* material_emit;
+    float* material_ior;
+    float* material_alpha;
+    int* light_types;      /* num_lights: 0 triangle, 1 sphere (include/lights/types.h:14-17) */
+    int* light_indices;
+    float* env_rgba;       /* env_width * env_height * 4 */
+    float* camera;         /* 11 floats: origin[3], target[3], up[3], vfov (radians), flip */
+} pt_scene_export;
+
+/* Launch shape and queue sizing (the autotuner's knobs). Zero fields keep the current value. */
+typedef struct pt_launch_config {
+    int wave_paths;        /* paths in flight per wave (queue capacity) */
+    int block_extend;      /* threads per block of the closest-hit stage */
+    int block_shade;
+    int block_shadow;
+    int blocks_per_sm;     /* persistent grid = SMs * blocks_per_sm */
+    int sort_materials;    /* 1: material-sorted shading, 2: off (0 keeps current) */
+    int use_graph;         /* 1: capture each frame's launch sequence in a CUDA graph, 2: off */
+} pt_launch_config;
+
+typedef struct pt_stats {
+    unsigned long long rays_camera;   /* camera rays of the last frame */
+    unsigned long long rays_extend;   /* closest-hit queries (camera + continuation) */
+    unsigned long long rays_shadow;   /* any-hit queries */
+    float last_frame_ms;              /* device time of the last completed frame */
+    int last_frame_spp;
+    int total_spp;
+    int frames;
+} pt_stats;
+
+/* Per-stage device time of the last frame (replaces the reference's single begin/end event
+ * pair and "CUDA Frame: X ms" print, path_tracer.cu:300-352). Stages: 0 camera, 1 extend
+ * (closest hit), 2 material sort, 3 shade, 4 shadow (any hit), 5 accumulate. Work counters
+ * are filled only for frames rendered with work counting on. */
+#define PT_NUM_STAGES 6
+typedef struct pt_profile {
+    float stage_ms[PT_NUM_STAGES];
+    int stage_launches[PT_NUM_STAGES];
+    unsigned long long extend_nodes;  /* wide BVH nodes loaded by closest-hit queries */
+    unsigned long long extend_prims;  /* leaf entries (triangles/spheres) tested */
+    unsigned long long shadow_nodes;
+    unsigned long long shadow_prims;
+    int bvh_width;
+    int node_bytes;                   /* bytes per wide node */
+    int prim_bytes;                   /* bytes per leaf entry */
+    int wave_paths;                   /* paths per wave of the last frame */
+} pt_profile;
+
+/* ---- session lifetime (RenderSession ctor, render_session.cu:55-117) ------------------ */
+int pt_create(int width, int height, pt_session** out);
+int pt_destroy(pt_session* s);
+const char* pt_last_error(const pt_session* s);
+/* Select the CUDA device for this session (default: current device). Call before any
+ * device work. */
+int pt_set_device(pt_session* s, int device);
+
+/* ---- scene (SceneParameters::getSceneData/getCamera, src/scene.cu:14-216) -------------- */
+/* Seeded procedural configuration: 0 Cornell box (36 triangles), 1 sixty-four spheres on a
+ * plane with 4 sphere emitters, 2 displaced icosphere (1,310,720 triangles) under a
+ * 2048x1024 environment map, 3 the same mesh in a closed room lit through a 0.05-wide slit.
+ * Also sets the camera and the default depth/NEE. Host work only (scene generation, BVH
+ * build); device upload is deferred to the first device call. */
+int pt_load_config(pt_session* s, int config, uint64_t seed);
+/* Same with an explicit icosphere level for configurations 2 and 3 (smaller test scenes). */
+int pt_load_config_level(pt_session* s, int config, uint64_t seed, int icosphere_level);
+int pt_load_arrays(pt_session* s, const pt_scene_desc* desc);
+int pt_scene_counts_get(const pt_session* s, pt_scene_counts* out);
+int pt_export_scene(const pt_session* s, pt_scene_export* out);
+/* Rebuild the BVH with a given width (2, 4, 8) and maximum leaf size (1..16). */
+int pt_set_bvh(pt_session* s, int width, int max_leaf);
+/* Host-side structural check of the BVH (containment, references); 0 if sound. */
+int pt_check_bvh(const pt_session* s);
+
+/* ---- scene model edits (SceneModel setters, src/scene_model.cu:41-347) ---------------- */
+/* Camera (Camera ctor + lookAt, src/core/camera.cu:5-21, src/transform.cu:7-33). */
+int pt_set_camera(pt_session* s, const float origin[3], const float target[3], const float up[3],
+                  float vfov_radians, int flip_handedness);
+/* Material edit of an existing id; changing the type resets the parameters to the
+ * reference's defaults for that type (Scene::setMaterialType, include/scene.h:36-61). */
+int pt_set_material(pt_session* s, int material_id, int type, const float albedo[3],
+                    const float emit[3], float ior, float alpha);
+int pt_set_max_depth(pt_session* s, int max_depth);  /* vertices per path (path_tracer.cu:165) */
+int pt_set_nee(pt_session* s, int enabled);          /* calculateLiNEE vs calculateLiNaive */
+int pt_set_seed(pt_session* s, uint64_t seed);
+/* Learned path guiding (not part of the reference). Returns PT_ERR_ARG when unavailable. */
+int pt_set_guiding(pt_session* s, int enabled);
+/* Restart progressive accumulation at the next frame (Renderer::reset). */
+int pt_reset(pt_session* s);
+int pt_set_launch(pt_session* s, const pt_launch_config* cfg);
+int pt_get_launch(const pt_session* s, pt_launch_config* out);
+
+/* ---- rendering (PathTracer::renderAsync/pollRender, path_tracer.cu:285-356) ----------- */
+int pt_render_async(pt_session* s, int spp);
+/* done = 1 when the frame in flight finished (its spp is then added to the running total);
+ * ms = its device time. done = 1 with no frame in flight. */
+int pt_poll(pt_session* s, int* done, float* ms);
+/* Block until the frame in flight finishes (pt_poll until done). */
+int pt_wait(pt_session* s, float* ms);
+int pt_get_spp(const pt_session* s, int* spp);
+int pt_get_stats(const pt_session* s, pt_stats* out);
+/* stage_timing: record an event after every launch of the following frames; work_counters:
+ * traversal kernels count nodes and leaf entries (slower; for roofline accounting). */
+int pt_set_profiling(pt_session* s, int stage_timing, int work_counters);
+int pt_get_profile(const pt_session* s, pt_profile* out);
+
+/* ---- readback (Renderer::getRadianceBuffer, src/renderers/renderer.cpp:20-42) --------- */
+/* Running-mean linear radiance, rows bottom-up like the reference (row 0 = image bottom),
+ * 3 floats per pixel; n = number of floats of `rgb` (>= 3 * width * height). */
+int pt_readback(pt_session* s, float* rgb, size_t n);
+/* Same for the last frame's own mean (passRadiances). */
+int pt_readback_pass(pt_session* s, float* rgb, size_t n);
+/* sRGB-encoded, clamped RGBA8 display buffer (framebuffer.cu:35-40); n bytes >= 4*W*H. */
+int pt_readback_rgba8(pt_session* s, uint8_t* rgba, size_t n);
+
+/* ---- queries --------------------------------------------------------------------------- */
+/* Material id under pixel (x = column, y = row) through its centre, -1 on a miss
+ * (RenderSession::hitTest, src/hit_test.cu:25-82). */
+int pt_hit_test(pt_session* s, int x, int y, int* material_id);
+/* Closest hit of n caller rays against the loaded scene, host arrays (parity entry for
+ * World::hit, src/world.cu:5-41). o, d: 3 floats per ray. Outputs per ray: prim_type (0
+ * triangle, 1 sphere, -1 miss), prim_id, mat_id (-1 on a miss), t. bary (2 per ray) may be
+ * NULL. */
+int pt_trace_rays(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax,
+                  int n, int* prim_type, int* prim_id, int* mat_id, float* t, float* bary);
+/* Same with device pointers (no copies; arrays must be device memory of this device). */
+int pt_trace_rays_device(pt_session* s, const float* o, const float* d, const float* tmin,
+                         const float* tmax, int n, int* prim_type, int* prim_id, int* mat_id,
+                         float* t, float* bary);
+/* Any-hit of n caller rays: occluded[i] = 1 when a primitive lies in [tmin, tmax]
+ * (the shadow query of directSampleLights, path_tracer.cu:101-113). */
+int pt_occluded(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax,
+                int n, int* occluded);
+
+/* Library version string. */
+const char* pt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PATHED_H */

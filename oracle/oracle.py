@@ -1,0 +1,220 @@
+"""ORACLE - test infrastructure, not product code.
+
+ctypes wrappers of liboracle.so (the CPU restatement of the reference integrator, built from
+oracle/oracle.cpp) and of _ref/libref_cpu.so (the reference's own sources compiled for the
+host CPU by `make -C oracle ref`). Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref_cpu.so")
+REF_TREE = os.environ.get("PATHED_REFERENCE", "/root/reference")
+
+
+def build(ref: bool = True) -> None:
+    """Compile liboracle.so, and the reference CPU library when the reference tree exists."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if ref and os.path.isdir(REF_TREE):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+
+
+def _f(a):
+    return np.ascontiguousarray(np.asarray(a, np.float32))
+
+
+def _i(a):
+    return np.ascontiguousarray(np.asarray(a, np.int32))
+
+
+class _SceneLib:
+    """Common scene handling of the two libraries (same create signature)."""
+
+    prefix = ""
+
+    def __init__(self, path):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        p = self.prefix
+        getattr(self.lib, p + "scene_create").restype = C.c_void_p
+        getattr(self.lib, p + "scene_create").argtypes = (
+            [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+            + [C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_void_p])
+        getattr(self.lib, p + "scene_destroy").argtypes = [C.c_void_p]
+
+    def scene(self, sc: dict):
+        """Create a scene from an export dict (pathed.Session.export_scene layout)."""
+        keep = [
+            _f(sc["tri_vertices"]), _f(sc["tri_normals"]), _i(sc["tri_materials"]), _f(sc["spheres"]),
+            _i(sc["sphere_materials"]), _i(sc["material_types"]), _f(sc["material_albedo"]),
+            _f(sc["material_emit"]), _f(sc["material_ior"]), _f(sc["material_alpha"]),
+        ]
+        env = sc.get("env_rgba")
+        env = None if env is None or env.size == 0 else _f(env)
+        ew, eh = (0, 0) if env is None else (env.shape[1], env.shape[0])
+        h = getattr(self.lib, self.prefix + "scene_create")(
+            keep[0].shape[0] if keep[0].ndim > 1 else keep[0].size // 9, keep[0].ctypes.data,
+            keep[1].ctypes.data, keep[2].ctypes.data,
+            keep[3].size // 4, keep[3].ctypes.data if keep[3].size else None,
+            keep[4].ctypes.data if keep[4].size else None,
+            keep[5].size, keep[5].ctypes.data, keep[6].ctypes.data, keep[7].ctypes.data, keep[8].ctypes.data,
+            keep[9].ctypes.data, ew, eh, None if env is None else env.ctypes.data)
+        return _SceneHandle(self, h, keep + [env])
+
+
+class _SceneHandle:
+    def __init__(self, owner, h, keep):
+        self.owner, self.h, self._keep = owner, h, keep
+
+    def __del__(self):
+        try:
+            getattr(self.owner.lib, self.owner.prefix + "scene_destroy")(self.h)
+        except Exception:
+            pass
+
+
+class Oracle(_SceneLib):
+    prefix = "oracle_"
+
+    def __init__(self, path=ORACLE_LIB):
+        super().__init__(path)
+        L = self.lib
+        L.oracle_trace.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_int]
+        L.oracle_render.argtypes = ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                     C.c_int, C.c_uint64, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_int])
+        L.oracle_bsdf_sample.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_float,
+                                         C.c_float, C.c_void_p]
+        L.oracle_bsdf_eval.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]
+        L.oracle_light_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_void_p]
+        L.oracle_camera_ray.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                        C.c_void_p]
+        L.oracle_dist1d.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
+        L.oracle_dist2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]
+        L.oracle_phitheta_pdf.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_int, C.c_void_p]
+        L.oracle_env_sample.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p]
+        L.oracle_rng.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, C.c_void_p]
+        L.oracle_num_lights.argtypes = [C.c_void_p]
+
+    def trace(self, scene, o, d, tmin, tmax, threads=0):
+        o, d = _f(o).reshape(-1, 3), _f(d).reshape(-1, 3)
+        n = o.shape[0]
+        tmin = _f(np.broadcast_to(np.asarray(tmin, np.float32), (n,)))
+        tmax = _f(np.broadcast_to(np.asarray(tmax, np.float32), (n,)))
+        out = {"prim_type": np.empty(n, np.int32), "prim_id": np.empty(n, np.int32),
+               "mat_id": np.empty(n, np.int32), "t": np.empty(n, np.float32)}
+        self.lib.oracle_trace(scene.h, o.ctypes.data, d.ctypes.data, tmin.ctypes.data, tmax.ctypes.data, n,
+                              out["prim_type"].ctypes.data, out["prim_id"].ctypes.data, out["mat_id"].ctypes.data,
+                              out["t"].ctypes.data, threads)
+        return out
+
+    def render(self, scene, camera, width, height, pixels, spp, max_depth, nee=True, seed=0x5EED, sample_base=0,
+               trace_once=True, threads=0):
+        pixels = _i(pixels)
+        n = pixels.size
+        mean = np.zeros((n, 3), np.float64)
+        var = np.zeros((n, 3), np.float64)
+        counts = np.zeros(3, np.uint64)
+        cam = _f(camera)
+        self.lib.oracle_render(scene.h, cam.ctypes.data, width, height, pixels.ctypes.data, n, spp, max_depth,
+                               int(bool(nee)), seed, sample_base, int(bool(trace_once)), mean.ctypes.data,
+                               var.ctypes.data, counts.ctypes.data, threads)
+        return mean, var, counts
+
+    def rng(self, seed, sample, pixel, n):
+        out = np.empty(n, np.float32)
+        self.lib.oracle_rng(seed, sample, pixel, n, out.ctypes.data)
+        return out
+
+
+class RefCPU(_SceneLib):
+    """The reference's own routines compiled for the host CPU."""
+
+    prefix = "ref_"
+
+    def __init__(self, path=REF_LIB):
+        super().__init__(path)
+        L = self.lib
+        L.ref_trace.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4
+        L.ref_bsdf_sample.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_float, C.c_float,
+                                      C.c_void_p]
+        L.ref_bsdf_eval.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_light_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_void_p]
+        L.ref_camera_ray.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                     C.c_void_p]
+        L.ref_dist1d.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]
+        L.ref_dist2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]
+        L.ref_phitheta_pdf.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_int, C.c_void_p]
+        L.ref_env_sample.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p]
+
+    def trace(self, scene, o, d, tmin, tmax):
+        o, d = _f(o).reshape(-1, 3), _f(d).reshape(-1, 3)
+        n = o.shape[0]
+        tmin = _f(np.broadcast_to(np.asarray(tmin, np.float32), (n,)))
+        tmax = _f(np.broadcast_to(np.asarray(tmax, np.float32), (n,)))
+        out = {"prim_type": np.empty(n, np.int32), "prim_id": np.empty(n, np.int32),
+               "mat_id": np.empty(n, np.int32), "t": np.empty(n, np.float32)}
+        self.lib.ref_trace(scene.h, o.ctypes.data, d.ctypes.data, tmin.ctypes.data, tmax.ctypes.data, n,
+                           out["prim_type"].ctypes.data, out["prim_id"].ctypes.data, out["mat_id"].ctypes.data,
+                           out["t"].ctypes.data)
+        return out
+
+
+def call_pair(fn_o, fn_r, *args, nout):
+    """Run the same unit routine in both libraries; returns (oracle_out, reference_out)."""
+    a = np.zeros(nout, np.float32)
+    b = np.zeros(nout, np.float32)
+    fn_o(*args, a.ctypes.data)
+    fn_r(*args, b.ctypes.data)
+    return a, b
+
+
+def dist1d(lib, values, xis):
+    """1-D distribution pmf/total/sample of either library ('oracle_' or 'ref_' prefix)."""
+    v, x = _f(values), _f(xis)
+    pmf = np.zeros(v.size, np.float32)
+    total = np.zeros(1, np.float32)
+    idx = np.zeros(x.size, np.int32)
+    spmf = np.zeros(x.size, np.float32)
+    fn = getattr(lib.lib, lib.prefix + "dist1d")
+    fn(v.ctypes.data, v.size, x.ctypes.data, x.size, pmf.ctypes.data, total.ctypes.data, idx.ctypes.data,
+       spmf.ctypes.data)
+    return pmf, float(total[0]), idx, spmf
+
+
+def dist2d(lib, values, w, h, xis):
+    v, x = _f(values), _f(xis).reshape(-1, 2)
+    pmf = np.zeros(w * h, np.float32)
+    sx = np.zeros(x.shape[0], np.int32)
+    sy = np.zeros(x.shape[0], np.int32)
+    spmf = np.zeros(x.shape[0], np.float32)
+    fn = getattr(lib.lib, lib.prefix + "dist2d")
+    fn(v.ctypes.data, w, h, x.ctypes.data, x.shape[0], pmf.ctypes.data, sx.ctypes.data, sy.ctypes.data,
+       spmf.ctypes.data)
+    return pmf.reshape(h, w), sx, sy, spmf
+
+
+def phitheta_pdf(lib, values, w, h, canon, dirs):
+    v = _f(values)
+    c = _f(canon).reshape(-1, 2)
+    d = _f(dirs).reshape(-1, 3)
+    pc = np.zeros(c.shape[0], np.float32)
+    pd = np.zeros(d.shape[0], np.float32)
+    fn = getattr(lib.lib, lib.prefix + "phitheta_pdf")
+    fn(v.ctypes.data, w, h, c.ctypes.data, c.shape[0], pc.ctypes.data, d.ctypes.data, d.shape[0], pd.ctypes.data)
+    return pc, pd

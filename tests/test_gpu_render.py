@@ -1,0 +1,172 @@
+"""Image parity of the wavefront integrator against the oracle, through the C ABI.
+
+Two checks per configuration:
+  * same streams: the GPU and the oracle consume identical PCG32 variates per path, so each
+    pixel's value must agree to FP32 rounding for nearly all pixels (a few paths may take a
+    different discrete branch after single-ulp differences in transcendental functions);
+  * statistics: the GPU's accumulated mean against the oracle run in the reference's own
+    trace convention (two traces per bounce, path_tracer.cu:51 and :177) with independent
+    samples, per-pixel |difference| <= 3 combined standard errors.
+"""
+import numpy as np
+import pytest
+
+import pathed
+from _util import pixel_subset, three_se_pass
+
+CASES = [(0, None, 96, 96, 8), (1, None, 96, 96, 8), (2, 4, 96, 54, 8), (3, 4, 96, 96, 8)]
+
+
+def _oracle_scene(oracle_lib, s):
+    sc = s.export_scene()
+    return sc, oracle_lib.scene(sc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"cfg{c[0]}")
+@pytest.mark.parametrize("nee", [True, False])
+def test_same_stream_agreement(oracle_lib, case, nee):
+    cfg, level, w, h, spp = case
+    s = pathed.Session(w, h)
+    s.load_config(cfg, level=level)
+    s.set_nee(nee)
+    s.render(spp)
+    img = s.readback().reshape(-1, 3).astype(np.float64)
+    sc, osc = _oracle_scene(oracle_lib, s)
+    pix = pixel_subset(w, h, 1500, seed=cfg)
+    mean, var, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, spp, s.counts().default_depth, nee=nee,
+                                     trace_once=True)
+    g = img[pix]
+    close = np.all(np.abs(g - mean) <= 1e-3 * np.abs(mean) + 1e-5, axis=1)
+    assert close.mean() >= 0.97, f"only {close.mean():.4f} of pixels agree"
+    assert abs(g.mean() - mean.mean()) <= 0.01 * abs(mean.mean()) + 1e-4
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES[:2], ids=lambda c: f"cfg{c[0]}")
+def test_statistical_parity_vs_reference_convention(oracle_lib, case):
+    cfg, level, w, h, _ = case
+    frames, spp = 8, 16
+    s = pathed.Session(w, h)
+    s.load_config(cfg, level=level)
+    s.set_seed(1234)
+    passes = []
+    for _ in range(frames):
+        s.render(spp)
+        passes.append(s.readback(pass_only=True).reshape(-1, 3).astype(np.float64))
+    passes = np.stack(passes)
+    sc, osc = _oracle_scene(oracle_lib, s)
+    pix = pixel_subset(w, h, 600, seed=1)
+    g_mean = passes[:, pix].mean(0)
+    g_se = passes[:, pix].std(0, ddof=1) / np.sqrt(frames)
+    o_mean, o_var, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, frames * spp, s.counts().default_depth,
+                                         nee=True, seed=99, trace_once=False)
+    frac = three_se_pass(g_mean, g_se, o_mean, np.sqrt(o_var))
+    assert frac >= 0.97, f"3-SE pass fraction {frac:.4f}"
+    s.close()
+
+
+@pytest.mark.gpu
+def test_depth_zero_and_one(oracle_lib):
+    s = pathed.Session(48, 48)
+    s.load_config(0)
+    s.set_max_depth(0)
+    s.render(2)
+    assert np.all(s.readback() == 0.0)  # calculateLiNEE returns 0 for maxDepth 0 (:148)
+    s.set_max_depth(1)
+    s.render(4)
+    img = s.readback().reshape(-1, 3)
+    sc, osc = _oracle_scene(oracle_lib, s)
+    pix = np.arange(48 * 48, dtype=np.int32)
+    mean, _, _ = oracle_lib.render(osc, sc["camera"], 48, 48, pix, 4, 1, nee=True)
+    assert np.allclose(img, mean, rtol=1e-4, atol=1e-5)  # emission seen directly only
+    s.close()
+
+
+@pytest.mark.gpu
+def test_progressive_running_mean():
+    s = pathed.Session(40, 40)
+    s.load_config(0)
+    s.render(4)
+    p1 = s.readback(pass_only=True).astype(np.float64)
+    s.render(12)
+    p2 = s.readback(pass_only=True).astype(np.float64)
+    acc = s.readback().astype(np.float64)
+    assert s.spp() == 16
+    # framebuffer.cu:23-33 running mean of the two passes
+    assert np.allclose(acc, (p1 * 4 + p2 * 12) / 16, rtol=1e-5, atol=1e-6)
+    s.reset()
+    s.render(4)
+    assert s.spp() == 4
+    s.close()
+
+
+@pytest.mark.gpu
+def test_rgba8_display_buffer():
+    s = pathed.Session(32, 32)
+    s.load_config(0)
+    s.render(8)
+    acc = s.readback().astype(np.float64)
+    rgba = s.readback_rgba8()
+    srgb = np.where(acc <= 0.0031308, acc * 12.92, 1.055 * np.power(np.maximum(acc, 0), 1 / 2.2) - 0.055)
+    expect = np.floor(np.clip(srgb, 0, 1) * 255)
+    assert np.max(np.abs(rgba[..., :3].astype(np.float64) - expect)) <= 1
+    assert np.all(rgba[..., 3] == 255)
+    s.close()
+
+
+@pytest.mark.gpu
+def test_material_and_camera_edits(oracle_lib):
+    w = h = 48
+    s = pathed.Session(w, h)
+    s.load_config(0)
+    s.set_material(0, pathed.MIRROR)      # white walls -> mirror (defaults of the new type)
+    s.set_material(1, pathed.LAMBERTIAN, albedo=(0.2, 0.8, 0.3), emit=(1.0, 0.5, 0.0))  # red wall now emits
+    s.set_camera((0.3, 1.1, 3.5), (0, 1, 0), (0, 1, 0), 0.7)
+    s.render(8)
+    img = s.readback().reshape(-1, 3)
+    sc, osc = _oracle_scene(oracle_lib, s)
+    assert sc["counts"].num_lights == 4  # the emitting wall's two triangles joined the emitter list
+    pix = pixel_subset(w, h, 800, seed=4)
+    mean, _, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, 8, s.counts().default_depth, nee=True)
+    close = np.all(np.abs(img[pix] - mean) <= 1e-3 * np.abs(mean) + 1e-5, axis=1)
+    assert close.mean() >= 0.97
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sort", [1, 2])
+@pytest.mark.parametrize("width", [2, 8])
+def test_launch_shapes_do_not_change_images(sort, width):
+    """queue capacity, block shape, BVH width and material sorting change scheduling only"""
+    s = pathed.Session(64, 64)
+    s.load_config(1)
+    s.render(4)
+    base = s.readback().copy()
+    s.set_bvh(width, 2)
+    s.set_launch(wave_paths=3000, block_extend=64, block_shade=256, block_shadow=96, blocks_per_sm=3,
+                 sort_materials=sort)
+    s.reset()
+    s.render(4)
+    other = s.readback()
+    # identical random streams and exact hits: only float summation order may differ
+    assert np.allclose(base, other, rtol=1e-5, atol=1e-6)
+    s.close()
+
+
+@pytest.mark.gpu
+def test_stats_count_canonical_queries(oracle_lib):
+    w = h = 32
+    s = pathed.Session(w, h)
+    s.load_config(0)
+    s.render(4)
+    st = s.stats()
+    assert st["rays_camera"] == w * h * 4
+    sc, osc = _oracle_scene(oracle_lib, s)
+    _, _, counts = oracle_lib.render(osc, sc["camera"], w, h, np.arange(w * h, dtype=np.int32), 4,
+                                     s.counts().default_depth, nee=True)
+    # same streams: the oracle's closest-hit and shadow query counts match the device counters
+    assert abs(int(counts[0]) - st["rays_extend"]) <= 0.01 * st["rays_extend"]
+    assert abs(int(counts[1]) - st["rays_shadow"]) <= 0.01 * st["rays_shadow"]
+    s.close()
