@@ -168,6 +168,10 @@ class Session:
             raise PathedError(rc, lib.pt_last_error(self._h).decode())
         return rc
 
+    def set_device(self, device: int):
+        """Select the CUDA device (the library's runtime keeps its own current device)."""
+        self._check(lib.pt_set_device(self._h, device))
+
     # ---- scene
     def load_config(self, config: int, seed: int = 0x5EED, level: int | None = None):
         if level is None:
