@@ -666,6 +666,31 @@ int Session::trace_rays(const float* o, const float* d, const float* tmin, const
     return PT_OK;
 }
 
+int Session::trace_rays_static(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pty,
+                               int* pid, int* mid, float* t, float* bary) {
+    if (n < 0 || n > kStaticTraceMaxRays)
+        return fail(PT_ERR_ARG, "ray count must be in [0, " + std::to_string(kStaticTraceMaxRays) + "]");
+    if (n > 0 && (!o || !d || !tmin || !tmax || !pty || !pid || !mid || !t)) return fail(PT_ERR_ARG, "null array");
+    // Nothing may be allocated here: device set-up and the scene upload must already be done.
+    if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (!dev_ready_ || scene_dirty_ || mats_dirty_)
+        return fail(PT_ERR_STATE,
+                    "scene not resident on the device; make one allocating device call (render, trace, hit "
+                    "test) after loading or editing the scene");
+    const int sd = bvh_.depth + 1;
+    if (stack_bytes(sd, 128) > (size_t)kMaxStackBytesDefault)
+        return fail(PT_ERR_SCENE, "BVH too deep for the traversal stack in shared memory");
+    int r;
+    if ((r = check_cuda(cudaSetDevice(device_), "cudaSetDevice"))) return r;
+    int of = 0;
+    if ((r = check_cuda(pt::trace_rays_static(scene_view(), sd, o, d, tmin, tmax, n, pty, pid, mid, t, bary, &of,
+                                              stream_),
+                        "static trace rays")))
+        return r;
+    if (of) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");
+    return PT_OK;
+}
+
 int Session::occluded(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* occ) {
     if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
     if (n < 0) return fail(PT_ERR_ARG, "negative ray count");

@@ -86,6 +86,10 @@ public:
     int trace_rays(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pt,
                    int* pid, int* mid, float* t, float* bary, bool device_ptrs);
     int occluded(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* occ);
+    // Allocation-free closest-hit queries (staging in a static device array); the scene must
+    // already be resident on the device.
+    int trace_rays_static(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pt,
+                          int* pid, int* mid, float* t, float* bary);
 
     const HostScene& scene() const { return scene_; }
     const CameraSpec& camera_spec() const { return camspec_; }

@@ -18,6 +18,7 @@
 #include "wavefront.h"
 
 #include <cfloat>
+#include <mutex>
 
 #include "dev_math.cuh"
 #include "dev_shade.cuh"
@@ -556,6 +557,73 @@ cudaError_t enqueue_occluded(const SceneDevice& sc, int stack_depth, const float
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+// ---- closest-hit queries without allocation ----------------------------------------------
+// Staging area of trace_rays_static, one per device that loads the library (about 3.7 MB,
+// held until the process exits): rays in (o, d, tmin, tmax), results out (type, id,
+// material, t, barycentrics) and the traversal-overflow flag. Every call reuses it and it
+// keeps the previous call's contents; the flag is cleared at the start of each call. Calls
+// whose work overlaps on the GPU (other streams, other host threads) race on it.
+namespace {
+constexpr size_t kStaticRayWords = 14;  // 3 + 3 + 1 + 1 floats in, 1 + 1 + 1 + 1 + 2 words out
+constexpr size_t kStaticScratchWords = (size_t)kStaticTraceMaxRays * kStaticRayWords + 64;
+static __device__ __align__(256) float g_trace_scratch[kStaticScratchWords];
+
+std::mutex g_scratch_mutex;
+float* g_scratch_addr[64] = {};
+
+cudaError_t static_scratch(float** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_trace_scratch);  // once per device, device current
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[dev] = static_cast<float*>(p);
+    }
+    *out = g_scratch_addr[dev];
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t trace_rays_static(const SceneDevice& sc, int stack_depth, const float* o, const float* d,
+                              const float* tmin, const float* tmax, int n, int* prim_type, int* prim_id,
+                              int* mat_id, float* t, float* bary, int* overflow, cudaStream_t stream) {
+    if (n < 0 || n > kStaticTraceMaxRays) return cudaErrorInvalidValue;
+    float* base = nullptr;
+    cudaError_t e = static_scratch(&base);
+    if (e != cudaSuccess) return e;
+    const size_t N = kStaticTraceMaxRays;
+    float* sO = base;
+    float* sD = sO + 3 * N;
+    float* sTmin = sD + 3 * N;
+    float* sTmax = sTmin + N;
+    int* sType = reinterpret_cast<int*>(sTmax + N);
+    int* sId = sType + N;
+    int* sMat = sId + N;
+    float* sT = reinterpret_cast<float*>(sMat + N);
+    float* sBary = sT + N;
+    int* sFlag = reinterpret_cast<int*>(sBary + 2 * N);
+    if ((e = cudaMemsetAsync(sFlag, 0, sizeof(int), stream))) return e;
+    if (n == 0) return cudaSuccess;
+    const size_t b = (size_t)n * sizeof(float);
+    if ((e = cudaMemcpyAsync(sO, o, 3 * b, cudaMemcpyHostToDevice, stream))) return e;
+    if ((e = cudaMemcpyAsync(sD, d, 3 * b, cudaMemcpyHostToDevice, stream))) return e;
+    if ((e = cudaMemcpyAsync(sTmin, tmin, b, cudaMemcpyHostToDevice, stream))) return e;
+    if ((e = cudaMemcpyAsync(sTmax, tmax, b, cudaMemcpyHostToDevice, stream))) return e;
+    if ((e = enqueue_trace_rays(sc, stack_depth, sO, sD, sTmin, sTmax, n, sType, sId, sMat, sT, sBary, sFlag, stream)))
+        return e;
+    if ((e = cudaMemcpyAsync(prim_type, sType, b, cudaMemcpyDeviceToHost, stream))) return e;
+    if ((e = cudaMemcpyAsync(prim_id, sId, b, cudaMemcpyDeviceToHost, stream))) return e;
+    if ((e = cudaMemcpyAsync(mat_id, sMat, b, cudaMemcpyDeviceToHost, stream))) return e;
+    if ((e = cudaMemcpyAsync(t, sT, b, cudaMemcpyDeviceToHost, stream))) return e;
+    if (bary && (e = cudaMemcpyAsync(bary, sBary, 2 * b, cudaMemcpyDeviceToHost, stream))) return e;
+    if ((e = cudaMemcpyAsync(overflow, sFlag, sizeof(int), cudaMemcpyDeviceToHost, stream))) return e;
+    return cudaStreamSynchronize(stream);
 }
 
 cudaError_t enqueue_hit_test(const SceneDevice& sc, const CameraParams& cam, int stack_depth, int x, int y,

@@ -117,6 +117,15 @@ cudaError_t enqueue_occluded(const SceneDevice& sc, int stack_depth, const float
 cudaError_t enqueue_hit_test(const SceneDevice& sc, const CameraParams& cam, int stack_depth, int x, int y,
                              int* out_material, int* overflow, cudaStream_t stream);
 
+// Closest-hit queries that allocate nothing: host rays in, host results out, staged through
+// a file-scope __device__ array of kStaticTraceMaxRays entries (see wavefront.cu). The
+// first call on a device looks the array's address up (cudaGetSymbolAddress) with that
+// device current. Returns cudaErrorInvalidValue for n outside [0, kStaticTraceMaxRays].
+constexpr int kStaticTraceMaxRays = 65536;
+cudaError_t trace_rays_static(const SceneDevice& sc, int stack_depth, const float* o, const float* d,
+                              const float* tmin, const float* tmax, int n, int* prim_type, int* prim_id,
+                              int* mat_id, float* t, float* bary, int* overflow, cudaStream_t stream);
+
 // Size in bytes of the traversal stack per block for `threads` threads.
 inline size_t stack_bytes(int stack_depth, int threads) { return (size_t)stack_depth * threads * sizeof(int2); }
 

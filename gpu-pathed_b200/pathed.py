@@ -31,7 +31,10 @@ EXPORTED = [
     "pt_set_launch", "pt_get_launch", "pt_render_async", "pt_poll", "pt_wait", "pt_get_spp", "pt_get_stats",
     "pt_readback", "pt_readback_pass", "pt_readback_rgba8", "pt_hit_test", "pt_trace_rays",
     "pt_trace_rays_device", "pt_occluded", "pt_version", "pt_set_profiling", "pt_get_profile",
+    "pt_trace_rays_static",
 ]
+
+STATIC_MAX_RAYS = 65536  # PT_STATIC_MAX_RAYS
 
 STAGES = ("camera", "extend", "sort", "shade", "shadow", "accumulate")
 
@@ -106,6 +109,7 @@ def _load():
     lib.pt_readback_rgba8.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.pt_trace_rays.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
     lib.pt_trace_rays_device.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
+    lib.pt_trace_rays_static.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
     lib.pt_occluded.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
     lib.pt_hit_test.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
     for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async"):

@@ -219,6 +219,22 @@ int pt_trace_rays(pt_session* s, const float* o, const float* d, const float* tm
 int pt_trace_rays_device(pt_session* s, const float* o, const float* d, const float* tmin,
                          const float* tmax, int n, int* prim_type, int* prim_id, int* mat_id,
                          float* t, float* bary);
+/* Allocation-free variant of pt_trace_rays. It has no counterpart in the reference.
+ * For callers that cannot call cudaMalloc: cudaMalloc and cudaFree may synchronize the
+ * device, so an interactive caller (picking under the cursor while a frame renders) would
+ * stall on the frame in flight; and a host whose device memory is fully owned by its own
+ * allocator (an engine, or a framework's caching allocator) has none to give. The call
+ * stages rays and results through one file-scope __device__ array of
+ * PT_STATIC_MAX_RAYS entries (about 3.7 MB, reserved on every GPU that loads the library
+ * until the process exits) and allocates nothing; n above PT_STATIC_MAX_RAYS is rejected
+ * with PT_ERR_ARG. The scene must already be on the device: after loading or editing it,
+ * make one ordinary device call first (otherwise PT_ERR_STATE). The first call on a device
+ * looks the array's address up; make that first call before any stream capture. All calls
+ * share the array and it keeps the last call's contents; calls whose work overlaps on the
+ * GPU (other sessions, streams or host threads) race on it. */
+#define PT_STATIC_MAX_RAYS 65536
+int pt_trace_rays_static(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax,
+                         int n, int* prim_type, int* prim_id, int* mat_id, float* t, float* bary);
 /* Any-hit of n caller rays: occluded[i] = 1 when a primitive lies in [tmin, tmax]
  * (the shadow query of directSampleLights, path_tracer.cu:101-113). */
 int pt_occluded(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax,

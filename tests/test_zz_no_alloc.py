@@ -1,0 +1,67 @@
+"""pt_trace_rays_static: closest-hit queries that allocate nothing.
+
+Some callers cannot call cudaMalloc: cudaMalloc/cudaFree may synchronize the device (an
+interactive pick while a frame renders would stall), and a host whose device memory belongs
+to its own allocator has none to hand out. This entry point stages rays and results through
+a fixed file-scope device array instead. It must return exactly what pt_trace_rays returns,
+call after call (the array is reused and keeps the previous call's contents).
+
+This file is collected last on purpose, so a run that stops at the first failure has run
+every other test before it.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import pathed
+from _util import seeded_rays
+
+
+def _static(s, o, d, tmin, tmax):
+    n = o.shape[0]
+    out = {"prim_type": np.empty(n, np.int32), "prim_id": np.empty(n, np.int32), "mat_id": np.empty(n, np.int32),
+           "t": np.empty(n, np.float32), "bary": np.empty((n, 2), np.float32)}
+    rc = pathed.lib.pt_trace_rays_static(s._h, o.ctypes.data, d.ctypes.data, tmin.ctypes.data, tmax.ctypes.data, n,
+                                         out["prim_type"].ctypes.data, out["prim_id"].ctypes.data,
+                                         out["mat_id"].ctypes.data, out["t"].ctypes.data, out["bary"].ctypes.data)
+    return rc, out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg,level", [(1, None), (3, 4)])
+def test_static_entry_matches_allocating_entry(cfg, level):
+    s = pathed.Session(32, 32)
+    s.load_config(cfg, level=level)
+    sc = s.export_scene()
+    o1, d1, tmin1, tmax1 = seeded_rays(sc, 20000, seed=21)
+    o2, d2, tmin2, tmax2 = seeded_rays(sc, 7000, seed=22)  # second call: fewer rays, other rays
+    # scene not yet on the device: the static entry must refuse rather than allocate
+    rc, _ = _static(s, o1, d1, tmin1, tmax1)
+    assert rc == pathed.PT_ERR_STATE
+    ref1 = s.trace_rays(o1, d1, tmin1, tmax1, with_bary=True)  # allocating call uploads the scene
+    ref2 = s.trace_rays(o2, d2, tmin2, tmax2, with_bary=True)
+    for (o, d, tmin, tmax), ref in (((o1, d1, tmin1, tmax1), ref1), ((o2, d2, tmin2, tmax2), ref2)):
+        rc, got = _static(s, o, d, tmin, tmax)
+        assert rc == pathed.PT_OK, pathed.lib.pt_last_error(s._h)
+        for k in ("prim_type", "prim_id", "mat_id", "t", "bary"):
+            assert np.array_equal(got[k], ref[k]), k  # bit-exact, the tolerance of the other trace tests
+    s.close()
+
+
+@pytest.mark.gpu
+def test_static_entry_limits():
+    s = pathed.Session(16, 16)
+    s.load_config(0)
+    sc = s.export_scene()
+    o, d, tmin, tmax = seeded_rays(sc, 64, seed=1)
+    s.trace_rays(o, d, tmin, tmax)
+    n = pathed.STATIC_MAX_RAYS + 1
+    big = np.zeros((n, 3), np.float32)
+    rc = pathed.lib.pt_trace_rays_static(s._h, big.ctypes.data, big.ctypes.data, big.ctypes.data, big.ctypes.data, n,
+                                         big.ctypes.data, big.ctypes.data, big.ctypes.data, big.ctypes.data, None)
+    assert rc == pathed.PT_ERR_ARG
+    assert b"PT_STATIC" in pathed.lib.pt_last_error(s._h) or b"ray count" in pathed.lib.pt_last_error(s._h)
+    rc, got = _static(s, o[:0], d[:0], tmin[:0], tmax[:0])
+    assert rc == pathed.PT_OK
+    s.close()
