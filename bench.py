@@ -287,8 +287,12 @@ def run_ours(args):
         per_launch_bytes = algo_bytes_frame / ext_launches
         ext_ms = stage_ms["extend"] / max(1, stage_launches["extend"])
         achieved = per_launch_bytes / (ext_ms / 1e3) / 1e9
+        bpq = _ncu_bytes_per_query()
+        # ncu measured one launch's DRAM bytes; scaled to the average launch by its queries
+        traffic = None if bpq is None else bpq * q_ext / ext_launches
         roof = {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": _ncu_traffic(),
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "traffic_source": "ncu dram bytes per query x queries per launch (profiles/k_extend_traffic.txt)",
                 "peak_source": peak_kind + " hbm_gbs (burst copy)",
                 "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": ext_ms,
                 "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
@@ -327,15 +331,16 @@ def run_ours(args):
     return 0
 
 
-def _ncu_traffic():
-    """DRAM bytes per extend launch from the committed ncu summary, when present."""
-    p = os.path.join(ROOT, "profiles", "extend_traffic.json")
-    if os.path.exists(p):
-        try:
-            with open(p) as f:
-                return json.load(f).get("dram_bytes_per_launch")
-        except Exception:
-            return None
+def _ncu_bytes_per_query():
+    """DRAM bytes per closest-hit query measured by ncu (profiles/k_extend_traffic.txt)."""
+    p = os.path.join(ROOT, "profiles", "k_extend_traffic.txt")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_query:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
     return None
 
 

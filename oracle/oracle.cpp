@@ -477,8 +477,8 @@ struct Beckmann {
         const float tan2 = (1.f - cos2) / cos2;
         if (std::isinf(tan2)) return 0.f;
         const float num = expf(-tan2 / a2);
-        const double den = M_PI * a2 * cos4;
-        return (float)(num / den);
+        const float den = M_PI * a2 * cos4;  // the double product is stored as float (microfacet.h:47-48)
+        return num / den;
     }
     Vec3 sampleWh(const Vec3& wo, float xi1, float xi2) const {
         const float phi = xi1 * M_PI * 2.f;
