@@ -158,6 +158,7 @@ def run_reference(args):
         vals.append(mr)
         per.append((mp, dt))
     v = sum(vals) / len(vals)
+    ref_cuda = _reference_cuda(args, rays_per_path=(v / per[0][0]) if per[0][0] > 0 else None)
     line = {
         "impl": "reference", "metric": "Mrays/s", "value": v, "unit": "Mrays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(p[1] for p in per) / len(per),
@@ -168,9 +169,50 @@ def run_reference(args):
         "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda": ref_cuda,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _reference_cuda(args, rays_per_path):
+    """The reference's own CUDA integrator (renderKernel from its sources, linear primitive
+    scan, curand) timed on this GPU on the same workload; Mrays/s from the canonical rays per
+    path of the CPU restatement (same estimator, same expected path lengths)."""
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        import pathed
+
+        if not os.path.exists(orc.REFBENCH_LIB):
+            return {"unavailable": "reference GPU build (oracle/_ref/librefbench.so) not built"}
+        wl = WORKLOADS[args.config]
+        w, h = wl["res"]
+        s = pathed.Session(w, h)
+        s.load_config(args.config)
+        sc = s.export_scene()
+        s.close()
+        rb = orc.RefBench()
+        rb.load(sc, w, h)
+        rb.render(1, wl["depth"], True)  # warm-up
+        ms = [rb.render(wl["spp"], wl["depth"], True) for _ in range(max(1, min(args.steps, 3)))]
+        rb.close()
+        mean_ms = sum(ms) / len(ms)
+        paths = w * h * wl["spp"]
+        out = {"ms_per_frame": mean_ms, "mpaths_per_s": paths / (mean_ms / 1e3) / 1e6,
+               "build": "reference sources (src/renderers/path_tracer.cu et al.), nvcc -O3 sm_100a, FMA on",
+               "frames": len(ms)}
+        if rays_per_path:
+            out["value"] = paths * rays_per_path / (mean_ms / 1e3) / 1e6
+            out["unit"] = "Mrays/s"
+            out["rays_per_path"] = rays_per_path
+        return out
+    except Exception as e:  # report, do not fail the arm
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def run_ours(args):

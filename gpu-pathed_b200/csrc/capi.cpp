@@ -200,6 +200,11 @@ int pt_get_launch(const pt_session* s, pt_launch_config* c) {
     return PT_OK;
 }
 
+int pt_autotune(pt_session* s, int spp, const char* cache_path, pt_tune_result* out) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.autotune(spp, cache_path, out); });
+}
+
 int pt_render_async(pt_session* s, int spp) {
     if (!s) return PT_ERR_ARG;
     return guarded(s, [&] { return s->impl.render_async(spp); });

@@ -191,10 +191,47 @@ struct TraceWork {
     unsigned prims = 0;  // leaf entries tested
 };
 
-// Stack entry: x = node index, y = (remaining count << 24) | 3-bit child slots, nearest first.
-// The stack holds at most one entry per tree level.
+// Next entry to process from the traversal stack, or kEmptyChild when it is empty.
+// Stack entry: x = node index, y = (remaining count << 24) | 3-bit child slots, nearest first;
+// the stack holds at most one entry per tree level. For closest-hit queries the popped child
+// is re-tested against the current hit distance; when it is culled, the siblings behind it
+// (sorted farther) are dropped with it.
+template <int W, bool ANY>
+__device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, const RayPre& r, float tmin, float tmax,
+                                         const Hit& best, int2* __restrict__ stk, int stride, int& sp) {
+    constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
+    while (sp > 0) {
+        const int2 ent = stk[(sp - 1) * stride];
+        const int parent = ent.x;
+        const uint32_t packed = (uint32_t)ent.y;
+        const int cnt = (int)(packed >> 24);
+        const uint32_t list = packed & 0xFFFFFFu;
+        const int sl = (int)(list & 7u);
+        if (cnt > 1) stk[(sp - 1) * stride] = make_int2(parent, (int)(((uint32_t)(cnt - 1) << 24) | (list >> 3)));
+        else sp--;
+        const float* pf = reinterpret_cast<const float*>(nodes + (size_t)parent * kNF4);
+        if (!ANY) {
+            const float tc = best.prim == kMissPrim ? tmax : best.t;
+            const float te = box_entry(r, __ldg(pf + 0 * W + sl), __ldg(pf + 1 * W + sl), __ldg(pf + 2 * W + sl),
+                                       __ldg(pf + 3 * W + sl), __ldg(pf + 4 * W + sl), __ldg(pf + 5 * W + sl), tmin,
+                                       tc * kBoxSlack);
+            if (te == __int_as_float(0x7f800000)) {
+                if (cnt > 1) sp--;
+                continue;
+            }
+        }
+        return __float_as_int(__ldg(pf + 6 * W + sl));
+    }
+    return kEmptyChild;
+}
+
+// Warp-synchronous traversal: every lane of the warp calls this together (`active` marks the
+// lanes that carry a query). Lanes advance through internal nodes in one phase and test
+// leaves in the next, re-converging at each phase boundary (the while-while organisation of
+// Aila and Laine, HPG 2009), so leaf tests and node visits execute as coherent SIMT
+// instructions instead of drifting apart. Returns whether the query hit.
 template <int W, bool ANY, bool CNT = false>
-__device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r, float tmin, float tmax,
+__device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r, float tmin, float tmax, bool active,
                                          int2* __restrict__ stk, int stride, int max_depth, Hit& best,
                                          int& overflow, TraceWork* work = nullptr) {
     constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
@@ -203,124 +240,95 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
     best.prim = kMissPrim;
     best.t = tmax;
     int sp = 0;
-    int node = sc.root;
-    for (;;) {
-        // ---- visit an internal node
-        NodeView<W> nv;
-        load_node<W>(nodes + (size_t)node * kNF4, nv);
-        if (CNT) work->nodes++;
-        const float tcur = best.prim == kMissPrim ? tmax : best.t;
-        const float tlim = tcur * kBoxSlack;
-        float key[W];
-        int slot[W];
-        int nhit = 0;
+    int cur = active ? sc.root : kEmptyChild;
+    bool alive = active;
+    bool hit_any = false;
+    while (__any_sync(0xffffffffu, alive)) {
+        // ---- phase 1: internal nodes, until this lane holds a leaf (or is finished)
+        while (__any_sync(0xffffffffu, alive && cur >= 0)) {
+            if (alive && cur >= 0) {
+                NodeView<W> nv;
+                load_node<W>(nodes + (size_t)cur * kNF4, nv);
+                if (CNT) work->nodes++;
+                const float tcur = best.prim == kMissPrim ? tmax : best.t;
+                const float tlim = tcur * kBoxSlack;
+                float key[W];
+                int slot[W];
+                int nhit = 0;
 #pragma unroll
-        for (int k = 0; k < W; k++) {
-            float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k],
-                                 tmin, tlim);
-            if (nv.child[k] == kEmptyChild) te = __int_as_float(0x7f800000);
-            key[k] = te;
-            slot[k] = k;
-            nhit += te != __int_as_float(0x7f800000) ? 1 : 0;
-        }
-        if (!ANY) {
-            // odd-even transposition sort of (key, slot), W <= 8
-#pragma unroll
-            for (int pass = 0; pass < W; pass++) {
-#pragma unroll
-                for (int k = (pass & 1); k + 1 < W; k += 2) {
-                    if (key[k + 1] < key[k]) {
-                        const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
-                        const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
-                    }
+                for (int k = 0; k < W; k++) {
+                    float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k],
+                                         tmin, tlim);
+                    if (nv.child[k] == kEmptyChild) te = __int_as_float(0x7f800000);
+                    key[k] = te;
+                    slot[k] = k;
+                    nhit += te != __int_as_float(0x7f800000) ? 1 : 0;
                 }
-            }
-        } else {
-            // any order; compact hits to the front
+                // odd-even transposition network: nearest first (closest hit) or hits first
 #pragma unroll
-            for (int pass = 0; pass < W; pass++) {
+                for (int pass = 0; pass < W; pass++) {
 #pragma unroll
-                for (int k = (pass & 1); k + 1 < W; k += 2) {
-                    const bool inf_k = key[k] == __int_as_float(0x7f800000);
-                    const bool inf_k1 = key[k + 1] == __int_as_float(0x7f800000);
-                    if (inf_k && !inf_k1) {
-                        const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
-                        const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
-                    }
-                }
-            }
-        }
-        int next_child = kEmptyChild;
-        if (nhit > 0) {
-            if (nhit > 1) {
-                uint32_t list = 0;
-#pragma unroll
-                for (int k = W - 1; k >= 1; k--) {
-                    if (k < nhit) list = (list << 3) | (uint32_t)slot[k];
-                }
-                if (sp >= max_depth) {
-                    overflow = 1;
-                    return best.prim != kMissPrim;
-                }
-                stk[sp * stride] = make_int2(node, (int)(((uint32_t)(nhit - 1) << 24) | list));
-                sp++;
-            }
-            int sel = slot[0];
-            int c = kEmptyChild;
-#pragma unroll
-            for (int k = 0; k < W; k++)
-                if (k == sel) c = nv.child[k];
-            next_child = c;
-        }
-        // ---- descend / process leaves / pop
-        for (;;) {
-            if (next_child != kEmptyChild) {
-                const int c = next_child;
-                next_child = kEmptyChild;
-                if (!child_is_leaf(c)) {
-                    node = c;
-                    break;
-                }
-                const int first = leaf_first(c), cnt = leaf_count(c);
-                if (CNT) work->prims += cnt;
-                if (ANY) {
-                    for (int e = first; e < first + cnt; e++) {
-                        if (leaf_entry_any(prims, e, r, tmin, tmax)) {
-                            best.prim = 0;
-                            return true;
+                    for (int k = (pass & 1); k + 1 < W; k += 2) {
+                        const bool swap = ANY ? (key[k] == __int_as_float(0x7f800000) &&
+                                                 key[k + 1] != __int_as_float(0x7f800000))
+                                              : (key[k + 1] < key[k]);
+                        if (swap) {
+                            const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
+                            const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
                         }
                     }
-                } else {
-                    for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
                 }
+                int next = kEmptyChild;
+                if (nhit > 0) {
+                    if (nhit > 1) {
+                        uint32_t list = 0;
+#pragma unroll
+                        for (int k = W - 1; k >= 1; k--)
+                            if (k < nhit) list = (list << 3) | (uint32_t)slot[k];
+                        if (sp >= max_depth) {
+                            overflow = 1;
+                            alive = false;  // reported to the host; the query gives up
+                        } else {
+                            stk[sp * stride] = make_int2(cur, (int)(((uint32_t)(nhit - 1) << 24) | list));
+                            sp++;
+                        }
+                    }
+                    const int sel = slot[0];
+#pragma unroll
+                    for (int k = 0; k < W; k++)
+                        if (k == sel) next = nv.child[k];
+                }
+                if (alive && next == kEmptyChild) next = stack_pop<W, ANY>(nodes, r, tmin, tmax, best, stk, stride, sp);
+                cur = next;
+                if (cur == kEmptyChild) alive = false;
             }
-            if (sp == 0) return best.prim != kMissPrim;
-            int2 ent = stk[(sp - 1) * stride];
-            const int parent = ent.x;
-            const uint32_t packed = (uint32_t)ent.y;
-            const int cnt = (int)(packed >> 24);
-            const uint32_t list = packed & 0xFFFFFFu;
-            const int sl = (int)(list & 7u);
-            if (cnt > 1) {
-                stk[(sp - 1) * stride] = make_int2(parent, (int)(((uint32_t)(cnt - 1) << 24) | (list >> 3)));
+        }
+        // ---- phase 2: leaves
+        if (alive) {
+            const int first = leaf_first(cur), cnt = leaf_count(cur);
+            if (CNT) work->prims += cnt;
+            if (ANY) {
+                for (int e = first; e < first + cnt; e++) {
+                    if (leaf_entry_any(prims, e, r, tmin, tmax)) {
+                        hit_any = true;
+                        break;
+                    }
+                }
+                if (hit_any) alive = false;
             } else {
-                sp--;
+                for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
             }
-            const float* pf = reinterpret_cast<const float*>(nodes + (size_t)parent * kNF4);
-            if (!ANY) {
-                // re-test against the shrunken interval; siblings behind it are farther
-                const float tc = best.prim == kMissPrim ? tmax : best.t;
-                const float te = box_entry(r, __ldg(pf + 0 * W + sl), __ldg(pf + 1 * W + sl), __ldg(pf + 2 * W + sl),
-                                           __ldg(pf + 3 * W + sl), __ldg(pf + 4 * W + sl), __ldg(pf + 5 * W + sl),
-                                           tmin, tc * kBoxSlack);
-                if (te == __int_as_float(0x7f800000)) {
-                    if (cnt > 1) sp--;
-                    continue;
-                }
+            if (alive) {
+                cur = stack_pop<W, ANY>(nodes, r, tmin, tmax, best, stk, stride, sp);
+                if (cur == kEmptyChild) alive = false;
             }
-            next_child = __float_as_int(__ldg(pf + 6 * W + sl));
         }
     }
+    if (ANY) {
+        if (hit_any) best.prim = 0;
+        return hit_any;
+    }
+    return best.prim != kMissPrim;
 }
 
 }  // namespace pt

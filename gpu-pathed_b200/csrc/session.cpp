@@ -2,6 +2,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "../../include/pathed.h"
@@ -24,6 +26,8 @@ Session::~Session() {
         if (ev_begin_) cudaEventDestroy(ev_begin_);
         if (ev_end_) cudaEventDestroy(ev_end_);
         for (cudaEvent_t e : mark_events_) cudaEventDestroy(e);
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (h_dyn_) cudaFreeHost(h_dyn_);
         if (stream_) cudaStreamDestroy(stream_);
         if (h_stats_) cudaFreeHost(h_stats_);
     }
@@ -70,8 +74,17 @@ int Session::ensure_device() {
     std::memset(h_stats_, 0, sizeof(FrameStats));
     if ((r = check_cuda(d_counters_.alloc(sizeof(WaveCounters)), "counters"))) return r;
     if ((r = check_cuda(d_stats_.alloc(sizeof(FrameStats)), "stats"))) return r;
+    if ((r = check_cuda(d_dyn_.alloc(sizeof(FrameDyn)), "frame constants"))) return r;
+    if ((r = check_cuda(cudaMallocHost((void**)&h_dyn_, sizeof(FrameDyn)), "cudaMallocHost"))) return r;
     dev_ready_ = true;
     return PT_OK;
+}
+
+void Session::update_material_classes() {
+    bool seen[4] = {false, false, false, false};
+    for (int m : scene_.tri_mat) seen[scene_.mats[m].type & 3] = true;
+    for (int m : scene_.sph_mat) seen[scene_.mats[m].type & 3] = true;
+    material_classes_ = (int)seen[0] + (int)seen[1] + (int)seen[2] + (int)seen[3];
 }
 
 int Session::load_config(int config, uint64_t seed, int level) {
@@ -105,6 +118,7 @@ int Session::load_scene(HostScene&& s) {
     have_scene_ = true;
     scene_dirty_ = true;
     mats_dirty_ = true;
+    update_material_classes();
     reset();
     return PT_OK;
 }
@@ -223,6 +237,7 @@ int Session::set_material(int id, int type, const float* albedo, const float* em
     }
     finalize_materials(scene_);
     lights_ = build_light_list(scene_);
+    update_material_classes();
     mats_dirty_ = true;
     reset();
     return PT_OK;
@@ -248,12 +263,14 @@ int Session::set_launch(const pt_launch_config* c) {
         return fail(PT_ERR_ARG, "block sizes must be multiples of 32 in [32, 1024]");
     if (c->wave_paths < 0 || c->blocks_per_sm < 0 || c->blocks_per_sm > 64)
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
+    if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2)
+        return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
     if (c->block_extend) shape_.block_extend = c->block_extend;
     if (c->block_shade) shape_.block_shade = c->block_shade;
     if (c->block_shadow) shape_.block_shadow = c->block_shadow;
     if (c->blocks_per_sm) shape_.blocks_per_sm = c->blocks_per_sm;
-    if (c->sort_materials) shape_.sort_materials = c->sort_materials == 1 ? 1 : 0;
+    if (c->sort_materials) sort_mode_ = c->sort_materials == 1 ? 1 : c->sort_materials == 2 ? 0 : -1;
     if (c->use_graph) use_graph_ = c->use_graph == 1 ? 1 : 0;
     return PT_OK;
 }
@@ -264,7 +281,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->block_shade = shape_.block_shade;
     c->block_shadow = shape_.block_shadow;
     c->blocks_per_sm = shape_.blocks_per_sm;
-    c->sort_materials = shape_.sort_materials ? 1 : 2;
+    c->sort_materials = sort_mode_ == 1 ? 1 : sort_mode_ == 0 ? 2 : 3;
     c->use_graph = use_graph_ ? 1 : 2;
 }
 
@@ -389,9 +406,10 @@ int Session::render_async(int spp) {
         total_spp_ = 0;
         reset_pending_ = false;
     }
-    FrameParams p{};
+    FrameParams p;
+    std::memset(&p, 0, sizeof(p));  // padding too: the graph cache compares these bytes
     p.sc = scene_view();
-    p.cam = cam_;
+    p.dyn = d_dyn_.as<FrameDyn>();
     for (int k = 0; k < 2; k++) {
         p.q[k].o = d_q_[k][0].as<float4>();
         p.q[k].d = d_q_[k][1].as<float4>();
@@ -413,17 +431,20 @@ int Session::render_async(int spp) {
     p.width = w_;
     p.height = h_;
     p.spp = spp;
-    p.prev_spp = total_spp_;
     p.max_depth = max_depth_;
     p.nee = nee_;
-    p.seed = seed_;
-    p.sample_base = (uint64_t)total_spp_;
     p.wave_pixels = queue_cap_ / spp;
     p.stack_depth = stack_depth;
     p.num_sms = num_sms_;
     p.count_work = work_counters_;
     p.shape = shape_;
+    p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 3 ? 1 : 0);
     last_wave_paths_ = p.wave_pixels * spp;
+    // per-frame constants: one pinned copy ahead of the frame's launches
+    h_dyn_->cam = cam_;
+    h_dyn_->seed = seed_;
+    h_dyn_->sample_base = (uint64_t)total_spp_;
+    h_dyn_->prev_spp = total_spp_;
     StageMarks* mk = nullptr;
     marks_active_ = false;
     if (stage_timing_) {
@@ -444,7 +465,37 @@ int Session::render_async(int spp) {
     }
     if ((r = check_cuda(cudaMemsetAsync(d_stats_.p, 0, sizeof(FrameStats), stream_), "stats reset"))) return r;
     if ((r = check_cuda(cudaEventRecord(ev_begin_, stream_), "cudaEventRecord"))) return r;
-    if ((r = check_cuda(enqueue_frame(p, stream_, mk), "frame launch"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(d_dyn_.p, h_dyn_, sizeof(FrameDyn), cudaMemcpyHostToDevice, stream_),
+                        "frame constants")))
+        return r;
+    if (use_graph_ && !mk) {
+        // replay the captured frame while every launch parameter is unchanged
+        if (!graph_valid_ || std::memcmp(&graph_params_, &p, sizeof(p)) != 0) {
+            if (graph_exec_) {
+                cudaGraphExecDestroy(graph_exec_);
+                graph_exec_ = nullptr;
+            }
+            graph_valid_ = false;
+            cudaGraph_t g = nullptr;
+            if ((r = check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture")))
+                return r;
+            const cudaError_t ce = enqueue_frame(p, stream_, nullptr);
+            const cudaError_t ee = cudaStreamEndCapture(stream_, &g);
+            if ((r = check_cuda(ce != cudaSuccess ? ce : ee, "graph capture"))) {
+                if (g) cudaGraphDestroy(g);
+                return r;
+            }
+            const cudaError_t ie = cudaGraphInstantiate(&graph_exec_, g, 0);
+            cudaGraphDestroy(g);
+            if ((r = check_cuda(ie, "graph instantiate"))) return r;
+            graph_params_ = p;
+            graph_valid_ = true;
+            graph_captures_++;
+        }
+        if ((r = check_cuda(cudaGraphLaunch(graph_exec_, stream_), "graph launch"))) return r;
+    } else if ((r = check_cuda(enqueue_frame(p, stream_, mk), "frame launch"))) {
+        return r;
+    }
     if ((r = check_cuda(cudaMemcpyAsync(h_stats_, d_stats_.p, sizeof(FrameStats), cudaMemcpyDeviceToHost, stream_),
                         "stats readback")))
         return r;
@@ -527,6 +578,154 @@ int Session::stats(pt_stats* out) const {
     out->last_frame_spp = last_spp_;
     out->total_spp = total_spp_;
     out->frames = frames_;
+    return PT_OK;
+}
+
+namespace {
+std::string tune_key(const HostScene& s, int classes, int w, int h, int spp, int depth, int nee) {
+    return "t" + std::to_string(s.num_tri()) + "_s" + std::to_string(s.num_sph()) + "_c" + std::to_string(classes) +
+           "_e" + std::to_string(s.env_w) + "_" + std::to_string(w) + "x" + std::to_string(h) + "_spp" +
+           std::to_string(spp) + "_d" + std::to_string(depth) + "_n" + std::to_string(nee);
+}
+int json_int(const std::string& line, const char* field, int dflt) {
+    const std::string k = std::string("\"") + field + "\": ";
+    const size_t p = line.find(k);
+    return p == std::string::npos ? dflt : std::atoi(line.c_str() + p + k.size());
+}
+double json_num(const std::string& line, const char* field, double dflt) {
+    const std::string k = std::string("\"") + field + "\": ";
+    const size_t p = line.find(k);
+    return p == std::string::npos ? dflt : std::atof(line.c_str() + p + k.size());
+}
+}  // namespace
+
+int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
+    if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    if (spp < 1) return fail(PT_ERR_ARG, "spp must be >= 1");
+    pt_tune_result res;
+    std::memset(&res, 0, sizeof(res));
+    const std::string key = tune_key(scene_, material_classes_, w_, h_, spp, max_depth_, nee_);
+    struct Cand {
+        int width, sort, bps, block;
+    };
+    auto apply = [&](const Cand& c) -> int {
+        int r;
+        if (c.width != bvh_width_ && (r = set_bvh(c.width, bvh_leaf_))) return r;
+        sort_mode_ = c.sort;
+        shape_.blocks_per_sm = c.bps;
+        shape_.block_extend = shape_.block_shadow = c.block;
+        return PT_OK;
+    };
+    if (cache_path) {
+        FILE* f = std::fopen(cache_path, "r");
+        if (f) {
+            char buf[1024];
+            const std::string want = "\"key\": \"" + key + "\"";
+            while (std::fgets(buf, sizeof(buf), f)) {
+                const std::string line(buf);
+                if (line.find(want) == std::string::npos) continue;
+                Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
+                       json_int(line, "block", 128)};
+                std::fclose(f);
+                int r;
+                if ((r = apply(c))) return r;
+                res.bvh_width = c.width;
+                res.sort_materials = c.sort == 1 ? 1 : 2;
+                res.blocks_per_sm = c.bps;
+                res.block = c.block;
+                res.wave_paths = wave_paths_;
+                res.best_ms = (float)json_num(line, "ms", 0.0);
+                res.from_cache = 1;
+                reset();
+                if (out) *out = res;
+                return PT_OK;
+            }
+            std::fclose(f);
+        }
+    }
+    const int saved_timing = stage_timing_;
+    stage_timing_ = 0;
+    int trials = 0;
+    auto measure = [&](const Cand& c, float& ms_out) -> int {
+        int r;
+        if ((r = apply(c))) return r;
+        float best = 1e30f;
+        for (int k = 0; k < 3; k++) {  // first frame warms up (and captures the graph)
+            reset();
+            if ((r = render_async(spp))) return r;
+            float ms = 0.f;
+            if ((r = wait(&ms))) return r;
+            if (k > 0) best = std::min(best, ms);
+        }
+        trials += 2;
+        ms_out = best;
+        return PT_OK;
+    };
+    const int prims = scene_.num_tri() + scene_.num_sph();
+    Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 3 ? 1 : 0), shape_.blocks_per_sm,
+              shape_.block_extend};
+    float best_ms;
+    int r;
+    if ((r = measure(best, best_ms))) return r;
+    res.default_ms = best_ms;
+    auto consider = [&](Cand c) -> int {
+        float ms;
+        int rr;
+        if ((rr = measure(c, ms))) return rr;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+        return PT_OK;
+    };
+    // coordinate descent: BVH width, then material sorting, then grid and block size
+    const int widths_small[3] = {2, 4, 8}, widths_large[2] = {4, 8};
+    const int* widths = prims < 100000 ? widths_small : widths_large;
+    const int nw = prims < 100000 ? 3 : 2;
+    const Cand start = best;
+    for (int i = 0; i < nw; i++)
+        if (widths[i] != start.width) {
+            Cand c = best;
+            c.width = widths[i];
+            if ((r = consider(c))) return r;
+        }
+    if (material_classes_ >= 2) {
+        Cand c = best;
+        c.sort = best.sort ? 0 : 1;
+        if ((r = consider(c))) return r;
+    }
+    for (int bps : {8, 24}) {
+        Cand c = best;
+        c.bps = bps;
+        if ((r = consider(c))) return r;
+    }
+    {
+        Cand c = best;
+        c.block = best.block == 128 ? 256 : 128;
+        if ((r = consider(c))) return r;
+    }
+    if ((r = apply(best))) return r;
+    stage_timing_ = saved_timing;
+    reset();
+    res.bvh_width = best.width;
+    res.sort_materials = best.sort == 1 ? 1 : 2;
+    res.blocks_per_sm = best.bps;
+    res.block = best.block;
+    res.wave_paths = wave_paths_;
+    res.best_ms = best_ms;
+    res.trials = trials;
+    if (cache_path) {
+        FILE* f = std::fopen(cache_path, "a");
+        if (f) {
+            std::fprintf(f,
+                         "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
+                         "\"wave_paths\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
+                         key.c_str(), best.width, best.sort, best.bps, best.block, wave_paths_, best_ms, res.default_ms);
+            std::fclose(f);
+        }
+    }
+    if (out) *out = res;
     return PT_OK;
 }
 

@@ -136,8 +136,8 @@ private:
     DevBuf d_L_, d_sort_, d_counters_, d_stats_, d_scratch_;
     int queue_cap_ = 0;
     LaunchShape shape_;
-    int wave_paths_ = 1 << 21;
-    int use_graph_ = 0;
+    int wave_paths_ = 1 << 25;  // 32M paths in flight (about 7.4 GB of queues)
+    int use_graph_ = 1;
     int total_spp_ = 0;
     bool reset_pending_ = true;
     bool in_flight_ = false;
@@ -159,6 +159,22 @@ private:
     int stage_launches_[kNumStages] = {};
     int last_wave_paths_ = 0;
     size_t smem_configured_ = 48 * 1024;
+    // per-frame constants (device) and their pinned staging copy
+    DevBuf d_dyn_;
+    FrameDyn* h_dyn_ = nullptr;
+    // CUDA graph of one frame's launches, valid while the captured FrameParams are unchanged
+    cudaGraphExec_t graph_exec_ = nullptr;
+    FrameParams graph_params_{};
+    bool graph_valid_ = false;
+    int graph_captures_ = 0;
+    // material sorting: 1 on, 0 off, -1 automatic (on when >= 3 material classes are present)
+    int sort_mode_ = -1;
+    int material_classes_ = 1;
+    void update_material_classes();
+
+public:
+    int graph_captures() const { return graph_captures_; }
+    int autotune(int spp, const char* cache_path, ::pt_tune_result* out);
 };
 
 }  // namespace pt

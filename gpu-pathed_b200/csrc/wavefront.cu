@@ -56,6 +56,14 @@ __device__ __forceinline__ int warp_fetch(int* cursor) {
 
 __global__ void k_camera(FrameParams p, long long wave_first, int n) {
     const PathQueue q = p.q[0];
+    __shared__ CameraParams cam;
+    __shared__ uint64_t seed, sample_base;
+    if (threadIdx.x == 0) {
+        cam = p.dyn->cam;
+        seed = p.dyn->seed;
+        sample_base = p.dyn->sample_base;
+    }
+    __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const long long gp = wave_first + i;
         const int pixel = (int)(gp / p.spp);
@@ -63,11 +71,11 @@ __global__ void k_camera(FrameParams p, long long wave_first, int n) {
         const int row = pixel / p.width;
         const int col = pixel - row * p.width;
         const uint64_t inc = pcg_inc((uint32_t)pixel);
-        uint64_t st = pcg_seed(p.seed, p.sample_base + (uint64_t)s, (uint32_t)pixel);
+        uint64_t st = pcg_seed(seed, sample_base + (uint64_t)s, (uint32_t)pixel);
         const float xi1 = pcg_uniform(st, inc);
         const float xi2 = pcg_uniform(st, inc);
         V o, d;
-        camera_ray(p.cam, row, col, xi1, xi2, o, d);
+        camera_ray(cam, row, col, xi1, xi2, o, d);
         q.o[i] = make_float4(o.x, o.y, o.z, __int_as_float(i));
         q.d[i] = make_float4(d.x, d.y, d.z, 0.f);
         q.beta[i] = make_float4(1.f, 1.f, 1.f, __int_as_float(1));  // camera ray: no MIS
@@ -113,15 +121,16 @@ __global__ void k_extend(FrameParams p, int depth) {
         const int base = warp_fetch(&p.counters->work_extend[depth]);
         if (base >= count) break;
         const int i = base + lane;
+        const bool valid = i < count;
         int key = -1;
-        if (i < count) {
-            const float4 o = q.o[i];
-            const float4 d = q.d[i];
-            const RayPre r = make_raypre(mkv(o), mkv(d));
-            Hit h;
-            int of = 0;
-            traverse<W, false, CNT>(p.sc, r, tmin, FLT_MAX, stk + threadIdx.x, blockDim.x, p.stack_depth, h, of,
-                                    &work);
+        const float4 o = valid ? q.o[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 d = valid ? q.d[i] : make_float4(0.f, 0.f, 1.f, 0.f);
+        const RayPre r = make_raypre(mkv(o), mkv(d));
+        Hit h;
+        int of = 0;
+        traverse<W, false, CNT>(p.sc, r, tmin, FLT_MAX, valid, stk + threadIdx.x, blockDim.x, p.stack_depth, h, of,
+                                &work);
+        if (valid) {
             if (of) atomicOr(&p.stats->error, 1);
             q.hit[i] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
             if (p.shape.sort_materials) {
@@ -323,14 +332,15 @@ __global__ void k_shadow(FrameParams p, int depth) {
         const int base = warp_fetch(&p.counters->work_shadow[depth]);
         if (base >= count) break;
         const int i = base + lane;
-        if (i < count) {
-            const float4 o = p.sq.o[i];
-            const float4 d = p.sq.d[i];
-            const RayPre r = make_raypre(mkv(o), mkv(d));
-            Hit h;
-            int of = 0;
-            const bool occ = traverse<W, true, CNT>(p.sc, r, kShadowTMin, o.w, stk + threadIdx.x, blockDim.x,
-                                                    p.stack_depth, h, of, &work);
+        const bool valid = i < count;
+        const float4 o = valid ? p.sq.o[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 d = valid ? p.sq.d[i] : make_float4(0.f, 0.f, 1.f, 0.f);
+        const RayPre r = make_raypre(mkv(o), mkv(d));
+        Hit h;
+        int of = 0;
+        const bool occ = traverse<W, true, CNT>(p.sc, r, kShadowTMin, o.w, valid, stk + threadIdx.x, blockDim.x,
+                                                p.stack_depth, h, of, &work);
+        if (valid) {
             if (of) atomicOr(&p.stats->error, 1);
             if (!occ) {
                 const float4 c = p.sq.c[i];
@@ -362,9 +372,10 @@ __global__ void k_accumulate(FrameParams p, int first_pixel, int npix) {
     p.pass_rgb[3 * (size_t)pixel + 1] = g;
     p.pass_rgb[3 * (size_t)pixel + 2] = b;
     float nr = r, ng = g, nb = b;
-    if (p.prev_spp > 0) {  // running mean (framebuffer.cu:23-33)
-        const float prev = (float)p.prev_spp;
-        const float total = (float)(p.prev_spp + p.spp);
+    const int prev_spp = p.dyn->prev_spp;
+    if (prev_spp > 0) {  // running mean (framebuffer.cu:23-33)
+        const float prev = (float)prev_spp;
+        const float total = (float)(prev_spp + p.spp);
         const float wpass = 1.f * p.spp / total;
         nr = p.accum_rgb[3 * (size_t)pixel + 0] * prev / total + r * wpass;
         ng = p.accum_rgb[3 * (size_t)pixel + 1] * prev / total + g * wpass;
@@ -450,11 +461,13 @@ __global__ void k_trace_rays(SceneDevice sc, int stack_depth, const float* __res
                              float* t, float* bary, int* overflow) {
     extern __shared__ int2 stk[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const RayPre r = make_raypre(mkv(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mkv(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
+    const bool valid = i < n;  // every lane enters the warp-synchronous traversal
+    const int j = valid ? i : 0;
+    const RayPre r = make_raypre(mkv(o[3 * j], o[3 * j + 1], o[3 * j + 2]), mkv(d[3 * j], d[3 * j + 1], d[3 * j + 2]));
     Hit h;
     int of = 0;
-    traverse<W, false>(sc, r, tmin[i], tmax[i], stk + threadIdx.x, blockDim.x, stack_depth, h, of);
+    traverse<W, false>(sc, r, tmin[j], tmax[j], valid, stk + threadIdx.x, blockDim.x, stack_depth, h, of);
+    if (!valid) return;
     if (of) atomicOr(overflow, 1);
     if (h.prim == kMissPrim) {
         prim_type[i] = -1;
@@ -483,24 +496,28 @@ __global__ void k_occluded(SceneDevice sc, int stack_depth, const float* __restr
                            const float* __restrict__ tmax, int n, int* occluded, int* overflow) {
     extern __shared__ int2 stk[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const RayPre r = make_raypre(mkv(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mkv(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
+    const bool valid = i < n;
+    const int j = valid ? i : 0;
+    const RayPre r = make_raypre(mkv(o[3 * j], o[3 * j + 1], o[3 * j + 2]), mkv(d[3 * j], d[3 * j + 1], d[3 * j + 2]));
     Hit h;
     int of = 0;
-    occluded[i] = traverse<W, true>(sc, r, tmin[i], tmax[i], stk + threadIdx.x, blockDim.x, stack_depth, h, of) ? 1 : 0;
+    const bool occ = traverse<W, true>(sc, r, tmin[j], tmax[j], valid, stk + threadIdx.x, blockDim.x, stack_depth, h, of);
+    if (!valid) return;
+    occluded[i] = occ ? 1 : 0;
     if (of) atomicOr(overflow, 1);
 }
 
 template <int W>
 __global__ void k_hit_test(SceneDevice sc, CameraParams cam, int stack_depth, int x, int y, int* out, int* overflow) {
     extern __shared__ int2 stk[];
-    if (threadIdx.x != 0) return;
     V o, d;
     camera_ray(cam, y, x, 0.5f, 0.5f, o, d);
     const RayPre r = make_raypre(o, d);
     Hit h;
     int of = 0;
-    traverse<W, false>(sc, r, 0.f, FLT_MAX, stk, 1, stack_depth, h, of);
+    // the whole warp enters the traversal; lane 0 carries the query and owns the stack
+    traverse<W, false>(sc, r, 0.f, FLT_MAX, threadIdx.x == 0, stk, 1, stack_depth, h, of);
+    if (threadIdx.x != 0) return;
     if (of) atomicOr(overflow, 1);
     if (h.prim == kMissPrim) *out = -1;
     else if (h.prim >= 0) *out = sc.tri_mat[h.prim];

@@ -65,13 +65,24 @@ struct LaunchShape {
     int block_extend = 128;
     int block_shade = 128;
     int block_shadow = 128;
-    int blocks_per_sm = 8;    // persistent grid = SMs * blocks_per_sm
+    int blocks_per_sm = 16;   // persistent grid = SMs * blocks_per_sm
     int sort_materials = 1;   // material-sorted shading
+};
+
+// Values that change from frame to frame live in device memory, so a captured CUDA graph
+// of the frame's launches stays valid across frames; the host updates them with one copy
+// before each launch.
+struct FrameDyn {
+    CameraParams cam;
+    uint64_t seed;
+    uint64_t sample_base;    // samples per pixel rendered before this frame (RNG offset)
+    int prev_spp;            // samples accumulated before this frame
+    int pad[3];
 };
 
 struct FrameParams {
     SceneDevice sc;
-    CameraParams cam;
+    const FrameDyn* dyn;     // device pointer
     PathQueue q[2];
     ShadowQueue sq;
     float4* L;               // wave-local path radiance
@@ -83,11 +94,8 @@ struct FrameParams {
     uchar4* rgba8;           // W*H display buffer
     int width, height;
     int spp;                 // samples per pixel of this frame
-    int prev_spp;            // samples accumulated before this frame
     int max_depth;
     int nee;
-    uint64_t seed;
-    uint64_t sample_base;    // samples per pixel rendered before this frame (RNG offset)
     int wave_pixels;         // pixels per wave
     int stack_depth;         // traversal stack entries per thread
     int num_sms;

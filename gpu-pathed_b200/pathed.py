@@ -31,7 +31,7 @@ EXPORTED = [
     "pt_set_launch", "pt_get_launch", "pt_render_async", "pt_poll", "pt_wait", "pt_get_spp", "pt_get_stats",
     "pt_readback", "pt_readback_pass", "pt_readback_rgba8", "pt_hit_test", "pt_trace_rays",
     "pt_trace_rays_device", "pt_occluded", "pt_version", "pt_set_profiling", "pt_get_profile",
-    "pt_trace_rays_static",
+    "pt_trace_rays_static", "pt_autotune",
 ]
 
 STATIC_MAX_RAYS = 65536  # PT_STATIC_MAX_RAYS
@@ -82,6 +82,11 @@ class Stats(C.Structure):
                 ("frames", C.c_int)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("bvh_width", "sort_materials", "blocks_per_sm", "block", "wave_paths")] + \
+               [("best_ms", C.c_float), ("default_ms", C.c_float), ("trials", C.c_int), ("from_cache", C.c_int)]
+
+
 class Profile(C.Structure):
     _fields_ = [("stage_ms", C.c_float * 6), ("stage_launches", C.c_int * 6), ("extend_nodes", C.c_ulonglong),
                 ("extend_prims", C.c_ulonglong), ("shadow_nodes", C.c_ulonglong), ("shadow_prims", C.c_ulonglong),
@@ -116,6 +121,7 @@ def _load():
         getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
     lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_set_profiling.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.pt_autotune.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p]
     lib.pt_get_profile.argtypes = [C.c_void_p, C.c_void_p]
     for name in ("pt_reset", "pt_check_bvh"):
         getattr(lib, name).argtypes = [C.c_void_p]
@@ -316,6 +322,11 @@ class Session:
         s = Stats()
         self._check(lib.pt_get_stats(self._h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def autotune(self, spp: int, cache_path: str | None = None) -> dict:
+        r = TuneResult()
+        self._check(lib.pt_autotune(self._h, spp, cache_path.encode() if cache_path else None, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_}
 
     def set_profiling(self, stage_timing: bool = True, work_counters: bool = False):
         self._check(lib.pt_set_profiling(self._h, int(bool(stage_timing)), int(bool(work_counters))))

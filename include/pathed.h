@@ -107,9 +107,24 @@ typedef struct pt_launch_config {
     int block_shade;
     int block_shadow;
     int blocks_per_sm;     /* persistent grid = SMs * blocks_per_sm */
-    int sort_materials;    /* 1: material-sorted shading, 2: off (0 keeps current) */
-    int use_graph;         /* 1: capture each frame's launch sequence in a CUDA graph, 2: off */
+    int sort_materials;    /* 1: material-sorted shading, 2: off, 3: automatic (on when the
+                              scene has 3 or more material classes; default) (0 keeps current) */
+    int use_graph;         /* 1: capture each frame's launches in a CUDA graph and replay it
+                              while the launch parameters are unchanged (default), 2: off */
 } pt_launch_config;
+
+/* Result of pt_autotune. */
+typedef struct pt_tune_result {
+    int bvh_width;          /* chosen BVH width (2, 4, 8) */
+    int sort_materials;     /* 1 on, 2 off */
+    int blocks_per_sm;
+    int block;              /* threads per block of the traversal stages */
+    int wave_paths;
+    float best_ms;          /* frame time of the chosen configuration */
+    float default_ms;       /* frame time of the configuration before tuning */
+    int trials;             /* frames measured (0 when taken from the cache) */
+    int from_cache;
+} pt_tune_result;
 
 typedef struct pt_stats {
     unsigned long long rays_camera;   /* camera rays of the last frame */
@@ -181,6 +196,13 @@ int pt_set_guiding(pt_session* s, int enabled);
 int pt_reset(pt_session* s);
 int pt_set_launch(pt_session* s, const pt_launch_config* cfg);
 int pt_get_launch(const pt_session* s, pt_launch_config* out);
+/* Autotuner (no counterpart in the reference, whose only tuning is SppOptimizer's spp
+ * budget, src/spp_optimizer.cpp:8-29): times frames of `spp` samples on the loaded scene over
+ * BVH width, material sorting, persistent-grid size and block size (coordinate descent),
+ * applies the fastest and restarts accumulation. With cache_path, results are stored as one
+ * JSON object per line keyed by scene size, material classes, resolution, spp, depth and
+ * NEE, and a cached key is applied without measuring. */
+int pt_autotune(pt_session* s, int spp, const char* cache_path, pt_tune_result* out);
 
 /* ---- rendering (PathTracer::renderAsync/pollRender, path_tracer.cu:285-356) ----------- */
 int pt_render_async(pt_session* s, int spp);

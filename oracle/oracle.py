@@ -20,10 +20,11 @@ REF_TREE = os.environ.get("PATHED_REFERENCE", "/root/reference")
 
 
 def build(ref: bool = True) -> None:
-    """Compile liboracle.so, and the reference CPU library when the reference tree exists."""
+    """Compile liboracle.so, and the reference's CPU and GPU builds when the reference tree
+    exists (on a machine without it, the prebuilt _ref/ libraries are used as they are)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref and os.path.isdir(REF_TREE):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "refbench", f"REF={REF_TREE}"], check=True)
 
 
 def _f(a):
@@ -173,6 +174,79 @@ class RefCPU(_SceneLib):
                            out["prim_type"].ctypes.data, out["prim_id"].ctypes.data, out["mat_id"].ctypes.data,
                            out["t"].ctypes.data)
         return out
+
+
+REFBENCH_LIB = os.path.join(HERE, "_ref", "librefbench.so")
+REFBENCH_NOFMA_LIB = os.path.join(HERE, "_ref", "librefbench_nofma.so")
+
+
+class RefBench:
+    """The reference's own CUDA integrator (renderKernel + updateFramebuffer, World::hit),
+    built from the reference sources by `make -C oracle refbench`. GPU only."""
+
+    def __init__(self, nofma: bool = False):
+        path = REFBENCH_NOFMA_LIB if nofma else REFBENCH_LIB
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = self.lib = C.CDLL(path)
+        L.refbench_create.restype = C.c_void_p
+        L.refbench_create.argtypes = ([C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_int] + [C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_void_p])
+        L.refbench_init.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.refbench_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]
+        L.refbench_readback.argtypes = [C.c_void_p, C.c_void_p]
+        L.refbench_trace.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4
+        L.refbench_destroy.argtypes = [C.c_void_p]
+        self.h = None
+
+    def load(self, sc: dict, width: int, height: int):
+        keep = [_f(sc["tri_vertices"]), _f(sc["tri_normals"]), _i(sc["tri_materials"]), _f(sc["spheres"]),
+                _i(sc["sphere_materials"]), _i(sc["material_types"]), _f(sc["material_albedo"]),
+                _f(sc["material_emit"]), _f(sc["material_ior"]), _f(sc["material_alpha"])]
+        env = sc.get("env_rgba")
+        env = None if env is None or env.size == 0 else _f(env)
+        ew, eh = (0, 0) if env is None else (env.shape[1], env.shape[0])
+        self.h = self.lib.refbench_create(
+            keep[0].size // 9, keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data, keep[3].size // 4,
+            keep[3].ctypes.data if keep[3].size else None, keep[4].ctypes.data if keep[4].size else None,
+            keep[5].size, keep[5].ctypes.data, keep[6].ctypes.data, keep[7].ctypes.data, keep[8].ctypes.data,
+            keep[9].ctypes.data, ew, eh, None if env is None else env.ctypes.data)
+        if not self.h:
+            raise RuntimeError("refbench_create failed")
+        cam = _f(sc["camera"])
+        self.w, self.hgt = width, height
+        if self.lib.refbench_init(self.h, cam.ctypes.data, width, height) != 0:
+            raise RuntimeError("refbench_init failed")
+
+    def render(self, spp, max_depth, nee=True) -> float:
+        ms = C.c_float()
+        if self.lib.refbench_render(self.h, spp, max_depth, int(bool(nee)), C.byref(ms)) != 0:
+            raise RuntimeError("refbench_render failed")
+        return ms.value
+
+    def readback(self):
+        out = np.empty((self.hgt, self.w, 3), np.float32)
+        if self.lib.refbench_readback(self.h, out.ctypes.data) != 0:
+            raise RuntimeError("refbench_readback failed")
+        return out
+
+    def trace(self, o, d, tmin, tmax):
+        o, d = _f(o).reshape(-1, 3), _f(d).reshape(-1, 3)
+        n = o.shape[0]
+        tmin = _f(np.broadcast_to(np.asarray(tmin, np.float32), (n,)))
+        tmax = _f(np.broadcast_to(np.asarray(tmax, np.float32), (n,)))
+        out = {"prim_type": np.empty(n, np.int32), "prim_id": np.empty(n, np.int32),
+               "mat_id": np.empty(n, np.int32), "t": np.empty(n, np.float32)}
+        if self.lib.refbench_trace(self.h, o.ctypes.data, d.ctypes.data, tmin.ctypes.data, tmax.ctypes.data, n,
+                                   out["prim_type"].ctypes.data, out["prim_id"].ctypes.data,
+                                   out["mat_id"].ctypes.data, out["t"].ctypes.data) != 0:
+            raise RuntimeError("refbench_trace failed")
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.refbench_destroy(self.h)
+            self.h = None
 
 
 def call_pair(fn_o, fn_r, *args, nout):

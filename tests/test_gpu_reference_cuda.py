@@ -1,0 +1,131 @@
+"""Parity against the reference's own CUDA backend run on the same GPU.
+
+oracle/_ref/librefbench*.so are built from the reference sources (renderKernel, World::hit,
+...) by `make -C oracle refbench`:
+  * librefbench_nofma.so (-fmad=false): the reference's arithmetic evaluated exactly as
+    written; closest-hit results must equal ours bit for bit.
+  * librefbench.so (nvcc defaults, FMA contraction): hit ids may differ only where two
+    candidates lie within a relative 1e-4 of each other (exact-distance ties, excluded), or
+    where a ray grazes an edge (counted and reported).
+  * images: the reference integrator with curand against ours with PCG32, per-pixel mean
+    within 3 combined standard errors (estimated from frame-to-frame spread on both sides).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import pathed
+from _util import pixel_subset, seeded_rays, three_se_pass
+
+pytestmark = pytest.mark.skipif(not os.path.exists(orc.REFBENCH_LIB), reason="reference GPU build not available")
+
+CASES = [(0, None), (1, None), (2, 4), (3, 4)]
+
+
+def _ours(cfg, level, w=64, h=64):
+    s = pathed.Session(w, h)
+    s.load_config(cfg, level=level)
+    return s, s.export_scene()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"cfg{c[0]}")
+def test_hit_ids_bitexact_vs_reference_nofma(case):
+    s, sc = _ours(*case)
+    rb = orc.RefBench(nofma=True)
+    rb.load(sc, 16, 16)
+    o, d, tmin, tmax = seeded_rays(sc, 20000, seed=31)
+    g = s.trace_rays(o, d, tmin, tmax)
+    r = rb.trace(o, d, tmin, tmax)
+    for k in ("prim_type", "prim_id", "mat_id", "t"):
+        bad = np.nonzero(g[k] != r[k])[0]
+        assert bad.size == 0, f"{k}: {bad.size} differ, e.g. gpu {g[k][bad[:4]]} reference {r[k][bad[:4]]}"
+    rb.close()
+    s.close()
+
+
+def _graze(sc, ptype, pid, o, d, eps=1e-5):
+    """True where the ray passes within a relative eps of the primitive's boundary: a
+    triangle edge (smallest barycentric, FP64) or a sphere silhouette."""
+    out = np.zeros(len(o), bool)
+    for i in np.nonzero(ptype >= 0)[0]:
+        ro, rd = o[i].astype(np.float64), d[i].astype(np.float64)
+        if ptype[i] == 0:
+            p = sc["tri_vertices"][pid[i]].reshape(3, 3).astype(np.float64)
+            e1, e2 = p[1] - p[0], p[2] - p[0]
+            s1 = np.cross(rd, e2)
+            div = s1 @ e1
+            s_ = ro - p[0]
+            b1 = (s_ @ s1) / div
+            b2 = (rd @ np.cross(s_, e1)) / div
+            out[i] = min(b1, b2, 1 - b1 - b2) < eps * 10
+        else:
+            c = sc["spheres"][pid[i]].astype(np.float64)
+            u = rd / np.linalg.norm(rd)
+            oc = ro - c[:3]
+            perp = np.linalg.norm(oc - (oc @ u) * u)
+            out[i] = abs(perp - c[3]) < 100 * eps * c[3]
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"cfg{c[0]}")
+def test_hit_ids_vs_reference_default_build(case):
+    """FMA-contracted reference: differences must be exact-distance ties (excluded) or
+    boundary grazes (counted and reported)."""
+    s, sc = _ours(*case)
+    rb = orc.RefBench(nofma=False)
+    rb.load(sc, 16, 16)
+    o, d, tmin, tmax = seeded_rays(sc, 20000, seed=32)
+    g = s.trace_rays(o, d, tmin, tmax)
+    r = rb.trace(o, d, tmin, tmax)
+    diff = (g["prim_type"] != r["prim_type"]) | (g["prim_id"] != r["prim_id"])
+    both = (g["prim_type"] >= 0) & (r["prim_type"] >= 0)
+    tie = both & (np.abs(g["t"] - r["t"]) <= 1e-4 * np.abs(r["t"]))
+    graze = _graze(sc, g["prim_type"], g["prim_id"], o, d) | _graze(sc, r["prim_type"], r["prim_id"], o, d)
+    unexplained = diff & ~tie & ~graze
+    print(f"cfg{case[0]}: {diff.sum()} id differences in {len(o)} rays: {(diff & tie).sum()} ties, "
+          f"{(diff & graze & ~tie).sum()} boundary grazes, {unexplained.sum()} other")
+    assert unexplained.sum() == 0
+    assert (diff & ~tie).mean() <= 1e-3
+    rb.close()
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [(0, None), (1, None), (3, 4)], ids=lambda c: f"cfg{c[0]}")
+def test_image_means_vs_reference_cuda(case):
+    cfg, level = case
+    w = h = 64
+    frames, spp = 8, 32
+    s, sc = _ours(cfg, level, w, h)
+    depth = s.counts().default_depth
+    ours = []
+    for _ in range(frames):
+        s.render(spp)
+        ours.append(s.readback(pass_only=True).reshape(-1, 3).astype(np.float64))
+    ours = np.stack(ours)
+    rb = orc.RefBench()
+    rb.load(sc, w, h)
+    ref, prev = [], np.zeros((w * h, 3))
+    for k in range(frames):
+        rb.render(spp, depth, True)
+        m = rb.readback().reshape(-1, 3).astype(np.float64)
+        ref.append((m * (k + 1) - prev * k))  # per-frame pass from the running mean
+        prev = m
+    ref = np.stack(ref)
+    pix = pixel_subset(w, h, 2000, seed=3)
+    a, b = ours[:, pix], ref[:, pix]
+    se_a = a.std(0, ddof=1) / np.sqrt(frames)
+    se_b = b.std(0, ddof=1) / np.sqrt(frames)
+    frac = three_se_pass(a.mean(0), se_a, b.mean(0), se_b, floor=1e-5)
+    # image mean: frame-to-frame spread of the per-frame image means on both sides
+    ma, mb = a.mean(axis=(1, 2)), b.mean(axis=(1, 2))
+    se = np.sqrt(ma.var(ddof=1) / frames + mb.var(ddof=1) / frames)
+    print(f"cfg{cfg}: 3-SE pass {frac:.4f}, image mean ours {ma.mean():.5f} reference {mb.mean():.5f} (SE {se:.5f})")
+    assert frac >= 0.97
+    assert abs(ma.mean() - mb.mean()) <= 4 * se + 1e-6
+    rb.close()
+    s.close()

@@ -174,3 +174,41 @@ def test_stats_count_canonical_queries(oracle_lib):
     assert abs(int(counts[0]) - st["rays_extend"]) <= 0.01 * st["rays_extend"]
     assert abs(int(counts[1]) - st["rays_shadow"]) <= 0.01 * st["rays_shadow"]
     s.close()
+
+
+@pytest.mark.gpu
+def test_graph_replay_matches_direct_launches():
+    """frames replayed from the captured CUDA graph equal frames launched directly"""
+    imgs = []
+    for graph in (1, 2):
+        s = pathed.Session(96, 96)
+        s.load_config(1)
+        s.set_launch(use_graph=graph)
+        for _ in range(3):  # first frame captures, the next ones replay with new constants
+            s.render(4)
+        s.set_camera((1.0, 5.0, 15.0), (0, 0.5, 0), (0, 1, 0), 0.7)  # constants change, launches do not
+        s.render(4)
+        imgs.append(s.readback().copy())
+        s.close()
+    assert np.array_equal(imgs[0], imgs[1])
+
+
+@pytest.mark.gpu
+def test_autotuner_and_cache(tmp_path):
+    cache = str(tmp_path / "tune.jsonl")
+    s = pathed.Session(128, 128)
+    s.load_config(0)
+    s.render(4)
+    base = s.readback().copy()
+    r = s.autotune(4, cache)
+    assert r["trials"] > 0 and r["from_cache"] == 0
+    assert r["bvh_width"] in (2, 4, 8) and r["best_ms"] <= r["default_ms"] * 1.05
+    s.render(4)
+    assert s.spp() == 4  # tuning restarts accumulation
+    assert np.allclose(s.readback(), base, rtol=1e-5, atol=1e-6)  # tuning changes scheduling only
+    t = pathed.Session(128, 128)
+    t.load_config(0)
+    r2 = t.autotune(4, cache)
+    assert r2["from_cache"] == 1 and r2["bvh_width"] == r["bvh_width"]
+    s.close()
+    t.close()
