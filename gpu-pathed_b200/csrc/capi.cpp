@@ -182,8 +182,39 @@ int pt_set_seed(pt_session* s, uint64_t seed) {
 }
 int pt_set_guiding(pt_session* s, int enabled) {
     if (!s) return PT_ERR_ARG;
-    if (enabled) return s->impl.fail(PT_ERR_ARG, "path guiding is not available in this build");
-    return PT_OK;
+    return guarded(s, [&] { return s->impl.set_guiding(enabled); });
+}
+int pt_guide_reset(pt_session* s) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.guide_reset(); });
+}
+int pt_set_guide_options(pt_session* s, int steps_per_frame, int batch, float lr, int warmup_steps) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.set_guide_options(steps_per_frame, batch, lr, warmup_steps);
+}
+int pt_set_consistent_mis(pt_session* s, int enabled) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.set_consistent_mis(enabled);
+}
+int pt_guide_get_info(const pt_session* s, pt_guide_info* out) {
+    if (!s || !out) return PT_ERR_ARG;
+    return s->impl.guide_info(out);
+}
+int pt_guide_get_params(pt_session* s, float* out, int n) {
+    if (!s || !out) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.guide_params(out, n, false); });
+}
+int pt_guide_set_params(pt_session* s, const float* in, int n) {
+    if (!s || !in) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.guide_params(const_cast<float*>(in), n, true); });
+}
+int pt_guide_forward(pt_session* s, const float* x, int n, float* raw) {
+    if (!s || (n > 0 && (!x || !raw))) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.guide_forward(x, n, raw); });
+}
+int pt_guide_gradients(pt_session* s, const float* x, const float* wi, const float* w, int n, float* grad) {
+    if (!s || !x || !wi || !w || !grad) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.guide_gradients(x, wi, w, n, grad); });
 }
 int pt_reset(pt_session* s) {
     if (!s) return PT_ERR_ARG;

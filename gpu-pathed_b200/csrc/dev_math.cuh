@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 namespace pt {
 
 constexpr float kPiF = 3.14159265358979323846f;

@@ -1,0 +1,60 @@
+// Host-visible interface of the path-guiding kernels (guide.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "guide.cuh"
+#include "pt_types.h"
+
+namespace pt {
+
+// Device buffers of the guide network and its training state.
+struct GuideDevice {
+    float* w;            // FP32 master parameters [kGuideParams]
+    uint32_t* wpack;     // BF16 pairs in mma B-fragment order + FP32 biases (see guide.cu)
+    float* grad;         // [kGuideParams]
+    float* adam_m;       // [kGuideParams]
+    float* adam_v;       // [kGuideParams]
+    float* wsum;         // [1] sum of sample weights of the current batch
+    GuideFrame frame;
+};
+
+// One training sample: where, which direction was sampled, and its weight F / p.
+struct GuideSample {
+    float p[3], n[3], wo[3], wi[3];
+    float weight;
+    float pad[3];
+};
+static_assert(sizeof(GuideSample) == 64, "GuideSample layout");
+
+// Vertex record written while shading a training path; resolved into a GuideSample once the
+// path's later contributions are known.
+struct GuideRecord {
+    float p[3], n[3], wo[3], wi[3];
+    float fcos_over_p;   // luminance of f |cos| / p_mix at the vertex
+    float beta_next;     // luminance of the throughput after the vertex
+    int tpath;           // training-path index within the wave
+    int depth;           // vertex depth
+};
+static_assert(sizeof(GuideRecord) == 64, "GuideRecord layout");
+
+// Bytes of the packed inference weights.
+constexpr int kGuidePackWords = (kGuideIn / 2) * kGuideHidden + 2 * (kGuideHidden / 2) * kGuideHidden +
+                                (kGuideHidden / 2) * kGuideOut + (kGuideHidden * 3 + kGuideOut);
+
+// Repack FP32 master weights into the inference layout (BF16 pairs + FP32 biases).
+cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s);
+// Raw network outputs for n explicit input vectors (inference kernel, tensor cores).
+cudaError_t guide_forward_features(const GuideDevice& g, const float* x, int n, float* raw, cudaStream_t s);
+// Gradient of the batch loss -sum_i w_i log q(wi_i | x_i) / sum_i w_i with respect to all
+// parameters, for explicit input vectors (training kernel); grad is overwritten.
+cudaError_t guide_gradients_features(const GuideDevice& g, const float* x, const float* wi, const float* w, int n,
+                                     cudaStream_t s);
+// Training on samples [first, first + n) of a ring of capacity `cap`: gradients then one
+// Adam step (lr, betas, eps) with step counter t (1-based).
+cudaError_t guide_train_step(const GuideDevice& g, const GuideSample* ring, int cap, const int* count, int batch,
+                             float lr, int t, cudaStream_t s);
+cudaError_t guide_adam(const GuideDevice& g, float lr, int t, cudaStream_t s);
+
+}  // namespace pt

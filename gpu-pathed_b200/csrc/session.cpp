@@ -119,8 +119,189 @@ int Session::load_scene(HostScene&& s) {
     scene_dirty_ = true;
     mats_dirty_ = true;
     update_material_classes();
+    // scene bounds for the guide's position encoding
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    for (size_t i = 0; i < scene_.tri_p.size(); i += 3)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = std::min(lo[k], scene_.tri_p[i + k]);
+            hi[k] = std::max(hi[k], scene_.tri_p[i + k]);
+        }
+    for (int s = 0; s < scene_.num_sph(); s++)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = std::min(lo[k], scene_.sph[4 * s + k] - scene_.sph[4 * s + 3]);
+            hi[k] = std::max(hi[k], scene_.sph[4 * s + k] + scene_.sph[4 * s + 3]);
+        }
+    for (int k = 0; k < 3; k++) {
+        const float ext = std::max(hi[k] - lo[k], 1e-6f);
+        gframe_.lo[k] = lo[k];
+        gframe_.inv_ext[k] = 2.f / ext;
+    }
     reset();
     return PT_OK;
+}
+
+GuideDevice Session::guide_view() const {
+    GuideDevice g{};
+    g.w = d_gw_.as<float>();
+    g.wpack = d_gwpack_.as<uint32_t>();
+    g.grad = d_ggrad_.as<float>();
+    g.adam_m = d_gm_.as<float>();
+    g.adam_v = d_gv_.as<float>();
+    g.wsum = d_gwsum_.as<float>();
+    g.frame = gframe_;
+    return g;
+}
+
+int Session::guide_init_weights() {
+    // He-normal initialisation from a seeded generator; zero biases; the output layer starts
+    // small so that the first mixture is broad (kappa about 1) and evenly weighted.
+    std::vector<float> w(kGuideParams, 0.f);
+    uint64_t s = guide_seed_;
+    auto next = [&]() {
+        s += 0x9E3779B97F4A7C15ULL;
+        uint64_t z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return (double)((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto normal = [&]() {
+        const double u1 = std::max(next(), 1e-300), u2 = next();
+        return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    };
+    auto fill = [&](int off, int fan_in, int count, double scale) {
+        const double sd = std::sqrt(2.0 / fan_in) * scale;
+        for (int i = 0; i < count; i++) w[off + i] = (float)(normal() * sd);
+    };
+    fill(kGW1, kGuideIn, kGuideIn * kGuideHidden, 1.0);
+    fill(kGW2, kGuideHidden, kGuideHidden * kGuideHidden, 1.0);
+    fill(kGW3, kGuideHidden, kGuideHidden * kGuideHidden, 1.0);
+    fill(kGW4, kGuideHidden, kGuideHidden * kGuideOut, 0.1);
+    for (int j = 0; j < kGuideLobes; j++) {  // mean directions spread by the bias
+        const double z = 2.0 * next() - 1.0, ph = 6.283185307179586 * next(), r = std::sqrt(1 - z * z);
+        w[kGB4 + 5 * j] = (float)(r * std::cos(ph));
+        w[kGB4 + 5 * j + 1] = (float)(r * std::sin(ph));
+        w[kGB4 + 5 * j + 2] = (float)z;
+    }
+    int r;
+    if ((r = check_cuda(cudaMemcpyAsync(d_gw_.p, w.data(), kGuideParams * 4, cudaMemcpyHostToDevice, stream_),
+                        "guide weights")))
+        return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_ggrad_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_gm_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_gv_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_gring_count_.p, 0, sizeof(int), stream_), "guide"))) return r;
+    if ((r = check_cuda(guide_pack(guide_view(), stream_), "guide pack"))) return r;
+    guide_iters_ = 0;
+    return check_cuda(cudaStreamSynchronize(stream_), "guide init");
+}
+
+int Session::ensure_guide() {
+    int r;
+    if ((r = ensure_device())) return r;
+    if (!guide_alloc_) {
+        if ((r = check_cuda(d_gw_.alloc(kGuideParams * 4), "guide"))) return r;
+        if ((r = check_cuda(d_gwpack_.alloc(kGuidePackWords * 4), "guide"))) return r;
+        if ((r = check_cuda(d_ggrad_.alloc(kGuideParams * 4), "guide"))) return r;
+        if ((r = check_cuda(d_gm_.alloc(kGuideParams * 4), "guide"))) return r;
+        if ((r = check_cuda(d_gv_.alloc(kGuideParams * 4), "guide"))) return r;
+        if ((r = check_cuda(d_gwsum_.alloc(16), "guide"))) return r;
+        if ((r = check_cuda(d_grec_.alloc((size_t)(1 << 20) * sizeof(GuideRecord)), "guide records"))) return r;
+        if ((r = check_cuda(d_grec_count_.alloc(16), "guide"))) return r;
+        if ((r = check_cuda(d_gring_.alloc((size_t)(1 << 21) * sizeof(GuideSample)), "guide samples"))) return r;
+        if ((r = check_cuda(d_gring_count_.alloc(16), "guide"))) return r;
+        guide_alloc_ = true;
+        if ((r = guide_init_weights())) return r;
+    }
+    return PT_OK;
+}
+
+int Session::set_guiding(int on) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    if (on) {
+        int r;
+        if ((r = ensure_guide())) return r;
+    }
+    guiding_ = on != 0;
+    reset();
+    return PT_OK;
+}
+
+int Session::guide_reset() {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    int r;
+    if ((r = ensure_guide())) return r;
+    if ((r = guide_init_weights())) return r;
+    reset();
+    return PT_OK;
+}
+
+int Session::guide_info(pt_guide_info* out) const {
+    std::memset(out, 0, sizeof(*out));
+    out->enabled = guiding_ ? 1 : 0;
+    out->mode = !guiding_ ? 0 : guide_iters_ >= guide_warmup_ ? 2 : 1;
+    out->steps = guide_iters_;
+    out->params = kGuideParams;
+    if (guide_alloc_) {
+        int c = 0;
+        float ws[2] = {0.f, 0.f};
+        cudaMemcpy(&c, d_gring_count_.p, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaMemcpy(ws, d_gwsum_.p, sizeof(ws), cudaMemcpyDeviceToHost);
+        out->samples = (unsigned long long)(unsigned)c;
+        out->loss = ws[1];
+    }
+    return PT_OK;
+}
+
+int Session::guide_params(float* out, int n, bool set) {
+    if (n != kGuideParams) return fail(PT_ERR_ARG, "parameter count must be 16104");
+    int r;
+    if ((r = ensure_guide())) return r;
+    if (in_flight_ && (r = wait(nullptr))) return r;
+    if (set) {
+        if ((r = check_cuda(cudaMemcpyAsync(d_gw_.p, out, n * 4, cudaMemcpyHostToDevice, stream_), "guide params")))
+            return r;
+        if ((r = check_cuda(guide_pack(guide_view(), stream_), "guide pack"))) return r;
+    } else if ((r = check_cuda(cudaMemcpyAsync(out, d_gw_.p, n * 4, cudaMemcpyDeviceToHost, stream_), "guide params"))) {
+        return r;
+    }
+    return check_cuda(cudaStreamSynchronize(stream_), "guide params");
+}
+
+int Session::guide_forward(const float* x, int n, float* raw) {
+    if (n < 0) return fail(PT_ERR_ARG, "negative count");
+    int r;
+    if ((r = ensure_guide())) return r;
+    if (in_flight_ && (r = wait(nullptr))) return r;
+    if (n == 0) return PT_OK;
+    if ((r = check_cuda(d_scratch_.alloc((size_t)n * (kGuideIn + kGuideOut) * 4), "scratch"))) return r;
+    float* dx = d_scratch_.as<float>();
+    float* dy = dx + (size_t)n * kGuideIn;
+    if ((r = check_cuda(cudaMemcpyAsync(dx, x, (size_t)n * kGuideIn * 4, cudaMemcpyHostToDevice, stream_), "copy")))
+        return r;
+    if ((r = check_cuda(guide_forward_features(guide_view(), dx, n, dy, stream_), "guide forward"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(raw, dy, (size_t)n * kGuideOut * 4, cudaMemcpyDeviceToHost, stream_), "copy")))
+        return r;
+    return check_cuda(cudaStreamSynchronize(stream_), "guide forward");
+}
+
+int Session::guide_gradients(const float* x, const float* wi, const float* w, int n, float* grad) {
+    if (n <= 0) return fail(PT_ERR_ARG, "need at least one sample");
+    int r;
+    if ((r = ensure_guide())) return r;
+    if (in_flight_ && (r = wait(nullptr))) return r;
+    if ((r = check_cuda(d_scratch_.alloc((size_t)n * (kGuideIn + 4) * 4), "scratch"))) return r;
+    float* dx = d_scratch_.as<float>();
+    float* dwi = dx + (size_t)n * kGuideIn;
+    float* dw = dwi + (size_t)n * 3;
+    if ((r = check_cuda(cudaMemcpyAsync(dx, x, (size_t)n * kGuideIn * 4, cudaMemcpyHostToDevice, stream_), "copy")))
+        return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dwi, wi, (size_t)n * 3 * 4, cudaMemcpyHostToDevice, stream_), "copy"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(dw, w, (size_t)n * 4, cudaMemcpyHostToDevice, stream_), "copy"))) return r;
+    if ((r = check_cuda(guide_gradients_features(guide_view(), dx, dwi, dw, n, stream_), "guide gradients"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(grad, d_ggrad_.p, kGuideParams * 4, cudaMemcpyDeviceToHost, stream_), "copy")))
+        return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_ggrad_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
+    return check_cuda(cudaStreamSynchronize(stream_), "guide gradients");
 }
 
 int Session::set_bvh(int width, int max_leaf) {
@@ -440,6 +621,28 @@ int Session::render_async(int spp) {
     p.shape = shape_;
     p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 3 ? 1 : 0);
     last_wave_paths_ = p.wave_pixels * spp;
+    p.consistent_mis = consistent_mis_ || guiding_;
+    if (guiding_) {
+        if ((r = ensure_guide())) return r;
+        const size_t mix_bytes = (size_t)queue_cap_ * kGuideOut * sizeof(float);
+        if ((r = check_cuda(d_gmix_.alloc(mix_bytes), "guide mixtures"))) return r;
+        const int gstride = std::max(1, queue_cap_ / 131072);  // about 2^17 training paths per wave
+        const size_t tpaths = (size_t)(queue_cap_ + gstride - 1) / gstride;
+        if ((r = check_cuda(d_gacc_.alloc(tpaths * kMaxDepthLimit * 3 * sizeof(float)), "guide accumulators")))
+            return r;
+        p.guide_mode = guide_iters_ >= guide_warmup_ ? 2 : 1;
+        p.gwpack = d_gwpack_.as<uint32_t>();
+        p.gmix = d_gmix_.as<float>();
+        p.gframe = gframe_;
+        p.grec = d_grec_.as<GuideRecord>();
+        p.grec_count = d_grec_count_.as<int>();
+        p.grec_cap = 1 << 20;
+        p.gacc = d_gacc_.as<float>();
+        p.gstride = gstride;
+        p.gring = d_gring_.as<GuideSample>();
+        p.gring_count = d_gring_count_.as<int>();
+        p.gring_cap = 1 << 21;
+    }
     // per-frame constants: one pinned copy ahead of the frame's launches
     h_dyn_->cam = cam_;
     h_dyn_->seed = seed_;
@@ -449,7 +652,7 @@ int Session::render_async(int spp) {
     marks_active_ = false;
     if (stage_timing_) {
         const int waves = (w_ * h_ + p.wave_pixels - 1) / p.wave_pixels;
-        const size_t need = (size_t)waves * (max_depth_ * 4 + 3) + 8;
+        const size_t need = (size_t)waves * (max_depth_ * 5 + 4) + 8;
         while (mark_events_.size() < need) {
             cudaEvent_t e;
             if ((r = check_cuda(cudaEventCreate(&e), "cudaEventCreate"))) return r;
@@ -495,6 +698,18 @@ int Session::render_async(int spp) {
         if ((r = check_cuda(cudaGraphLaunch(graph_exec_, stream_), "graph launch"))) return r;
     } else if ((r = check_cuda(enqueue_frame(p, stream_, mk), "frame launch"))) {
         return r;
+    }
+    if (guiding_) {
+        // online training on the newest samples: one Adam step per frame, inside the frame's
+        // timed region
+        for (int k = 0; k < guide_steps_per_frame_; k++) {
+            guide_iters_++;
+            if ((r = check_cuda(guide_train_step(guide_view(), d_gring_.as<GuideSample>(), 1 << 21,
+                                                 d_gring_count_.as<int>(), guide_batch_, guide_lr_, guide_iters_,
+                                                 stream_),
+                                "guide training")))
+                return r;
+        }
     }
     if ((r = check_cuda(cudaMemcpyAsync(h_stats_, d_stats_.p, sizeof(FrameStats), cudaMemcpyDeviceToHost, stream_),
                         "stats readback")))

@@ -172,9 +172,46 @@ private:
     int material_classes_ = 1;
     void update_material_classes();
 
+    // ---- learned path guiding ----
+    bool guiding_ = false;
+    int consistent_mis_ = 0;
+    bool guide_alloc_ = false;
+    DevBuf d_gw_, d_gwpack_, d_ggrad_, d_gm_, d_gv_, d_gwsum_, d_gmix_, d_grec_, d_grec_count_, d_gacc_, d_gring_,
+        d_gring_count_;
+    size_t gmix_cap_ = 0;
+    int guide_iters_ = 0;       // Adam steps taken
+    int guide_warmup_ = 4;      // steps before the guide is used for sampling
+    int guide_batch_ = 1 << 18;
+    int guide_steps_per_frame_ = 1;
+    float guide_lr_ = 1e-3f;
+    uint64_t guide_seed_ = 0x9e11deULL;
+    GuideFrame gframe_{};
+    int ensure_guide();
+    int guide_init_weights();
+    GuideDevice guide_view() const;
+
 public:
     int graph_captures() const { return graph_captures_; }
     int autotune(int spp, const char* cache_path, ::pt_tune_result* out);
+    int set_guiding(int on);
+    int set_consistent_mis(int on) {
+        consistent_mis_ = on ? 1 : 0;
+        reset();
+        return 0;
+    }
+    int guide_reset();
+    int set_guide_options(int steps, int batch, float lr, int warmup) {
+        if (batch > (1 << 21)) return fail(-1, "batch must be at most 2^21 samples");
+        if (steps > 0) guide_steps_per_frame_ = steps;
+        if (batch > 0) guide_batch_ = batch;
+        if (lr > 0.f) guide_lr_ = lr;
+        if (warmup >= 0) guide_warmup_ = warmup;
+        return 0;
+    }
+    int guide_info(::pt_guide_info* out) const;
+    int guide_params(float* out, int n, bool set);
+    int guide_forward(const float* x, int n, float* raw);
+    int guide_gradients(const float* x, const float* wi, const float* w, int n, float* grad);
 };
 
 }  // namespace pt

@@ -23,6 +23,7 @@
 #include "dev_math.cuh"
 #include "dev_shade.cuh"
 #include "dev_trace.cuh"
+#include "guide_mlp.cuh"
 
 namespace pt {
 
@@ -180,6 +181,56 @@ __global__ void k_sort(FrameParams p, int depth) {
     }
 }
 
+// Hit point, shading normal and material of a closest hit (Triangle::hit / Sphere::hit's
+// record, src/primitives/*.cu): the triangle normal is the interpolated, unnormalised one.
+__device__ __forceinline__ void hit_info(const SceneDevice& sc, V o, V dir, float4 h4, V& point, V& n, int& mat) {
+    const int prim = __float_as_int(h4.w);
+    if (prim >= 0) {
+        const float b1 = h4.y, b2 = h4.z;
+        const float w0 = 1.f - b1 - b2;
+        const V p0 = mkv(__ldg(sc.tri_p + 3 * prim + 0));
+        const V p1 = mkv(__ldg(sc.tri_p + 3 * prim + 1));
+        const V p2 = mkv(__ldg(sc.tri_p + 3 * prim + 2));
+        const V n0 = mkv(__ldg(sc.tri_n + 3 * prim + 0));
+        const V n1 = mkv(__ldg(sc.tri_n + 3 * prim + 1));
+        const V n2 = mkv(__ldg(sc.tri_n + 3 * prim + 2));
+        point = p0 * w0 + p1 * b1 + p2 * b2;
+        n = w0 * n0 + b1 * n1 + b2 * n2;
+        mat = __ldg(sc.tri_mat + prim);
+    } else {
+        const float4 s = __ldg(sc.sph + ~prim);
+        point = o + h4.x * dir;
+        n = normalized((point - mkv(s.x, s.y, s.z)) / s.w);
+        mat = __ldg(sc.sph_mat + ~prim);
+    }
+}
+
+// The BSDF sampler's own density of a direction (the reference's Microfacet::pdf evaluates D
+// with alpha(wi), microfacet.h:124-134, while sampling uses alpha(wo), :148-158).
+__device__ __forceinline__ float bsdf_sampling_pdf(const Material& m, V wo, V wi) {
+    if (m.type == kLambertian) return lambert_pdf(wi);
+    if (m.type == kMicrofacet) {
+        const V wh = normalized(wo + wi);
+        return mf_D(m.alpha, wo, wh) * fabsf(wh.z) / (4.f * fabsf(dot(wo, wh)));
+    }
+    return 0.f;
+}
+
+__device__ __forceinline__ float lum(V c) { return (c.x + c.y + c.z) * (1.f / 3.f); }
+
+// Per training path and depth: U (unweighted emission), R (NEE + MIS-weighted emission),
+// W (MIS-weighted emission), luminance times throughput.
+__device__ __forceinline__ void guide_account(const FrameParams& p, int path, int depth, float u, float r, float w) {
+    if (p.guide_mode == 0 || path % p.gstride != 0) return;
+    float* a = p.gacc + ((size_t)(path / p.gstride) * p.max_depth + depth) * 3;
+    a[0] += u;
+    a[1] += r;
+    a[2] += w;
+}
+
+// GUIDE: compiled with the path-guiding code (used when guide_mode != 0); the plain
+// instantiation keeps the reference integrator's register budget.
+template <bool GUIDE>
 __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
     const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
@@ -187,13 +238,15 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
     const bool last = depth >= p.max_depth - 1;
     const int n_choice = p.sc.num_lights + (p.sc.env.present ? 1 : 0);
     const bool do_nee = p.nee && n_choice > 0;
+    const bool guided = GUIDE && p.guide_mode == 2;
     for (;;) {
         const int base = warp_fetch(&p.counters->work_shade[depth]);
         if (base >= count) break;
         const int i = base + (threadIdx.x & 31);
-        bool cont = false, shadow = false;
+        bool cont = false, shadow = false, record = false;
         float4 co, cd, cb, so, sd, sc4;
         uint2 crng;
+        GuideRecord rec;
         if (i < count) {
             const int slot = p.shape.sort_materials ? p.sort_index[i] : i;
             const float4 o4 = q.o[slot];
@@ -212,56 +265,66 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                 if (!is_zero(Le)) {
                     const float w = nomis ? 1.f : balance(d4.w, pdf_env_light(p.sc, dir));
                     Ladd = beta * Le * w;
+                    if (GUIDE) guide_account(p, path, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
                 }
             } else {
                 V point, n;
                 int mat;
-                if (prim >= 0) {
-                    // Triangle::hit's hit point and interpolated (unnormalised) shading normal
-                    const float b1 = h4.y, b2 = h4.z;
-                    const float w0 = 1.f - b1 - b2;
-                    const V p0 = mkv(__ldg(p.sc.tri_p + 3 * prim + 0));
-                    const V p1 = mkv(__ldg(p.sc.tri_p + 3 * prim + 1));
-                    const V p2 = mkv(__ldg(p.sc.tri_p + 3 * prim + 2));
-                    const V n0 = mkv(__ldg(p.sc.tri_n + 3 * prim + 0));
-                    const V n1 = mkv(__ldg(p.sc.tri_n + 3 * prim + 1));
-                    const V n2 = mkv(__ldg(p.sc.tri_n + 3 * prim + 2));
-                    point = p0 * w0 + p1 * b1 + p2 * b2;
-                    n = w0 * n0 + b1 * n1 + b2 * n2;
-                    mat = __ldg(p.sc.tri_mat + prim);
-                } else {
-                    const float4 s = __ldg(p.sc.sph + ~prim);
-                    point = o + h4.x * dir;
-                    n = normalized((point - mkv(s.x, s.y, s.z)) / s.w);
-                    mat = __ldg(p.sc.sph_mat + ~prim);
-                }
+                hit_info(p.sc, o, dir, h4, point, n, mat);
+                // guided modes shade in an orthonormal frame (the reference's frame is built
+                // from the unnormalised interpolated normal)
+                if (GUIDE && p.guide_mode) n = normalized(n);
                 const Frame fr = make_frame(n);
                 const V wo = normalized(to_local(fr, -dir));
                 const Material m = p.sc.mats[mat];
                 if (m.emitting && wo.z >= 0.f) {  // front-face emission (lambertian.cu:5-11)
+                    const V Le = mkv(m.emit[0], m.emit[1], m.emit[2]);
                     const float w = nomis ? 1.f : balance(d4.w, pdf_scene_light(p.sc, o, point, n, prim));
-                    Ladd = beta * mkv(m.emit[0], m.emit[1], m.emit[2]) * w;
+                    Ladd = beta * Le * w;
+                    if (GUIDE) guide_account(p, path, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
                 }
                 if (!last) {
                     const long long gp = wave_first + path;
                     const uint32_t pixel = (uint32_t)(gp / p.spp);
                     const uint64_t inc = pcg_inc(pixel);
                     uint64_t st = ((uint64_t)q.rng[slot].y << 32) | q.rng[slot].x;
+                    const bool delta_mat = m.type == kMirror || m.type == kGlass;
+                    const bool use_guide = guided && !delta_mat;
+                    const float* mix = use_guide ? p.gmix + (size_t)slot * kGuideOut : nullptr;
+                    bool from_guide = false;
+                    if (use_guide) from_guide = pcg_uniform(st, inc) >= 0.5f;  // one-sample MIS, fraction 0.5
                     BsdfSample bs;
-                    switch (m.type) {
-                        case kLambertian: {
-                            const float x1 = pcg_uniform(st, inc);
-                            const float x2 = pcg_uniform(st, inc);
-                            bs = lambert_sample(m, wo, x1, x2);
-                            break;
+                    V wworld;
+                    if (from_guide) {
+                        const float u0 = pcg_uniform(st, inc), u1 = pcg_uniform(st, inc), u2 = pcg_uniform(st, inc);
+                        wworld = normalized(guide_sample(mix, u0, u1, u2));
+                        bs.wi = to_local(fr, wworld);
+                        bs.f = bsdf_f(m, wo, bs.wi);
+                        bs.delta = false;
+                    } else {
+                        switch (m.type) {
+                            case kLambertian: {
+                                const float x1 = pcg_uniform(st, inc);
+                                const float x2 = pcg_uniform(st, inc);
+                                bs = lambert_sample(m, wo, x1, x2);
+                                break;
+                            }
+                            case kMirror: bs = mirror_sample(wo); break;
+                            case kGlass: bs = glass_sample(m, wo, pcg_uniform(st, inc)); break;
+                            default: {
+                                const float x1 = pcg_uniform(st, inc);
+                                const float x2 = pcg_uniform(st, inc);
+                                bs = mf_sample(m.alpha, wo, x1, x2);
+                            }
                         }
-                        case kMirror: bs = mirror_sample(wo); break;
-                        case kGlass: bs = glass_sample(m, wo, pcg_uniform(st, inc)); break;
-                        default: {
-                            const float x1 = pcg_uniform(st, inc);
-                            const float x2 = pcg_uniform(st, inc);
-                            bs = mf_sample(m.alpha, wo, x1, x2);
-                        }
+                        wworld = to_world(fr, bs.wi);
+                    }
+                    if (use_guide) {
+                        // mixture density of the direction, whichever strategy produced it
+                        const float pb = bsdf_sampling_pdf(m, wo, bs.wi);
+                        float pg = guide_pdf(mix, normalized(wworld));
+                        if (!isfinite(pg)) pg = 0.f;
+                        bs.pdf = 0.5f * pb + 0.5f * pg;
                     }
                     if (do_nee && !bs.delta) {
                         // directSampleLights (path_tracer.cu:83-126)
@@ -271,7 +334,11 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                         const LightSample ls = sample_lights(p.sc, point, x1, x2, x3);
                         if (dot(ls.normal, ls.wi) < 0.f && ls.pdf > 0.f) {
                             const V wil = to_local(fr, ls.wi);
-                            const float bpdf = bsdf_pdf(m, wo, wil);
+                            float bpdf = p.consistent_mis ? bsdf_sampling_pdf(m, wo, wil) : bsdf_pdf(m, wo, wil);
+                            if (use_guide) {
+                                const float pg = guide_pdf(mix, ls.wi);
+                                bpdf = 0.5f * bpdf + 0.5f * (isfinite(pg) ? pg : 0.f);
+                            }
                             const float wl = balance(ls.pdf, bpdf);
                             const V f = bsdf_f(m, wo, wil);
                             const V contrib = beta * (ls.emitted * wl * f * fabsf(dot(n, ls.wi)) / ls.pdf);
@@ -285,14 +352,21 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                     }
                     // beta *= f * |cos| / pdf (path_tracer.cu:171-173)
                     if (bs.pdf > 0.f) {
-                        const V nb = beta * (bs.f * fabsf(bs.wi.z) / bs.pdf);
+                        const V fc = bs.f * fabsf(bs.wi.z) / bs.pdf;
+                        const V nb = beta * fc;
                         if (!is_zero(nb) && isfinite(nb.x + nb.y + nb.z)) {
-                            const V wd = to_world(fr, bs.wi);
                             cont = true;
                             co = make_float4(point.x, point.y, point.z, __int_as_float(path));
-                            cd = make_float4(wd.x, wd.y, wd.z, bs.pdf);
+                            cd = make_float4(wworld.x, wworld.y, wworld.z, bs.pdf);
                             cb = make_float4(nb.x, nb.y, nb.z, __int_as_float(bs.delta ? 1 : 0));
                             crng = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
+                            if (GUIDE && p.guide_mode && !delta_mat && path % p.gstride == 0) {
+                                const V wn = normalized(wworld);
+                                const V won = normalized(-dir);
+                                rec = GuideRecord{{point.x, point.y, point.z}, {n.x, n.y, n.z}, {won.x, won.y, won.z},
+                                                  {wn.x, wn.y, wn.z}, lum(fc), lum(nb), path / p.gstride, depth};
+                                record = true;
+                            }
                         }
                     }
                 }
@@ -304,6 +378,10 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                 l.z += Ladd.z;
                 p.L[path] = l;
             }
+        }
+        if (GUIDE && p.guide_mode) {
+            const int r = warp_append(p.grec_count, record);
+            if (record && r < p.grec_cap) p.grec[r] = rec;
         }
         const int cslot = warp_append(&p.counters->ray_count[depth + 1], cont);
         if (cont) {
@@ -350,10 +428,96 @@ __global__ void k_shadow(FrameParams p, int depth) {
                 l.y += c.y;
                 l.z += c.z;
                 p.L[path] = l;
+                guide_account(p, path, depth, 0.f, (c.x + c.y + c.z) * (1.f / 3.f), 0.f);
             }
         }
     }
     if (CNT) flush_work(work, &p.stats->shadow_nodes, &p.stats->shadow_prims);
+}
+
+// Guide inference for the rays of the queue consumed at `depth`: features of each hit, the
+// network on the tensor cores (16 rays per warp), the mixture written per queue slot.
+__global__ void __launch_bounds__(128) k_guide_infer(FrameParams p, int depth) {
+    __shared__ uint32_t sw[kSWords];
+    __shared__ uint32_t sx[4][16 * kSXStride];
+    // outputs overwrite the inputs: every lane has loaded its input fragments into registers
+    // before the warp-synchronous mma chain reaches the output stores
+    float(*sy)[16 * kSXStride] = reinterpret_cast<float(*)[16 * kSXStride]>(sx);
+    guide_load_weights(p.gwpack, sw);
+    __syncthreads();
+    const int count = p.counters->ray_count[depth];
+    const PathQueue q = p.q[depth & 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int groups = (count + 15) / 16;
+    for (int grp = blockIdx.x * 4 + warp; grp < groups; grp += gridDim.x * 4) {
+        const int slot = grp * 16 + (lane & 15);
+        bool hit = false;
+        if (lane < 16) {
+            float x[kGuideIn];
+            if (slot < count) {
+                const float4 o4 = q.o[slot], d4 = q.d[slot], h4 = q.hit[slot];
+                if (__float_as_int(h4.w) != kMissPrim) {
+                    V point, n;
+                    int mat;
+                    hit_info(p.sc, mkv(o4), mkv(d4), h4, point, n, mat);
+                    n = normalized(n);
+                    const V wo = normalized(-mkv(d4));
+                    const float pp[3] = {point.x, point.y, point.z}, nn[3] = {n.x, n.y, n.z}, ww[3] = {wo.x, wo.y, wo.z};
+                    guide_encode(p.gframe, pp, nn, ww, x);
+                    hit = true;
+                }
+            }
+            if (!hit)
+                for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
+            guide_store_input(sx[warp], lane, x);
+        }
+        __syncwarp();
+        guide_mlp_warp16(sw, sx[warp], sy[warp]);
+        __syncwarp();
+        if (lane < 16) {
+            float raw[kGuideOut], mix[kGuideOut];
+            for (int j = 0; j < kGuideOut; j++) raw[j] = sy[warp][lane * kGuideOut + j];
+            guide_activate(raw, mix);
+            for (int j = 0; j < kGuideOut; j++) sy[warp][lane * kGuideOut + j] = mix[j];
+        }
+        __syncwarp();
+        // 16 consecutive slots: one contiguous 2560-byte store by the whole warp
+        const int rows = count - grp * 16 < 16 ? count - grp * 16 : 16;
+        float* dst = p.gmix + (size_t)grp * 16 * kGuideOut;
+        for (int e = lane; e < rows * kGuideOut; e += 32) dst[e] = sy[warp][e];
+        __syncwarp();
+    }
+}
+
+// Resolve this wave's training records into samples: the radiance that arrived along each
+// sampled direction is the path's later contributions (unweighted emission at the next
+// vertex, everything after it) divided by the throughput after the vertex.
+__global__ void k_guide_collect(FrameParams p) {
+    const int n = min(*p.grec_count, p.grec_cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const GuideRecord r = p.grec[i];
+        const float* a = p.gacc + (size_t)r.tpath * p.max_depth * 3;
+        float lin = 0.f;
+        const int k1 = r.depth + 1;
+        if (k1 < p.max_depth) {
+            float sum_r = 0.f;
+            for (int d = k1; d < p.max_depth; d++) sum_r += a[3 * d + 1];
+            lin = (a[3 * k1] + sum_r - a[3 * k1 + 2]) / r.beta_next;
+        }
+        const float weight = r.fcos_over_p * lin;
+        if (!(weight > 0.f) || !isfinite(weight)) continue;
+        const int idx = atomicAdd(p.gring_count, 1);
+        GuideSample smp;
+        for (int k = 0; k < 3; k++) {
+            smp.p[k] = r.p[k];
+            smp.n[k] = r.n[k];
+            smp.wo[k] = r.wo[k];
+            smp.wi[k] = r.wi[k];
+        }
+        smp.weight = weight;
+        smp.pad[0] = smp.pad[1] = smp.pad[2] = 0.f;
+        p.gring[(unsigned)idx % (unsigned)p.gring_cap] = smp;
+    }
 }
 
 __global__ void k_accumulate(FrameParams p, int first_pixel, int npix) {
@@ -417,6 +581,11 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
         const long long wave_first = (long long)first * p.spp;
         cudaError_t e = cudaMemsetAsync(p.counters, 0, sizeof(WaveCounters), stream);
         if (e != cudaSuccess) return e;
+        if (p.guide_mode) {
+            const size_t tpaths = (size_t)(n + p.gstride - 1) / p.gstride;
+            if ((e = cudaMemsetAsync(p.gacc, 0, tpaths * p.max_depth * 3 * sizeof(float), stream))) return e;
+            if ((e = cudaMemsetAsync(p.grec_count, 0, sizeof(int), stream))) return e;
+        }
         mark(-1);
         k_camera<<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
         mark(kStageCamera);
@@ -427,7 +596,12 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
                 k_sort<<<(n + 255) / 256, 256, 0, stream>>>(p, d);
                 mark(kStageSort);
             }
-            k_shade<<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
+            if (p.guide_mode == 2 && d < p.max_depth - 1) {
+                k_guide_infer<<<p.num_sms * 4, 128, 0, stream>>>(p, d);
+                mark(kStageGuide);
+            }
+            if (p.guide_mode) k_shade<true><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
+            else k_shade<false><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {
                 k_shadow<W, CNT><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d);
@@ -436,6 +610,10 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
         }
         k_accumulate<<<(npix + 127) / 128, 128, 0, stream>>>(p, first, npix);
         mark(kStageAccum);
+        if (p.guide_mode) {
+            k_guide_collect<<<p.num_sms * 2, 256, 0, stream>>>(p);
+            mark(kStageGuide);
+        }
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (mark.err != cudaSuccess) return mark.err;

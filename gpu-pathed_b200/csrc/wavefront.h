@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "guide.h"
 #include "pt_types.h"
 
 namespace pt {
@@ -51,7 +52,16 @@ struct FrameStats {
 };
 
 // Stages of a frame, for per-stage device timing.
-enum Stage : int { kStageCamera = 0, kStageExtend, kStageSort, kStageShade, kStageShadow, kStageAccum, kNumStages };
+enum Stage : int {
+    kStageCamera = 0,
+    kStageExtend,
+    kStageSort,
+    kStageShade,
+    kStageShadow,
+    kStageAccum,
+    kStageGuide,  // guide inference + training-sample collection
+    kNumStages
+};
 
 // Host-side recorder of stage boundaries: an event is recorded after every launch.
 struct StageMarks {
@@ -101,6 +111,20 @@ struct FrameParams {
     int num_sms;
     int count_work;          // 1: traversal kernels count nodes and leaf entries (slower)
     LaunchShape shape;
+    // ---- learned path guiding (guide.cuh) ----
+    int guide_mode;          // 0 off, 1 collect training data only, 2 guided sampling + collect
+    int consistent_mis;      // NEE weights use the BSDF's true sampling density (microfacet)
+    const uint32_t* gwpack;  // packed inference weights
+    float* gmix;             // per queue slot: mixture (40 floats)
+    GuideFrame gframe;       // scene bounds for the position encoding
+    GuideRecord* grec;       // vertex records of training paths (this wave)
+    int* grec_count;
+    int grec_cap;
+    float* gacc;             // per training path and depth: U, R, W luminance (3 floats)
+    int gstride;             // paths whose wave index is a multiple of gstride are training paths
+    GuideSample* gring;      // training-sample ring
+    int* gring_count;
+    int gring_cap;
 };
 
 // Enqueue one frame (all waves) on `stream`. Grid sizes do not depend on queue lengths,

@@ -31,12 +31,15 @@ EXPORTED = [
     "pt_set_launch", "pt_get_launch", "pt_render_async", "pt_poll", "pt_wait", "pt_get_spp", "pt_get_stats",
     "pt_readback", "pt_readback_pass", "pt_readback_rgba8", "pt_hit_test", "pt_trace_rays",
     "pt_trace_rays_device", "pt_occluded", "pt_version", "pt_set_profiling", "pt_get_profile",
-    "pt_trace_rays_static", "pt_autotune",
+    "pt_trace_rays_static", "pt_autotune", "pt_guide_reset", "pt_set_consistent_mis", "pt_guide_get_info",
+    "pt_guide_get_params", "pt_guide_set_params", "pt_guide_forward", "pt_guide_gradients", "pt_set_guide_options",
 ]
+
+GUIDE_PARAMS = 16104
 
 STATIC_MAX_RAYS = 65536  # PT_STATIC_MAX_RAYS
 
-STAGES = ("camera", "extend", "sort", "shade", "shadow", "accumulate")
+STAGES = ("camera", "extend", "sort", "shade", "shadow", "accumulate", "guide")
 
 
 class PathedError(RuntimeError):
@@ -82,13 +85,18 @@ class Stats(C.Structure):
                 ("frames", C.c_int)]
 
 
+class GuideInfo(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("mode", C.c_int), ("steps", C.c_int), ("params", C.c_int),
+                ("samples", C.c_ulonglong), ("loss", C.c_float)]
+
+
 class TuneResult(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("bvh_width", "sort_materials", "blocks_per_sm", "block", "wave_paths")] + \
                [("best_ms", C.c_float), ("default_ms", C.c_float), ("trials", C.c_int), ("from_cache", C.c_int)]
 
 
 class Profile(C.Structure):
-    _fields_ = [("stage_ms", C.c_float * 6), ("stage_launches", C.c_int * 6), ("extend_nodes", C.c_ulonglong),
+    _fields_ = [("stage_ms", C.c_float * 7), ("stage_launches", C.c_int * 7), ("extend_nodes", C.c_ulonglong),
                 ("extend_prims", C.c_ulonglong), ("shadow_nodes", C.c_ulonglong), ("shadow_prims", C.c_ulonglong),
                 ("bvh_width", C.c_int), ("node_bytes", C.c_int), ("prim_bytes", C.c_int), ("wave_paths", C.c_int)]
 
@@ -122,6 +130,14 @@ def _load():
     lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_set_profiling.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_autotune.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p]
+    lib.pt_guide_reset.argtypes = [C.c_void_p]
+    lib.pt_set_guide_options.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]
+    lib.pt_set_consistent_mis.argtypes = [C.c_void_p, C.c_int]
+    lib.pt_guide_get_info.argtypes = [C.c_void_p, C.c_void_p]
+    lib.pt_guide_get_params.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.pt_guide_set_params.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.pt_guide_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    lib.pt_guide_gradients.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
     lib.pt_get_profile.argtypes = [C.c_void_p, C.c_void_p]
     for name in ("pt_reset", "pt_check_bvh"):
         getattr(lib, name).argtypes = [C.c_void_p]
@@ -322,6 +338,43 @@ class Session:
         s = Stats()
         self._check(lib.pt_get_stats(self._h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    # ---- learned path guiding
+    def guide_reset(self):
+        self._check(lib.pt_guide_reset(self._h))
+
+    def set_guide_options(self, steps_per_frame=0, batch=0, lr=0.0, warmup_steps=-1):
+        self._check(lib.pt_set_guide_options(self._h, steps_per_frame, batch, lr, warmup_steps))
+
+    def set_consistent_mis(self, on: bool):
+        self._check(lib.pt_set_consistent_mis(self._h, int(bool(on))))
+
+    def guide_info(self) -> dict:
+        g = GuideInfo()
+        self._check(lib.pt_guide_get_info(self._h, C.byref(g)))
+        return {k: getattr(g, k) for k, _ in GuideInfo._fields_}
+
+    def guide_params(self) -> np.ndarray:
+        out = np.empty(GUIDE_PARAMS, np.float32)
+        self._check(lib.pt_guide_get_params(self._h, out.ctypes.data, out.size))
+        return out
+
+    def set_guide_params(self, p):
+        p = _f32(p, GUIDE_PARAMS)
+        self._check(lib.pt_guide_set_params(self._h, p.ctypes.data, p.size))
+
+    def guide_forward(self, x) -> np.ndarray:
+        x = _f32(x).reshape(-1, 80)
+        raw = np.empty((x.shape[0], 40), np.float32)
+        self._check(lib.pt_guide_forward(self._h, x.ctypes.data, x.shape[0], raw.ctypes.data))
+        return raw
+
+    def guide_gradients(self, x, wi, w) -> np.ndarray:
+        x, wi, w = _f32(x).reshape(-1, 80), _f32(wi).reshape(-1, 3), _f32(w).reshape(-1)
+        g = np.empty(GUIDE_PARAMS, np.float32)
+        self._check(lib.pt_guide_gradients(self._h, x.ctypes.data, wi.ctypes.data, w.ctypes.data, x.shape[0],
+                                           g.ctypes.data))
+        return g
 
     def autotune(self, spp: int, cache_path: str | None = None) -> dict:
         r = TuneResult()

@@ -138,9 +138,10 @@ typedef struct pt_stats {
 
 /* Per-stage device time of the last frame (replaces the reference's single begin/end event
  * pair and "CUDA Frame: X ms" print, path_tracer.cu:300-352). Stages: 0 camera, 1 extend
- * (closest hit), 2 material sort, 3 shade, 4 shadow (any hit), 5 accumulate. Work counters
- * are filled only for frames rendered with work counting on. */
-#define PT_NUM_STAGES 6
+ * (closest hit), 2 material sort, 3 shade, 4 shadow (any hit), 5 accumulate, 6 guide
+ * (inference and training-sample collection). Work counters are filled only for frames
+ * rendered with work counting on. */
+#define PT_NUM_STAGES 7
 typedef struct pt_profile {
     float stage_ms[PT_NUM_STAGES];
     int stage_launches[PT_NUM_STAGES];
@@ -190,8 +191,44 @@ int pt_set_material(pt_session* s, int material_id, int type, const float albedo
 int pt_set_max_depth(pt_session* s, int max_depth);  /* vertices per path (path_tracer.cu:165) */
 int pt_set_nee(pt_session* s, int enabled);          /* calculateLiNEE vs calculateLiNaive */
 int pt_set_seed(pt_session* s, uint64_t seed);
-/* Learned path guiding (not part of the reference). Returns PT_ERR_ARG when unavailable. */
+/* ---- learned path guiding (no counterpart in the reference) -----------------------------
+ * A network (80 -> 64 -> 64 -> 64 -> 40, ReLU; 16,104 parameters, BF16 weights on the
+ * tensor cores, FP32 master copy) maps a 12-frequency sin/cos encoding of the hit position,
+ * the shading normal and the outgoing direction to an 8-lobe von Mises-Fisher mixture. It is
+ * trained online (Adam, lr 1e-3, 2^18 samples per step, one step per frame) on radiance
+ * samples the integrator produces, and combined with BSDF sampling by one-sample MIS (guide
+ * fraction 0.5) so the estimator stays unbiased; MIS weights of emitter sampling then use
+ * the mixture density. Before the first steps have been taken, paths are sampled from the
+ * BSDF alone while training data is collected. */
 int pt_set_guiding(pt_session* s, int enabled);
+/* Re-initialise the guide network (seeded) and its optimiser state. */
+int pt_guide_reset(pt_session* s);
+/* Training schedule: Adam steps per frame (default 1), samples per step (default 2^18),
+ * learning rate (default 1e-3), steps before the guide is used for sampling (default 4).
+ * Zero or negative values keep the current setting. */
+int pt_set_guide_options(pt_session* s, int steps_per_frame, int batch, float lr, int warmup_steps);
+/* MIS weights of emitter samples use the BSDF's own sampling density (the reference's
+ * Microfacet::pdf evaluates alpha at the incident direction instead, microfacet.h:124-134,
+ * which biases the combination slightly). On by itself when guiding is on. */
+int pt_set_consistent_mis(pt_session* s, int enabled);
+typedef struct pt_guide_info {
+    int enabled;
+    int mode;              /* 0 off, 1 collecting only, 2 guided sampling */
+    int steps;             /* Adam steps taken */
+    int params;            /* 16104 */
+    unsigned long long samples;  /* training samples collected so far */
+    float loss;            /* weighted mean of -log q(wi|x) over the last training batch */
+} pt_guide_info;
+int pt_guide_get_info(const pt_session* s, pt_guide_info* out);
+/* Network parameters (FP32 master copy): W1[80][64], b1[64], W2[64][64], b2, W3[64][64], b3,
+ * W4[64][40], b4[40], row-major, concatenated; n must be 16104. */
+int pt_guide_get_params(pt_session* s, float* out, int n);
+int pt_guide_set_params(pt_session* s, const float* in, int n);
+/* Raw outputs (n x 40) of the inference kernel for n explicit input vectors (n x 80). */
+int pt_guide_forward(pt_session* s, const float* x, int n, float* raw);
+/* Gradient (16104 floats) of -sum w_i log q(wi_i | x_i) / sum w_i computed by the training
+ * kernel for n explicit samples (x: n x 80, wi: n x 3 unit vectors, w: n weights). */
+int pt_guide_gradients(pt_session* s, const float* x, const float* wi, const float* w, int n, float* grad);
 /* Restart progressive accumulation at the next frame (Renderer::reset). */
 int pt_reset(pt_session* s);
 int pt_set_launch(pt_session* s, const pt_launch_config* cfg);

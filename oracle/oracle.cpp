@@ -996,3 +996,181 @@ void oracle_rng(uint64_t seed, uint64_t sample, uint32_t pixel, int n, float* ou
 }
 
 }  // extern "C"
+
+// ---- guide network in FP64 (checker of the guide kernels) ----------------------------------
+// Network 80 -> 64 -> 64 -> 64 (ReLU) -> 40, parameters W1[80][64] b1 W2[64][64] b2
+// W3[64][64] b3 W4[64][40] b4 concatenated; outputs per lobe (mu_raw.xyz, kappa_raw, logit).
+namespace oracle {
+namespace guide {
+constexpr int IN = 80, H = 64, OUT = 40, L = 8;
+constexpr int W1 = 0, B1 = W1 + IN * H, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H * H, W4 = B3 + H,
+              B4 = W4 + H * OUT, NP = B4 + OUT;
+
+inline float bf16(float x) {  // round to nearest even, to BF16 precision
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    u &= 0xFFFF0000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+struct Net {
+    std::vector<double> w;
+    explicit Net(const float* p) : w(NP) {
+        for (int i = 0; i < NP; i++) w[i] = bf16(p[i]);  // the kernels use BF16-rounded weights
+    }
+};
+
+// forward; act[l] holds post-ReLU activations of hidden layer l; quant: round layer inputs to BF16
+inline void forward(const Net& n, const double* x, bool quant, double (&a1)[H], double (&a2)[H], double (&a3)[H],
+                    double (&y)[OUT]) {
+    auto q = [&](double v) { return quant ? (double)bf16((float)v) : v; };
+    double xin[IN];
+    for (int k = 0; k < IN; k++) xin[k] = q(x[k]);
+    for (int j = 0; j < H; j++) {
+        double s = n.w[B1 + j];
+        for (int k = 0; k < IN; k++) s += xin[k] * n.w[W1 + k * H + j];
+        a1[j] = s > 0 ? s : 0;
+    }
+    for (int j = 0; j < H; j++) {
+        double s = n.w[B2 + j];
+        for (int k = 0; k < H; k++) s += q(a1[k]) * n.w[W2 + k * H + j];
+        a2[j] = s > 0 ? s : 0;
+    }
+    for (int j = 0; j < H; j++) {
+        double s = n.w[B3 + j];
+        for (int k = 0; k < H; k++) s += q(a2[k]) * n.w[W3 + k * H + j];
+        a3[j] = s > 0 ? s : 0;
+    }
+    for (int j = 0; j < OUT; j++) {
+        double s = n.w[B4 + j];
+        for (int k = 0; k < H; k++) s += q(a3[k]) * n.w[W4 + k * OUT + j];
+        y[j] = s;
+    }
+}
+
+// -w log q(wi) and its gradient with respect to the raw outputs
+inline double loss_and_grad(const double (&y)[OUT], const double* wi, double w, double (&dy)[OUT]) {
+    double pi[L], kap[L], mu[L][3], len[L], dt[L], lf[L];
+    double mx = -1e300;
+    for (int j = 0; j < L; j++) mx = std::max(mx, y[5 * j + 4]);
+    double se = 0;
+    for (int j = 0; j < L; j++) se += std::exp(y[5 * j + 4] - mx);
+    double lmax = -1e300;
+    for (int j = 0; j < L; j++) {
+        pi[j] = std::exp(y[5 * j + 4] - mx) / se;
+        len[j] = std::sqrt(y[5 * j] * y[5 * j] + y[5 * j + 1] * y[5 * j + 1] + y[5 * j + 2] * y[5 * j + 2]) + 1e-12;
+        for (int a = 0; a < 3; a++) mu[j][a] = y[5 * j + a] / len[j];
+        kap[j] = std::exp(std::min(10.0, std::max(-4.0, y[5 * j + 3])));
+        dt[j] = mu[j][0] * wi[0] + mu[j][1] * wi[1] + mu[j][2] * wi[2];
+        const double lognorm = std::log(kap[j]) - std::log(2 * M_PI) - std::log1p(-std::exp(-2 * kap[j]));
+        lf[j] = std::log(pi[j] + 1e-300) + lognorm + kap[j] * (dt[j] - 1);
+        lmax = std::max(lmax, lf[j]);
+    }
+    double sq = 0;
+    for (int j = 0; j < L; j++) sq += std::exp(lf[j] - lmax);
+    const double logq = lmax + std::log(sq);
+    for (int j = 0; j < L; j++) {
+        const double s = std::exp(lf[j] - logq);
+        dy[5 * j + 4] = -w * (s - pi[j]);
+        const double kr = y[5 * j + 3], k = kap[j];
+        const double dlogc = 1 / k - 2 * std::exp(-2 * k) / (-std::expm1(-2 * k));
+        dy[5 * j + 3] = (kr > -4 && kr < 10) ? -w * s * (dlogc + dt[j] - 1) * k : 0.0;
+        const double c = -w * s * k / len[j];
+        for (int a = 0; a < 3; a++) dy[5 * j + a] = c * (wi[a] - dt[j] * mu[j][a]);
+    }
+    return -w * logq;
+}
+}  // namespace guide
+}  // namespace oracle
+
+extern "C" {
+
+// Raw outputs (n x 40). quant = 1 rounds each layer's inputs to BF16 (as the inference
+// kernel's operands are); FP64 accumulation.
+void oracle_guide_forward(const float* params, const float* x, int n, int quant, double* out) {
+    using namespace oracle::guide;
+    const Net net(params);
+    for (int i = 0; i < n; i++) {
+        double xi[IN], a1[H], a2[H], a3[H], y[OUT];
+        for (int k = 0; k < IN; k++) xi[k] = x[(size_t)i * IN + k];
+        forward(net, xi, quant != 0, a1, a2, a3, y);
+        for (int j = 0; j < OUT; j++) out[(size_t)i * OUT + j] = y[j];
+    }
+}
+
+// Loss -sum w_i log q / sum w_i and its gradient (16104 values) in FP64, FP32 activations
+// not emulated (exact arithmetic on the BF16-rounded weights).
+double oracle_guide_grad(const float* params, const float* x, const float* wi, const float* w, int n, double* grad) {
+    using namespace oracle::guide;
+    const Net net(params);
+    for (int i = 0; i < NP; i++) grad[i] = 0;
+    double wsum = 0;
+    for (int i = 0; i < n; i++) wsum += w[i];
+    const double inv = wsum > 0 ? 1 / wsum : 0;
+    double loss = 0;
+    for (int i = 0; i < n; i++) {
+        double xi[IN], a1[H], a2[H], a3[H], y[OUT], dy[OUT];
+        for (int k = 0; k < IN; k++) xi[k] = x[(size_t)i * IN + k];
+        forward(net, xi, false, a1, a2, a3, y);
+        const double d[3] = {wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
+        if (w[i] == 0) continue;
+        loss += loss_and_grad(y, d, w[i] * inv, dy);
+        double d3[H], d2[H], d1[H];
+        for (int k = 0; k < H; k++) {
+            double s = 0;
+            for (int j = 0; j < OUT; j++) {
+                grad[W4 + k * OUT + j] += a3[k] * dy[j];
+                s += dy[j] * net.w[W4 + k * OUT + j];
+            }
+            d3[k] = a3[k] > 0 ? s : 0;
+        }
+        for (int j = 0; j < OUT; j++) grad[B4 + j] += dy[j];
+        for (int k = 0; k < H; k++) {
+            double s = 0;
+            for (int j = 0; j < H; j++) {
+                grad[W3 + k * H + j] += a2[k] * d3[j];
+                s += d3[j] * net.w[W3 + k * H + j];
+            }
+            d2[k] = a2[k] > 0 ? s : 0;
+        }
+        for (int j = 0; j < H; j++) grad[B3 + j] += d3[j];
+        for (int k = 0; k < H; k++) {
+            double s = 0;
+            for (int j = 0; j < H; j++) {
+                grad[W2 + k * H + j] += a1[k] * d2[j];
+                s += d2[j] * net.w[W2 + k * H + j];
+            }
+            d1[k] = a1[k] > 0 ? s : 0;
+        }
+        for (int j = 0; j < H; j++) grad[B2 + j] += d2[j];
+        for (int k = 0; k < IN; k++)
+            for (int j = 0; j < H; j++) grad[W1 + k * H + j] += xi[k] * d1[j];
+        for (int j = 0; j < H; j++) grad[B1 + j] += d1[j];
+    }
+    return loss;
+}
+
+// Loss only (for finite differences): the parameters are used as given (no BF16 rounding).
+double oracle_guide_loss_exact(const double* params, const float* x, const float* wi, const float* w, int n) {
+    using namespace oracle::guide;
+    std::vector<float> dummy(NP, 0.f);
+    Net net(dummy.data());
+    for (int i = 0; i < NP; i++) net.w[i] = params[i];
+    double wsum = 0;
+    for (int i = 0; i < n; i++) wsum += w[i];
+    double loss = 0;
+    for (int i = 0; i < n; i++) {
+        double xi[IN], a1[H], a2[H], a3[H], y[OUT], dy[OUT];
+        for (int k = 0; k < IN; k++) xi[k] = x[(size_t)i * IN + k];
+        forward(net, xi, false, a1, a2, a3, y);
+        const double d[3] = {wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
+        if (w[i] == 0) continue;
+        loss += loss_and_grad(y, d, w[i] / wsum, dy);
+    }
+    return loss;
+}
+
+}  // extern "C"
