@@ -1,13 +1,14 @@
 // Path-guiding network kernels: weight packing, tensor-core inference on explicit inputs,
-// the fused training kernel (forward + loss + backward + per-block gradient accumulation)
-// and the Adam update.
+// the fused tensor-core training kernel (forward + loss + backward + weight gradients) and
+// the Adam update.
 //
 // Loss (neural importance sampling, Mueller et al. 2019): for samples wi_i drawn with
 // density p_i, F_i the integrand value and w_i = F_i / p_i, minimise
 //     L = - sum_i w_i log q(wi_i | x_i) / sum_i w_i,
 // a Monte Carlo estimate of the KL divergence from the normalised integrand to q (up to a
-// constant). Training arithmetic is FP32 with the BF16-rounded weights the inference kernel
-// uses, so the trained and the evaluated network are the same function.
+// constant). Every matrix product of training runs on BF16 mma.sync tiles with FP32
+// accumulation, with the same BF16 weights and FP32 biases as the inference kernel, so the
+// trained and the evaluated network are the same function.
 #include "guide.h"
 
 #include <cuda_bf16.h>
@@ -16,41 +17,55 @@
 
 namespace pt {
 
+static_assert(kPackWords == kGuidePackWords, "packed weight layout");
+
 namespace {
 
-constexpr int kTile = 64;      // samples per training tile
-constexpr int kTrainThreads = 256;
-constexpr int kOwned = (kGuideParams + kTrainThreads - 1) / kTrainThreads;  // 63 parameters per thread
-// padded row strides (odd) so that column-wise walks hit distinct banks
-constexpr int kXS = 81, kAS = 65, kYS = 41;
-constexpr int kSmemFloats = kGuideParams + kTile * kXS + 3 * kTile * kAS + kTile * kYS + 2 * kTile * kAS +
-                            kTile * 3 + kTile;
-
-__device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-
+// FP32 master parameters -> the two shared-memory images (forward, transposed).
 __global__ void k_guide_pack(const float* __restrict__ w, uint32_t* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kGuidePackWords) return;
+    // forward: pair of rows (2 kp, 2 kp + 1) at column n
     auto pair = [&](int base, int ncol, int kp, int n) {
         return pack_bf16(w[base + (2 * kp) * ncol + n], w[base + (2 * kp + 1) * ncol + n]);
     };
-    uint32_t v;
-    if (i < kGP2) v = pair(kGW1, 64, i / 64, i % 64);
-    else if (i < kGP3) v = pair(kGW2, 64, (i - kGP2) / 64, (i - kGP2) % 64);
-    else if (i < kGP4) v = pair(kGW3, 64, (i - kGP3) / 64, (i - kGP3) % 64);
-    else if (i < kGPB) v = pair(kGW4, 40, (i - kGP4) / 40, (i - kGP4) % 40);
-    else {
-        const int j = i - kGPB;  // b1 64, b2 64, b3 64, b4 40
+    // backward: pair of columns (2 c, 2 c + 1) of row k, zero past the last column
+    auto tpair = [&](int base, int ncol, int k, int c) {
+        const float lo = 2 * c < ncol ? w[base + k * ncol + 2 * c] : 0.f;
+        const float hi = 2 * c + 1 < ncol ? w[base + k * ncol + 2 * c + 1] : 0.f;
+        return pack_bf16(lo, hi);
+    };
+    uint32_t v = 0u;
+    if (i < kSW2) {
+        const int r = i / 72, c = i % 72;
+        if (c < 64) v = pair(kGW1, 64, r, c);
+    } else if (i < kSW3) {
+        const int r = (i - kSW2) / 72, c = (i - kSW2) % 72;
+        if (c < 64) v = pair(kGW2, 64, r, c);
+    } else if (i < kSW4) {
+        const int r = (i - kSW3) / 72, c = (i - kSW3) % 72;
+        if (c < 64) v = pair(kGW3, 64, r, c);
+    } else if (i < kSB) {
+        v = pair(kGW4, 40, (i - kSW4) / 40, (i - kSW4) % 40);
+    } else if (i < kSWords) {
+        const int j = i - kSB;  // b1 64, b2 64, b3 64, b4 40
         const float b = j < 64 ? w[kGB1 + j] : j < 128 ? w[kGB2 + j - 64] : j < 192 ? w[kGB3 + j - 128] : w[kGB4 + j - 192];
         v = __float_as_uint(b);
+    } else {
+        const int j = i - kPackT, layer = j / (64 * kSTStride), r = (j % (64 * kSTStride)) / kSTStride,
+                  c = j % kSTStride;
+        if (layer == 0 && c < 32) v = tpair(kGW2, 64, r, c);
+        else if (layer == 1 && c < 32) v = tpair(kGW3, 64, r, c);
+        else if (layer == 2 && c < 24) v = tpair(kGW4, 40, r, c);
     }
     out[i] = v;
 }
 
 // Inference on explicit input vectors (tests, tools): 4 warps per block, 16 rows per warp.
+// Inputs 78 and 79 are padding and read as zero.
 __global__ void k_guide_forward_x(const uint32_t* __restrict__ wpack, const float* __restrict__ x, int n,
                                   float* __restrict__ raw) {
-    __shared__ uint32_t sw[kSWords];
+    __shared__ __align__(16) uint32_t sw[kSWords];
     __shared__ uint32_t sx[4][16 * kSXStride];
     // outputs overwrite the inputs (all input fragments are in registers before the stores)
     float(*sy)[16 * kSXStride] = reinterpret_cast<float(*)[16 * kSXStride]>(sx);
@@ -63,8 +78,9 @@ __global__ void k_guide_forward_x(const uint32_t* __restrict__ wpack, const floa
         for (int e = lane; e < 16 * (kGuideIn / 2); e += 32) {
             const int r = e / (kGuideIn / 2), k = e % (kGuideIn / 2);
             const int gi = row0 + r;
-            const float a = gi < n ? x[(size_t)gi * kGuideIn + 2 * k] : 0.f;
-            const float b = gi < n ? x[(size_t)gi * kGuideIn + 2 * k + 1] : 0.f;
+            const bool ok = gi < n && k < kGuideIn / 2 - 1;
+            const float a = ok ? x[(size_t)gi * kGuideIn + 2 * k] : 0.f;
+            const float b = ok ? x[(size_t)gi * kGuideIn + 2 * k + 1] : 0.f;
             sx[warp][r * kSXStride + k] = pack_bf16(a, b);
         }
         __syncwarp();
@@ -108,9 +124,7 @@ __device__ __forceinline__ void source_sample(const TrainSource& s, const GuideF
                                               float* xrow, float wi[3], float& w) {
     if (s.ring) {
         const GuideSample sm = s.ring[(unsigned)(first + i) % (unsigned)s.cap];
-        float x[kGuideIn];
-        guide_encode(gf, sm.p, sm.n, sm.wo, x);
-        for (int k = 0; k < kGuideIn; k++) xrow[k] = x[k];
+        guide_encode(gf, sm.p, sm.n, sm.wo, xrow);
         wi[0] = sm.wi[0]; wi[1] = sm.wi[1]; wi[2] = sm.wi[2];
         w = sm.weight;
     } else {
@@ -118,6 +132,8 @@ __device__ __forceinline__ void source_sample(const TrainSource& s, const GuideF
         wi[0] = s.wi[3 * i]; wi[1] = s.wi[3 * i + 1]; wi[2] = s.wi[3 * i + 2];
         w = s.w[i];
     }
+    xrow[kGuideIn - 2] = 0.f;  // padding inputs
+    xrow[kGuideIn - 1] = 0.f;
 }
 
 __global__ void k_guide_wsum(TrainSource s, float* wsum) {
@@ -129,30 +145,6 @@ __global__ void k_guide_wsum(TrainSource s, float* wsum) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0 && acc != 0.f) atomicAdd(wsum, acc);
-}
-
-// out[t][n] = act(b[n] + sum_k in[t][k] W[k][n]) for a tile of kTile rows.
-template <bool RELU>
-__device__ __forceinline__ void dense_fwd(const float* in, int in_stride, int K, const float* W, const float* b, int N,
-                                          float* out, int out_stride) {
-    for (int o = threadIdx.x; o < kTile * N; o += blockDim.x) {
-        const int t = o % kTile, n = o / kTile;
-        float acc = b[n];
-        for (int k = 0; k < K; k++) acc = fmaf(in[t * in_stride + k], W[k * N + n], acc);
-        out[t * out_stride + n] = RELU ? fmaxf(acc, 0.f) : acc;
-    }
-}
-
-// dA[t][k] = (sum_n dZ[t][n] W[k][n]) * (A[t][k] > 0): backward through a dense layer and the
-// ReLU of its input.
-__device__ __forceinline__ void dense_bwd(const float* dz, int dz_stride, int N, const float* W, int K, const float* a,
-                                          float* da) {
-    for (int o = threadIdx.x; o < kTile * K; o += blockDim.x) {
-        const int t = o % kTile, k = o / kTile;
-        float acc = 0.f;
-        for (int n = 0; n < N; n++) acc = fmaf(dz[t * dz_stride + n], W[k * N + n], acc);
-        da[t * kAS + k] = a[t * kAS + k] > 0.f ? acc : 0.f;
-    }
 }
 
 // Gradient of -w log q(wi) with respect to the 40 raw outputs of one sample; returns the loss.
@@ -196,97 +188,283 @@ __device__ __forceinline__ float loss_grad(const float* raw, const float wi[3], 
     return -w * logq;
 }
 
-__global__ void __launch_bounds__(kTrainThreads) k_guide_train(GuideDevice g, TrainSource src) {
-    extern __shared__ float sm[];
-    float* sW = sm;
-    float* sX = sW + kGuideParams;
-    float* sA1 = sX + kTile * kXS;
-    float* sA2 = sA1 + kTile * kAS;
-    float* sA3 = sA2 + kTile * kAS;
-    float* sY = sA3 + kTile * kAS;
-    float* sD0 = sY + kTile * kYS;
-    float* sD1 = sD0 + kTile * kAS;
-    float* sWi = sD1 + kTile * kAS;
-    float* sWt = sWi + kTile * 3;
-    for (int i = threadIdx.x; i < kGuideParams; i += blockDim.x) sW[i] = bf16_round(g.w[i]);
+// ---- fused training kernel -------------------------------------------------------------
+//
+// One block of 8 warps per SM walks tiles of 128 samples (16 per warp). Per tile:
+//   1. each warp stages its 16 samples (encoded inputs, direction, normalised weight);
+//   2. forward through the four layers on mma.sync (the inference code path), storing the
+//      BF16 activations X, A1, A2, A3 in the warp's shared-memory tiles;
+//   3. the loss gradient dY of each sample (FP32), stored as BF16;
+//   4. backward dZ3 = (dY W4^T) . [A3 > 0], dZ2 = (dZ3 W3^T) . [A2 > 0],
+//      dZ1 = (dZ2 W2^T) . [A1 > 0] on mma.sync, chained in registers, each stored as BF16;
+//   5. weight gradients G = A^T dZ over the block's 128 samples as 16x8 output tiles on
+//      mma.sync (operands transposed by ldmatrix.trans): 145 tiles (W1 40, W2 32, W3 32,
+//      W4 20, and bias tiles b2 8, b3 8, b4 5 computed as ones^T dZ), 19 per warp, each held
+//      in FP32 registers across every tile the block processes. The bias of layer 1 rides on
+//      W1's padding input 78, set to one in the stored X tile after the forward pass.
+// At the end each block adds its register accumulators to the global gradient.
+
+constexpr int kTrainWarps = 8;
+constexpr int kTrainThreads = 32 * kTrainWarps;
+constexpr int kBlockRows = 16 * kTrainWarps;  // samples per block tile
+// per-warp tile row strides in 32-bit words (rows are multiples of 16 bytes for ldmatrix and
+// spread 8 consecutive rows over distinct 16-byte bank groups)
+constexpr int kXW = kSXStride;  // 44: 80 BF16 inputs
+constexpr int kAW = 36;         // 64 BF16 activations
+constexpr int kYW = 28;         // 48 BF16 (40 output gradients, zero-padded)
+constexpr int kRawW = 41;       // FP32 raw outputs
+constexpr int kWX = 0;
+constexpr int kWA1 = kWX + 16 * kXW;
+constexpr int kWA2 = kWA1 + 16 * kAW;
+constexpr int kWA3 = kWA2 + 16 * kAW;
+constexpr int kWD1 = kWA3 + 16 * kAW;
+constexpr int kWD2 = kWD1 + 16 * kAW;
+constexpr int kWD3 = kWD2 + 16 * kAW;
+constexpr int kWDY = kWD3 + 16 * kAW;
+constexpr int kWWi = kWDY + 16 * kYW;  // 16 x (wi.xyz, normalised weight)
+constexpr int kWarpWords = kWWi + 16 * 4;
+constexpr int kWRaw = kWD2;  // raw outputs alias dZ2/dZ3, consumed before either is written
+static_assert(16 * kRawW <= 2 * 16 * kAW, "raw outputs must fit the dZ2/dZ3 tiles");
+static_assert((kSWords + kSTWords) % 4 == 0 && kWarpWords % 4 == 0, "16-byte aligned warp tiles");
+constexpr int kTrainSmemWords = kSWords + kSTWords + kTrainWarps * kWarpWords;
+constexpr int kGradTiles = 145;
+constexpr int kOwnTiles = (kGradTiles + kTrainWarps - 1) / kTrainWarps;  // 19
+
+// Operands and destination of weight-gradient tile `id`.
+struct GradTile {
+    int a_off, a_stride, a_col;  // A^T source tile (a_off < 0: ones, a bias tile)
+    int b_off, b_stride, b_col;  // dZ source tile
+    int out, out_stride;         // parameter index of element (0, 0), row stride
+};
+
+__device__ __forceinline__ GradTile grad_tile(int id) {
+    GradTile t;
+    if (id < 40) {  // W1 = X^T dZ1 (row 78 is b1, row 79 unused)
+        t = {kWX, kXW, (id / 8) * 16, kWD1, kAW, (id % 8) * 8, kGW1 + (id / 8) * 16 * 64 + (id % 8) * 8, 64};
+    } else if (id < 72) {  // W2 = A1^T dZ2
+        const int j = id - 40;
+        t = {kWA1, kAW, (j / 8) * 16, kWD2, kAW, (j % 8) * 8, kGW2 + (j / 8) * 16 * 64 + (j % 8) * 8, 64};
+    } else if (id < 104) {  // W3 = A2^T dZ3
+        const int j = id - 72;
+        t = {kWA2, kAW, (j / 8) * 16, kWD3, kAW, (j % 8) * 8, kGW3 + (j / 8) * 16 * 64 + (j % 8) * 8, 64};
+    } else if (id < 124) {  // W4 = A3^T dY
+        const int j = id - 104;
+        t = {kWA3, kAW, (j / 5) * 16, kWDY, kYW, (j % 5) * 8, kGW4 + (j / 5) * 16 * 40 + (j % 5) * 8, 40};
+    } else if (id < 132) {  // b2 = 1^T dZ2
+        const int j = id - 124;
+        t = {-1, 0, 0, kWD2, kAW, j * 8, kGB2 + j * 8, 0};
+    } else if (id < 140) {  // b3 = 1^T dZ3
+        const int j = id - 132;
+        t = {-1, 0, 0, kWD3, kAW, j * 8, kGB3 + j * 8, 0};
+    } else {  // b4 = 1^T dY
+        const int j = id - 140;
+        t = {-1, 0, 0, kWDY, kYW, j * 8, kGB4 + j * 8, 0};
+    }
+    return t;
+}
+
+// Backward through one layer: dA = dZ W^T (KT k-steps of 16 over the layer's outputs, 64
+// inputs), masked by the layer input's ReLU ([A > 0], read from the stored BF16 tile) and
+// re-packed as BF16 A fragments.
+template <int KT>
+__device__ __forceinline__ void guide_backward(const uint32_t* swt_layer, const uint32_t (&dz)[KT][4],
+                                               const uint32_t* a_tile, uint32_t (&out)[4][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float c[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < KT; kt++) {
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const uint32_t b0 = swt_layer[(nt * 8 + g) * kSTStride + kt * 8 + t];
+            const uint32_t b1 = swt_layer[(nt * 8 + g) * kSTStride + kt * 8 + 4 + t];
+            mma16816(c[nt], dz[kt][0], dz[kt][1], dz[kt][2], dz[kt][3], b0, b1);
+        }
+    }
+    auto masked = [&](float lo, float hi, uint32_t a) {
+        return pack_bf16((a & 0x7FFFu) ? lo : 0.f, (a & 0x7FFF0000u) ? hi : 0.f);
+    };
+#pragma unroll
+    for (int kt = 0; kt < 4; kt++) {
+        out[kt][0] = masked(c[2 * kt][0], c[2 * kt][1], a_tile[g * kAW + kt * 8 + t]);
+        out[kt][1] = masked(c[2 * kt][2], c[2 * kt][3], a_tile[(g + 8) * kAW + kt * 8 + t]);
+        out[kt][2] = masked(c[2 * kt + 1][0], c[2 * kt + 1][1], a_tile[g * kAW + kt * 8 + 4 + t]);
+        out[kt][3] = masked(c[2 * kt + 1][2], c[2 * kt + 1][3], a_tile[(g + 8) * kAW + kt * 8 + 4 + t]);
+    }
+}
+
+__global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideDevice g, TrainSource src) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    uint32_t* sw = smem;               // forward weights and biases (inference layout)
+    uint32_t* swt = sw + kSWords;      // transposed weights
+    uint32_t* tiles = swt + kSTWords;  // per-warp tiles
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g8 = lane >> 2, t4 = lane & 3;
+    uint32_t* my = tiles + warp * kWarpWords;
+    float* myf = reinterpret_cast<float*>(my);
+    guide_load_weights(g.wpack, sw);
+    guide_load_weights_t(g.wpack, swt);
     int first, n;
     source_range(src, first, n);
     const float wsum = g.wsum[0];
     const float inv_wsum = wsum > 0.f ? 1.f / wsum : 0.f;
-    float gacc[kOwned];
+    float acc[kOwnTiles][4];
 #pragma unroll
-    for (int i = 0; i < kOwned; i++) gacc[i] = 0.f;
+    for (int j = 0; j < kOwnTiles; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    float loss = 0.f;
     __syncthreads();
-    // accumulate the gradients of the parameters this thread owns that lie in [lo, hi)
-    auto own = [&](int lo, int hi, const float* a, int a_stride, int K, const float* dz, int dz_stride, int N,
-                   int blo) {
-#pragma unroll
-        for (int i = 0; i < kOwned; i++) {
-            const int gi = threadIdx.x + kTrainThreads * i;
-            if (gi >= lo && gi < hi) {
-                const int k = (gi - lo) / N, nn = (gi - lo) % N;
-                float acc = 0.f;
-                for (int t = 0; t < kTile; t++) acc = fmaf(a[t * a_stride + k], dz[t * dz_stride + nn], acc);
-                gacc[i] += acc;
-            } else if (gi >= blo && gi < blo + N) {
-                const int nn = gi - blo;
-                float acc = 0.f;
-                for (int t = 0; t < kTile; t++) acc += dz[t * dz_stride + nn];
-                gacc[i] += acc;
-            }
-        }
-        (void)K;
-    };
-    for (int tile = blockIdx.x; tile * kTile < n; tile += gridDim.x) {
-        if (threadIdx.x < kTile) {
-            const int t = threadIdx.x, i = tile * kTile + t;
-            float wi[3] = {0.f, 0.f, 1.f}, w = 0.f;
+    for (int tile = blockIdx.x; tile * kBlockRows < n; tile += gridDim.x) {
+        // 1. stage this warp's 16 samples
+        if (lane < 16) {
+            const int i = tile * kBlockRows + warp * 16 + lane;
+            float x[kGuideIn], wi[3] = {0.f, 0.f, 1.f}, w = 0.f;
             if (i < n) {
-                source_sample(src, g.frame, first, i, sX + t * kXS, wi, w);
+                source_sample(src, g.frame, first, i, x, wi, w);
             } else {
-                for (int k = 0; k < kGuideIn; k++) sX[t * kXS + k] = 0.f;
+#pragma unroll
+                for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
             }
-            sWi[3 * t] = wi[0]; sWi[3 * t + 1] = wi[1]; sWi[3 * t + 2] = wi[2];
-            sWt[t] = w * inv_wsum;
+            guide_store_input(my + kWX, lane, x);
+            float* f = myf + kWWi + 4 * lane;
+            f[0] = wi[0]; f[1] = wi[1]; f[2] = wi[2];
+            f[3] = w * inv_wsum;
         }
-        __syncthreads();
-        dense_fwd<true>(sX, kXS, kGuideIn, sW + kGW1, sW + kGB1, kGuideHidden, sA1, kAS);
-        __syncthreads();
-        dense_fwd<true>(sA1, kAS, kGuideHidden, sW + kGW2, sW + kGB2, kGuideHidden, sA2, kAS);
-        __syncthreads();
-        dense_fwd<true>(sA2, kAS, kGuideHidden, sW + kGW3, sW + kGB3, kGuideHidden, sA3, kAS);
-        __syncthreads();
-        dense_fwd<false>(sA3, kAS, kGuideHidden, sW + kGW4, sW + kGB4, kGuideOut, sY, kYS);
-        __syncthreads();
-        if (threadIdx.x < kTile) {
-            const int t = threadIdx.x;
+        __syncwarp();
+        // 2. forward
+        {
+            uint32_t a1[5][4];
+#pragma unroll
+            for (int kt = 0; kt < 5; kt++) {
+                a1[kt][0] = my[kWX + g8 * kXW + kt * 8 + t4];
+                a1[kt][1] = my[kWX + (g8 + 8) * kXW + kt * 8 + t4];
+                a1[kt][2] = my[kWX + g8 * kXW + kt * 8 + 4 + t4];
+                a1[kt][3] = my[kWX + (g8 + 8) * kXW + kt * 8 + 4 + t4];
+            }
+            __syncwarp();
+            if (lane < 16) my[kWX + lane * kXW + kGuideIn / 2 - 1] = pack_bf16(1.f, 0.f);  // b1 rides on input 78
+            uint32_t h[4][4], h2[4][4];
+            guide_hidden<5>(sw, kSW1, kSB, a1, h);
+            guide_store_frag(my + kWA1, kAW, h);
+            guide_hidden<4>(sw, kSW2, kSB + 64, h, h2);
+            guide_store_frag(my + kWA2, kAW, h2);
+            guide_hidden<4>(sw, kSW3, kSB + 128, h2, h);
+            guide_store_frag(my + kWA3, kAW, h);
+            float y[5][4];
+#pragma unroll
+            for (int nt = 0; nt < 5; nt++) {
+                const float b0 = __uint_as_float(sw[kSB + 192 + nt * 8 + 2 * t4]);
+                const float b1 = __uint_as_float(sw[kSB + 192 + nt * 8 + 2 * t4 + 1]);
+                y[nt][0] = b0; y[nt][1] = b1; y[nt][2] = b0; y[nt][3] = b1;
+            }
+#pragma unroll
+            for (int kt = 0; kt < 4; kt++) {
+#pragma unroll
+                for (int nt = 0; nt < 5; nt++) {
+                    const uint32_t b0 = sw[kSW4 + (kt * 8 + t4) * 40 + nt * 8 + g8];
+                    const uint32_t b1 = sw[kSW4 + (kt * 8 + 4 + t4) * 40 + nt * 8 + g8];
+                    mma16816(y[nt], h[kt][0], h[kt][1], h[kt][2], h[kt][3], b0, b1);
+                }
+            }
+#pragma unroll
+            for (int nt = 0; nt < 5; nt++) {
+                myf[kWRaw + g8 * kRawW + nt * 8 + 2 * t4] = y[nt][0];
+                myf[kWRaw + g8 * kRawW + nt * 8 + 2 * t4 + 1] = y[nt][1];
+                myf[kWRaw + (g8 + 8) * kRawW + nt * 8 + 2 * t4] = y[nt][2];
+                myf[kWRaw + (g8 + 8) * kRawW + nt * 8 + 2 * t4 + 1] = y[nt][3];
+            }
+        }
+        __syncwarp();
+        // 3. loss gradient per sample
+        if (lane < 16) {
             float raw[kGuideOut], dy[kGuideOut];
-            for (int j = 0; j < kGuideOut; j++) raw[j] = sY[t * kYS + j];
-            const float wi[3] = {sWi[3 * t], sWi[3 * t + 1], sWi[3 * t + 2]};
-            const float l = loss_grad(raw, wi, sWt[t], dy);
-            if (l != 0.f) atomicAdd(g.wsum + 1, l);  // batch loss, for monitoring
-            for (int j = 0; j < kGuideOut; j++) sY[t * kYS + j] = dy[j];
+#pragma unroll
+            for (int j = 0; j < kGuideOut; j++) raw[j] = myf[kWRaw + lane * kRawW + j];
+            const float* f = myf + kWWi + 4 * lane;
+            const float wi[3] = {f[0], f[1], f[2]};
+            loss += loss_grad(raw, wi, f[3], dy);
+#pragma unroll
+            for (int j = 0; j < kGuideOut / 2; j++) my[kWDY + lane * kYW + j] = pack_bf16(dy[2 * j], dy[2 * j + 1]);
+#pragma unroll
+            for (int j = kGuideOut / 2; j < 24; j++) my[kWDY + lane * kYW + j] = 0u;
+        }
+        __syncwarp();
+        // 4. backward, chained in registers
+        {
+            uint32_t ay[3][4];
+#pragma unroll
+            for (int kt = 0; kt < 3; kt++) {
+                ay[kt][0] = my[kWDY + g8 * kYW + kt * 8 + t4];
+                ay[kt][1] = my[kWDY + (g8 + 8) * kYW + kt * 8 + t4];
+                ay[kt][2] = my[kWDY + g8 * kYW + kt * 8 + 4 + t4];
+                ay[kt][3] = my[kWDY + (g8 + 8) * kYW + kt * 8 + 4 + t4];
+            }
+            uint32_t d[4][4], d2[4][4];
+            guide_backward<3>(swt + kST4, ay, my + kWA3, d);
+            guide_store_frag(my + kWD3, kAW, d);
+            guide_backward<4>(swt + kST3, d, my + kWA2, d2);
+            guide_store_frag(my + kWD2, kAW, d2);
+            guide_backward<4>(swt + kST2, d2, my + kWA1, d);
+            guide_store_frag(my + kWD1, kAW, d);
         }
         __syncthreads();
-        // layer 4: dW4 = A3^T dY, db4 = sum dY; dZ3 = (dY W4^T) * relu'(Z3)
-        own(kGW4, kGB4, sA3, kAS, kGuideHidden, sY, kYS, kGuideOut, kGB4);
-        dense_bwd(sY, kYS, kGuideOut, sW + kGW4, kGuideHidden, sA3, sD0);
+        // 5. weight gradients over the block's 128 samples
+        {
+            // ldmatrix row addresses: A^T from four 8x8 tiles (samples 0-7 / 8-15 x columns
+            // a_col + 0-7 / 8-15), dZ from two (samples 0-7 / 8-15)
+            const int mi = lane >> 3, mr = lane & 7;
+            const int a_row = mr + ((mi >> 1) << 3), a_half = (mi & 1) << 2;
+            const int b_row = lane & 15;
+#pragma unroll
+            for (int j = 0; j < kOwnTiles; j++) {
+                const int id = warp * kOwnTiles + j;
+                if (id < kGradTiles) {
+                    const GradTile gt = grad_tile(id);
+                    const int a_addr = gt.a_off + a_row * gt.a_stride + (gt.a_col >> 1) + a_half;
+                    const int b_addr = gt.b_off + b_row * gt.b_stride + (gt.b_col >> 1);
+#pragma unroll 2
+                    for (int s = 0; s < kTrainWarps; s++) {
+                        const uint32_t* base = tiles + s * kWarpWords;
+                        uint32_t a[4] = {0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u};  // BF16 ones
+                        if (gt.a_off >= 0) ldsm_x4_t(a, base + a_addr);
+                        uint32_t b0, b1;
+                        ldsm_x2_t(b0, b1, base + b_addr);
+                        mma16816(acc[j], a[0], a[1], a[2], a[3], b0, b1);
+                    }
+                }
+            }
+        }
         __syncthreads();
-        own(kGW3, kGB3, sA2, kAS, kGuideHidden, sD0, kAS, kGuideHidden, kGB3);
-        dense_bwd(sD0, kAS, kGuideHidden, sW + kGW3, kGuideHidden, sA2, sD1);
-        __syncthreads();
-        own(kGW2, kGB2, sA1, kAS, kGuideHidden, sD1, kAS, kGuideHidden, kGB2);
-        __syncthreads();  // sD0 is overwritten next
-        dense_bwd(sD1, kAS, kGuideHidden, sW + kGW2, kGuideHidden, sA1, sD0);
-        __syncthreads();
-        own(kGW1, kGB1, sX, kXS, kGuideIn, sD0, kAS, kGuideHidden, kGB1);
-        __syncthreads();
+    }
+    // 6. add this block's partial gradients
+#pragma unroll
+    for (int j = 0; j < kOwnTiles; j++) {
+        const int id = warp * kOwnTiles + j;
+        if (id < kGradTiles) {
+            const GradTile gt = grad_tile(id);
+            if (gt.a_off < 0) {  // bias tile: every row holds the column sums
+                if (g8 == 0) {
+                    if (acc[j][0] != 0.f) atomicAdd(&g.grad[gt.out + 2 * t4], acc[j][0]);
+                    if (acc[j][1] != 0.f) atomicAdd(&g.grad[gt.out + 2 * t4 + 1], acc[j][1]);
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int row = gt.a_col + g8 + 8 * h;
+                    int o = gt.out + (g8 + 8 * h) * gt.out_stride + 2 * t4;
+                    bool skip = false;
+                    if (id < 40 && row >= kGuideIn - 2) {
+                        skip = row == kGuideIn - 1;          // padding input
+                        o = kGB1 + gt.b_col + 2 * t4;        // the ones column: b1
+                    }
+                    if (!skip && acc[j][2 * h] != 0.f) atomicAdd(&g.grad[o], acc[j][2 * h]);
+                    if (!skip && acc[j][2 * h + 1] != 0.f) atomicAdd(&g.grad[o + 1], acc[j][2 * h + 1]);
+                }
+            }
+        }
     }
 #pragma unroll
-    for (int i = 0; i < kOwned; i++) {
-        const int gi = threadIdx.x + kTrainThreads * i;
-        if (gi < kGuideParams && gacc[i] != 0.f) atomicAdd(&g.grad[gi], gacc[i]);
-    }
+    for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if (lane == 0 && loss != 0.f) atomicAdd(g.wsum + 1, loss);  // batch loss, for monitoring
 }
 
 __global__ void k_guide_adam(GuideDevice g, float lr, float c1, float c2) {
@@ -306,7 +484,7 @@ __global__ void k_guide_adam(GuideDevice g, float lr, float c1, float c2) {
 
 cudaError_t launch_train(const GuideDevice& g, const TrainSource& src, cudaStream_t s) {
     static bool configured = false;
-    const size_t smem = (size_t)kSmemFloats * sizeof(float);
+    const size_t smem = (size_t)kTrainSmemWords * sizeof(uint32_t);
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

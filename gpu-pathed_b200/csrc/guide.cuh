@@ -3,9 +3,9 @@
 // integrator combines the guide with BSDF sampling by one-sample MIS.
 //
 // Network: 80 inputs -> 64 -> 64 -> 64 (ReLU) -> 40 outputs.
-//   inputs  : sin/cos(2^k pi p_a), k = 0..11, for the 3 axes of the position normalised to
-//             [-1, 1] over the scene bounds (72), shading normal (3), outgoing direction
-//             (3, world space), two zeros of padding
+//   inputs  : sin/cos(f_k p_a), f_k = pi r^k, r = 2^(5/11), k = 0..11 (pi .. 32 pi), for the
+//             3 axes of the position normalised to [-1, 1] over the scene bounds (72),
+//             shading normal (3), outgoing direction (3, world space), two zeros of padding
 //   outputs : 8 lobes x (mu_raw.xyz, kappa_raw, logit)
 //   lobe j  : mu = normalize(mu_raw), kappa = exp(clamp(kappa_raw, -4, 10)), weight = softmax(logit)
 //   vMF pdf : kappa / (2 pi (1 - exp(-2 kappa))) exp(kappa (mu . w - 1))
@@ -35,16 +35,15 @@ constexpr int kGB4 = kGW4 + kGuideHidden * kGuideOut;       // 16064
 constexpr int kGuideParams = kGB4 + kGuideOut;              // 16104
 constexpr float kKappaLogMin = -4.f, kKappaLogMax = 10.f;
 
-// Mixture as stored per queue slot: for each lobe mu.xyz, kappa, weight (40 floats).
-struct GuideMixture {
-    float v[kGuideOut];
-};
-
 // Scene bounds for the position encoding.
 struct GuideFrame {
     float lo[3];
     float inv_ext[3];  // 2 / (hi - lo)
 };
+
+#ifndef PT_GUIDE_FREQ_RATIO
+#define PT_GUIDE_FREQ_RATIO 1.37035f  // 2^(5/11): frequencies pi .. 32 pi
+#endif
 
 __host__ __device__ __forceinline__ void guide_encode(const GuideFrame& gf, const float p[3], const float n[3],
                                                       const float wo[3], float out[kGuideIn]) {
@@ -55,14 +54,14 @@ __host__ __device__ __forceinline__ void guide_encode(const GuideFrame& gf, cons
         for (int k = 0; k < kGuideFreqs; k++) {
             float s, c;
 #if defined(__CUDA_ARCH__)
-            sincosf(f * x, &s, &c);
+            __sincosf(f * x, &s, &c);  // |f x| <= 32 pi: the hardware approximation suffices for features
 #else
             s = sinf(f * x);
             c = cosf(f * x);
 #endif
             out[o++] = s;
             out[o++] = c;
-            f *= 2.f;
+            f *= PT_GUIDE_FREQ_RATIO;
         }
     }
     for (int a = 0; a < 3; a++) out[o++] = n[a];
@@ -71,39 +70,58 @@ __host__ __device__ __forceinline__ void guide_encode(const GuideFrame& gf, cons
     out[o++] = 0.f;
 }
 
-// Raw network outputs -> mixture parameters (mu normalised, kappa, softmax weight).
-__host__ __device__ __forceinline__ void guide_activate(const float raw[kGuideOut], float mix[kGuideOut]) {
-    float mx = -1e30f;
-    for (int j = 0; j < kGuideLobes; j++) mx = fmaxf(mx, raw[5 * j + 4]);
-    float sum = 0.f;
-    float e[kGuideLobes];
-    for (int j = 0; j < kGuideLobes; j++) {
-        e[j] = expf(raw[5 * j + 4] - mx);
-        sum += e[j];
-    }
-    for (int j = 0; j < kGuideLobes; j++) {
-        const float mxr = raw[5 * j], myr = raw[5 * j + 1], mzr = raw[5 * j + 2];
-        const float len = sqrtf(mxr * mxr + myr * myr + mzr * mzr) + 1e-12f;
-        mix[5 * j] = mxr / len;
-        mix[5 * j + 1] = myr / len;
-        mix[5 * j + 2] = mzr / len;
-        mix[5 * j + 3] = expf(fminf(kKappaLogMax, fmaxf(kKappaLogMin, raw[5 * j + 3])));
-        mix[5 * j + 4] = e[j] / sum;
-    }
-}
-
 // log of the vMF normaliser kappa / (2 pi (1 - exp(-2 kappa)))
 __host__ __device__ __forceinline__ float vmf_log_norm(float kappa) {
     return logf(kappa) - 1.8378770664093453f /* log(2 pi) */ - log1pf(-expf(-2.f * kappa));
 }
 
+// Mixture as stored per queue slot for sampling and evaluation (40 floats): lobe j as the
+// float4 (kappa_j mu_j, c_j) with c_j = log pi_j + log C(kappa_j) - kappa_j, then the 8
+// cumulative lobe weights. The density is then sum_j exp(c_j + kappa_j mu_j . w): one
+// exponential per lobe.
+constexpr int kMixCdf = 4 * kGuideLobes;
+
+#if defined(__CUDACC__)
+// Raw network outputs -> stored mixture. The stored values define the distribution that is
+// both sampled and evaluated, so hardware approximations of exp/log are exact enough here.
+__device__ __forceinline__ void guide_activate(const float raw[kGuideOut], float mix[kGuideOut]) {
+    float mx = -1e30f;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) mx = fmaxf(mx, raw[5 * j + 4]);
+    float sum = 0.f;
+    float e[kGuideLobes];
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        e[j] = __expf(raw[5 * j + 4] - mx);
+        sum += e[j];
+    }
+    const float inv_sum = 1.f / sum;
+    float cdf = 0.f;
+#pragma unroll
+    for (int j = 0; j < kGuideLobes; j++) {
+        const float mxr = raw[5 * j], myr = raw[5 * j + 1], mzr = raw[5 * j + 2];
+        const float il = rsqrtf(mxr * mxr + myr * myr + mzr * mzr + 1e-24f);
+        const float lk = fminf(kKappaLogMax, fmaxf(kKappaLogMin, raw[5 * j + 3]));
+        const float kappa = __expf(lk);
+        const float pi = e[j] * inv_sum;
+        mix[4 * j] = kappa * mxr * il;
+        mix[4 * j + 1] = kappa * myr * il;
+        mix[4 * j + 2] = kappa * mzr * il;
+        // log pi + log kappa - log(2 pi) - log(1 - exp(-2 kappa)) - kappa
+        mix[4 * j + 3] = __logf(pi) + lk - 1.8378770664093453f - __logf(1.f - __expf(-2.f * kappa)) - kappa;
+        cdf += pi;
+        mix[kMixCdf + j] = cdf;
+    }
+}
+
+// Density of the stored mixture at unit direction w.
 __device__ __forceinline__ float guide_pdf(const float* mix, V w) {
+    const float4* l = reinterpret_cast<const float4*>(mix);
     float p = 0.f;
 #pragma unroll
     for (int j = 0; j < kGuideLobes; j++) {
-        const float k = mix[5 * j + 3];
-        const float d = mix[5 * j] * w.x + mix[5 * j + 1] * w.y + mix[5 * j + 2] * w.z;
-        p += mix[5 * j + 4] * expf(vmf_log_norm(k) + k * (d - 1.f));
+        const float4 v = l[j];
+        p += __expf(v.w + v.x * w.x + v.y * w.y + v.z * w.z);
     }
     return p;
 }
@@ -112,25 +130,22 @@ __device__ __forceinline__ float guide_pdf(const float* mix, V w) {
 // (Jakob, "Numerically stable sampling of the von Mises-Fisher distribution on S^2", 2012).
 __device__ __forceinline__ V guide_sample(const float* mix, float u0, float u1, float u2) {
     int j = kGuideLobes - 1;
-    float acc = 0.f;
 #pragma unroll
-    for (int k = 0; k < kGuideLobes; k++) {
-        acc += mix[5 * k + 4];
-        if (u0 < acc) {
-            j = k;
-            break;
-        }
-    }
-    const float kappa = mix[5 * j + 3];
+    for (int k = kGuideLobes - 2; k >= 0; k--)
+        if (u0 < mix[kMixCdf + k]) j = k;
+    const float4 v = reinterpret_cast<const float4*>(mix)[j];
+    const float kappa = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
     const float u = fmaxf(u1, 1e-7f);
     const float wz = fminf(1.f, fmaxf(-1.f, 1.f + logf(u + (1.f - u) * expf(-2.f * kappa)) / kappa));
     const float r = sqrtf(fmaxf(0.f, 1.f - wz * wz));
     float s, c;
     sincosf(kTwoPiF * u2, &s, &c);
-    const V mu = V{mix[5 * j], mix[5 * j + 1], mix[5 * j + 2]};
+    const float ik = 1.f / kappa;
+    const V mu = V{v.x * ik, v.y * ik, v.z * ik};
     // orthonormal frame around mu
     const Frame f = make_frame(mu);
     return to_world(f, V{r * c, r * s, wz});
 }
+#endif  // __CUDACC__
 
 }  // namespace pt

@@ -12,11 +12,11 @@ namespace pt {
 // Device buffers of the guide network and its training state.
 struct GuideDevice {
     float* w;            // FP32 master parameters [kGuideParams]
-    uint32_t* wpack;     // BF16 pairs in mma B-fragment order + FP32 biases (see guide.cu)
+    uint32_t* wpack;     // [kGuidePackWords] shared-memory images of the BF16 weights
     float* grad;         // [kGuideParams]
     float* adam_m;       // [kGuideParams]
     float* adam_v;       // [kGuideParams]
-    float* wsum;         // [1] sum of sample weights of the current batch
+    float* wsum;         // [2] sum of sample weights of the current batch, batch loss
     GuideFrame frame;
 };
 
@@ -39,11 +39,12 @@ struct GuideRecord {
 };
 static_assert(sizeof(GuideRecord) == 64, "GuideRecord layout");
 
-// Bytes of the packed inference weights.
-constexpr int kGuidePackWords = (kGuideIn / 2) * kGuideHidden + 2 * (kGuideHidden / 2) * kGuideHidden +
-                                (kGuideHidden / 2) * kGuideOut + (kGuideHidden * 3 + kGuideOut);
+// 32-bit words of the packed weights: the shared-memory images of the forward weights (BF16
+// pairs of consecutive inputs, padded rows, FP32 biases; 9000 words) and of the transposed
+// backward weights (BF16 pairs of consecutive outputs, padded rows; 6912 words).
+constexpr int kGuidePackWords = 15912;
 
-// Repack FP32 master weights into the inference layout (BF16 pairs + FP32 biases).
+// Repack the FP32 master weights into the packed images.
 cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s);
 // Raw network outputs for n explicit input vectors (inference kernel, tensor cores).
 cudaError_t guide_forward_features(const GuideDevice& g, const float* x, int n, float* raw, cudaStream_t s);

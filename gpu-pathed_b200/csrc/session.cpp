@@ -8,6 +8,10 @@
 
 #include "../../include/pathed.h"
 
+#ifndef PT_GUIDE_TRAIN_PATHS
+#define PT_GUIDE_TRAIN_PATHS 524288
+#endif
+
 namespace pt {
 
 namespace {
@@ -205,8 +209,8 @@ int Session::ensure_guide() {
         if ((r = check_cuda(d_gm_.alloc(kGuideParams * 4), "guide"))) return r;
         if ((r = check_cuda(d_gv_.alloc(kGuideParams * 4), "guide"))) return r;
         if ((r = check_cuda(d_gwsum_.alloc(16), "guide"))) return r;
-        if ((r = check_cuda(d_grec_.alloc((size_t)(1 << 20) * sizeof(GuideRecord)), "guide records"))) return r;
         if ((r = check_cuda(d_grec_count_.alloc(16), "guide"))) return r;
+        if ((r = check_cuda(configure_guide_infer(), "guide inference configuration"))) return r;
         if ((r = check_cuda(d_gring_.alloc((size_t)(1 << 21) * sizeof(GuideSample)), "guide samples"))) return r;
         if ((r = check_cuda(d_gring_count_.alloc(16), "guide"))) return r;
         guide_alloc_ = true;
@@ -626,17 +630,21 @@ int Session::render_async(int spp) {
         if ((r = ensure_guide())) return r;
         const size_t mix_bytes = (size_t)queue_cap_ * kGuideOut * sizeof(float);
         if ((r = check_cuda(d_gmix_.alloc(mix_bytes), "guide mixtures"))) return r;
-        const int gstride = std::max(1, queue_cap_ / 131072);  // about 2^17 training paths per wave
+        // every gstride-th path of a wave records training data: about 2^19 training paths
+        const int gstride = std::max(1, queue_cap_ / PT_GUIDE_TRAIN_PATHS);
         const size_t tpaths = (size_t)(queue_cap_ + gstride - 1) / gstride;
         if ((r = check_cuda(d_gacc_.alloc(tpaths * kMaxDepthLimit * 3 * sizeof(float)), "guide accumulators")))
             return r;
+        // one record per scattering vertex of a training path
+        const size_t rec_cap = tpaths * (size_t)std::max(1, max_depth_ - 1);
+        if ((r = check_cuda(d_grec_.alloc(rec_cap * sizeof(GuideRecord)), "guide records"))) return r;
         p.guide_mode = guide_iters_ >= guide_warmup_ ? 2 : 1;
         p.gwpack = d_gwpack_.as<uint32_t>();
         p.gmix = d_gmix_.as<float>();
         p.gframe = gframe_;
         p.grec = d_grec_.as<GuideRecord>();
         p.grec_count = d_grec_count_.as<int>();
-        p.grec_cap = 1 << 20;
+        p.grec_cap = (int)rec_cap;
         p.gacc = d_gacc_.as<float>();
         p.gstride = gstride;
         p.gring = d_gring_.as<GuideSample>();

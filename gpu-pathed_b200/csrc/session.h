@@ -178,7 +178,6 @@ private:
     bool guide_alloc_ = false;
     DevBuf d_gw_, d_gwpack_, d_ggrad_, d_gm_, d_gv_, d_gwsum_, d_gmix_, d_grec_, d_grec_count_, d_gacc_, d_gring_,
         d_gring_count_;
-    size_t gmix_cap_ = 0;
     int guide_iters_ = 0;       // Adam steps taken
     int guide_warmup_ = 4;      // steps before the guide is used for sampling
     int guide_batch_ = 1 << 18;

@@ -435,56 +435,62 @@ __global__ void k_shadow(FrameParams p, int depth) {
     if (CNT) flush_work(work, &p.stats->shadow_nodes, &p.stats->shadow_prims);
 }
 
-// Guide inference for the rays of the queue consumed at `depth`: features of each hit, the
-// network on the tensor cores (16 rays per warp), the mixture written per queue slot.
-__global__ void __launch_bounds__(128) k_guide_infer(FrameParams p, int depth) {
-    __shared__ uint32_t sw[kSWords];
-    __shared__ uint32_t sx[4][16 * kSXStride];
-    // outputs overwrite the inputs: every lane has loaded its input fragments into registers
-    // before the warp-synchronous mma chain reaches the output stores
-    float(*sy)[16 * kSXStride] = reinterpret_cast<float(*)[16 * kSXStride]>(sx);
+// Guide inference for the rays of the queue consumed at `depth`: each lane computes the
+// features of one hit, the warp runs the network on the tensor cores for its 32 rays (two
+// 16-row groups sharing each weight fragment), each lane activates its own row and the warp
+// writes the 32 mixtures of consecutive queue slots as one contiguous 5120-byte store.
+constexpr int kInferWarps = 8;
+constexpr int kInferSmemBytes = (kSWords + kInferWarps * 32 * kSXStride) * 4;  // 81 KB: 2 blocks per SM
+
+__global__ void __launch_bounds__(32 * kInferWarps, 2) k_guide_infer(FrameParams p, int depth) {
+    extern __shared__ __align__(16) uint32_t ism[];
+    const int count = p.counters->ray_count[depth];
+    const int groups = (count + 31) / 32;
+    if (blockIdx.x * kInferWarps >= groups) return;  // no rays for this block: skip the weight copy
+    uint32_t* sw = ism;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* sx = ism + kSWords + warp * 32 * kSXStride;
+    // outputs overwrite the inputs of the same 16-row group: every lane has loaded its input
+    // fragments into registers before the warp-synchronous mma chain reaches the output stores
+    const float* sy = reinterpret_cast<const float*>(sx);
     guide_load_weights(p.gwpack, sw);
     __syncthreads();
-    const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int groups = (count + 15) / 16;
-    for (int grp = blockIdx.x * 4 + warp; grp < groups; grp += gridDim.x * 4) {
-        const int slot = grp * 16 + (lane & 15);
+    for (int grp = blockIdx.x * kInferWarps + warp; grp < groups; grp += gridDim.x * kInferWarps) {
+        const int slot = grp * 32 + lane;
+        float x[kGuideIn];
         bool hit = false;
-        if (lane < 16) {
-            float x[kGuideIn];
-            if (slot < count) {
-                const float4 o4 = q.o[slot], d4 = q.d[slot], h4 = q.hit[slot];
-                if (__float_as_int(h4.w) != kMissPrim) {
-                    V point, n;
-                    int mat;
-                    hit_info(p.sc, mkv(o4), mkv(d4), h4, point, n, mat);
-                    n = normalized(n);
-                    const V wo = normalized(-mkv(d4));
-                    const float pp[3] = {point.x, point.y, point.z}, nn[3] = {n.x, n.y, n.z}, ww[3] = {wo.x, wo.y, wo.z};
-                    guide_encode(p.gframe, pp, nn, ww, x);
-                    hit = true;
-                }
+        if (slot < count) {
+            const float4 o4 = q.o[slot], d4 = q.d[slot], h4 = q.hit[slot];
+            if (__float_as_int(h4.w) != kMissPrim) {
+                V point, n;
+                int mat;
+                hit_info(p.sc, mkv(o4), mkv(d4), h4, point, n, mat);
+                n = normalized(n);
+                const V wo = normalized(-mkv(d4));
+                const float pp[3] = {point.x, point.y, point.z}, nn[3] = {n.x, n.y, n.z}, ww[3] = {wo.x, wo.y, wo.z};
+                guide_encode(p.gframe, pp, nn, ww, x);
+                hit = true;
             }
-            if (!hit)
-                for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
-            guide_store_input(sx[warp], lane, x);
         }
+        if (!hit)
+            for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
+        guide_store_input(sx, lane, x);
         __syncwarp();
-        guide_mlp_warp16(sw, sx[warp], sy[warp]);
+        guide_mlp_warp32(sw, sx);
         __syncwarp();
-        if (lane < 16) {
+        {
+            float* row = reinterpret_cast<float*>(sx) + (lane >> 4) * 16 * kSXStride + (lane & 15) * kGuideOut;
             float raw[kGuideOut], mix[kGuideOut];
-            for (int j = 0; j < kGuideOut; j++) raw[j] = sy[warp][lane * kGuideOut + j];
+            for (int j = 0; j < kGuideOut; j++) raw[j] = row[j];
             guide_activate(raw, mix);
-            for (int j = 0; j < kGuideOut; j++) sy[warp][lane * kGuideOut + j] = mix[j];
+            for (int j = 0; j < kGuideOut; j++) row[j] = mix[j];
         }
         __syncwarp();
-        // 16 consecutive slots: one contiguous 2560-byte store by the whole warp
-        const int rows = count - grp * 16 < 16 ? count - grp * 16 : 16;
-        float* dst = p.gmix + (size_t)grp * 16 * kGuideOut;
-        for (int e = lane; e < rows * kGuideOut; e += 32) dst[e] = sy[warp][e];
+        const int rows = count - grp * 32 < 32 ? count - grp * 32 : 32;
+        float* dst = p.gmix + (size_t)grp * 32 * kGuideOut;
+        for (int e = lane; e < rows * kGuideOut; e += 32)
+            dst[e] = sy[(e / (16 * kGuideOut)) * 16 * kSXStride + e % (16 * kGuideOut)];
         __syncwarp();
     }
 }
@@ -597,7 +603,7 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
                 mark(kStageSort);
             }
             if (p.guide_mode == 2 && d < p.max_depth - 1) {
-                k_guide_infer<<<p.num_sms * 4, 128, 0, stream>>>(p, d);
+                k_guide_infer<<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
                 mark(kStageGuide);
             }
             if (p.guide_mode) k_shade<true><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
@@ -713,6 +719,10 @@ cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks*
         case 8: return cnt ? enqueue_frame_w<8, true>(p, stream, marks) : enqueue_frame_w<8, false>(p, stream, marks);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t configure_guide_infer() {
+    return cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmemBytes);
 }
 
 cudaError_t configure_traversal_smem(size_t bytes) {

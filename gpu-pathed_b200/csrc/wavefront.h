@@ -115,8 +115,8 @@ struct FrameParams {
     int guide_mode;          // 0 off, 1 collect training data only, 2 guided sampling + collect
     int consistent_mis;      // NEE weights use the BSDF's true sampling density (microfacet)
     const uint32_t* gwpack;  // packed inference weights
-    float* gmix;             // per queue slot: mixture (40 floats)
     GuideFrame gframe;       // scene bounds for the position encoding
+    float* gmix;             // per queue slot: mixture (40 floats)
     GuideRecord* grec;       // vertex records of training paths (this wave)
     int* grec_count;
     int grec_cap;
@@ -134,6 +134,8 @@ cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks*
 
 // Raise the dynamic shared-memory limit of the traversal kernels to `bytes`.
 cudaError_t configure_traversal_smem(size_t bytes);
+// Opt the guide inference kernel into its dynamic shared memory (weights + 8 warps x 32 rows).
+cudaError_t configure_guide_infer();
 
 // Closest-hit queries for caller-provided rays (parity entry). Arrays are device pointers.
 cudaError_t enqueue_trace_rays(const SceneDevice& sc, int stack_depth, const float* o, const float* d,

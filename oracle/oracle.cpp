@@ -1016,10 +1016,13 @@ inline float bf16(float x) {  // round to nearest even, to BF16 precision
     return r;
 }
 
+inline bool is_bias(int i) { return i >= B4 || (i >= B1 && i < W2) || (i >= B2 && i < W3) || (i >= B3 && i < W4); }
+
 struct Net {
     std::vector<double> w;
+    // the kernels multiply with BF16-rounded weights and add FP32 biases
     explicit Net(const float* p) : w(NP) {
-        for (int i = 0; i < NP; i++) w[i] = bf16(p[i]);  // the kernels use BF16-rounded weights
+        for (int i = 0; i < NP; i++) w[i] = is_bias(i) ? (double)p[i] : (double)bf16(p[i]);
     }
 };
 
@@ -1089,23 +1092,28 @@ inline double loss_and_grad(const double (&y)[OUT], const double* wi, double w, 
 extern "C" {
 
 // Raw outputs (n x 40). quant = 1 rounds each layer's inputs to BF16 (as the inference
-// kernel's operands are); FP64 accumulation.
+// kernel's operands are); FP64 accumulation. Inputs 78 and 79 are padding and read as zero.
 void oracle_guide_forward(const float* params, const float* x, int n, int quant, double* out) {
     using namespace oracle::guide;
     const Net net(params);
     for (int i = 0; i < n; i++) {
         double xi[IN], a1[H], a2[H], a3[H], y[OUT];
-        for (int k = 0; k < IN; k++) xi[k] = x[(size_t)i * IN + k];
+        for (int k = 0; k < IN; k++) xi[k] = k < IN - 2 ? x[(size_t)i * IN + k] : 0.0;
         forward(net, xi, quant != 0, a1, a2, a3, y);
         for (int j = 0; j < OUT; j++) out[(size_t)i * OUT + j] = y[j];
     }
 }
 
-// Loss -sum w_i log q / sum w_i and its gradient (16104 values) in FP64, FP32 activations
-// not emulated (exact arithmetic on the BF16-rounded weights).
-double oracle_guide_grad(const float* params, const float* x, const float* wi, const float* w, int n, double* grad) {
+// Loss -sum w_i log q / sum w_i and its gradient (16104 values) in FP64 on the BF16-rounded
+// weights. quant = 1 also rounds every matrix-product operand to BF16 where the tensor-core
+// training kernel does: the inputs and activations X, A1..A3 and the back-propagated dY,
+// dZ3, dZ2, dZ1 (the ReLU masks use the unrounded activations). Inputs 78 and 79 are padding
+// and read as zero.
+double oracle_guide_grad(const float* params, const float* x, const float* wi, const float* w, int n, int quant,
+                         double* grad) {
     using namespace oracle::guide;
     const Net net(params);
+    auto q = [&](double v) { return quant ? (double)bf16((float)v) : v; };
     for (int i = 0; i < NP; i++) grad[i] = 0;
     double wsum = 0;
     for (int i = 0; i < n; i++) wsum += w[i];
@@ -1113,37 +1121,38 @@ double oracle_guide_grad(const float* params, const float* x, const float* wi, c
     double loss = 0;
     for (int i = 0; i < n; i++) {
         double xi[IN], a1[H], a2[H], a3[H], y[OUT], dy[OUT];
-        for (int k = 0; k < IN; k++) xi[k] = x[(size_t)i * IN + k];
-        forward(net, xi, false, a1, a2, a3, y);
+        for (int k = 0; k < IN; k++) xi[k] = k < IN - 2 ? q(x[(size_t)i * IN + k]) : 0.0;
+        forward(net, xi, quant != 0, a1, a2, a3, y);
         const double d[3] = {wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
         if (w[i] == 0) continue;
         loss += loss_and_grad(y, d, w[i] * inv, dy);
         double d3[H], d2[H], d1[H];
+        for (int j = 0; j < OUT; j++) dy[j] = q(dy[j]);
         for (int k = 0; k < H; k++) {
             double s = 0;
             for (int j = 0; j < OUT; j++) {
-                grad[W4 + k * OUT + j] += a3[k] * dy[j];
+                grad[W4 + k * OUT + j] += q(a3[k]) * dy[j];
                 s += dy[j] * net.w[W4 + k * OUT + j];
             }
-            d3[k] = a3[k] > 0 ? s : 0;
+            d3[k] = a3[k] > 0 ? q(s) : 0;
         }
         for (int j = 0; j < OUT; j++) grad[B4 + j] += dy[j];
         for (int k = 0; k < H; k++) {
             double s = 0;
             for (int j = 0; j < H; j++) {
-                grad[W3 + k * H + j] += a2[k] * d3[j];
+                grad[W3 + k * H + j] += q(a2[k]) * d3[j];
                 s += d3[j] * net.w[W3 + k * H + j];
             }
-            d2[k] = a2[k] > 0 ? s : 0;
+            d2[k] = a2[k] > 0 ? q(s) : 0;
         }
         for (int j = 0; j < H; j++) grad[B3 + j] += d3[j];
         for (int k = 0; k < H; k++) {
             double s = 0;
             for (int j = 0; j < H; j++) {
-                grad[W2 + k * H + j] += a1[k] * d2[j];
+                grad[W2 + k * H + j] += q(a1[k]) * d2[j];
                 s += d2[j] * net.w[W2 + k * H + j];
             }
-            d1[k] = a1[k] > 0 ? s : 0;
+            d1[k] = a1[k] > 0 ? q(s) : 0;
         }
         for (int j = 0; j < H; j++) grad[B2 + j] += d2[j];
         for (int k = 0; k < IN; k++)

@@ -109,7 +109,7 @@ class Oracle(_SceneLib):
         L.oracle_rng.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, C.c_void_p]
         L.oracle_num_lights.argtypes = [C.c_void_p]
         L.oracle_guide_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
-        L.oracle_guide_grad.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
+        L.oracle_guide_grad.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_void_p]
         L.oracle_guide_grad.restype = C.c_double
         L.oracle_guide_loss_exact.argtypes = [C.c_void_p] * 4 + [C.c_int]
         L.oracle_guide_loss_exact.restype = C.c_double
@@ -120,11 +120,11 @@ class Oracle(_SceneLib):
         self.lib.oracle_guide_forward(params.ctypes.data, x.ctypes.data, x.shape[0], int(quant), out.ctypes.data)
         return out
 
-    def guide_grad(self, params, x, wi, w):
+    def guide_grad(self, params, x, wi, w, quant=False):
         params, x, wi, w = _f(params), _f(x).reshape(-1, 80), _f(wi).reshape(-1, 3), _f(w)
         g = np.zeros(params.size, np.float64)
         loss = self.lib.oracle_guide_grad(params.ctypes.data, x.ctypes.data, wi.ctypes.data, w.ctypes.data,
-                                          x.shape[0], g.ctypes.data)
+                                          x.shape[0], int(quant), g.ctypes.data)
         return loss, g
 
     def guide_loss_exact(self, params64, x, wi, w):

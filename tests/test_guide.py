@@ -76,17 +76,45 @@ def test_inference_kernel_matches_oracle(oracle_lib):
     s.close()
 
 
+def _compare(g, ref):
+    rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
+    cos = g @ ref / (np.linalg.norm(g) * np.linalg.norm(ref))
+    return rel, cos
+
+
+def test_bf16_operand_rounding_is_a_small_perturbation(oracle_lib):
+    """the oracle's BF16 emulation of the training kernel stays close to exact FP64 training"""
+    p = random_params(9)
+    x, wi, w = random_batch(500, seed=10)
+    _, exact = oracle_lib.guide_grad(p, x, wi, w)
+    _, quant = oracle_lib.guide_grad(p, x, wi, w, quant=True)
+    rel, cos = _compare(quant, exact)
+    assert rel <= 3e-2 and cos >= 0.999, (rel, cos)
+
+
 @pytest.mark.gpu
-def test_training_gradients_match_oracle(oracle_lib):
+@pytest.mark.parametrize("n", [3000, 40000])
+def test_training_gradients_match_oracle(oracle_lib, n):
+    """tensor-core training kernel (BF16 operands, FP32 accumulation) against the FP64 oracle
+    that rounds the same operands to BF16; n = 40000 gives blocks several sample tiles"""
     s = pathed.Session(8, 8)
     p = random_params(9)
     s.set_guide_params(p)
-    x, wi, w = random_batch(3000, seed=10)
+    x, wi, w = random_batch(n, seed=10)
     g = s.guide_gradients(x, wi, w).astype(np.float64)
+    _, ref_q = oracle_lib.guide_grad(p, x, wi, w, quant=True)
     _, ref = oracle_lib.guide_grad(p, x, wi, w)
-    rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
-    cos = g @ ref / (np.linalg.norm(g) * np.linalg.norm(ref))
-    assert rel <= 1e-3 and cos >= 0.999999, (rel, cos)
+    rel_q, cos_q = _compare(g, ref_q)
+    rel, cos = _compare(g, ref)
+    print(f"n {n}: vs BF16-emulating oracle rel {rel_q:.2e} cos {cos_q:.8f}; vs exact rel {rel:.2e}")
+    # FP32 accumulation order and rare BF16 rounding-boundary flips are all that differ
+    assert rel_q <= 2e-3 and cos_q >= 0.99999, (rel_q, cos_q)
+    assert rel <= 3e-2 and cos >= 0.999, (rel, cos)
+    # every parameter block is trained: per-block agreement
+    for lo, hi in [(0, 5120), (5120, 5184), (5184, 9280), (9280, 9344), (9344, 13440), (13440, 13504),
+                   (13504, 16064), (16064, 16104)]:
+        r, _ = _compare(g[lo:hi], ref_q[lo:hi])
+        assert r <= 1e-2, (lo, hi, r)
     s.close()
 
 
@@ -124,13 +152,15 @@ def test_guided_estimator_is_unbiased():
 
 @pytest.mark.gpu
 def test_trained_guide_reduces_error():
-    """hard lighting (environment seen through a slit): at equal samples, the trained guide's
-    relMSE against a converged plain render is lower than plain BSDF + NEE sampling's"""
-    w = h = 48
+    """hard lighting (environment seen through a slit): after online training, the guided
+    render's relMSE against a converged plain render is clearly below plain BSDF + NEE
+    sampling's at the same sample count"""
+    w = h = 128
     ref = _slit_room(w, h)
     ref.set_consistent_mis(True)
+    ref.set_seed(1234)
     for _ in range(16):
-        ref.render(256)
+        ref.render(512)
     img_ref = ref.readback().astype(np.float64)
     ref.close()
 
@@ -140,23 +170,24 @@ def test_trained_guide_reduces_error():
     plain = _slit_room(w, h)
     plain.set_consistent_mis(True)
     plain.set_seed(77)
-    for _ in range(8):
-        plain.render(16)
+    for _ in range(16):
+        plain.render(4)
     e_plain = relmse(plain.readback().astype(np.float64))
     plain.close()
 
     g = _slit_room(w, h)
     g.set_guiding(True)
-    g.set_guide_options(steps_per_frame=8, warmup_steps=16)
-    for _ in range(12):  # training frames (discarded)
-        g.render(16)
+    g.set_guide_options(steps_per_frame=8, batch=1 << 16, warmup_steps=4)
+    for _ in range(96):  # online training frames (discarded)
+        g.render(4)
     g.reset()
     g.set_seed(77)
-    for _ in range(8):
-        g.render(16)
+    for _ in range(16):
+        g.render(4)
     e_guided = relmse(g.readback().astype(np.float64))
     info = g.guide_info()
     g.close()
-    print(f"relMSE at 128 spp: plain {e_plain:.5f} guided {e_guided:.5f} (steps {info['steps']}, "
-          f"samples {info['samples']})")
-    assert e_guided < e_plain
+    print(f"relMSE at 64 spp: plain {e_plain:.6f} guided {e_guided:.6f} (ratio {e_plain / e_guided:.2f}; "
+          f"steps {info['steps']}, samples {info['samples']}, loss {info['loss']:.3f})")
+    assert info["mode"] == 2
+    assert e_guided < 0.8 * e_plain
