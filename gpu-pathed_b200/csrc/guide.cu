@@ -467,10 +467,12 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideDevice g,
     if (lane == 0 && loss != 0.f) atomicAdd(g.wsum + 1, loss);  // batch loss, for monitoring
 }
 
-__global__ void k_guide_adam(GuideDevice g, float lr, float c1, float c2) {
+__global__ void k_guide_adam(GuideDevice g, float lr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kGuideParams) return;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float t = (float)(*g.step + 1);
+    const float c1 = 1.f - powf(b1, t), c2 = 1.f - powf(b2, t);
     float gr = g.grad[i];
     if (!isfinite(gr)) gr = 0.f;
     gr = fminf(10.f, fmaxf(-10.f, gr));
@@ -482,25 +484,23 @@ __global__ void k_guide_adam(GuideDevice g, float lr, float c1, float c2) {
     g.grad[i] = 0.f;
 }
 
+__global__ void k_guide_step(int* step) { *step += 1; }
+
+constexpr size_t kTrainSmemBytes = (size_t)kTrainSmemWords * sizeof(uint32_t);
+
 cudaError_t launch_train(const GuideDevice& g, const TrainSource& src, cudaStream_t s) {
-    static bool configured = false;
-    const size_t smem = (size_t)kTrainSmemWords * sizeof(uint32_t);
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
     cudaError_t e = cudaMemsetAsync(g.wsum, 0, 2 * sizeof(float), s);  // weight sum, batch loss
     if (e != cudaSuccess) return e;
-    k_guide_wsum<<<148, 256, 0, s>>>(src, g.wsum);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_guide_train<<<sms, kTrainThreads, smem, s>>>(g, src);
+    k_guide_wsum<<<g.num_sms, 256, 0, s>>>(src, g.wsum);
+    k_guide_train<<<g.num_sms, kTrainThreads, kTrainSmemBytes, s>>>(g, src);
     return cudaGetLastError();
 }
 
 }  // namespace
+
+cudaError_t guide_configure() {
+    return cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmemBytes);
+}
 
 cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s) {
     k_guide_pack<<<(kGuidePackWords + 255) / 256, 256, 0, s>>>(g.w, g.wpack);
@@ -523,20 +523,15 @@ cudaError_t guide_gradients_features(const GuideDevice& g, const float* x, const
     return launch_train(g, src, s);
 }
 
-cudaError_t guide_adam(const GuideDevice& g, float lr, int t, cudaStream_t s) {
-    const float c1 = 1.f - powf(0.9f, (float)t), c2 = 1.f - powf(0.999f, (float)t);
-    k_guide_adam<<<(kGuideParams + 255) / 256, 256, 0, s>>>(g, lr, c1, c2);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    return guide_pack(g, s);
-}
-
 cudaError_t guide_train_step(const GuideDevice& g, const GuideSample* ring, int cap, const int* count, int batch,
-                             float lr, int t, cudaStream_t s) {
+                             float lr, cudaStream_t s) {
     TrainSource src{nullptr, nullptr, nullptr, ring, cap, count, batch};
     cudaError_t e = launch_train(g, src, s);
     if (e != cudaSuccess) return e;
-    return guide_adam(g, lr, t, s);
+    k_guide_adam<<<(kGuideParams + 255) / 256, 256, 0, s>>>(g, lr);
+    k_guide_step<<<1, 1, 0, s>>>(g.step);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return guide_pack(g, s);
 }
 
 }  // namespace pt

@@ -17,6 +17,8 @@ struct GuideDevice {
     float* adam_m;       // [kGuideParams]
     float* adam_v;       // [kGuideParams]
     float* wsum;         // [2] sum of sample weights of the current batch, batch loss
+    int* step;           // Adam steps taken (device counter, so training launches replay in graphs)
+    int num_sms;         // training grid: one block per SM
     GuideFrame frame;
 };
 
@@ -44,6 +46,8 @@ static_assert(sizeof(GuideRecord) == 64, "GuideRecord layout");
 // backward weights (BF16 pairs of consecutive outputs, padded rows; 6912 words).
 constexpr int kGuidePackWords = 15912;
 
+// Opt the training kernel into its dynamic shared memory (once per device, before capture).
+cudaError_t guide_configure();
 // Repack the FP32 master weights into the packed images.
 cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s);
 // Raw network outputs for n explicit input vectors (inference kernel, tensor cores).
@@ -52,10 +56,11 @@ cudaError_t guide_forward_features(const GuideDevice& g, const float* x, int n, 
 // parameters, for explicit input vectors (training kernel); grad is overwritten.
 cudaError_t guide_gradients_features(const GuideDevice& g, const float* x, const float* wi, const float* w, int n,
                                      cudaStream_t s);
-// Training on samples [first, first + n) of a ring of capacity `cap`: gradients then one
-// Adam step (lr, betas, eps) with step counter t (1-based).
+// Training on the newest `batch` samples of a ring of capacity `cap` (`count` samples written
+// so far): gradients, then one Adam step (lr, betas 0.9 / 0.999, eps 1e-8) whose bias
+// correction uses the device step counter, then the repack. Graph-capturable: no argument
+// changes from step to step.
 cudaError_t guide_train_step(const GuideDevice& g, const GuideSample* ring, int cap, const int* count, int batch,
-                             float lr, int t, cudaStream_t s);
-cudaError_t guide_adam(const GuideDevice& g, float lr, int t, cudaStream_t s);
+                             float lr, cudaStream_t s);
 
 }  // namespace pt

@@ -152,6 +152,8 @@ GuideDevice Session::guide_view() const {
     g.adam_m = d_gm_.as<float>();
     g.adam_v = d_gv_.as<float>();
     g.wsum = d_gwsum_.as<float>();
+    g.step = reinterpret_cast<int*>(d_gwsum_.as<float>() + 3);
+    g.num_sms = num_sms_;
     g.frame = gframe_;
     return g;
 }
@@ -194,6 +196,7 @@ int Session::guide_init_weights() {
     if ((r = check_cuda(cudaMemsetAsync(d_gm_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
     if ((r = check_cuda(cudaMemsetAsync(d_gv_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
     if ((r = check_cuda(cudaMemsetAsync(d_gring_count_.p, 0, sizeof(int), stream_), "guide"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_gwsum_.p, 0, 16, stream_), "guide"))) return r;  // sums, step counter
     if ((r = check_cuda(guide_pack(guide_view(), stream_), "guide pack"))) return r;
     guide_iters_ = 0;
     return check_cuda(cudaStreamSynchronize(stream_), "guide init");
@@ -211,6 +214,7 @@ int Session::ensure_guide() {
         if ((r = check_cuda(d_gwsum_.alloc(16), "guide"))) return r;
         if ((r = check_cuda(d_grec_count_.alloc(16), "guide"))) return r;
         if ((r = check_cuda(configure_guide_infer(), "guide inference configuration"))) return r;
+        if ((r = check_cuda(guide_configure(), "guide training configuration"))) return r;
         if ((r = check_cuda(d_gring_.alloc((size_t)(1 << 21) * sizeof(GuideSample)), "guide samples"))) return r;
         if ((r = check_cuda(d_gring_count_.alloc(16), "guide"))) return r;
         guide_alloc_ = true;
@@ -650,6 +654,13 @@ int Session::render_async(int spp) {
         p.gring = d_gring_.as<GuideSample>();
         p.gring_count = d_gring_count_.as<int>();
         p.gring_cap = 1 << 21;
+        // Adam steps this frame: automatic schedule (many while the network is young) unless set
+        p.gtrain_steps = guide_steps_per_frame_ > 0 ? guide_steps_per_frame_
+                         : guide_iters_ < 256      ? 8
+                         : guide_iters_ < 1024     ? 4
+                                                   : 2;
+        p.gtrain_batch = guide_batch_;
+        p.gtrain_lr = guide_lr_;
     }
     // per-frame constants: one pinned copy ahead of the frame's launches
     h_dyn_->cam = cam_;
@@ -690,7 +701,7 @@ int Session::render_async(int spp) {
             cudaGraph_t g = nullptr;
             if ((r = check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture")))
                 return r;
-            const cudaError_t ce = enqueue_frame(p, stream_, nullptr);
+            const cudaError_t ce = enqueue_frame_and_training(p, nullptr);
             const cudaError_t ee = cudaStreamEndCapture(stream_, &g);
             if ((r = check_cuda(ce != cudaSuccess ? ce : ee, "graph capture"))) {
                 if (g) cudaGraphDestroy(g);
@@ -704,21 +715,10 @@ int Session::render_async(int spp) {
             graph_captures_++;
         }
         if ((r = check_cuda(cudaGraphLaunch(graph_exec_, stream_), "graph launch"))) return r;
-    } else if ((r = check_cuda(enqueue_frame(p, stream_, mk), "frame launch"))) {
+    } else if ((r = check_cuda(enqueue_frame_and_training(p, mk), "frame launch"))) {
         return r;
     }
-    if (guiding_) {
-        // online training on the newest samples: one Adam step per frame, inside the frame's
-        // timed region
-        for (int k = 0; k < guide_steps_per_frame_; k++) {
-            guide_iters_++;
-            if ((r = check_cuda(guide_train_step(guide_view(), d_gring_.as<GuideSample>(), 1 << 21,
-                                                 d_gring_count_.as<int>(), guide_batch_, guide_lr_, guide_iters_,
-                                                 stream_),
-                                "guide training")))
-                return r;
-        }
-    }
+    if (guiding_) guide_iters_ += p.gtrain_steps;
     if ((r = check_cuda(cudaMemcpyAsync(h_stats_, d_stats_.p, sizeof(FrameStats), cudaMemcpyDeviceToHost, stream_),
                         "stats readback")))
         return r;
@@ -726,6 +726,18 @@ int Session::render_async(int spp) {
     in_flight_ = true;
     inflight_spp_ = spp;
     return PT_OK;
+}
+
+// The frame's launches, then (guiding) online training on the newest samples inside the
+// frame's timed region.
+cudaError_t Session::enqueue_frame_and_training(const FrameParams& p, StageMarks* marks) {
+    cudaError_t e = enqueue_frame(p, stream_, marks);
+    if (e != cudaSuccess || !p.guide_mode) return e;
+    for (int k = 0; k < p.gtrain_steps; k++) {
+        e = guide_train_step(guide_view(), p.gring, p.gring_cap, p.gring_count, p.gtrain_batch, p.gtrain_lr, stream_);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 int Session::finish_frame(float* ms) {

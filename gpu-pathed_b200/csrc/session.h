@@ -103,6 +103,7 @@ private:
     int ensure_frame_buffers(int spp);
     int check_cuda(cudaError_t e, const char* what);
     int finish_frame(float* ms);
+    cudaError_t enqueue_frame_and_training(const FrameParams& p, StageMarks* marks);
     SceneDevice scene_view() const;
 
     int w_, h_;
@@ -180,8 +181,8 @@ private:
         d_gring_count_;
     int guide_iters_ = 0;       // Adam steps taken
     int guide_warmup_ = 4;      // steps before the guide is used for sampling
-    int guide_batch_ = 1 << 18;
-    int guide_steps_per_frame_ = 1;
+    int guide_batch_ = 1 << 16;      // samples per Adam step
+    int guide_steps_per_frame_ = 0;  // 0: automatic schedule
     float guide_lr_ = 1e-3f;
     uint64_t guide_seed_ = 0x9e11deULL;
     GuideFrame gframe_{};
@@ -201,7 +202,8 @@ public:
     int guide_reset();
     int set_guide_options(int steps, int batch, float lr, int warmup) {
         if (batch > (1 << 21)) return fail(-1, "batch must be at most 2^21 samples");
-        if (steps > 0) guide_steps_per_frame_ = steps;
+        if (steps > 64) return fail(-1, "at most 64 Adam steps per frame");
+        if (steps >= 0) guide_steps_per_frame_ = steps;
         if (batch > 0) guide_batch_ = batch;
         if (lr > 0.f) guide_lr_ = lr;
         if (warmup >= 0) guide_warmup_ = warmup;

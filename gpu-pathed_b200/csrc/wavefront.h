@@ -125,6 +125,10 @@ struct FrameParams {
     GuideSample* gring;      // training-sample ring
     int* gring_count;
     int gring_cap;
+    // training launched after the frame (captured with it): Adam steps, minibatch, rate
+    int gtrain_steps;
+    int gtrain_batch;
+    float gtrain_lr;
 };
 
 // Enqueue one frame (all waves) on `stream`. Grid sizes do not depend on queue lengths,

@@ -343,7 +343,9 @@ class Session:
     def guide_reset(self):
         self._check(lib.pt_guide_reset(self._h))
 
-    def set_guide_options(self, steps_per_frame=0, batch=0, lr=0.0, warmup_steps=-1):
+    def set_guide_options(self, steps_per_frame=-1, batch=0, lr=0.0, warmup_steps=-1):
+        """steps_per_frame 0 selects the automatic schedule; -1 (and batch 0, lr 0, warmup
+        -1) keep the current setting."""
         self._check(lib.pt_set_guide_options(self._h, steps_per_frame, batch, lr, warmup_steps))
 
     def set_consistent_mis(self, on: bool):

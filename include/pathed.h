@@ -203,9 +203,10 @@ int pt_set_seed(pt_session* s, uint64_t seed);
 int pt_set_guiding(pt_session* s, int enabled);
 /* Re-initialise the guide network (seeded) and its optimiser state. */
 int pt_guide_reset(pt_session* s);
-/* Training schedule: Adam steps per frame (default 1), samples per step (default 2^18),
- * learning rate (default 1e-3), steps before the guide is used for sampling (default 4).
- * Zero or negative values keep the current setting. */
+/* Training schedule: Adam steps per frame (0, the default: automatic, 8 steps per frame for
+ * the first 256 steps, 4 up to 1024, then 2), samples per step (default 2^16), learning rate
+ * (default 1e-3), steps before the guide is used for sampling (default 4). Negative values
+ * (zero for batch and lr) keep the current setting. */
 int pt_set_guide_options(pt_session* s, int steps_per_frame, int batch, float lr, int warmup_steps);
 /* MIS weights of emitter samples use the BSDF's own sampling density (the reference's
  * Microfacet::pdf evaluates alpha at the incident direction instead, microfacet.h:124-134,
