@@ -15,6 +15,10 @@ contributing shadow rays); Mpaths/s is reported beside it.
   roofline  the extend (closest-hit) stage, timed live with events around its launches.
   cpu_baseline  the oracle's restatement of the reference integrator (two traces per bounce,
           linear primitive scan) on the host cores, on a bounded pixel sample.
+  guiding  time-to-relMSE on the slit room (1024x1024, depth 10): device time of the plain
+          render at a fixed sample budget, and of the guided render (network trained online
+          from scratch, training inside the timed frames) until its relMSE against a converged
+          plain render reaches the plain render's (rank 0, N = 1; --no-guiding skips it).
 
 --impl reference runs that CPU restatement as the reference arm (rank 0 only).
 """
@@ -348,6 +352,10 @@ def run_ours(args):
         cpu = {"value": mr, "unit": "Mrays/s", "cores": thr, "kind": "port", "sample": sample,
                "mpaths_per_s": mp, "algorithm": "reference integrator restated (two traces per bounce, linear scan)"}
 
+    guiding = None
+    if rank == 0 and world == 1 and not args.no_guiding:
+        guiding = guided_time_to_relmse()
+
     gpu_launches = sum(stage_launches.values())
     if rank == 0:
         line = {
@@ -363,6 +371,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": w * h * 3 * 4},
             "roofline": roof,
             "cpu_baseline": cpu,
+            "guiding": guiding,
             "clocks": clk,
             "gpu_launches": gpu_launches,
         }
@@ -371,6 +380,68 @@ def run_ours(args):
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def guided_time_to_relmse(budget_spp=128, ref_spp=2048, res=1024):
+    """Plain vs guided on the slit room: device ms for the plain render to reach `budget_spp`
+    and for the guided render (trained online from scratch) to reach the same relMSE,
+    relMSE = mean((I - I_ref)^2 / (I_ref^2 + 1e-2)) against a `ref_spp` plain render."""
+    import numpy as np
+
+    import pathed
+
+    def session():
+        s = pathed.Session(res, res)
+        s.load_config(3)
+        s.set_consistent_mis(True)
+        return s
+
+    r = session()
+    r.set_seed(12345)
+    for _ in range(ref_spp // 64):
+        r.render(64)
+    ref = r.readback().astype(np.float64)
+    r.close()
+    den = ref ** 2 + 1e-2
+
+    def relmse(s):
+        return float(np.mean((s.readback().astype(np.float64) - ref) ** 2 / den))
+
+    p = session()
+    p.set_seed(77)
+    p.render(1)
+    p.reset()
+    t_plain = sum(p.render(1) for _ in range(budget_spp))
+    target = relmse(p)
+    p.close()
+
+    g = session()
+    g.set_seed(77)
+    g.set_guiding(True)
+    t_guided, spp, prev, crossed = 0.0, 0, None, None
+    while t_guided < 3 * t_plain:
+        t_guided += g.render(1)
+        spp += 1
+        if spp >= 16 and spp % 4 == 0:
+            e = relmse(g)
+            if e <= target:
+                # interpolate the crossing in log relMSE between the last two checks
+                if prev is not None:
+                    (t0, e0) = prev
+                    f = (np.log(e0) - np.log(target)) / max(1e-12, np.log(e0) - np.log(e))
+                    crossed = t0 + f * (t_guided - t0)
+                else:
+                    crossed = t_guided
+                break
+            prev = (t_guided, e)
+    info = g.guide_info()
+    g.close()
+    return {"workload": f"slit-room {res}x{res} depth 10 (2002 + 1310720 triangles, env through a 0.05 slit)",
+            "reference": f"plain render, {ref_spp} spp, consistent MIS", "plain_spp": budget_spp,
+            "plain_ms": t_plain, "target_relmse": target, "guided_ms": crossed,
+            "guided_spp": spp if crossed is not None else None,
+            "speedup": (t_plain / crossed) if crossed else None, "guide_steps": info["steps"],
+            "training": "online from scratch inside the timed frames (automatic Adam schedule)"}
 
 
 def _ncu_bytes_per_query():
@@ -397,6 +468,7 @@ def main():
     ap.add_argument("--wave-paths", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-guiding", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -78,7 +78,23 @@ def build(verbose: bool = False, clean: bool = False, ptxas_info: bool = False) 
             relink = True
     if relink:
         _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs, "-lpthread"], verbose)
+    build_module(verbose, relink)
     return LIB
+
+
+def build_module(verbose: bool = False, force: bool = False) -> str:
+    """The pybind11 module `path_tracer` (the reference GUI's binding surface) over
+    libpathed.so, next to it in the package directory."""
+    import pybind11
+
+    src = os.path.join(CSRC, "path_tracer_module.cpp")
+    out = os.path.join(HERE, "path_tracer" + sysconfig.get_config_var("EXT_SUFFIX"))
+    deps = [src, LIB, os.path.join(HERE, "..", "include", "pathed.h")]
+    if force or _newer(deps, out):
+        _run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden", "-I", pybind11.get_include(),
+              "-I", sysconfig.get_paths()["include"], src, "-o", out, "-L", HERE, "-lpathed",
+              "-Wl,-rpath,$ORIGIN"], verbose)
+    return out
 
 
 if __name__ == "__main__":
