@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["wavefront.cu", "guide.cu"]
-CPP_SOURCES = ["host_scene.cpp", "bvh_build.cpp", "host_util.cpp", "session.cpp", "capi.cpp"]
+CPP_SOURCES = ["host_scene.cpp", "bvh_build.cpp", "host_util.cpp", "session.cpp", "session_batch.cpp", "capi.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] if os.path.isdir(CSRC) else []
 
 

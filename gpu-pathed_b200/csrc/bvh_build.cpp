@@ -407,4 +407,53 @@ bool check_bvh(const HostScene& s, const BvhBuild& b, std::string& err) {
     return false;
 }
 
+// Append `b` (a scene's own BVH over its own primitive ids) to `into`, the BVH of a batch
+// whose scenes share one node array, one leaf-entry array and one id space: internal child
+// indices move by the node count already present, leaf ranges by the leaf entries present,
+// triangle and sphere ids by the scene's first triangle and sphere. Returns the scene's root.
+template <int W>
+static int append_nodes(const BvhBuild& b, int node_base, int entry_base, BvhBuild& into) {
+    const size_t nbytes = sizeof(BvhNode<W>);
+    const size_t old = into.nodes.size();
+    into.nodes.resize(old + (size_t)b.num_nodes * nbytes);
+    for (int i = 0; i < b.num_nodes; i++) {
+        BvhNode<W> nd;
+        std::memcpy(&nd, b.nodes.data() + (size_t)i * nbytes, nbytes);
+        for (int k = 0; k < W; k++) {
+            const int c = nd.child[k];
+            if (c == kEmptyChild) continue;
+            if (child_is_leaf(c)) nd.child[k] = leaf_code(leaf_first(c) + entry_base, leaf_count(c));
+            else nd.child[k] = c + node_base;
+        }
+        std::memcpy(into.nodes.data() + old + (size_t)i * nbytes, &nd, nbytes);
+    }
+    return b.root + node_base;
+}
+
+int append_bvh(const BvhBuild& b, int tri_base, int sph_base, BvhBuild& into) {
+    const int node_base = into.num_nodes;
+    const int entry_base = (int)(into.prims.size() / 12);
+    if (node_base == 0 && into.prims.empty()) into.width = b.width;
+    int root = 0;
+    if (b.width == 2) root = append_nodes<2>(b, node_base, entry_base, into);
+    else if (b.width == 4) root = append_nodes<4>(b, node_base, entry_base, into);
+    else root = append_nodes<8>(b, node_base, entry_base, into);
+    const size_t old = into.prims.size();
+    into.prims.insert(into.prims.end(), b.prims.begin(), b.prims.end());
+    for (size_t e = 0; e < b.prims.size() / 12; e++) {
+        float* r = &into.prims[old + e * 12];
+        int id;
+        std::memcpy(&id, &r[3], 4);
+        id = id >= 0 ? id + tri_base : ~(~id + sph_base);
+        std::memcpy(&r[3], &id, 4);
+        const int po = b.prim_order[e];
+        into.prim_order.push_back(po >= 0 ? po + tri_base : ~(~po + sph_base));
+    }
+    into.num_nodes += b.num_nodes;
+    into.depth = std::max(into.depth, b.depth);
+    into.max_leaf = std::max(into.max_leaf, b.max_leaf);
+    into.build_ms += b.build_ms;
+    return root;
+}
+
 }  // namespace pt

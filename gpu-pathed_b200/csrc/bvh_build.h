@@ -36,4 +36,8 @@ bool build_bvh(const HostScene& s, int width, int max_leaf, BvhBuild& out, std::
 // primitive contained in the padded boxes of all its ancestors, child codes in range.
 bool check_bvh(const HostScene& s, const BvhBuild& b, std::string& err);
 
+// Append a scene's BVH to the shared BVH of a batch (node, leaf-entry and primitive-id
+// offsets applied; the scene's primitives start at tri_base / sph_base). Returns its root.
+int append_bvh(const BvhBuild& b, int tri_base, int sph_base, BvhBuild& into);
+
 }  // namespace pt

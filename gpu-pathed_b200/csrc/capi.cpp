@@ -295,4 +295,55 @@ int pt_occluded(pt_session* s, const float* o, const float* d, const float* tmin
     return guarded(s, [&] { return s->impl.occluded(o, d, tmin, tmax, n, occluded); });
 }
 
+int pt_batch_generate(unsigned long long seed, int n, pt_batch_scene* out) {
+    if (n < 1 || n > pt::kMaxBatchScenes || !out) return PT_ERR_ARG;
+    try {
+        const std::vector<pt::BatchSpec> specs = pt::generate_batch_specs(seed, n);
+        for (int i = 0; i < n; i++) {
+            pt_batch_scene& o = out[i];
+            std::memset(&o, 0, sizeof(o));
+            o.config = specs[i].config;
+            o.level = specs[i].level;
+            o.seed = specs[i].seed;
+            o.width = specs[i].width;
+            o.height = specs[i].height;
+            o.spp = specs[i].spp;
+            o.max_depth = specs[i].max_depth;
+            o.guided = specs[i].guided;
+        }
+    } catch (const std::exception&) {
+        return PT_ERR_ARG;
+    }
+    return PT_OK;
+}
+
+int pt_load_batch(pt_session* s, const pt_batch_scene* scenes, int n) {
+    if (!s) return PT_ERR_ARG;
+    if (!scenes || n < 1) return s->impl.fail(PT_ERR_ARG, "empty batch");
+    return guarded(s, [&] {
+        std::vector<pt::BatchSpec> specs(n);
+        for (int i = 0; i < n; i++) {
+            specs[i].config = scenes[i].config;
+            specs[i].level = scenes[i].level;
+            specs[i].seed = scenes[i].seed;
+            specs[i].width = scenes[i].width;
+            specs[i].height = scenes[i].height;
+            specs[i].spp = scenes[i].spp;
+            specs[i].max_depth = scenes[i].max_depth;
+            specs[i].guided = scenes[i].guided;
+        }
+        return s->impl.load_batch(specs);
+    });
+}
+
+int pt_batch_get_info(const pt_session* s, int scene, pt_batch_info* out) {
+    if (!s || !out) return PT_ERR_ARG;
+    return s->impl.batch_info(scene, out);
+}
+
+int pt_batch_readback(pt_session* s, int scene, float* rgb, size_t n, int pass_only) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.batch_readback(scene, rgb, n, pass_only != 0); });
+}
+
 }  // extern "C"

@@ -426,8 +426,21 @@ bool generate_config(int config, uint64_t seed, HostScene& out, std::string& err
     out = HostScene();
     const uint64_t s = seed + (uint64_t)config;
     switch (config) {
-        case 0: gen_cornell(s, out); break;
-        case 1: gen_spheres(s, out); break;
+        case 0:
+            gen_cornell(s, out);
+            // batched workloads: a displaced icosphere (Beckmann 0.3) floating in the box
+            if (level >= 0) {
+                out.mats.push_back(microfacet(0.3f));
+                push_displaced_icosphere(out, level, 0.3, 0.05, s, {0.05, 1.15, 0.35}, (int)out.mats.size() - 1);
+            }
+            break;
+        case 1:
+            gen_spheres(s, out);
+            if (level >= 0) {  // batched workloads: a displaced icosphere among the spheres
+                out.mats.push_back(microfacet(0.3f));
+                push_displaced_icosphere(out, level, 1.2, 0.05, s, {0.0, 2.5, 0.0}, (int)out.mats.size() - 1);
+            }
+            break;
         case 2: gen_env_mesh(s, out, level < 0 ? 8 : level); break;
         case 3: gen_slit_room(s, out, level < 0 ? 8 : level); break;
         default:
@@ -436,6 +449,30 @@ bool generate_config(int config, uint64_t seed, HostScene& out, std::string& err
     }
     finalize_materials(out);
     return true;
+}
+
+std::vector<BatchSpec> generate_batch_specs(uint64_t seed, int n) {
+    // Configuration 4: scenes drawn from configurations 0-3 with log-uniform triangle counts
+    // (1k-2M, realised as the nearest icosphere level 3-8: 1,280 to 1,310,720 mesh triangles),
+    // square resolutions 256-1024 in steps of 64, spp 4-64 (powers of two), depth 4-10, and a
+    // guide network for about half of them.
+    HostRng rng(seed ^ 0xB47C4ULL);
+    std::vector<BatchSpec> out;
+    for (int i = 0; i < n; i++) {
+        BatchSpec b;
+        b.config = (int)(rng.uniform() * 4.0) & 3;
+        b.seed = seed + 1000003ULL * (uint64_t)(i + 1);
+        const double tris = std::exp(rng.uniform(std::log(1e3), std::log(2e6)));
+        int level = (int)std::lround(std::log(tris / 20.0) / std::log(4.0));
+        b.level = std::max(3, std::min(8, level));
+        const int res = 256 + 64 * (int)(rng.uniform() * 13.0);
+        b.width = b.height = std::min(1024, res);
+        b.spp = 4 << (int)(rng.uniform() * 5.0);
+        b.max_depth = 4 + (int)(rng.uniform() * 7.0);
+        b.guided = rng.uniform() < 0.5 ? 1 : 0;
+        out.push_back(b);
+    }
+    return out;
 }
 
 bool validate_scene(const HostScene& s, std::string& err) {

@@ -58,10 +58,23 @@ void finalize_materials(HostScene& s);
 //      lognormal + 3-sun environment, 1920x1080, 32 spp, depth 6.
 //   3: closed room (~2k triangles) with a 0.05-wide ceiling slit around the config-2 mesh,
 //      lit by the config-2 environment through the slit, 1024x1024, depth 10.
-// Returns false (and leaves `err`) for an unknown id. `scale` < 1 shrinks the triangle
-// count of configs 2 and 3 (icosphere level) for quick tests; 1.0 is the full size.
+// Returns false (and leaves `err`) for an unknown id. `icosphere_level` >= 0 sets the mesh
+// level of configs 2 and 3 and adds a displaced icosphere of that level to configs 0 and 1
+// (batched workloads); -1 keeps each configuration as described.
 bool generate_config(int config, uint64_t seed, HostScene& out, std::string& err,
                      int icosphere_level = -1);
+
+// One scene of a batched frame (configuration 4).
+struct BatchSpec {
+    int config = 0;          // generated configuration 0-3
+    uint64_t seed = 0;
+    int level = -1;          // icosphere level (configs 0-1: an added mesh; -1: none/default)
+    int width = 256, height = 256, spp = 4, max_depth = 4;
+    int guided = 0;          // own guide network
+};
+
+// Configuration 4's draw of n scenes from configurations 0-3 (seeded).
+std::vector<BatchSpec> generate_batch_specs(uint64_t seed, int n);
 
 // Environment map of configuration 2 (lognormal background + 3 Gaussian suns).
 void generate_sun_env(uint64_t seed, int w, int h, std::vector<float>& rgba);

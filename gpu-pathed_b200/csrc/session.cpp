@@ -32,6 +32,7 @@ Session::~Session() {
         for (cudaEvent_t e : mark_events_) cudaEventDestroy(e);
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         if (h_dyn_) cudaFreeHost(h_dyn_);
+        if (h_batch_) cudaFreeHost(h_batch_);
         if (stream_) cudaStreamDestroy(stream_);
         if (h_stats_) cudaFreeHost(h_stats_);
     }
@@ -123,25 +124,32 @@ int Session::load_scene(HostScene&& s) {
     scene_dirty_ = true;
     mats_dirty_ = true;
     update_material_classes();
+    gframe_ = guide_frame_of(scene_);
+    clear_batch();
+    reset();
+    return PT_OK;
+}
+
+GuideFrame guide_frame_of(const HostScene& s) {
     // scene bounds for the guide's position encoding
+    GuideFrame g{};
     float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
-    for (size_t i = 0; i < scene_.tri_p.size(); i += 3)
+    for (size_t i = 0; i < s.tri_p.size(); i += 3)
         for (int k = 0; k < 3; k++) {
-            lo[k] = std::min(lo[k], scene_.tri_p[i + k]);
-            hi[k] = std::max(hi[k], scene_.tri_p[i + k]);
+            lo[k] = std::min(lo[k], s.tri_p[i + k]);
+            hi[k] = std::max(hi[k], s.tri_p[i + k]);
         }
-    for (int s = 0; s < scene_.num_sph(); s++)
+    for (int j = 0; j < s.num_sph(); j++)
         for (int k = 0; k < 3; k++) {
-            lo[k] = std::min(lo[k], scene_.sph[4 * s + k] - scene_.sph[4 * s + 3]);
-            hi[k] = std::max(hi[k], scene_.sph[4 * s + k] + scene_.sph[4 * s + 3]);
+            lo[k] = std::min(lo[k], s.sph[4 * j + k] - s.sph[4 * j + 3]);
+            hi[k] = std::max(hi[k], s.sph[4 * j + k] + s.sph[4 * j + 3]);
         }
     for (int k = 0; k < 3; k++) {
         const float ext = std::max(hi[k] - lo[k], 1e-6f);
-        gframe_.lo[k] = lo[k];
-        gframe_.inv_ext[k] = 2.f / ext;
+        g.lo[k] = lo[k];
+        g.inv_ext[k] = 2.f / ext;
     }
-    reset();
-    return PT_OK;
+    return g;
 }
 
 GuideDevice Session::guide_view() const {
@@ -319,6 +327,10 @@ int Session::set_bvh(int width, int max_leaf) {
     bvh_width_ = width;
     bvh_leaf_ = max_leaf;
     if (!have_scene_) return PT_OK;
+    if (batch_mode()) {  // rebuild every scene of the batch with the new shape
+        const std::vector<BatchSpec> specs = batch_specs_;
+        return load_batch(specs);
+    }
     BvhBuild b;
     std::string err;
     if (!build_bvh(scene_, bvh_width_, bvh_leaf_, b, err)) return fail(PT_ERR_SCENE, err);
@@ -356,7 +368,7 @@ int Session::counts(pt_scene_counts* out) const {
 }
 
 int Session::export_scene(pt_scene_export* o) const {
-    if (!have_scene_) return PT_ERR_STATE;
+    if (!have_scene_ || batch_mode()) return PT_ERR_STATE;
     const HostScene& s = scene_;
     if (o->tri_vertices) std::memcpy(o->tri_vertices, s.tri_p.data(), s.tri_p.size() * 4);
     if (o->tri_normals) std::memcpy(o->tri_normals, s.tri_n.data(), s.tri_n.size() * 4);
@@ -391,6 +403,7 @@ int Session::export_scene(pt_scene_export* o) const {
 }
 
 int Session::set_camera(const CameraSpec& c) {
+    if (batch_mode()) return fail(PT_ERR_STATE, "not available for a batch (one query per scene session)");
     CameraParams tmp;
     std::string err;
     if (!make_camera(c, w_, h_, tmp, err)) return fail(PT_ERR_ARG, err);
@@ -401,6 +414,7 @@ int Session::set_camera(const CameraSpec& c) {
 
 int Session::set_material(int id, int type, const float* albedo, const float* emit, float ior, float alpha) {
     if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (batch_mode()) return fail(PT_ERR_STATE, "not available for a batch (one query per scene session)");
     if (id < 0 || id >= (int)scene_.mats.size()) return fail(PT_ERR_ARG, "material id out of range");
     if (type < kLambertian || type > kMicrofacet) return fail(PT_ERR_ARG, "unknown material type");
     Material& m = scene_.mats[id];
@@ -474,13 +488,6 @@ void Session::get_launch(pt_launch_config* c) const {
     c->use_graph = use_graph_ ? 1 : 2;
 }
 
-template <class T>
-static cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
-    cudaError_t e = b.alloc(v.size() * sizeof(T));
-    if (e != cudaSuccess || v.empty()) return e;
-    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
-}
-
 int Session::upload_materials() {
     int r;
     if ((r = check_cuda(upload(d_mats_, scene_.mats, stream_), "upload materials"))) return r;
@@ -515,6 +522,7 @@ int Session::upload_scene() {
     }
     // host vectors above must outlive the async copies
     if ((r = check_cuda(cudaStreamSynchronize(stream_), "scene upload"))) return r;
+    if (batch_mode() && (r = upload_batch())) return r;
     scene_dirty_ = false;
     return upload_materials();
 }
@@ -551,12 +559,35 @@ SceneDevice Session::scene_view() const {
 
 int Session::ensure_frame_buffers(int spp) {
     int r;
-    const size_t np = (size_t)w_ * h_;
+    const size_t np = batch_mode() ? (size_t)batch_pixels_ : (size_t)w_ * h_;
     if ((r = check_cuda(d_pass_.alloc(np * 3 * 4), "frame buffer"))) return r;
     if ((r = check_cuda(d_accum_.alloc(np * 3 * 4), "frame buffer"))) return r;
     if ((r = check_cuda(d_rgba8_.alloc(np * 4), "frame buffer"))) return r;
     const int wave_pixels = std::max(1, std::min((int)np, wave_paths_ / spp));
-    const size_t cap = (size_t)wave_pixels * spp;
+    size_t cap = (size_t)wave_pixels * spp;
+    if (batch_mode()) {  // waves of whole pixels of the batch's global pixel order
+        cap = (size_t)std::min<long long>(wave_paths_, batch_paths_);
+        batch_waves_.clear();
+        long long px = 0;
+        for (const BatchHost& b : batch_) {
+            const long long npx = (long long)b.spec.width * b.spec.height;
+            for (long long q = 0; q < npx;) {
+                if (batch_waves_.empty() || (long long)batch_waves_.back().npaths + b.spec.spp > (long long)cap) {
+                    WaveRange w{};
+                    w.first_pixel = (int)(b.pixel_base + q);
+                    w.first_path = b.path_base + q * b.spec.spp;
+                    batch_waves_.push_back(w);
+                }
+                WaveRange& w = batch_waves_.back();
+                const long long room = ((long long)cap - w.npaths) / b.spec.spp;
+                const long long take = std::min(room, npx - q);
+                w.npix += (int)take;
+                w.npaths += (int)(take * b.spec.spp);
+                q += take;
+            }
+            px += npx;
+        }
+    }
     const size_t f4 = cap * sizeof(float4);
     for (int k = 0; k < 2; k++) {
         for (int a = 0; a < 6; a++) {
@@ -575,6 +606,8 @@ int Session::ensure_frame_buffers(int spp) {
 int Session::render_async(int spp) {
     if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
     if (in_flight_) return fail(PT_ERR_STATE, "a frame is already in flight");
+    const bool batch = batch_mode();
+    if (batch) spp = 1;  // each scene of a batch renders its own spp
     if (spp < 1) return fail(PT_ERR_ARG, "spp must be >= 1");
     int r;
     if ((r = ensure_device())) return r;
@@ -582,7 +615,7 @@ int Session::render_async(int spp) {
     if (mats_dirty_ && (r = upload_materials())) return r;
     if ((r = ensure_frame_buffers(spp))) return r;
     std::string err;
-    if (!make_camera(camspec_, w_, h_, cam_, err)) return fail(PT_ERR_ARG, err);
+    if (!batch && !make_camera(camspec_, w_, h_, cam_, err)) return fail(PT_ERR_ARG, err);
     const int stack_depth = bvh_.depth + 1;
     const int maxb = std::max(shape_.block_extend, shape_.block_shadow);
     const size_t smem = stack_bytes(stack_depth, maxb);
@@ -593,6 +626,7 @@ int Session::render_async(int spp) {
     }
     if (reset_pending_) {  // PathTracer::renderAsync resets m_currentSamples (path_tracer.cu:306-309)
         total_spp_ = 0;
+        for (BatchHost& b : batch_) b.total_spp = 0;
         reset_pending_ = false;
     }
     FrameParams p;
@@ -620,9 +654,16 @@ int Session::render_async(int spp) {
     p.width = w_;
     p.height = h_;
     p.spp = spp;
-    p.max_depth = max_depth_;
+    p.max_depth = batch ? batch_max_depth_ : max_depth_;
     p.nee = nee_;
     p.wave_pixels = queue_cap_ / spp;
+    if (batch) {
+        p.width = p.height = 0;
+        p.batch = d_batch_.as<BatchScene>();
+        p.batch_path_base = d_batch_path_base_.as<long long>();
+        p.batch_pixel_base = d_batch_pixel_base_.as<long long>();
+        p.num_scenes = (int)batch_.size();
+    }
     p.stack_depth = stack_depth;
     p.num_sms = num_sms_;
     p.count_work = work_counters_;
@@ -640,7 +681,7 @@ int Session::render_async(int spp) {
         if ((r = check_cuda(d_gacc_.alloc(tpaths * kMaxDepthLimit * 3 * sizeof(float)), "guide accumulators")))
             return r;
         // one record per scattering vertex of a training path
-        const size_t rec_cap = tpaths * (size_t)std::max(1, max_depth_ - 1);
+        const size_t rec_cap = tpaths * (size_t)std::max(1, p.max_depth - 1);
         if ((r = check_cuda(d_grec_.alloc(rec_cap * sizeof(GuideRecord)), "guide records"))) return r;
         p.guide_mode = guide_iters_ >= guide_warmup_ ? 2 : 1;
         p.gwpack = d_gwpack_.as<uint32_t>();
@@ -667,11 +708,18 @@ int Session::render_async(int spp) {
     h_dyn_->seed = seed_;
     h_dyn_->sample_base = (uint64_t)total_spp_;
     h_dyn_->prev_spp = total_spp_;
+    if (batch) {
+        for (size_t i = 0; i < batch_.size(); i++) {
+            h_batch_[i].seed = seed_;
+            h_batch_[i].sample_base = (uint64_t)batch_[i].total_spp;
+            h_batch_[i].prev_spp = batch_[i].total_spp;
+        }
+    }
     StageMarks* mk = nullptr;
     marks_active_ = false;
     if (stage_timing_) {
-        const int waves = (w_ * h_ + p.wave_pixels - 1) / p.wave_pixels;
-        const size_t need = (size_t)waves * (max_depth_ * 5 + 4) + 8;
+        const int waves = batch ? (int)batch_waves_.size() : (w_ * h_ + p.wave_pixels - 1) / p.wave_pixels;
+        const size_t need = (size_t)waves * (p.max_depth * 5 + 4) + 8;
         while (mark_events_.size() < need) {
             cudaEvent_t e;
             if ((r = check_cuda(cudaEventCreate(&e), "cudaEventCreate"))) return r;
@@ -689,6 +737,10 @@ int Session::render_async(int spp) {
     if ((r = check_cuda(cudaEventRecord(ev_begin_, stream_), "cudaEventRecord"))) return r;
     if ((r = check_cuda(cudaMemcpyAsync(d_dyn_.p, h_dyn_, sizeof(FrameDyn), cudaMemcpyHostToDevice, stream_),
                         "frame constants")))
+        return r;
+    if (batch && (r = check_cuda(cudaMemcpyAsync(d_batch_.p, h_batch_, batch_.size() * sizeof(BatchScene),
+                                                 cudaMemcpyHostToDevice, stream_),
+                                 "batch scene table")))
         return r;
     if (use_graph_ && !mk) {
         // replay the captured frame while every launch parameter is unchanged
@@ -731,7 +783,9 @@ int Session::render_async(int spp) {
 // The frame's launches, then (guiding) online training on the newest samples inside the
 // frame's timed region.
 cudaError_t Session::enqueue_frame_and_training(const FrameParams& p, StageMarks* marks) {
-    cudaError_t e = enqueue_frame(p, stream_, marks);
+    cudaError_t e = p.num_scenes > 0
+                        ? enqueue_batch_frame(p, batch_waves_.data(), (int)batch_waves_.size(), stream_, marks)
+                        : enqueue_frame(p, stream_, marks);
     if (e != cudaSuccess || !p.guide_mode) return e;
     for (int k = 0; k < p.gtrain_steps; k++) {
         e = guide_train_step(guide_view(), p.gring, p.gring_cap, p.gring_count, p.gtrain_batch, p.gtrain_lr, stream_);
@@ -748,6 +802,7 @@ int Session::finish_frame(float* ms) {
     last_ms_ = t;
     last_spp_ = inflight_spp_;
     total_spp_ += inflight_spp_;  // PathTracer::pollRender (path_tracer.cu:354)
+    for (BatchHost& b : batch_) b.total_spp += b.spec.spp;
     frames_++;
     last_stats_ = *h_stats_;
     if (ms) *ms = t;
@@ -1011,6 +1066,7 @@ int Session::readback_rgba8(uint8_t* out, size_t n) {
 
 int Session::hit_test(int x, int y, int* mat) {
     if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (batch_mode()) return fail(PT_ERR_STATE, "not available for a batch (one query per scene session)");
     if (x < 0 || y < 0 || x >= w_ || y >= h_) {
         // the reference's kernel matches no thread and reports no hit
         *mat = -1;
@@ -1039,6 +1095,7 @@ int Session::hit_test(int x, int y, int* mat) {
 int Session::trace_rays(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pty,
                         int* pid, int* mid, float* t, float* bary, bool device_ptrs) {
     if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (batch_mode()) return fail(PT_ERR_STATE, "not available for a batch (one query per scene session)");
     if (n < 0) return fail(PT_ERR_ARG, "negative ray count");
     if (n == 0) return PT_OK;
     if (!o || !d || !tmin || !tmax || !pty || !pid || !mid || !t) return fail(PT_ERR_ARG, "null array");
@@ -1102,6 +1159,7 @@ int Session::trace_rays(const float* o, const float* d, const float* tmin, const
 
 int Session::trace_rays_static(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pty,
                                int* pid, int* mid, float* t, float* bary) {
+    if (batch_mode()) return fail(PT_ERR_STATE, "not available for a batch (one query per scene session)");
     if (n < 0 || n > kStaticTraceMaxRays)
         return fail(PT_ERR_ARG, "ray count must be in [0, " + std::to_string(kStaticTraceMaxRays) + "]");
     if (n > 0 && (!o || !d || !tmin || !tmax || !pty || !pid || !mid || !t)) return fail(PT_ERR_ARG, "null array");
@@ -1127,6 +1185,7 @@ int Session::trace_rays_static(const float* o, const float* d, const float* tmin
 
 int Session::occluded(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* occ) {
     if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
+    if (batch_mode()) return fail(PT_ERR_STATE, "not available for a batch (one query per scene session)");
     if (n < 0) return fail(PT_ERR_ARG, "negative ray count");
     if (n == 0) return PT_OK;
     if (!o || !d || !tmin || !tmax || !occ) return fail(PT_ERR_ARG, "null array");

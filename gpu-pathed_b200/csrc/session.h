@@ -16,6 +16,10 @@
 
 namespace pt {
 
+struct DevBuf;
+template <class T>
+cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st);
+
 // Owning device allocation.
 struct DevBuf {
     void* p = nullptr;
@@ -41,6 +45,31 @@ struct DevBuf {
     template <class T>
     T* as() const { return static_cast<T*>(p); }
 };
+
+// Guide position-encoding frame from a scene's bounds.
+GuideFrame guide_frame_of(const HostScene& s);
+
+// Host state of one scene of a batch (configuration 4).
+struct BatchHost {
+    BatchSpec spec;
+    CameraSpec camspec;
+    int root = 0, light_first = 0, num_lights = 0;
+    int num_tri = 0, num_sph = 0;
+    long long path_base = 0, pixel_base = 0;
+    int env_w = 0, env_h = 0;
+    std::vector<float> env_rgba;
+    EnvCdf env_cdf;
+    GuideFrame gframe{};
+    int total_spp = 0;
+};
+
+// Allocate (grow) `b` and copy `v` into it on stream `st`.
+template <class T>
+cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    cudaError_t e = b.alloc(v.size() * sizeof(T));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
 
 class Session {
 public:
@@ -187,6 +216,18 @@ private:
     uint64_t guide_seed_ = 0x9e11deULL;
     GuideFrame gframe_{};
     int ensure_guide();
+    // batch mode
+    std::vector<BatchHost> batch_;
+    std::vector<BatchSpec> batch_specs_;
+    std::vector<WaveRange> batch_waves_;
+    std::vector<std::unique_ptr<DevBuf[]>> d_batch_env_;  // per scene: rgba, marg, cond, row
+    DevBuf d_batch_, d_batch_path_base_, d_batch_pixel_base_;
+    BatchScene* h_batch_ = nullptr;  // pinned
+    int batch_max_depth_ = 0;
+    long long batch_pixels_ = 0, batch_paths_ = 0;
+    void clear_batch();
+    int upload_batch();
+    int render_async_batch();
     int guide_init_weights();
     GuideDevice guide_view() const;
 
@@ -210,6 +251,13 @@ public:
         return 0;
     }
     int guide_info(::pt_guide_info* out) const;
+
+    // ---- batched frames (configuration 4): every scene rendered by one launch per stage ----
+    int load_batch(const std::vector<BatchSpec>& specs);
+    int batch_readback(int scene, float* rgb, size_t n, bool pass);
+    int batch_info(int scene, ::pt_batch_info* out) const;
+    bool batch_mode() const { return !batch_.empty(); }
+    int num_batch_scenes() const { return (int)batch_.size(); }
     int guide_params(float* out, int n, bool set);
     int guide_forward(const float* x, int n, float* raw);
     int guide_gradients(const float* x, const float* wi, const float* w, int n, float* grad);

@@ -25,6 +25,8 @@
 #include "dev_trace.cuh"
 #include "guide_mlp.cuh"
 
+#include <vector>
+
 namespace pt {
 
 namespace {
@@ -55,29 +57,75 @@ __device__ __forceinline__ int warp_fetch(int* cursor) {
     return __shfl_sync(0xffffffffu, base, 0);
 }
 
+__device__ __forceinline__ int tag_path(int tag) { return tag & kTagPathMask; }
+__device__ __forceinline__ int tag_scene(int tag) { return tag >> kTagPathBits; }
+
+// Index s with base[s] <= v < base[s + 1] (binary search over a batch's prefix offsets).
+__device__ __forceinline__ int batch_find(const long long* base, int n, long long v) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(base + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The scene a path belongs to: in batched frames its root, emitter range and environment come
+// from the scene table (the geometry arrays are shared, with global primitive ids).
+__device__ __forceinline__ SceneDevice batch_scene_view(const FrameParams& p, int sid) {
+    SceneDevice sc = p.sc;
+    const BatchScene& b = p.batch[sid];
+    sc.root = b.root;
+    sc.lights = p.sc.lights + b.light_first;
+    sc.num_lights = b.num_lights;
+    sc.env = b.env;
+    return sc;
+}
+
+template <bool B>
 __global__ void k_camera(FrameParams p, long long wave_first, int n) {
     const PathQueue q = p.q[0];
     __shared__ CameraParams cam;
     __shared__ uint64_t seed, sample_base;
-    if (threadIdx.x == 0) {
-        cam = p.dyn->cam;
-        seed = p.dyn->seed;
-        sample_base = p.dyn->sample_base;
+    if (!B) {
+        if (threadIdx.x == 0) {
+            cam = p.dyn->cam;
+            seed = p.dyn->seed;
+            sample_base = p.dyn->sample_base;
+        }
+        __syncthreads();
     }
-    __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const long long gp = wave_first + i;
-        const int pixel = (int)(gp / p.spp);
-        const int s = (int)(gp - (long long)pixel * p.spp);
-        const int row = pixel / p.width;
-        const int col = pixel - row * p.width;
+        long long local = gp;
+        int sid = 0, spp = p.spp, width = p.width;
+        const CameraParams* cp = &cam;
+        uint64_t sd = 0, sb = 0;
+        if (B) {
+            sid = batch_find(p.batch_path_base, p.num_scenes, gp);
+            const BatchScene& b = p.batch[sid];
+            local = gp - b.path_base;
+            spp = b.spp;
+            width = b.width;
+            cp = &b.cam;
+            sd = b.seed;
+            sb = b.sample_base;
+        } else {
+            sd = seed;
+            sb = sample_base;
+        }
+        const int pixel = (int)(local / spp);
+        const int s = (int)(local - (long long)pixel * spp);
+        const int row = pixel / width;
+        const int col = pixel - row * width;
         const uint64_t inc = pcg_inc((uint32_t)pixel);
-        uint64_t st = pcg_seed(seed, sample_base + (uint64_t)s, (uint32_t)pixel);
+        uint64_t st = pcg_seed(sd, sb + (uint64_t)s, (uint32_t)pixel);
         const float xi1 = pcg_uniform(st, inc);
         const float xi2 = pcg_uniform(st, inc);
         V o, d;
-        camera_ray(cam, row, col, xi1, xi2, o, d);
-        q.o[i] = make_float4(o.x, o.y, o.z, __int_as_float(i));
+        camera_ray(*cp, row, col, xi1, xi2, o, d);
+        q.o[i] = make_float4(o.x, o.y, o.z, __int_as_float(i | (sid << kTagPathBits)));
         q.d[i] = make_float4(d.x, d.y, d.z, 0.f);
         q.beta[i] = make_float4(1.f, 1.f, 1.f, __int_as_float(1));  // camera ray: no MIS
         q.rng[i] = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
@@ -109,7 +157,7 @@ __device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long lon
     }
 }
 
-template <int W, bool CNT>
+template <int W, bool CNT, bool B>
 __global__ void k_extend(FrameParams p, int depth) {
     extern __shared__ int2 stk[];
     const int count = p.counters->ray_count[depth];
@@ -129,7 +177,10 @@ __global__ void k_extend(FrameParams p, int depth) {
         const RayPre r = make_raypre(mkv(o), mkv(d));
         Hit h;
         int of = 0;
-        traverse<W, false, CNT>(p.sc, r, tmin, FLT_MAX, valid, stk + threadIdx.x, blockDim.x, p.stack_depth, h, of,
+        SceneDevice scb;
+        if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(o.w)));
+        const SceneDevice& sc = B ? scb : p.sc;
+        traverse<W, false, CNT>(sc, r, tmin, FLT_MAX, valid, stk + threadIdx.x, blockDim.x, p.stack_depth, h, of,
                                 &work);
         if (valid) {
             if (of) atomicOr(&p.stats->error, 1);
@@ -229,16 +280,15 @@ __device__ __forceinline__ void guide_account(const FrameParams& p, int path, in
 }
 
 // GUIDE: compiled with the path-guiding code (used when guide_mode != 0); the plain
-// instantiation keeps the reference integrator's register budget.
-template <bool GUIDE>
+// instantiation keeps the reference integrator's register budget. B: batched frame (the
+// scene, its depth, spp and guide come from the path's tag and the scene table).
+template <bool GUIDE, bool B>
 __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
     const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
     const PathQueue qn = p.q[(depth + 1) & 1];
-    const bool last = depth >= p.max_depth - 1;
-    const int n_choice = p.sc.num_lights + (p.sc.env.present ? 1 : 0);
-    const bool do_nee = p.nee && n_choice > 0;
-    const bool guided = GUIDE && p.guide_mode == 2;
+    const bool last_frame = depth >= p.max_depth - 1;
+    const bool guided_frame = GUIDE && p.guide_mode == 2;
     for (;;) {
         const int base = warp_fetch(&p.counters->work_shade[depth]);
         if (base >= count) break;
@@ -253,7 +303,15 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
             const float4 d4 = q.d[slot];
             const float4 b4 = q.beta[slot];
             const float4 h4 = q.hit[slot];
-            const int path = __float_as_int(o4.w);
+            const int tag = __float_as_int(o4.w);
+            const int path = tag_path(tag);
+            const int sid = B ? tag_scene(tag) : 0;
+            SceneDevice scb;
+            if (B) scb = batch_scene_view(p, sid);
+            const SceneDevice& sc = B ? scb : p.sc;
+            const bool last = B ? depth >= p.batch[sid].max_depth - 1 : last_frame;
+            const bool guided = B ? GUIDE && p.batch[sid].guide_mode == 2 : guided_frame;
+            const bool do_nee = p.nee && sc.num_lights + (sc.env.present ? 1 : 0) > 0;
             const int flags = __float_as_int(b4.w);
             const V o = mkv(o4), dir = mkv(d4), beta = mkv(b4);
             const int prim = __float_as_int(h4.w);
@@ -261,31 +319,32 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
             V Ladd = mkv(0.f);
             if (prim == kMissPrim) {
                 // escaped: environment radiance (path_tracer.cu:68-79, :162, :206, :228)
-                const V Le = env_emit(p.sc.env, dir);
+                const V Le = env_emit(sc.env, dir);
                 if (!is_zero(Le)) {
-                    const float w = nomis ? 1.f : balance(d4.w, pdf_env_light(p.sc, dir));
+                    const float w = nomis ? 1.f : balance(d4.w, pdf_env_light(sc, dir));
                     Ladd = beta * Le * w;
                     if (GUIDE) guide_account(p, path, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
                 }
             } else {
                 V point, n;
                 int mat;
-                hit_info(p.sc, o, dir, h4, point, n, mat);
+                hit_info(sc, o, dir, h4, point, n, mat);
                 // guided modes shade in an orthonormal frame (the reference's frame is built
                 // from the unnormalised interpolated normal)
                 if (GUIDE && p.guide_mode) n = normalized(n);
                 const Frame fr = make_frame(n);
                 const V wo = normalized(to_local(fr, -dir));
-                const Material m = p.sc.mats[mat];
+                const Material m = sc.mats[mat];
                 if (m.emitting && wo.z >= 0.f) {  // front-face emission (lambertian.cu:5-11)
                     const V Le = mkv(m.emit[0], m.emit[1], m.emit[2]);
-                    const float w = nomis ? 1.f : balance(d4.w, pdf_scene_light(p.sc, o, point, n, prim));
+                    const float w = nomis ? 1.f : balance(d4.w, pdf_scene_light(sc, o, point, n, prim));
                     Ladd = beta * Le * w;
                     if (GUIDE) guide_account(p, path, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
                 }
                 if (!last) {
                     const long long gp = wave_first + path;
-                    const uint32_t pixel = (uint32_t)(gp / p.spp);
+                    const uint32_t pixel =
+                        B ? (uint32_t)((gp - p.batch[sid].path_base) / p.batch[sid].spp) : (uint32_t)(gp / p.spp);
                     const uint64_t inc = pcg_inc(pixel);
                     uint64_t st = ((uint64_t)q.rng[slot].y << 32) | q.rng[slot].x;
                     const bool delta_mat = m.type == kMirror || m.type == kGlass;
@@ -331,7 +390,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                         const float x1 = pcg_uniform(st, inc);
                         const float x2 = pcg_uniform(st, inc);
                         const float x3 = pcg_uniform(st, inc);
-                        const LightSample ls = sample_lights(p.sc, point, x1, x2, x3);
+                        const LightSample ls = sample_lights(sc, point, x1, x2, x3);
                         if (dot(ls.normal, ls.wi) < 0.f && ls.pdf > 0.f) {
                             const V wil = to_local(fr, ls.wi);
                             float bpdf = p.consistent_mis ? bsdf_sampling_pdf(m, wo, wil) : bsdf_pdf(m, wo, wil);
@@ -345,7 +404,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                             if (!is_zero(contrib)) {
                                 shadow = true;
                                 so = make_float4(point.x, point.y, point.z, ls.distance - 2e-4f);
-                                sd = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, __int_as_float(path));
+                                sd = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, __int_as_float(tag));
                                 sc4 = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
                             }
                         }
@@ -356,15 +415,17 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                         const V nb = beta * fc;
                         if (!is_zero(nb) && isfinite(nb.x + nb.y + nb.z)) {
                             cont = true;
-                            co = make_float4(point.x, point.y, point.z, __int_as_float(path));
+                            co = make_float4(point.x, point.y, point.z, __int_as_float(tag));
                             cd = make_float4(wworld.x, wworld.y, wworld.z, bs.pdf);
                             cb = make_float4(nb.x, nb.y, nb.z, __int_as_float(bs.delta ? 1 : 0));
                             crng = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
-                            if (GUIDE && p.guide_mode && !delta_mat && path % p.gstride == 0) {
+                            if (GUIDE && p.guide_mode && !delta_mat && path % p.gstride == 0 &&
+                                (!B || p.batch[sid].guide_net >= 0)) {
                                 const V wn = normalized(wworld);
                                 const V won = normalized(-dir);
                                 rec = GuideRecord{{point.x, point.y, point.z}, {n.x, n.y, n.z}, {won.x, won.y, won.z},
-                                                  {wn.x, wn.y, wn.z}, lum(fc), lum(nb), path / p.gstride, depth};
+                                                  {wn.x, wn.y, wn.z}, lum(fc), lum(nb), path / p.gstride,
+                                                  depth | (sid << 8)};
                                 record = true;
                             }
                         }
@@ -399,7 +460,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
     }
 }
 
-template <int W, bool CNT>
+template <int W, bool CNT, bool B>
 __global__ void k_shadow(FrameParams p, int depth) {
     extern __shared__ int2 stk[];
     const int count = p.counters->shadow_count[depth];
@@ -416,13 +477,16 @@ __global__ void k_shadow(FrameParams p, int depth) {
         const RayPre r = make_raypre(mkv(o), mkv(d));
         Hit h;
         int of = 0;
-        const bool occ = traverse<W, true, CNT>(p.sc, r, kShadowTMin, o.w, valid, stk + threadIdx.x, blockDim.x,
+        SceneDevice scb;
+        if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(d.w)));
+        const SceneDevice& sc = B ? scb : p.sc;
+        const bool occ = traverse<W, true, CNT>(sc, r, kShadowTMin, o.w, valid, stk + threadIdx.x, blockDim.x,
                                                 p.stack_depth, h, of, &work);
         if (valid) {
             if (of) atomicOr(&p.stats->error, 1);
             if (!occ) {
                 const float4 c = p.sq.c[i];
-                const int path = __float_as_int(d.w);
+                const int path = tag_path(__float_as_int(d.w));
                 float4 l = p.L[path];
                 l.x += c.x;
                 l.y += c.y;
@@ -442,6 +506,40 @@ __global__ void k_shadow(FrameParams p, int depth) {
 constexpr int kInferWarps = 8;
 constexpr int kInferSmemBytes = (kSWords + kInferWarps * 32 * kSXStride) * 4;  // 81 KB: 2 blocks per SM
 
+// Features of one queued hit (zeros for a miss).
+__device__ __forceinline__ bool guide_features(const FrameParams& p, const GuideFrame& gf, float4 o4, float4 d4,
+                                               float4 h4, float x[kGuideIn]) {
+    if (__float_as_int(h4.w) == kMissPrim) {
+        for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
+        return false;
+    }
+    V point, n;
+    int mat;
+    hit_info(p.sc, mkv(o4), mkv(d4), h4, point, n, mat);
+    n = normalized(n);
+    const V wo = normalized(-mkv(d4));
+    const float pp[3] = {point.x, point.y, point.z}, nn[3] = {n.x, n.y, n.z}, ww[3] = {wo.x, wo.y, wo.z};
+    guide_encode(gf, pp, nn, ww, x);
+    return true;
+}
+
+// Raw outputs of row `lane` (left in the tile by guide_mlp_warp32) -> mixture, in place.
+__device__ __forceinline__ float* guide_activate_row(uint32_t* sx, int lane) {
+    float* row = reinterpret_cast<float*>(sx) + (lane >> 4) * 16 * kSXStride + (lane & 15) * kGuideOut;
+    float raw[kGuideOut], mix[kGuideOut];
+    for (int j = 0; j < kGuideOut; j++) raw[j] = row[j];
+    guide_activate(raw, mix);
+    for (int j = 0; j < kGuideOut; j++) row[j] = mix[j];
+    return row;
+}
+
+// Guide inference for the rays of the queue consumed at `depth`: each lane computes the
+// features of one hit, the warp runs the network on the tensor cores for its 32 rays (two
+// 16-row groups sharing each weight fragment), each lane activates its own row and the warp
+// writes the 32 mixtures of consecutive queue slots as one contiguous 5120-byte store.
+// Batched frames (B): each scene has its own network (weights read through L1/L2); a warp
+// evaluates each distinct network among its lanes in turn.
+template <bool B>
 __global__ void __launch_bounds__(32 * kInferWarps, 2) k_guide_infer(FrameParams p, int depth) {
     extern __shared__ __align__(16) uint32_t ism[];
     const int count = p.counters->ray_count[depth];
@@ -453,58 +551,76 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2) k_guide_infer(FrameParams
     // outputs overwrite the inputs of the same 16-row group: every lane has loaded its input
     // fragments into registers before the warp-synchronous mma chain reaches the output stores
     const float* sy = reinterpret_cast<const float*>(sx);
-    guide_load_weights(p.gwpack, sw);
+    if (!B) guide_load_weights(p.gwpack, sw);
     __syncthreads();
     const PathQueue q = p.q[depth & 1];
     for (int grp = blockIdx.x * kInferWarps + warp; grp < groups; grp += gridDim.x * kInferWarps) {
         const int slot = grp * 32 + lane;
         float x[kGuideIn];
-        bool hit = false;
-        if (slot < count) {
-            const float4 o4 = q.o[slot], d4 = q.d[slot], h4 = q.hit[slot];
-            if (__float_as_int(h4.w) != kMissPrim) {
-                V point, n;
-                int mat;
-                hit_info(p.sc, mkv(o4), mkv(d4), h4, point, n, mat);
-                n = normalized(n);
-                const V wo = normalized(-mkv(d4));
-                const float pp[3] = {point.x, point.y, point.z}, nn[3] = {n.x, n.y, n.z}, ww[3] = {wo.x, wo.y, wo.z};
-                guide_encode(p.gframe, pp, nn, ww, x);
-                hit = true;
+        if (!B) {
+            if (slot < count) guide_features(p, p.gframe, q.o[slot], q.d[slot], q.hit[slot], x);
+            else
+                for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
+            guide_store_input(sx, lane, x);
+            __syncwarp();
+            guide_mlp_warp32(sw, sx);
+            __syncwarp();
+            guide_activate_row(sx, lane);
+            __syncwarp();
+            const int rows = count - grp * 32 < 32 ? count - grp * 32 : 32;
+            float* dst = p.gmix + (size_t)grp * 32 * kGuideOut;
+            for (int e = lane; e < rows * kGuideOut; e += 32)
+                dst[e] = sy[(e / (16 * kGuideOut)) * 16 * kSXStride + e % (16 * kGuideOut)];
+            __syncwarp();
+        } else {
+            int net = -1, sid = 0;
+            float4 o4 = make_float4(0.f, 0.f, 0.f, 0.f), d4 = o4, h4 = o4;
+            if (slot < count) {
+                o4 = q.o[slot];
+                d4 = q.d[slot];
+                h4 = q.hit[slot];
+                sid = tag_scene(__float_as_int(o4.w));
+                const BatchScene& sb = p.batch[sid];
+                if (sb.guide_mode == 2 && __float_as_int(h4.w) != kMissPrim) net = sb.guide_net;
             }
+            unsigned pending = __ballot_sync(0xffffffffu, net >= 0);
+            while (pending) {
+                const int lnet = __shfl_sync(0xffffffffu, net, __ffs(pending) - 1);
+                const bool mine = net == lnet;
+                if (mine) guide_features(p, p.batch[sid].gframe, o4, d4, h4, x);
+                else
+                    for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
+                __syncwarp();
+                guide_store_input(sx, lane, x);
+                __syncwarp();
+                guide_mlp_warp32(p.gwpack + (size_t)lnet * kGuidePackWords, sx);
+                __syncwarp();
+                const float* row = guide_activate_row(sx, lane);
+                if (mine) {
+                    float4* dst = reinterpret_cast<float4*>(p.gmix + (size_t)slot * kGuideOut);
+                    const float4* src = reinterpret_cast<const float4*>(row);
+                    for (int j = 0; j < kGuideOut / 4; j++) dst[j] = src[j];
+                }
+                pending &= ~__ballot_sync(0xffffffffu, mine);
+            }
+            __syncwarp();
         }
-        if (!hit)
-            for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
-        guide_store_input(sx, lane, x);
-        __syncwarp();
-        guide_mlp_warp32(sw, sx);
-        __syncwarp();
-        {
-            float* row = reinterpret_cast<float*>(sx) + (lane >> 4) * 16 * kSXStride + (lane & 15) * kGuideOut;
-            float raw[kGuideOut], mix[kGuideOut];
-            for (int j = 0; j < kGuideOut; j++) raw[j] = row[j];
-            guide_activate(raw, mix);
-            for (int j = 0; j < kGuideOut; j++) row[j] = mix[j];
-        }
-        __syncwarp();
-        const int rows = count - grp * 32 < 32 ? count - grp * 32 : 32;
-        float* dst = p.gmix + (size_t)grp * 32 * kGuideOut;
-        for (int e = lane; e < rows * kGuideOut; e += 32)
-            dst[e] = sy[(e / (16 * kGuideOut)) * 16 * kSXStride + e % (16 * kGuideOut)];
-        __syncwarp();
     }
 }
 
 // Resolve this wave's training records into samples: the radiance that arrived along each
 // sampled direction is the path's later contributions (unweighted emission at the next
 // vertex, everything after it) divided by the throughput after the vertex.
+template <bool B>
 __global__ void k_guide_collect(FrameParams p) {
     const int n = min(*p.grec_count, p.grec_cap);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const GuideRecord r = p.grec[i];
+        const int net = B ? p.batch[r.depth >> 8].guide_net : 0;  // the record's scene's network
+        if (net < 0) continue;
         const float* a = p.gacc + (size_t)r.tpath * p.max_depth * 3;
         float lin = 0.f;
-        const int k1 = r.depth + 1;
+        const int k1 = (r.depth & 0xFF) + 1;
         if (k1 < p.max_depth) {
             float sum_r = 0.f;
             for (int d = k1; d < p.max_depth; d++) sum_r += a[3 * d + 1];
@@ -512,7 +628,7 @@ __global__ void k_guide_collect(FrameParams p) {
         }
         const float weight = r.fcos_over_p * lin;
         if (!(weight > 0.f) || !isfinite(weight)) continue;
-        const int idx = atomicAdd(p.gring_count, 1);
+        const int idx = atomicAdd(p.gring_count + net, 1);
         GuideSample smp;
         for (int k = 0; k < 3; k++) {
             smp.p[k] = r.p[k];
@@ -522,18 +638,30 @@ __global__ void k_guide_collect(FrameParams p) {
         }
         smp.weight = weight;
         smp.pad[0] = smp.pad[1] = smp.pad[2] = 0.f;
-        p.gring[(unsigned)idx % (unsigned)p.gring_cap] = smp;
+        p.gring[(size_t)net * p.gring_cap + (unsigned)idx % (unsigned)p.gring_cap] = smp;
     }
 }
 
-__global__ void k_accumulate(FrameParams p, int first_pixel, int npix) {
+template <bool B>
+__global__ void k_accumulate(FrameParams p, int first_pixel, int npix, long long wave_first) {
     const int pi = blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= npix) return;
     const int pixel = first_pixel + pi;
+    int spp = p.spp, prev_spp;
+    long long path0 = (long long)pi * p.spp;  // wave-local index of the pixel's first sample
+    if (B) {
+        const int sid = batch_find(p.batch_pixel_base, p.num_scenes, pixel);
+        const BatchScene& sb = p.batch[sid];
+        spp = sb.spp;
+        path0 = sb.path_base + (pixel - sb.pixel_base) * (long long)spp - wave_first;
+        prev_spp = sb.prev_spp;
+    } else {
+        prev_spp = p.dyn->prev_spp;
+    }
     float r = 0.f, g = 0.f, b = 0.f;
-    const float inv_spp = (float)p.spp;
-    for (int s = 0; s < p.spp; s++) {  // passRadiances += Li / spp (path_tracer.cu:258-262)
-        const float4 l = p.L[(size_t)pi * p.spp + s];
+    const float inv_spp = (float)spp;
+    for (int s = 0; s < spp; s++) {  // passRadiances += Li / spp (path_tracer.cu:258-262)
+        const float4 l = p.L[path0 + s];
         r += l.x / inv_spp;
         g += l.y / inv_spp;
         b += l.z / inv_spp;
@@ -542,11 +670,10 @@ __global__ void k_accumulate(FrameParams p, int first_pixel, int npix) {
     p.pass_rgb[3 * (size_t)pixel + 1] = g;
     p.pass_rgb[3 * (size_t)pixel + 2] = b;
     float nr = r, ng = g, nb = b;
-    const int prev_spp = p.dyn->prev_spp;
     if (prev_spp > 0) {  // running mean (framebuffer.cu:23-33)
         const float prev = (float)prev_spp;
-        const float total = (float)(prev_spp + p.spp);
-        const float wpass = 1.f * p.spp / total;
+        const float total = (float)(prev_spp + spp);
+        const float wpass = 1.f * spp / total;
         nr = p.accum_rgb[3 * (size_t)pixel + 0] * prev / total + r * wpass;
         ng = p.accum_rgb[3 * (size_t)pixel + 1] * prev / total + g * wpass;
         nb = p.accum_rgb[3 * (size_t)pixel + 2] * prev / total + b * wpass;
@@ -574,17 +701,17 @@ struct Marker {
     }
 };
 
-template <int W, bool CNT>
-cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
-    const int npixels = p.width * p.height;
+template <int W, bool CNT, bool B>
+cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
+                          StageMarks* marks) {
     const int grid_e = p.num_sms * p.shape.blocks_per_sm;
     const size_t smem_e = stack_bytes(p.stack_depth, p.shape.block_extend);
     const size_t smem_s = stack_bytes(p.stack_depth, p.shape.block_shadow);
     Marker mark{marks, stream};
-    for (int first = 0; first < npixels; first += p.wave_pixels) {
-        const int npix = npixels - first < p.wave_pixels ? npixels - first : p.wave_pixels;
-        const int n = npix * p.spp;
-        const long long wave_first = (long long)first * p.spp;
+    for (int wv = 0; wv < nwaves; wv++) {
+        const WaveRange& w = waves[wv];
+        const int n = w.npaths;
+        const long long wave_first = w.first_path;
         cudaError_t e = cudaMemsetAsync(p.counters, 0, sizeof(WaveCounters), stream);
         if (e != cudaSuccess) return e;
         if (p.guide_mode) {
@@ -593,31 +720,31 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
             if ((e = cudaMemsetAsync(p.grec_count, 0, sizeof(int), stream))) return e;
         }
         mark(-1);
-        k_camera<<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
+        k_camera<B><<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
         mark(kStageCamera);
         for (int d = 0; d < p.max_depth; d++) {
-            k_extend<W, CNT><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+            k_extend<W, CNT, B><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
             mark(kStageExtend);
             if (p.shape.sort_materials) {
                 k_sort<<<(n + 255) / 256, 256, 0, stream>>>(p, d);
                 mark(kStageSort);
             }
             if (p.guide_mode == 2 && d < p.max_depth - 1) {
-                k_guide_infer<<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
+                k_guide_infer<B><<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
                 mark(kStageGuide);
             }
-            if (p.guide_mode) k_shade<true><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
-            else k_shade<false><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
+            if (p.guide_mode) k_shade<true, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
+            else k_shade<false, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {
-                k_shadow<W, CNT><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d);
+                k_shadow<W, CNT, B><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d);
                 mark(kStageShadow);
             }
         }
-        k_accumulate<<<(npix + 127) / 128, 128, 0, stream>>>(p, first, npix);
+        k_accumulate<B><<<(w.npix + 127) / 128, 128, 0, stream>>>(p, w.first_pixel, w.npix, wave_first);
         mark(kStageAccum);
         if (p.guide_mode) {
-            k_guide_collect<<<p.num_sms * 2, 256, 0, stream>>>(p);
+            k_guide_collect<B><<<p.num_sms * 2, 256, 0, stream>>>(p);
             mark(kStageGuide);
         }
         e = cudaGetLastError();
@@ -627,14 +754,39 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
     return cudaSuccess;
 }
 
+// Single-scene frame: waves of whole pixels, p.wave_pixels each.
+template <int W, bool CNT>
+cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
+    const int npixels = p.width * p.height;
+    const int nwaves = (npixels + p.wave_pixels - 1) / p.wave_pixels;
+    WaveRange local[64];
+    std::vector<WaveRange> heap;
+    WaveRange* waves = local;
+    if (nwaves > 64) {
+        heap.resize(nwaves);
+        waves = heap.data();
+    }
+    for (int k = 0; k < nwaves; k++) {
+        const int first = k * p.wave_pixels;
+        const int npix = npixels - first < p.wave_pixels ? npixels - first : p.wave_pixels;
+        waves[k] = WaveRange{first, npix, (long long)first * p.spp, npix * p.spp, 0};
+    }
+    return enqueue_waves<W, CNT, false>(p, waves, nwaves, stream, marks);
+}
+
 template <int W>
 cudaError_t set_smem_w(size_t bytes) {
     const int b = (int)bytes;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_extend<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_extend<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_shadow<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_shadow<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((e = cudaFuncSetAttribute(k_extend<W, false, false>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, true, false>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, false, false>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, true, false>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, false, true>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, true, true>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, false, true>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, true, true>, a, b))) return e;
     return cudaSuccess;
 }
 
@@ -721,8 +873,26 @@ cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks*
     }
 }
 
+cudaError_t enqueue_batch_frame(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
+                                StageMarks* marks) {
+    if (p.max_depth < 0 || p.max_depth > kMaxDepthLimit || p.num_scenes <= 0) return cudaErrorInvalidValue;
+    const bool cnt = p.count_work != 0;
+    switch (p.sc.bvh_width) {
+        case 2: return cnt ? enqueue_waves<2, true, true>(p, waves, nwaves, stream, marks)
+                           : enqueue_waves<2, false, true>(p, waves, nwaves, stream, marks);
+        case 4: return cnt ? enqueue_waves<4, true, true>(p, waves, nwaves, stream, marks)
+                           : enqueue_waves<4, false, true>(p, waves, nwaves, stream, marks);
+        case 8: return cnt ? enqueue_waves<8, true, true>(p, waves, nwaves, stream, marks)
+                           : enqueue_waves<8, false, true>(p, waves, nwaves, stream, marks);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t configure_guide_infer() {
-    return cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmemBytes);
+    cudaError_t e = cudaFuncSetAttribute(k_guide_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kInferSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_guide_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmemBytes);
 }
 
 cudaError_t configure_traversal_smem(size_t bytes) {

@@ -90,6 +90,44 @@ struct FrameDyn {
     int pad[3];
 };
 
+// Queue tag carried in the origin's w (and the shadow direction's w): the path's index within
+// its wave in the low 25 bits, the scene of a batched frame above them. A wave therefore holds
+// at most 2^25 paths.
+constexpr int kTagPathBits = 25;
+constexpr int kTagPathMask = (1 << kTagPathBits) - 1;
+constexpr int kMaxWavePaths = 1 << kTagPathBits;
+constexpr int kMaxBatchScenes = 64;
+
+// One scene of a batched frame: its part of the concatenated geometry, its image and sampling
+// parameters and its guide network. The host rewrites the per-frame fields (camera, seed,
+// sample base, previous spp) before every frame.
+struct BatchScene {
+    int root;                // root node in the concatenated BVH
+    int light_first;         // first emitter in the concatenated emitter list
+    int num_lights;
+    int width, height, spp, max_depth;
+    int guide_net;           // network index, -1 without guiding
+    int guide_mode;          // 0 off, 1 collect, 2 guided sampling
+    int pad0;
+    long long path_base;     // first path of this scene in the frame's global path order
+    long long pixel_base;    // first pixel in the concatenated image buffers
+    EnvDevice env;
+    GuideFrame gframe;
+    CameraParams cam;
+    uint64_t seed;
+    uint64_t sample_base;    // samples per pixel rendered before this frame
+    int prev_spp;
+    int pad1[3];
+};
+
+// A wave of a frame: whole pixels [first_pixel, first_pixel + npix) of the global pixel order,
+// whose paths are [first_path, first_path + npaths).
+struct WaveRange {
+    int first_pixel, npix;
+    long long first_path;
+    int npaths, pad;
+};
+
 struct FrameParams {
     SceneDevice sc;
     const FrameDyn* dyn;     // device pointer
@@ -129,7 +167,18 @@ struct FrameParams {
     int gtrain_steps;
     int gtrain_batch;
     float gtrain_lr;
+    // ---- batched frames (num_scenes > 0): the scene table and its prefix offsets ----
+    const BatchScene* batch;
+    const long long* batch_path_base;   // num_scenes + 1 entries
+    const long long* batch_pixel_base;  // num_scenes + 1 entries
+    int num_scenes;
+    int gnets;               // guide networks trained after the frame
 };
+
+// Enqueue one batched frame (p.num_scenes > 0): the given waves over the scenes' global path
+// order, every stage one launch for all scenes of the wave.
+cudaError_t enqueue_batch_frame(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
+                                StageMarks* marks = nullptr);
 
 // Enqueue one frame (all waves) on `stream`. Grid sizes do not depend on queue lengths,
 // so the sequence can be captured into a CUDA graph. With `marks`, an event is recorded

@@ -33,6 +33,7 @@ EXPORTED = [
     "pt_trace_rays_device", "pt_occluded", "pt_version", "pt_set_profiling", "pt_get_profile",
     "pt_trace_rays_static", "pt_autotune", "pt_guide_reset", "pt_set_consistent_mis", "pt_guide_get_info",
     "pt_guide_get_params", "pt_guide_set_params", "pt_guide_forward", "pt_guide_gradients", "pt_set_guide_options",
+    "pt_batch_generate", "pt_load_batch", "pt_batch_get_info", "pt_batch_readback",
 ]
 
 GUIDE_PARAMS = 16104
@@ -95,6 +96,30 @@ class TuneResult(C.Structure):
                [("best_ms", C.c_float), ("default_ms", C.c_float), ("trials", C.c_int), ("from_cache", C.c_int)]
 
 
+class BatchScene(C.Structure):
+    _fields_ = [("config", C.c_int), ("level", C.c_int), ("seed", C.c_ulonglong), ("width", C.c_int),
+                ("height", C.c_int), ("spp", C.c_int), ("max_depth", C.c_int), ("guided", C.c_int),
+                ("pad", C.c_int)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("num_triangles", "num_spheres", "num_lights", "width", "height", "spp",
+                                       "max_depth", "guided", "spp_accumulated")] + \
+               [("first_pixel", C.c_longlong), ("first_path", C.c_longlong)]
+
+
+BATCH_FIELDS = ("config", "level", "seed", "width", "height", "spp", "max_depth", "guided")
+
+
+def batch_generate(seed: int, n: int) -> list[dict]:
+    """Configuration 4's seeded draw of n scenes (dicts of BATCH_FIELDS)."""
+    arr = (BatchScene * n)()
+    rc = lib.pt_batch_generate(C.c_ulonglong(seed), n, arr)
+    if rc != 0:
+        raise PathedError(rc, "pt_batch_generate failed")
+    return [{k: getattr(a, k) for k in BATCH_FIELDS} for a in arr]
+
+
 class Profile(C.Structure):
     _fields_ = [("stage_ms", C.c_float * 7), ("stage_launches", C.c_int * 7), ("extend_nodes", C.c_ulonglong),
                 ("extend_prims", C.c_ulonglong), ("shadow_nodes", C.c_ulonglong), ("shadow_prims", C.c_ulonglong),
@@ -120,6 +145,10 @@ def _load():
     lib.pt_readback.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.pt_readback_pass.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.pt_readback_rgba8.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.pt_batch_generate.argtypes = [C.c_ulonglong, C.c_int, C.c_void_p]
+    lib.pt_load_batch.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.pt_batch_get_info.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    lib.pt_batch_readback.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_int]
     lib.pt_trace_rays.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
     lib.pt_trace_rays_device.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
     lib.pt_trace_rays_static.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
@@ -399,6 +428,25 @@ class Session:
             out = np.empty((self.height, self.width, 3), np.float32)
         fn = lib.pt_readback_pass if pass_only else lib.pt_readback
         self._check(fn(self._h, out.ctypes.data, out.size))
+        return out
+
+    # ---- batched frames (configuration 4)
+    def load_batch(self, scenes: list[dict]):
+        arr = (BatchScene * len(scenes))()
+        for a, d in zip(arr, scenes):
+            for k in BATCH_FIELDS:
+                setattr(a, k, int(d.get(k, -1 if k == "level" else 0)))
+        self._check(lib.pt_load_batch(self._h, arr, len(scenes)))
+
+    def batch_info(self, scene: int) -> dict:
+        b = BatchInfo()
+        self._check(lib.pt_batch_get_info(self._h, scene, C.byref(b)))
+        return {k: getattr(b, k) for k, _ in BatchInfo._fields_}
+
+    def batch_readback(self, scene: int, pass_only: bool = False) -> np.ndarray:
+        i = self.batch_info(scene)
+        out = np.empty((i["height"], i["width"], 3), np.float32)
+        self._check(lib.pt_batch_readback(self._h, scene, out.ctypes.data, out.size, int(pass_only)))
         return out
 
     def readback_rgba8(self) -> np.ndarray:

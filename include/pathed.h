@@ -300,6 +300,45 @@ int pt_trace_rays_static(pt_session* s, const float* o, const float* d, const fl
 int pt_occluded(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax,
                 int n, int* occluded);
 
+/* ---- batched frames (configuration 4) -------------------------------------------------
+ * No counterpart in the reference, which renders one scene per session. A session loaded
+ * with pt_load_batch renders all its scenes in every frame: each stage of the wavefront
+ * (camera, closest hit, shading, shadow rays, accumulation, guide inference) is one launch
+ * over the rays of all scenes, whose queue entries carry their scene's id. Each scene keeps
+ * its own resolution, spp per frame, depth, camera, emitters, environment and, when
+ * `guided`, its own guide network. pt_render_async's spp argument is ignored (pass 0);
+ * pt_get_spp reports frames rendered. Single-scene queries (pt_hit_test, pt_trace_rays*,
+ * pt_set_camera, pt_set_material, pt_export_scene) are refused in batch mode. */
+typedef struct pt_batch_scene {
+    int config;            /* generated configuration 0-3 */
+    int level;             /* icosphere level: configs 2-3 their mesh, configs 0-1 an added
+                              mesh; -1 = configuration default (no added mesh) */
+    unsigned long long seed;
+    int width, height;
+    int spp;               /* samples per pixel per frame */
+    int max_depth;
+    int guided;            /* 1: own guide network (needs pt_set_guiding(s, 1)) */
+    int pad;
+} pt_batch_scene;
+
+typedef struct pt_batch_info {
+    int num_triangles, num_spheres, num_lights;
+    int width, height, spp, max_depth, guided;
+    int spp_accumulated;   /* samples per pixel in the scene's running mean */
+    long long first_pixel; /* offset of the scene's pixels in the batch's pixel order */
+    long long first_path;  /* offset of the scene's paths in a frame's path order */
+} pt_batch_info;
+
+/* Configuration 4's seeded draw of n scenes from configurations 0-3: log-uniform triangle
+ * counts 1k-2M (icosphere levels 3-8), square resolutions 256-1024, spp 4-64, depth 4-10,
+ * about half guided. */
+int pt_batch_generate(unsigned long long seed, int n, pt_batch_scene* out);
+/* Generate every scene, build its BVH and merge them into the session (n <= 64). */
+int pt_load_batch(pt_session* s, const pt_batch_scene* scenes, int n);
+int pt_batch_get_info(const pt_session* s, int scene, pt_batch_info* out);
+/* Running mean (pass_only = 0) or last frame's pass of one scene: width * height * 3 floats. */
+int pt_batch_readback(pt_session* s, int scene, float* rgb, size_t n, int pass_only);
+
 /* Library version string. */
 const char* pt_version(void);
 
