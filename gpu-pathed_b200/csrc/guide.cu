@@ -13,6 +13,8 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "guide_mlp.cuh"
 
 namespace pt {
@@ -25,6 +27,8 @@ namespace {
 __global__ void k_guide_pack(const float* __restrict__ w, uint32_t* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kGuidePackWords) return;
+    w += (size_t)blockIdx.y * kGuideParams;  // network blockIdx.y
+    out += (size_t)blockIdx.y * kGuidePackWords;
     // forward: pair of rows (2 kp, 2 kp + 1) at column n
     auto pair = [&](int base, int ncol, int kp, int n) {
         return pack_bf16(w[base + (2 * kp) * ncol + n], w[base + (2 * kp + 1) * ncol + n]);
@@ -105,6 +109,15 @@ struct TrainSource {
     int n;                 // explicit count, or the batch size for the ring
 };
 
+// The sample source of network `net` (its own ring and counter).
+__device__ __forceinline__ TrainSource source_of_net(TrainSource s, int net) {
+    if (s.ring) {
+        s.ring += (size_t)net * s.cap;
+        s.count += net;
+    }
+    return s;
+}
+
 __device__ __forceinline__ void source_range(const TrainSource& s, int& first, int& n) {
     if (s.ring) {
         // the counter only grows (and may wrap past 2^31): unsigned arithmetic, newest n samples
@@ -136,7 +149,9 @@ __device__ __forceinline__ void source_sample(const TrainSource& s, const GuideF
     xrow[kGuideIn - 1] = 0.f;
 }
 
-__global__ void k_guide_wsum(TrainSource s, float* wsum) {
+__global__ void k_guide_wsum(TrainSource s0, float* wsum) {
+    const TrainSource s = source_of_net(s0, blockIdx.y);
+    wsum += 4 * blockIdx.y;
     int first, n;
     source_range(s, first, n);
     float acc = 0.f;
@@ -294,8 +309,14 @@ __device__ __forceinline__ void guide_backward(const uint32_t* swt_layer, const 
     }
 }
 
-__global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideDevice g, TrainSource src) {
+__global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideDevice g, TrainSource src0) {
     extern __shared__ __align__(16) uint32_t smem[];
+    // network blockIdx.y: its weights, gradient, sums and samples
+    const int net = blockIdx.y;
+    g.wpack += (size_t)net * kGuidePackWords;
+    g.grad += (size_t)net * kGuideParams;
+    g.wsum += 4 * net;
+    const TrainSource src = source_of_net(src0, net);
     uint32_t* sw = smem;               // forward weights and biases (inference layout)
     uint32_t* swt = sw + kSWords;      // transposed weights
     uint32_t* tiles = swt + kSTWords;  // per-warp tiles
@@ -319,7 +340,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideDevice g,
             const int i = tile * kBlockRows + warp * 16 + lane;
             float x[kGuideIn], wi[3] = {0.f, 0.f, 1.f}, w = 0.f;
             if (i < n) {
-                source_sample(src, g.frame, first, i, x, wi, w);
+                source_sample(src, g.frames ? g.frames[net] : g.frame, first, i, x, wi, w);
             } else {
 #pragma unroll
                 for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
@@ -470,8 +491,13 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideDevice g,
 __global__ void k_guide_adam(GuideDevice g, float lr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kGuideParams) return;
+    const size_t off = (size_t)blockIdx.y * kGuideParams;  // network blockIdx.y
+    g.w += off;
+    g.grad += off;
+    g.adam_m += off;
+    g.adam_v += off;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    const float t = (float)(*g.step + 1);
+    const float t = (float)(*(g.step + 4 * blockIdx.y) + 1);
     const float c1 = 1.f - powf(b1, t), c2 = 1.f - powf(b2, t);
     float gr = g.grad[i];
     if (!isfinite(gr)) gr = 0.f;
@@ -484,15 +510,26 @@ __global__ void k_guide_adam(GuideDevice g, float lr) {
     g.grad[i] = 0.f;
 }
 
-__global__ void k_guide_step(int* step) { *step += 1; }
+__global__ void k_guide_step(int* step, int nets) {
+    if (threadIdx.x < nets) step[4 * threadIdx.x] += 1;  // one counter per network, 4 words apart
+}
 
 constexpr size_t kTrainSmemBytes = (size_t)kTrainSmemWords * sizeof(uint32_t);
 
+__global__ void k_guide_clear_sums(float* wsum, int nets) {
+    if (threadIdx.x < nets) {  // weight sum, batch loss of each network
+        wsum[4 * threadIdx.x] = 0.f;
+        wsum[4 * threadIdx.x + 1] = 0.f;
+    }
+}
+
 cudaError_t launch_train(const GuideDevice& g, const TrainSource& src, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(g.wsum, 0, 2 * sizeof(float), s);  // weight sum, batch loss
-    if (e != cudaSuccess) return e;
-    k_guide_wsum<<<g.num_sms, 256, 0, s>>>(src, g.wsum);
-    k_guide_train<<<g.num_sms, kTrainThreads, kTrainSmemBytes, s>>>(g, src);
+    const int nets = g.nets > 0 ? g.nets : 1;
+    k_guide_clear_sums<<<1, 64, 0, s>>>(g.wsum, nets);
+    // about one block per SM in total, at least 4 per network
+    const int per = std::max(4, g.num_sms / nets);
+    k_guide_wsum<<<dim3(per, nets), 256, 0, s>>>(src, g.wsum);
+    k_guide_train<<<dim3(per, nets), kTrainThreads, kTrainSmemBytes, s>>>(g, src);
     return cudaGetLastError();
 }
 
@@ -503,7 +540,7 @@ cudaError_t guide_configure() {
 }
 
 cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s) {
-    k_guide_pack<<<(kGuidePackWords + 255) / 256, 256, 0, s>>>(g.w, g.wpack);
+    k_guide_pack<<<dim3((kGuidePackWords + 255) / 256, g.nets > 0 ? g.nets : 1), 256, 0, s>>>(g.w, g.wpack);
     return cudaGetLastError();
 }
 
@@ -520,7 +557,9 @@ cudaError_t guide_gradients_features(const GuideDevice& g, const float* x, const
     cudaError_t e = cudaMemsetAsync(g.grad, 0, kGuideParams * sizeof(float), s);
     if (e != cudaSuccess) return e;
     TrainSource src{x, wi, w, nullptr, 0, nullptr, n};
-    return launch_train(g, src, s);
+    GuideDevice g1 = g;  // explicit samples train network 0
+    g1.nets = 1;
+    return launch_train(g1, src, s);
 }
 
 cudaError_t guide_train_step(const GuideDevice& g, const GuideSample* ring, int cap, const int* count, int batch,
@@ -528,8 +567,9 @@ cudaError_t guide_train_step(const GuideDevice& g, const GuideSample* ring, int 
     TrainSource src{nullptr, nullptr, nullptr, ring, cap, count, batch};
     cudaError_t e = launch_train(g, src, s);
     if (e != cudaSuccess) return e;
-    k_guide_adam<<<(kGuideParams + 255) / 256, 256, 0, s>>>(g, lr);
-    k_guide_step<<<1, 1, 0, s>>>(g.step);
+    const int nets = g.nets > 0 ? g.nets : 1;
+    k_guide_adam<<<dim3((kGuideParams + 255) / 256, nets), 256, 0, s>>>(g, lr);
+    k_guide_step<<<1, 64, 0, s>>>(g.step, nets);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return guide_pack(g, s);
 }

@@ -9,7 +9,10 @@
 
 namespace pt {
 
-// Device buffers of the guide network and its training state.
+// Device buffers of the guide networks and their training state. With nets > 1 (batched
+// frames, one network per guided scene) every array holds `nets` consecutive copies: per net
+// kGuideParams parameters, kGuidePackWords packed words, 4 words of sums (weight sum, loss,
+// unused, step counter) and its own sample ring.
 struct GuideDevice {
     float* w;            // FP32 master parameters [kGuideParams]
     uint32_t* wpack;     // [kGuidePackWords] shared-memory images of the BF16 weights
@@ -19,6 +22,8 @@ struct GuideDevice {
     float* wsum;         // [2] sum of sample weights of the current batch, batch loss
     int* step;           // Adam steps taken (device counter, so training launches replay in graphs)
     int num_sms;         // training grid: one block per SM
+    int nets;            // networks trained together (1 for a single scene)
+    const GuideFrame* frames;  // per-network encoding frames (nets > 1), else `frame`
     GuideFrame frame;
 };
 
@@ -62,5 +67,7 @@ cudaError_t guide_gradients_features(const GuideDevice& g, const float* x, const
 // changes from step to step.
 cudaError_t guide_train_step(const GuideDevice& g, const GuideSample* ring, int cap, const int* count, int batch,
                              float lr, cudaStream_t s);
+// Per-net views of a multi-net GuideDevice.
+inline float* guide_net_params(const GuideDevice& g, int net) { return g.w + (size_t)net * kGuideParams; }
 
 }  // namespace pt

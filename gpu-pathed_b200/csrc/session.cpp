@@ -162,14 +162,25 @@ GuideDevice Session::guide_view() const {
     g.wsum = d_gwsum_.as<float>();
     g.step = reinterpret_cast<int*>(d_gwsum_.as<float>() + 3);
     g.num_sms = num_sms_;
+    g.nets = guide_nets_;
     g.frame = gframe_;
+    g.frames = guide_nets_ > 1 || batch_mode() ? d_gframes_.as<GuideFrame>() : nullptr;
     return g;
+}
+
+// Networks a frame needs: one per guided scene of a batch, else one.
+int Session::wanted_guide_nets() const {
+    if (!batch_mode()) return 1;
+    int n = 0;
+    for (const BatchHost& b : batch_) n += b.spec.guided ? 1 : 0;
+    return std::max(1, n);
 }
 
 int Session::guide_init_weights() {
     // He-normal initialisation from a seeded generator; zero biases; the output layer starts
-    // small so that the first mixture is broad (kappa about 1) and evenly weighted.
-    std::vector<float> w(kGuideParams, 0.f);
+    // small so that the first mixture is broad (kappa about 1) and evenly weighted. Network k
+    // of a batch continues the generator of network k - 1.
+    std::vector<float> w((size_t)kGuideParams * guide_nets_, 0.f);
     uint64_t s = guide_seed_;
     auto next = [&]() {
         s += 0x9E3779B97F4A7C15ULL;
@@ -186,25 +197,36 @@ int Session::guide_init_weights() {
         const double sd = std::sqrt(2.0 / fan_in) * scale;
         for (int i = 0; i < count; i++) w[off + i] = (float)(normal() * sd);
     };
-    fill(kGW1, kGuideIn, kGuideIn * kGuideHidden, 1.0);
-    fill(kGW2, kGuideHidden, kGuideHidden * kGuideHidden, 1.0);
-    fill(kGW3, kGuideHidden, kGuideHidden * kGuideHidden, 1.0);
-    fill(kGW4, kGuideHidden, kGuideHidden * kGuideOut, 0.1);
-    for (int j = 0; j < kGuideLobes; j++) {  // mean directions spread by the bias
-        const double z = 2.0 * next() - 1.0, ph = 6.283185307179586 * next(), r = std::sqrt(1 - z * z);
-        w[kGB4 + 5 * j] = (float)(r * std::cos(ph));
-        w[kGB4 + 5 * j + 1] = (float)(r * std::sin(ph));
-        w[kGB4 + 5 * j + 2] = (float)z;
+    for (int net = 0; net < guide_nets_; net++) {
+        const int base = net * kGuideParams;
+        fill(base + kGW1, kGuideIn, kGuideIn * kGuideHidden, 1.0);
+        fill(base + kGW2, kGuideHidden, kGuideHidden * kGuideHidden, 1.0);
+        fill(base + kGW3, kGuideHidden, kGuideHidden * kGuideHidden, 1.0);
+        fill(base + kGW4, kGuideHidden, kGuideHidden * kGuideOut, 0.1);
+        for (int j = 0; j < kGuideLobes; j++) {  // mean directions spread by the bias
+            const double z = 2.0 * next() - 1.0, ph = 6.283185307179586 * next(), r = std::sqrt(1 - z * z);
+            w[base + kGB4 + 5 * j] = (float)(r * std::cos(ph));
+            w[base + kGB4 + 5 * j + 1] = (float)(r * std::sin(ph));
+            w[base + kGB4 + 5 * j + 2] = (float)z;
+        }
     }
+    const size_t pbytes = (size_t)kGuideParams * 4 * guide_nets_;
     int r;
-    if ((r = check_cuda(cudaMemcpyAsync(d_gw_.p, w.data(), kGuideParams * 4, cudaMemcpyHostToDevice, stream_),
-                        "guide weights")))
+    if ((r = check_cuda(cudaMemcpyAsync(d_gw_.p, w.data(), pbytes, cudaMemcpyHostToDevice, stream_), "guide weights")))
         return r;
-    if ((r = check_cuda(cudaMemsetAsync(d_ggrad_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
-    if ((r = check_cuda(cudaMemsetAsync(d_gm_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
-    if ((r = check_cuda(cudaMemsetAsync(d_gv_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
-    if ((r = check_cuda(cudaMemsetAsync(d_gring_count_.p, 0, sizeof(int), stream_), "guide"))) return r;
-    if ((r = check_cuda(cudaMemsetAsync(d_gwsum_.p, 0, 16, stream_), "guide"))) return r;  // sums, step counter
+    if ((r = check_cuda(cudaMemsetAsync(d_ggrad_.p, 0, pbytes, stream_), "guide"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_gm_.p, 0, pbytes, stream_), "guide"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_gv_.p, 0, pbytes, stream_), "guide"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(d_gring_count_.p, 0, sizeof(int) * guide_nets_, stream_), "guide"))) return r;
+    // weight sums, losses and step counters (4 words per network)
+    if ((r = check_cuda(cudaMemsetAsync(d_gwsum_.p, 0, 16 * guide_nets_, stream_), "guide"))) return r;
+    if (batch_mode()) {  // per-network position-encoding frames: the guided scenes' bounds
+        std::vector<GuideFrame> frames;
+        for (const BatchHost& b : batch_)
+            if (b.spec.guided) frames.push_back(b.gframe);
+        if (frames.empty()) frames.push_back(gframe_);
+        if ((r = check_cuda(upload(d_gframes_, frames, stream_), "guide frames"))) return r;
+    }
     if ((r = check_cuda(guide_pack(guide_view(), stream_), "guide pack"))) return r;
     guide_iters_ = 0;
     return check_cuda(cudaStreamSynchronize(stream_), "guide init");
@@ -213,18 +235,23 @@ int Session::guide_init_weights() {
 int Session::ensure_guide() {
     int r;
     if ((r = ensure_device())) return r;
-    if (!guide_alloc_) {
-        if ((r = check_cuda(d_gw_.alloc(kGuideParams * 4), "guide"))) return r;
-        if ((r = check_cuda(d_gwpack_.alloc(kGuidePackWords * 4), "guide"))) return r;
-        if ((r = check_cuda(d_ggrad_.alloc(kGuideParams * 4), "guide"))) return r;
-        if ((r = check_cuda(d_gm_.alloc(kGuideParams * 4), "guide"))) return r;
-        if ((r = check_cuda(d_gv_.alloc(kGuideParams * 4), "guide"))) return r;
-        if ((r = check_cuda(d_gwsum_.alloc(16), "guide"))) return r;
+    const int nets = wanted_guide_nets();
+    if (!guide_alloc_ || nets != guide_nets_) {
+        guide_nets_ = nets;
+        guide_ring_cap_ = nets > 1 ? 1 << 20 : 1 << 21;
+        const size_t pbytes = (size_t)kGuideParams * 4 * nets;
+        if ((r = check_cuda(d_gw_.alloc(pbytes), "guide"))) return r;
+        if ((r = check_cuda(d_gwpack_.alloc((size_t)kGuidePackWords * 4 * nets), "guide"))) return r;
+        if ((r = check_cuda(d_ggrad_.alloc(pbytes), "guide"))) return r;
+        if ((r = check_cuda(d_gm_.alloc(pbytes), "guide"))) return r;
+        if ((r = check_cuda(d_gv_.alloc(pbytes), "guide"))) return r;
+        if ((r = check_cuda(d_gwsum_.alloc(16 * nets), "guide"))) return r;
         if ((r = check_cuda(d_grec_count_.alloc(16), "guide"))) return r;
         if ((r = check_cuda(configure_guide_infer(), "guide inference configuration"))) return r;
         if ((r = check_cuda(guide_configure(), "guide training configuration"))) return r;
-        if ((r = check_cuda(d_gring_.alloc((size_t)(1 << 21) * sizeof(GuideSample)), "guide samples"))) return r;
-        if ((r = check_cuda(d_gring_count_.alloc(16), "guide"))) return r;
+        if ((r = check_cuda(d_gring_.alloc((size_t)guide_ring_cap_ * nets * sizeof(GuideSample)), "guide samples")))
+            return r;
+        if ((r = check_cuda(d_gring_count_.alloc(4 * nets), "guide"))) return r;
         guide_alloc_ = true;
         if ((r = guide_init_weights())) return r;
     }
@@ -694,7 +721,8 @@ int Session::render_async(int spp) {
         p.gstride = gstride;
         p.gring = d_gring_.as<GuideSample>();
         p.gring_count = d_gring_count_.as<int>();
-        p.gring_cap = 1 << 21;
+        p.gring_cap = guide_ring_cap_;
+        p.gnets = guide_nets_;
         // Adam steps this frame: automatic schedule (many while the network is young) unless set
         p.gtrain_steps = guide_steps_per_frame_ > 0 ? guide_steps_per_frame_
                          : guide_iters_ < 256      ? 8
@@ -709,7 +737,11 @@ int Session::render_async(int spp) {
     h_dyn_->sample_base = (uint64_t)total_spp_;
     h_dyn_->prev_spp = total_spp_;
     if (batch) {
+        int net = 0;
         for (size_t i = 0; i < batch_.size(); i++) {
+            const bool g = guiding_ && batch_[i].spec.guided;
+            h_batch_[i].guide_net = g ? net++ : -1;
+            h_batch_[i].guide_mode = g ? p.guide_mode : 0;
             h_batch_[i].seed = seed_;
             h_batch_[i].sample_base = (uint64_t)batch_[i].total_spp;
             h_batch_[i].prev_spp = batch_[i].total_spp;

@@ -216,6 +216,10 @@ private:
     uint64_t guide_seed_ = 0x9e11deULL;
     GuideFrame gframe_{};
     int ensure_guide();
+    int guide_nets_ = 1;
+    int guide_ring_cap_ = 1 << 21;
+    DevBuf d_gframes_;
+    int wanted_guide_nets() const;
     // batch mode
     std::vector<BatchHost> batch_;
     std::vector<BatchSpec> batch_specs_;

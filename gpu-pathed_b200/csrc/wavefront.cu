@@ -331,7 +331,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                 hit_info(sc, o, dir, h4, point, n, mat);
                 // guided modes shade in an orthonormal frame (the reference's frame is built
                 // from the unnormalised interpolated normal)
-                if (GUIDE && p.guide_mode) n = normalized(n);
+                if (GUIDE && (B ? p.batch[sid].guide_mode : p.guide_mode)) n = normalized(n);
                 const Frame fr = make_frame(n);
                 const V wo = normalized(to_local(fr, -dir));
                 const Material m = sc.mats[mat];

@@ -108,3 +108,45 @@ def test_batch_reset_and_graph_replay():
     assert np.array_equal(a, b)  # same seeds after a reset
     assert s.batch_info(0)["spp_accumulated"] == 2 * SMALL[0]["spp"]
     s.close()
+
+
+@pytest.mark.gpu
+def test_guided_batch_one_network_per_guided_scene():
+    specs = [dict(config=3, level=3, seed=21, width=64, height=64, spp=4, max_depth=8, guided=1),
+             dict(config=0, level=-1, seed=22, width=64, height=64, spp=4, max_depth=5, guided=0),
+             dict(config=2, level=3, seed=23, width=64, height=48, spp=4, max_depth=5, guided=1)]
+    frames, skip = 32, 8
+    s = pathed.Session(16, 16)
+    s.load_batch(specs)
+    s.set_guiding(True)
+    means = []
+    for k in range(frames):
+        s.render(0)
+        if k >= skip:
+            means.append(s.batch_readback(0, pass_only=True).mean())
+    info = s.guide_info()
+    assert info["mode"] == 2 and info["steps"] > 0 and info["samples"] > 0
+    # the unguided scene's paths are untouched by guiding (consistent MIS is on for the batch)
+    ref = pathed.Session(64, 64)
+    ref.load_config(0, seed=22)
+    ref.set_max_depth(5)
+    ref.set_consistent_mis(True)
+    for _ in range(frames):
+        ref.render(4)
+    assert np.array_equal(s.batch_readback(1), ref.readback())
+    ref.close()
+    s.close()
+    # the guided scene converges to its plain image: frame means within 4.5 standard errors
+    plain = pathed.Session(64, 64)
+    plain.load_config(3, seed=21, level=3)
+    plain.set_max_depth(8)
+    plain.set_consistent_mis(True)
+    pm = []
+    for _ in range(frames - skip):
+        plain.render(4)
+        pm.append(plain.readback(pass_only=True).mean())
+    plain.close()
+    m0, e0 = np.mean(pm), np.std(pm, ddof=1) / np.sqrt(len(pm))
+    m1, e1 = np.mean(means), np.std(means, ddof=1) / np.sqrt(len(means))
+    print(f"slit room in a guided batch: {m1:.6f} +- {e1:.6f}, alone plain {m0:.6f} +- {e0:.6f}")
+    assert abs(m0 - m1) <= 4.5 * np.hypot(e0, e1)
