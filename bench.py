@@ -40,6 +40,9 @@ WORKLOADS = {
     1: dict(name="spheres-64+4-emitters-plane", res=(1024, 1024), spp=64, depth=8),
     2: dict(name="icosphere-1310720tri-env2048x1024", res=(1920, 1080), spp=32, depth=6),
     3: dict(name="slit-room-2002tri+icosphere-1310720tri", res=(1024, 1024), spp=16, depth=10),
+    # 48 scenes drawn from 0-3 (seed 0x5EED + 4), one launch per stage for all of them,
+    # about half with their own guide network
+    4: dict(name="batch-48-scenes", res=(0, 0), spp=0, depth=0),
 }
 
 
@@ -153,6 +156,10 @@ def run_reference(args):
     if rank != 0:
         return 0
     wl = WORKLOADS[args.config]
+    if args.config == 4:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference renders one scene per session: no "
+                          "batched form of configuration 4 exists (per-scene reference arms: --config 0-3)"}))
+        return 0
     vals = []
     for _ in range(args.warmup):
         cpu_reference_run(args.config, 1.0)
@@ -236,9 +243,21 @@ def run_ours(args):
     wl = WORKLOADS[args.config]
     w, h = wl["res"]
     spp = args.spp or wl["spp"]
+    batch = args.config == 4
+    if batch:
+        w = h = 16
     s = pathed.Session(w, h)
     s.set_device(local)  # the library's CUDA runtime keeps its own current device
-    s.load_config(args.config)
+    specs = None
+    if batch:
+        specs = pathed.batch_generate(0x5EED + 4, 48)
+        s.load_batch(specs)
+        s.set_guiding(True)
+        spp = 0
+    else:
+        s.load_config(args.config)
+        if args.guided:  # learned guiding on the main workload (trained online during warm-up)
+            s.set_guiding(True)
     s.set_seed(0x5EED + 7919 * rank)
     if args.wave_paths:
         s.set_launch(wave_paths=args.wave_paths)
@@ -294,16 +313,24 @@ def run_ours(args):
     value = rays_all / (t_max / 1e3) / 1e6
 
     # ---- end to end through the C ABI with host buffers
-    cam = s.export_scene()["camera"]
-    host = torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
-    cam_host = torch.from_numpy(cam.copy()).pin_memory().numpy()
+    if batch:  # every scene's image read back each step
+        hosts = [torch.empty((d["height"], d["width"], 3), dtype=torch.float32).pin_memory().numpy() for d in specs]
+    else:
+        cam = s.export_scene()["camera"]
+        host = torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
+        cam_host = torch.from_numpy(cam.copy()).pin_memory().numpy()
     barrier()
     e2e_rays = 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        s.set_camera(cam_host[0:3], cam_host[3:6], cam_host[6:9], float(cam_host[9]), bool(cam_host[10]))
-        s.render(spp)
-        s.readback(out=host)
+        if batch:
+            s.render(0)
+            for k, hb in enumerate(hosts):
+                s._check(pathed.lib.pt_batch_readback(s._h, k, hb.ctypes.data, hb.size, 0))
+        else:
+            s.set_camera(cam_host[0:3], cam_host[3:6], cam_host[6:9], float(cam_host[9]), bool(cam_host[10]))
+            s.render(spp)
+            s.readback(out=host)
         st = s.stats()
         e2e_rays += st["rays_extend"] + st["rays_shadow"]
     barrier()
@@ -333,7 +360,7 @@ def run_ours(args):
         per_launch_bytes = algo_bytes_frame / ext_launches
         ext_ms = stage_ms["extend"] / max(1, stage_launches["extend"])
         achieved = per_launch_bytes / (ext_ms / 1e3) / 1e9
-        bpq = _ncu_bytes_per_query()
+        bpq = _ncu_bytes_per_query(wl["name"])
         # ncu measured one launch's DRAM bytes; scaled to the average launch by its queries
         traffic = None if bpq is None else bpq * q_ext / ext_launches
         roof = {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm", "achieved": achieved, "peak": hbm,
@@ -347,13 +374,13 @@ def run_ours(args):
                 "prims_per_query": prims / max(1, q_ext)}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not batch:
         mr, mp, sample, thr, _ = cpu_reference_run(args.config, args.cpu_seconds)
         cpu = {"value": mr, "unit": "Mrays/s", "cores": thr, "kind": "port", "sample": sample,
                "mpaths_per_s": mp, "algorithm": "reference integrator restated (two traces per bounce, linear scan)"}
 
     guiding = None
-    if rank == 0 and world == 1 and not args.no_guiding:
+    if rank == 0 and world == 1 and not args.no_guiding and not batch:
         guiding = guided_time_to_relmse()
 
     gpu_launches = sum(stage_launches.values())
@@ -363,12 +390,19 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "mpaths_per_s": paths_all / (t_max / 1e3) / 1e6,
-            "config": {"workload": wl["name"], "resolution": [w, h], "spp": spp, "max_depth": wl["depth"],
-                       "nee": True, "triangles": counts.num_triangles, "spheres": counts.num_spheres,
-                       "bvh_width": counts.bvh_width, "parallelism": f"replicas{world}",
-                       "l2": "flushed between steps (256 MiB write)"},
-            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 44,
-                    "d2h_bytes_per_step": w * h * 3 * 4},
+            "config": ({"workload": wl["name"], "resolution": [w, h], "spp": spp, "max_depth": wl["depth"],
+                        "nee": True, "triangles": counts.num_triangles, "spheres": counts.num_spheres,
+                        "bvh_width": counts.bvh_width, "parallelism": f"replicas{world}",
+                        "guided": bool(args.guided),
+                        "l2": "flushed between steps (256 MiB write)"} if not batch else
+                       {"workload": wl["name"], "scenes": len(specs), "guided_scenes": sum(d["guided"] for d in specs),
+                        "paths_per_frame": sum(d["width"] * d["height"] * d["spp"] for d in specs),
+                        "pixels": sum(d["width"] * d["height"] for d in specs), "triangles": counts.num_triangles,
+                        "spheres": counts.num_spheres, "bvh_width": counts.bvh_width, "nee": True,
+                        "draw": "pathed.batch_generate(0x5EED + 4, 48)", "parallelism": f"replicas{world}",
+                        "l2": "flushed between steps (256 MiB write)"}),
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0 if batch else 44,
+                    "d2h_bytes_per_step": (sum(d["width"] * d["height"] for d in specs) if batch else w * h) * 3 * 4},
             "roofline": roof,
             "cpu_baseline": cpu,
             "guiding": guiding,
@@ -444,14 +478,16 @@ def guided_time_to_relmse(budget_spp=128, ref_spp=2048, res=1024):
             "training": "online from scratch inside the timed frames (automatic Adam schedule)"}
 
 
-def _ncu_bytes_per_query():
-    """DRAM bytes per closest-hit query measured by ncu (profiles/k_extend_traffic.txt)."""
+def _ncu_bytes_per_query(workload):
+    """DRAM bytes per closest-hit query that ncu measured on this workload
+    (profiles/k_extend_traffic.txt, one `<workload> dram_bytes_per_query: B` line each), or None."""
     p = os.path.join(ROOT, "profiles", "k_extend_traffic.txt")
     try:
         with open(p) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_query:"):
-                    return float(line.split(":")[1])
+                parts = line.split()
+                if len(parts) == 3 and parts[0] == workload and parts[1] == "dram_bytes_per_query:":
+                    return float(parts[2])
     except OSError:
         pass
     return None
@@ -463,12 +499,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3])
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4])
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--wave-paths", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guiding", action="store_true")
+    ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
