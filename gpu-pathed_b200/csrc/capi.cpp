@@ -212,6 +212,10 @@ int pt_guide_forward(pt_session* s, const float* x, int n, float* raw) {
     if (!s || (n > 0 && (!x || !raw))) return PT_ERR_ARG;
     return guarded(s, [&] { return s->impl.guide_forward(x, n, raw); });
 }
+int pt_set_guide_inference(pt_session* s, int tc) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.set_guide_inference(tc);
+}
 int pt_guide_gradients(pt_session* s, const float* x, const float* wi, const float* w, int n, float* grad) {
     if (!s || !x || !wi || !w || !grad) return PT_ERR_ARG;
     return guarded(s, [&] { return s->impl.guide_gradients(x, wi, w, n, grad); });

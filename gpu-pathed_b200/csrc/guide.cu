@@ -16,10 +16,11 @@
 #include <algorithm>
 
 #include "guide_mlp.cuh"
+#include "guide_tc.cuh"
 
 namespace pt {
 
-static_assert(kPackWords == kGuidePackWords, "packed weight layout");
+static_assert(kPackWords + kTcPackWords == kGuidePackWords, "packed weight layout");
 
 namespace {
 
@@ -55,12 +56,23 @@ __global__ void k_guide_pack(const float* __restrict__ w, uint32_t* __restrict__
         const int j = i - kSB;  // b1 64, b2 64, b3 64, b4 40
         const float b = j < 64 ? w[kGB1 + j] : j < 128 ? w[kGB2 + j - 64] : j < 192 ? w[kGB3 + j - 128] : w[kGB4 + j - 192];
         v = __float_as_uint(b);
-    } else {
+    } else if (i < kPackWords) {
         const int j = i - kPackT, layer = j / (64 * kSTStride), r = (j % (64 * kSTStride)) / kSTStride,
                   c = j % kSTStride;
         if (layer == 0 && c < 32) v = tpair(kGW2, 64, r, c);
         else if (layer == 1 && c < 32) v = tpair(kGW3, 64, r, c);
         else if (layer == 2 && c < 24) v = tpair(kGW4, 40, r, c);
+    } else {
+        // K-major operand images of the tensor-memory inference: element (n, k) = W[k][n]
+        const int b = 4 * (i - kPackWords);
+        int base, ncol, lbo, off;
+        if (b < kTcW2) { base = kGW1; ncol = 64; lbo = kTcLboW; off = b - kTcW1; }
+        else if (b < kTcW3) { base = kGW2; ncol = 64; lbo = kTcLboW; off = b - kTcW2; }
+        else if (b < kTcW4) { base = kGW3; ncol = 64; lbo = kTcLboW; off = b - kTcW3; }
+        else { base = kGW4; ncol = 40; lbo = kTcLboW4; off = b - kTcW4; }
+        const int kc = off / lbo, rem = off % lbo;
+        const int n = (rem / 128) * 8 + (rem % 128) / 16, k = kc * 8 + (rem % 16) / 2;
+        if (n < ncol) v = pack_bf16(w[base + k * ncol + n], w[base + (k + 1) * ncol + n]);
     }
     out[i] = v;
 }
@@ -96,6 +108,37 @@ __global__ void k_guide_forward_x(const uint32_t* __restrict__ wpack, const floa
         }
         __syncwarp();
     }
+}
+
+// Inference on explicit input vectors on the tensor cores (tcgen05, TMEM accumulators):
+// 128 inputs per tile, one thread each. Raw outputs like k_guide_forward_x.
+__global__ void __launch_bounds__(kTcRows) k_guide_forward_x_tc(const uint32_t* __restrict__ wpack,
+                                                                const float* __restrict__ x, int n,
+                                                                float* __restrict__ raw, int* error) {
+    extern __shared__ __align__(1024) uint8_t tsm[];
+    TcSmem& s = *reinterpret_cast<TcSmem*>(tsm);
+    const int tiles = (n + kTcRows - 1) / kTcRows;
+    if ((int)blockIdx.x >= tiles) return;
+    const uint32_t tmem = tc_setup(s, wpack, wpack + kPackWords);
+    uint32_t phase = 0;
+    const int t = threadIdx.x;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int row = tile * kTcRows + t;
+        float xi[kGuideIn];
+        for (int k = 0; k < kGuideIn; k++) xi[k] = row < n ? x[(size_t)row * kGuideIn + k] : 0.f;
+        tc_store_input(s.a, t, xi);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        float out[kGuideOut];
+        if (!tc_network(s, tmem, phase, out)) {
+            if (t == 0) atomicOr(error, 2);
+            break;
+        }
+        if (row < n)
+            for (int j = 0; j < kGuideOut; j++) raw[(size_t)row * kGuideOut + j] = out[j];
+    }
+    tc_teardown(tmem);
 }
 
 // Sample source of the training kernel: explicit inputs, or a ring of GuideSamples.
@@ -536,7 +579,20 @@ cudaError_t launch_train(const GuideDevice& g, const TrainSource& src, cudaStrea
 }  // namespace
 
 cudaError_t guide_configure() {
-    return cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmemBytes);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_guide_forward_x_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TcSmem));
+}
+
+cudaError_t guide_forward_features_tc(const GuideDevice& g, const float* x, int n, float* raw, int* error,
+                                      cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int tiles = (n + kTcRows - 1) / kTcRows;
+    const int grid = tiles < g.num_sms * 4 ? tiles : g.num_sms * 4;
+    k_guide_forward_x_tc<<<grid, kTcRows, sizeof(TcSmem), s>>>(g.wpack, x, n, raw, error);
+    return cudaGetLastError();
 }
 
 cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s) {

@@ -47,9 +47,10 @@ struct GuideRecord {
 static_assert(sizeof(GuideRecord) == 64, "GuideRecord layout");
 
 // 32-bit words of the packed weights: the shared-memory images of the forward weights (BF16
-// pairs of consecutive inputs, padded rows, FP32 biases; 9000 words) and of the transposed
-// backward weights (BF16 pairs of consecutive outputs, padded rows; 6912 words).
-constexpr int kGuidePackWords = 15912;
+// pairs of consecutive inputs, padded rows, FP32 biases; 9000 words), of the transposed
+// backward weights (BF16 pairs of consecutive outputs, padded rows; 6912 words) and of the
+// tensor-memory inference's K-major operand images (8192 words).
+constexpr int kGuidePackWords = 24104;
 
 // Opt the training kernel into its dynamic shared memory (once per device, before capture).
 cudaError_t guide_configure();
@@ -57,6 +58,10 @@ cudaError_t guide_configure();
 cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s);
 // Raw network outputs for n explicit input vectors (inference kernel, tensor cores).
 cudaError_t guide_forward_features(const GuideDevice& g, const float* x, int n, float* raw, cudaStream_t s);
+// The same on the 5th-generation tensor cores (tcgen05.mma into tensor memory); a wait that
+// gives up sets bit 1 of *error (device int).
+cudaError_t guide_forward_features_tc(const GuideDevice& g, const float* x, int n, float* raw, int* error,
+                                      cudaStream_t s);
 // Gradient of the batch loss -sum_i w_i log q(wi_i | x_i) / sum_i w_i with respect to all
 // parameters, for explicit input vectors (training kernel); grad is overwritten.
 cudaError_t guide_gradients_features(const GuideDevice& g, const float* x, const float* wi, const float* w, int n,

@@ -316,15 +316,23 @@ int Session::guide_forward(const float* x, int n, float* raw) {
     if ((r = ensure_guide())) return r;
     if (in_flight_ && (r = wait(nullptr))) return r;
     if (n == 0) return PT_OK;
-    if ((r = check_cuda(d_scratch_.alloc((size_t)n * (kGuideIn + kGuideOut) * 4), "scratch"))) return r;
+    if ((r = check_cuda(d_scratch_.alloc((size_t)n * (kGuideIn + kGuideOut) * 4 + 16), "scratch"))) return r;
     float* dx = d_scratch_.as<float>();
     float* dy = dx + (size_t)n * kGuideIn;
+    int* derr = reinterpret_cast<int*>(dy + (size_t)n * kGuideOut);
     if ((r = check_cuda(cudaMemcpyAsync(dx, x, (size_t)n * kGuideIn * 4, cudaMemcpyHostToDevice, stream_), "copy")))
         return r;
-    if ((r = check_cuda(guide_forward_features(guide_view(), dx, n, dy, stream_), "guide forward"))) return r;
+    if ((r = check_cuda(cudaMemsetAsync(derr, 0, sizeof(int), stream_), "copy"))) return r;
+    const cudaError_t e = guide_infer_tc_ ? guide_forward_features_tc(guide_view(), dx, n, dy, derr, stream_)
+                                          : guide_forward_features(guide_view(), dx, n, dy, stream_);
+    if ((r = check_cuda(e, "guide forward"))) return r;
     if ((r = check_cuda(cudaMemcpyAsync(raw, dy, (size_t)n * kGuideOut * 4, cudaMemcpyDeviceToHost, stream_), "copy")))
         return r;
-    return check_cuda(cudaStreamSynchronize(stream_), "guide forward");
+    int herr = 0;
+    if ((r = check_cuda(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, stream_), "copy"))) return r;
+    if ((r = check_cuda(cudaStreamSynchronize(stream_), "guide forward"))) return r;
+    if (herr) return fail(PT_ERR_DEVICE, "tensor-core inference: a wait for the MMA completion gave up");
+    return PT_OK;
 }
 
 int Session::guide_gradients(const float* x, const float* wi, const float* w, int n, float* grad) {
@@ -711,6 +719,7 @@ int Session::render_async(int spp) {
         const size_t rec_cap = tpaths * (size_t)std::max(1, p.max_depth - 1);
         if ((r = check_cuda(d_grec_.alloc(rec_cap * sizeof(GuideRecord)), "guide records"))) return r;
         p.guide_mode = guide_iters_ >= guide_warmup_ ? 2 : 1;
+        p.guide_tc = guide_infer_tc_ ? 1 : 0;
         p.gwpack = d_gwpack_.as<uint32_t>();
         p.gmix = d_gmix_.as<float>();
         p.gframe = gframe_;
@@ -855,6 +864,7 @@ int Session::finish_frame(float* ms) {
         marks_active_ = false;
     }
     if (last_stats_.error & 1) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");
+    if (last_stats_.error & 2) return fail(PT_ERR_DEVICE, "tensor-core inference: a wait for the MMA completion gave up");
     return PT_OK;
 }
 

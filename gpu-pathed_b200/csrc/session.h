@@ -255,6 +255,12 @@ public:
         return 0;
     }
     int guide_info(::pt_guide_info* out) const;
+    // guide inference on tcgen05 / TMEM (1) or on mma.sync (0)
+    int set_guide_inference(int tc) {
+        guide_infer_tc_ = tc != 0;
+        return PT_OK;
+    }
+    bool guide_infer_tc_ = false;
 
     // ---- batched frames (configuration 4): every scene rendered by one launch per stage ----
     int load_batch(const std::vector<BatchSpec>& specs);

@@ -24,6 +24,7 @@
 #include "dev_shade.cuh"
 #include "dev_trace.cuh"
 #include "guide_mlp.cuh"
+#include "guide_tc.cuh"
 
 #include <vector>
 
@@ -608,6 +609,45 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2) k_guide_infer(FrameParams
     }
 }
 
+// Guide inference on the 5th-generation tensor cores: tiles of 128 queue slots, one thread
+// per slot; the network runs as tcgen05.mma into tensor memory (guide_tc.cuh).
+__global__ void __launch_bounds__(kTcRows) k_guide_infer_tc(FrameParams p, int depth) {
+    extern __shared__ __align__(1024) uint8_t tsm[];
+    TcSmem& s = *reinterpret_cast<TcSmem*>(tsm);
+    const int count = p.counters->ray_count[depth];
+    const int tiles = (count + kTcRows - 1) / kTcRows;
+    if ((int)blockIdx.x >= tiles) return;  // no work: skip the setup and the TMEM allocation
+    const uint32_t tmem = tc_setup(s, p.gwpack, p.gwpack + kPackWords);
+    uint32_t phase = 0;
+    const PathQueue q = p.q[depth & 1];
+    const int t = threadIdx.x;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int slot = tile * kTcRows + t;
+        float x[kGuideIn];
+        if (slot < count) guide_features(p, p.gframe, q.o[slot], q.d[slot], q.hit[slot], x);
+        else
+            for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
+        tc_store_input(s.a, t, x);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        float raw[kGuideOut];
+        if (!tc_network(s, tmem, phase, raw)) {
+            if (t == 0) atomicOr(&p.stats->error, 2);
+            break;
+        }
+        if (slot < count) {
+            float mix[kGuideOut];
+            guide_activate(raw, mix);
+            float4* dst = reinterpret_cast<float4*>(p.gmix + (size_t)slot * kGuideOut);
+#pragma unroll
+            for (int j = 0; j < kGuideOut / 4; j++)
+                dst[j] = make_float4(mix[4 * j], mix[4 * j + 1], mix[4 * j + 2], mix[4 * j + 3]);
+        }
+    }
+    tc_teardown(tmem);
+}
+
 // Resolve this wave's training records into samples: the radiance that arrived along each
 // sampled direction is the path's later contributions (unweighted emission at the next
 // vertex, everything after it) divided by the throughput after the vertex.
@@ -730,7 +770,10 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                 mark(kStageSort);
             }
             if (p.guide_mode == 2 && d < p.max_depth - 1) {
-                k_guide_infer<B><<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
+                if (!B && p.guide_tc)
+                    k_guide_infer_tc<<<p.num_sms * 4, kTcRows, sizeof(TcSmem), stream>>>(p, d);
+                else
+                    k_guide_infer<B><<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
                 mark(kStageGuide);
             }
             if (p.guide_mode) k_shade<true, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
@@ -891,6 +934,8 @@ cudaError_t enqueue_batch_frame(const FrameParams& p, const WaveRange* waves, in
 cudaError_t configure_guide_infer() {
     cudaError_t e = cudaFuncSetAttribute(k_guide_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kInferSmemBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_guide_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_guide_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmemBytes);
 }

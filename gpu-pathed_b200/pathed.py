@@ -33,7 +33,7 @@ EXPORTED = [
     "pt_trace_rays_device", "pt_occluded", "pt_version", "pt_set_profiling", "pt_get_profile",
     "pt_trace_rays_static", "pt_autotune", "pt_guide_reset", "pt_set_consistent_mis", "pt_guide_get_info",
     "pt_guide_get_params", "pt_guide_set_params", "pt_guide_forward", "pt_guide_gradients", "pt_set_guide_options",
-    "pt_batch_generate", "pt_load_batch", "pt_batch_get_info", "pt_batch_readback",
+    "pt_batch_generate", "pt_load_batch", "pt_batch_get_info", "pt_batch_readback", "pt_set_guide_inference",
 ]
 
 GUIDE_PARAMS = 16104
@@ -384,6 +384,10 @@ class Session:
         g = GuideInfo()
         self._check(lib.pt_guide_get_info(self._h, C.byref(g)))
         return {k: getattr(g, k) for k, _ in GuideInfo._fields_}
+
+    def set_guide_inference(self, tc: bool):
+        """Guide inference on tcgen05 / tensor memory (True) or mma.sync (False)."""
+        self._check(lib.pt_set_guide_inference(self._h, int(bool(tc))))
 
     def guide_params(self) -> np.ndarray:
         out = np.empty(GUIDE_PARAMS, np.float32)

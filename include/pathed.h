@@ -227,6 +227,9 @@ int pt_guide_get_params(pt_session* s, float* out, int n);
 int pt_guide_set_params(pt_session* s, const float* in, int n);
 /* Raw outputs (n x 40) of the inference kernel for n explicit input vectors (n x 80). */
 int pt_guide_forward(pt_session* s, const float* x, int n, float* raw);
+/* Guide inference on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor
+ * memory; tc = 1) or on warp-level mma.sync (tc = 0, the default and the fallback). */
+int pt_set_guide_inference(pt_session* s, int tc);
 /* Gradient (16104 floats) of -sum w_i log q(wi_i | x_i) / sum w_i computed by the training
  * kernel for n explicit samples (x: n x 80, wi: n x 3 unit vectors, w: n weights). */
 int pt_guide_gradients(pt_session* s, const float* x, const float* wi, const float* w, int n, float* grad);

@@ -61,8 +61,10 @@ def test_oracle_gradient_matches_finite_differences(oracle_lib):
 
 
 @pytest.mark.gpu
-def test_inference_kernel_matches_oracle(oracle_lib):
+@pytest.mark.parametrize("tc", [False, True], ids=["mma.sync", "tcgen05"])
+def test_inference_kernel_matches_oracle(oracle_lib, tc):
     s = pathed.Session(8, 8)
+    s.set_guide_inference(tc)
     p = random_params(7)
     s.set_guide_params(p)
     x, _, _ = random_batch(1000, seed=8)
@@ -74,6 +76,21 @@ def test_inference_kernel_matches_oracle(oracle_lib):
     assert np.percentile(err, 99) <= 2e-2 * scale
     assert np.mean(err) <= 2e-3 * scale
     s.close()
+
+
+@pytest.mark.gpu
+def test_tensor_memory_inference_equals_mma_sync():
+    """both inference paths round the same operands: outputs agree to FP32 accumulation order"""
+    s = pathed.Session(8, 8)
+    s.set_guide_params(random_params(11))
+    x, _, _ = random_batch(5000, seed=12)  # 40 tiles of 128 (one partial)
+    a = s.guide_forward(x)
+    s.set_guide_inference(True)
+    b = s.guide_forward(x)
+    s.close()
+    scale = np.abs(a).max()
+    assert np.percentile(np.abs(a - b), 99.9) <= 1e-2 * scale
+    assert np.mean(np.abs(a - b)) <= 1e-4 * scale
 
 
 def _compare(g, ref):
@@ -125,7 +142,8 @@ def _slit_room(w, h):
 
 
 @pytest.mark.gpu
-def test_guided_estimator_is_unbiased():
+@pytest.mark.parametrize("tc", [False, True], ids=["mma.sync", "tcgen05"])
+def test_guided_estimator_is_unbiased(tc):
     """guided frames converge to the plain (consistent-MIS) image: image mean within 4 SE"""
     w = h = 48
     frames, spp = 24, 16
@@ -134,6 +152,7 @@ def test_guided_estimator_is_unbiased():
         s = _slit_room(w, h)
         s.set_consistent_mis(True)
         if guided:
+            s.set_guide_inference(tc)
             s.set_guiding(True)
             s.set_guide_options(steps_per_frame=4, warmup_steps=8)
         vals = []
