@@ -416,7 +416,7 @@ def run_ours(args):
     return 0
 
 
-def guided_time_to_relmse(budget_spp=128, ref_spp=2048, res=1024):
+def guided_time_to_relmse(budget_spp=256, ref_spp=2048, res=1024):
     """Plain vs guided on the slit room: device ms for the plain render to reach `budget_spp`
     and for the guided render (trained online from scratch) to reach the same relMSE,
     relMSE = mean((I - I_ref)^2 / (I_ref^2 + 1e-2)) against a `ref_spp` plain render."""

@@ -1104,7 +1104,7 @@ void oracle_guide_forward(const float* params, const float* x, int n, int quant,
     }
 }
 
-// Loss -sum w_i log q / sum w_i and its gradient (16104 values) in FP64 on the BF16-rounded
+// Loss -sum_i min(w_i / sum w, 500 / n) log q_i and its gradient (16104 values) in FP64 on the BF16-rounded
 // weights. quant = 1 also rounds every matrix-product operand to BF16 where the tensor-core
 // training kernel does: the inputs and activations X, A1..A3 and the back-propagated dY,
 // dZ3, dZ2, dZ1 (the ReLU masks use the unrounded activations). Inputs 78 and 79 are padding
@@ -1125,7 +1125,7 @@ double oracle_guide_grad(const float* params, const float* x, const float* wi, c
         forward(net, xi, quant != 0, a1, a2, a3, y);
         const double d[3] = {wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
         if (w[i] == 0) continue;
-        loss += loss_and_grad(y, d, w[i] * inv, dy);
+        loss += loss_and_grad(y, d, std::min(w[i] * inv, 500.0 / n), dy);  // per-sample weight cap
         double d3[H], d2[H], d1[H];
         for (int j = 0; j < OUT; j++) dy[j] = q(dy[j]);
         for (int k = 0; k < H; k++) {
@@ -1177,7 +1177,7 @@ double oracle_guide_loss_exact(const double* params, const float* x, const float
         forward(net, xi, false, a1, a2, a3, y);
         const double d[3] = {wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
         if (w[i] == 0) continue;
-        loss += loss_and_grad(y, d, w[i] / wsum, dy);
+        loss += loss_and_grad(y, d, std::min(w[i] / wsum, 500.0 / n), dy);
     }
     return loss;
 }
