@@ -610,8 +610,9 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2) k_guide_infer(FrameParams
 }
 
 // Guide inference on the 5th-generation tensor cores: tiles of 128 queue slots, one thread
-// per slot; the network runs as tcgen05.mma into tensor memory (guide_tc.cuh).
-__global__ void __launch_bounds__(kTcRows) k_guide_infer_tc(FrameParams p, int depth) {
+// per slot; the network runs as tcgen05.mma into tensor memory (guide_tc.cuh). 128 registers
+// keep 4 CTAs (512 slots) resident per SM.
+__global__ void __launch_bounds__(kTcRows, 4) k_guide_infer_tc(FrameParams p, int depth) {
     extern __shared__ __align__(1024) uint8_t tsm[];
     TcSmem& s = *reinterpret_cast<TcSmem*>(tsm);
     const int count = p.counters->ray_count[depth];
