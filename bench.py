@@ -255,6 +255,8 @@ def run_ours(args):
         s.set_guiding(True)
         spp = 0
     else:
+        if args.gpu_bvh:  # BVH built on the device (LBVH collapsed to the wide format)
+            s.set_bvh_builder(True)
         s.load_config(args.config)
         if args.guided:  # learned guiding on the main workload (trained online during warm-up)
             s.set_guiding(True)
@@ -393,7 +395,7 @@ def run_ours(args):
             "config": ({"workload": wl["name"], "resolution": [w, h], "spp": spp, "max_depth": wl["depth"],
                         "nee": True, "triangles": counts.num_triangles, "spheres": counts.num_spheres,
                         "bvh_width": counts.bvh_width, "parallelism": f"replicas{world}",
-                        "guided": bool(args.guided),
+                        "guided": bool(args.guided), "bvh_builder": "gpu-lbvh" if args.gpu_bvh else "host-sah",
                         "l2": "flushed between steps (256 MiB write)"} if not batch else
                        {"workload": wl["name"], "scenes": len(specs), "guided_scenes": sum(d["guided"] for d in specs),
                         "paths_per_frame": sum(d["width"] * d["height"] * d["spp"] for d in specs),
@@ -506,6 +508,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guiding", action="store_true")
     ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
+    ap.add_argument("--gpu-bvh", action="store_true", help="build the BVH on the GPU instead of the host")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

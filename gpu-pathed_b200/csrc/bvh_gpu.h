@@ -1,0 +1,28 @@
+// GPU construction of the wide BVH (bvh_gpu.cu): a Morton-order linear BVH collapsed to the
+// host builder's node format.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "devbuf.h"
+#include "pt_types.h"
+
+namespace pt {
+
+// Scratch buffers, kept between builds.
+struct GpuBvhScratch {
+    DevBuf box_lo, box_hi, cen, bounds, keys, ids, tree, nbox, visits, queue, counters, sort_tmp;
+};
+
+struct GpuBvhInfo {
+    int root = 0, num_nodes = 0, depth = 0, max_leaf = 0, width = 4;
+};
+
+// Build over nt triangles (3 float4 each: p0 p1 p2) and ns spheres (centre, radius) already on
+// the device: wide nodes into nodes_out, leaf entries (3 float4 each, Morton order) into
+// prims_out. Synchronises `st` once per tree level.
+cudaError_t gpu_build_bvh(const float4* tri_p, int nt, const float4* sph, int ns, int width, int max_leaf,
+                          GpuBvhScratch& scratch, DevBuf& nodes_out, DevBuf& prims_out, GpuBvhInfo& info,
+                          cudaStream_t st);
+
+}  // namespace pt

@@ -149,7 +149,8 @@ int pt_set_bvh(pt_session* s, int width, int max_leaf) {
 
 int pt_check_bvh(const pt_session* s) {
     if (!s) return PT_ERR_ARG;
-    return s->impl.check_bvh();
+    // a GPU-built tree is built (if still pending) and downloaded first: no visible state changes
+    return const_cast<pt_session*>(s)->impl.check_bvh();
 }
 
 int pt_set_camera(pt_session* s, const float origin[3], const float target[3], const float up[3], float vfov,
@@ -297,6 +298,11 @@ int pt_occluded(pt_session* s, const float* o, const float* d, const float* tmin
                 int* occluded) {
     if (!s) return PT_ERR_ARG;
     return guarded(s, [&] { return s->impl.occluded(o, d, tmin, tmax, n, occluded); });
+}
+
+int pt_set_bvh_builder(pt_session* s, int gpu) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.set_bvh_builder(gpu); });
 }
 
 int pt_batch_generate(unsigned long long seed, int n, pt_batch_scene* out) {

@@ -114,7 +114,9 @@ int Session::load_scene(HostScene&& s) {
     finalize_materials(s);
     if (!validate_scene(s, err)) return fail(PT_ERR_SCENE, err);
     BvhBuild b;
-    if (!build_bvh(s, bvh_width_, bvh_leaf_, b, err)) return fail(PT_ERR_SCENE, err);
+    b.width = bvh_width_;
+    if (!bvh_gpu_ && !build_bvh(s, bvh_width_, bvh_leaf_, b, err)) return fail(PT_ERR_SCENE, err);
+    if (bvh_gpu_ && s.num_tri() + s.num_sph() == 0) return fail(PT_ERR_SCENE, "scene has no primitives");
     scene_ = std::move(s);
     bvh_ = std::move(b);
     lights_ = build_light_list(scene_);
@@ -366,6 +368,12 @@ int Session::set_bvh(int width, int max_leaf) {
         const std::vector<BatchSpec> specs = batch_specs_;
         return load_batch(specs);
     }
+    if (bvh_gpu_) {  // rebuilt on the device at the next upload
+        bvh_ = BvhBuild();
+        bvh_.width = width;
+        scene_dirty_ = true;
+        return PT_OK;
+    }
     BvhBuild b;
     std::string err;
     if (!build_bvh(scene_, bvh_width_, bvh_leaf_, b, err)) return fail(PT_ERR_SCENE, err);
@@ -374,10 +382,35 @@ int Session::set_bvh(int width, int max_leaf) {
     return PT_OK;
 }
 
-int Session::check_bvh() const {
+int Session::set_bvh_builder(int gpu) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    const bool g = gpu != 0;
+    if (g == bvh_gpu_) return PT_OK;
+    bvh_gpu_ = g;
+    if (have_scene_ && !batch_mode()) return set_bvh(bvh_width_, bvh_leaf_);  // rebuild with the new builder
+    return PT_OK;
+}
+
+int Session::check_bvh() {
     if (!have_scene_) return PT_ERR_STATE;
     std::string err;
-    return pt::check_bvh(scene_, bvh_, err) ? PT_OK : PT_ERR_SCENE;
+    if (!bvh_gpu_ || batch_mode()) return pt::check_bvh(scene_, bvh_, err) ? PT_OK : fail(PT_ERR_SCENE, err);
+    // GPU-built tree: build it if still pending, bring it to the host, run the same check
+    int r;
+    if ((r = ensure_device())) return r;
+    if (scene_dirty_ && (r = upload_scene())) return r;
+    BvhBuild h = bvh_;
+    const size_t nb = (size_t)bvh_.num_nodes * (bvh_.width == 2 ? 64 : bvh_.width == 4 ? 128 : 256);
+    const int ne = scene_.num_tri() + scene_.num_sph();
+    h.nodes.resize(nb);
+    h.prims.resize((size_t)ne * 12);
+    if ((r = check_cuda(cudaMemcpy(h.nodes.data(), d_nodes_.p, nb, cudaMemcpyDeviceToHost), "BVH download"))) return r;
+    if ((r = check_cuda(cudaMemcpy(h.prims.data(), d_prims_.p, h.prims.size() * 4, cudaMemcpyDeviceToHost),
+                        "BVH download")))
+        return r;
+    h.prim_order.resize(ne);
+    for (int e = 0; e < ne; e++) std::memcpy(&h.prim_order[e], &h.prims[(size_t)e * 12 + 3], 4);
+    return pt::check_bvh(scene_, h, err) ? PT_OK : fail(PT_ERR_SCENE, err);
 }
 
 int Session::counts(pt_scene_counts* out) const {
@@ -542,8 +575,11 @@ int Session::upload_scene() {
                 tp[(size_t)i * 12 + v * 4 + k] = scene_.tri_p[(size_t)i * 9 + v * 3 + k];
                 tn[(size_t)i * 12 + v * 4 + k] = scene_.tri_n[(size_t)i * 9 + v * 3 + k];
             }
-    if ((r = check_cuda(upload(d_nodes_, bvh_.nodes, stream_), "upload BVH nodes"))) return r;
-    if ((r = check_cuda(upload(d_prims_, bvh_.prims, stream_), "upload BVH primitives"))) return r;
+    const bool gpu_tree = bvh_gpu_ && !batch_mode();
+    if (!gpu_tree) {
+        if ((r = check_cuda(upload(d_nodes_, bvh_.nodes, stream_), "upload BVH nodes"))) return r;
+        if ((r = check_cuda(upload(d_prims_, bvh_.prims, stream_), "upload BVH primitives"))) return r;
+    }
     if ((r = check_cuda(upload(d_tri_p_, tp, stream_), "upload triangles"))) return r;
     if ((r = check_cuda(upload(d_tri_n_, tn, stream_), "upload normals"))) return r;
     if ((r = check_cuda(upload(d_tri_mat_, scene_.tri_mat, stream_), "upload triangle materials"))) return r;
@@ -554,6 +590,29 @@ int Session::upload_scene() {
         if ((r = check_cuda(upload(d_env_marg_, env_cdf_.marg, stream_), "upload environment CDF"))) return r;
         if ((r = check_cuda(upload(d_env_cond_, env_cdf_.cond, stream_), "upload environment CDF"))) return r;
         if ((r = check_cuda(upload(d_env_row_, env_cdf_.row_mass, stream_), "upload environment CDF"))) return r;
+    }
+    if (gpu_tree) {  // the wide BVH built on the device from the uploaded primitives
+        cudaEvent_t e0, e1;
+        if ((r = check_cuda(cudaEventCreate(&e0), "cudaEventCreate"))) return r;
+        if ((r = check_cuda(cudaEventCreate(&e1), "cudaEventCreate"))) return r;
+        cudaEventRecord(e0, stream_);
+        GpuBvhInfo info;
+        const cudaError_t be = gpu_build_bvh(d_tri_p_.as<float4>(), nt, d_sph_.as<float4>(), scene_.num_sph(),
+                                             bvh_width_, bvh_leaf_, gbvh_, d_nodes_, d_prims_, info, stream_);
+        cudaEventRecord(e1, stream_);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if ((r = check_cuda(be, "GPU BVH build"))) return r;
+        bvh_ = BvhBuild();
+        bvh_.width = info.width;
+        bvh_.root = info.root;
+        bvh_.num_nodes = info.num_nodes;
+        bvh_.depth = info.depth;
+        bvh_.max_leaf = info.max_leaf;
+        bvh_.build_ms = ms;
     }
     // host vectors above must outlive the async copies
     if ((r = check_cuda(cudaStreamSynchronize(stream_), "scene upload"))) return r;

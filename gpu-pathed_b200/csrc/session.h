@@ -10,41 +10,13 @@
 
 #include "../../include/pathed.h"
 #include "bvh_build.h"
+#include "bvh_gpu.h"
+#include "devbuf.h"
 #include "host_scene.h"
 #include "host_util.h"
 #include "wavefront.h"
 
 namespace pt {
-
-struct DevBuf;
-template <class T>
-cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st);
-
-// Owning device allocation.
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    cudaError_t alloc(size_t n) {
-        if (n <= bytes && p) return cudaSuccess;
-        release();
-        if (n == 0) n = 16;
-        cudaError_t e = cudaMalloc(&p, n);
-        if (e == cudaSuccess) bytes = n;
-        else p = nullptr;
-        return e;
-    }
-    template <class T>
-    T* as() const { return static_cast<T*>(p); }
-};
 
 // Guide position-encoding frame from a scene's bounds.
 GuideFrame guide_frame_of(const HostScene& s);
@@ -88,7 +60,10 @@ public:
     int load_config(int config, uint64_t seed, int level);
     int load_scene(HostScene&& s);
     int set_bvh(int width, int max_leaf);
-    int check_bvh() const;
+    int check_bvh();
+    // 1: build the BVH on the GPU (Morton-order LBVH collapsed to the wide format) at the next
+    // upload; 0: the host's binned-SAH builder (default)
+    int set_bvh_builder(int gpu);
     int counts(::pt_scene_counts* out) const;
     int export_scene(::pt_scene_export* out) const;
 
@@ -216,6 +191,8 @@ private:
     uint64_t guide_seed_ = 0x9e11deULL;
     GuideFrame gframe_{};
     int ensure_guide();
+    bool bvh_gpu_ = false;
+    GpuBvhScratch gbvh_;
     int guide_nets_ = 1;
     int guide_ring_cap_ = 1 << 21;
     DevBuf d_gframes_;

@@ -34,6 +34,7 @@ EXPORTED = [
     "pt_trace_rays_static", "pt_autotune", "pt_guide_reset", "pt_set_consistent_mis", "pt_guide_get_info",
     "pt_guide_get_params", "pt_guide_set_params", "pt_guide_forward", "pt_guide_gradients", "pt_set_guide_options",
     "pt_batch_generate", "pt_load_batch", "pt_batch_get_info", "pt_batch_readback", "pt_set_guide_inference",
+    "pt_set_bvh_builder",
 ]
 
 GUIDE_PARAMS = 16104
@@ -433,6 +434,10 @@ class Session:
         fn = lib.pt_readback_pass if pass_only else lib.pt_readback
         self._check(fn(self._h, out.ctypes.data, out.size))
         return out
+
+    def set_bvh_builder(self, gpu: bool):
+        """Build the BVH on the GPU (LBVH collapsed to the wide format) or on the host (SAH)."""
+        self._check(lib.pt_set_bvh_builder(self._h, int(bool(gpu))))
 
     # ---- batched frames (configuration 4)
     def load_batch(self, scenes: list[dict]):

@@ -342,6 +342,14 @@ int pt_batch_get_info(const pt_session* s, int scene, pt_batch_info* out);
 /* Running mean (pass_only = 0) or last frame's pass of one scene: width * height * 3 floats. */
 int pt_batch_readback(pt_session* s, int scene, float* rgb, size_t n, int pass_only);
 
+/* BVH construction on the GPU (gpu = 1): primitive boxes, 63-bit Morton codes, radix sort,
+ * a Karras radix tree, bottom-up bounds and a top-down collapse to the same wide-node format,
+ * run when the scene is next uploaded (the first render or query after a load or edit).
+ * gpu = 0 (default) selects the host's binned-SAH builder. Closest hits are identical with
+ * either tree. No counterpart in the reference, whose CUDA backend scans every primitive
+ * (src/world.cu:5-41). Batches always use the host builder. */
+int pt_set_bvh_builder(pt_session* s, int gpu);
+
 /* Library version string. */
 const char* pt_version(void);
 
