@@ -305,6 +305,11 @@ int pt_set_bvh_builder(pt_session* s, int gpu) {
     return guarded(s, [&] { return s->impl.set_bvh_builder(gpu); });
 }
 
+int pt_set_renderer(pt_session* s, int kind) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.set_renderer(kind); });
+}
+
 int pt_batch_generate(unsigned long long seed, int n, pt_batch_scene* out) {
     if (n < 1 || n > pt::kMaxBatchScenes || !out) return PT_ERR_ARG;
     try {

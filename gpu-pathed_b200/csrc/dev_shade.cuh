@@ -349,15 +349,19 @@ __device__ __forceinline__ float balance(float p1, float p2) { return p1 / (p1 +
 // ---- Camera (include/core/camera.h:40-61) -------------------------------------------------
 __device__ __forceinline__ void camera_ray(const CameraParams& c, int row, int col, float xi1, float xi2, V& o,
                                            V& d) {
-    const float xc = (col + xi1) / c.res_x;
-    const float yc = (row + xi2) / c.res_y;
-    const float y = yc * c.height - c.top;
-    const float x = xc * c.width - c.right;
-    const V dir = normalized(mkv(x, y, -1.f));
+    // every operation rounded on its own, in the order written (no FMA contraction), so a
+    // camera ray is bit-identical to the one the reference's arithmetic gives on the host
+    const float xc = __fdiv_rn(__fadd_rn((float)col, xi1), (float)c.res_x);
+    const float yc = __fdiv_rn(__fadd_rn((float)row, xi2), (float)c.res_y);
+    const float y = __fsub_rn(__fmul_rn(yc, c.height), c.top);
+    const float x = __fsub_rn(__fmul_rn(xc, c.width), c.right);
+    const float len = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), 1.f));
+    const V dir = mkv(__fdiv_rn(x, len), __fdiv_rn(y, len), __fdiv_rn(-1.f, len));
+    // Transform::apply: the origin (0, 0, 0) maps to the translation column
     o = mkv(c.m[0][3], c.m[1][3], c.m[2][3]);
-    d = mkv(c.m[0][0] * dir.x + c.m[0][1] * dir.y + c.m[0][2] * dir.z,
-            c.m[1][0] * dir.x + c.m[1][1] * dir.y + c.m[1][2] * dir.z,
-            c.m[2][0] * dir.x + c.m[2][1] * dir.y + c.m[2][2] * dir.z);
+    d = mkv(__fadd_rn(__fadd_rn(__fmul_rn(c.m[0][0], dir.x), __fmul_rn(c.m[0][1], dir.y)), __fmul_rn(c.m[0][2], dir.z)),
+            __fadd_rn(__fadd_rn(__fmul_rn(c.m[1][0], dir.x), __fmul_rn(c.m[1][1], dir.y)), __fmul_rn(c.m[1][2], dir.z)),
+            __fadd_rn(__fadd_rn(__fmul_rn(c.m[2][0], dir.x), __fmul_rn(c.m[2][1], dir.y)), __fmul_rn(c.m[2][2], dir.z)));
 }
 
 // ---- sRGB (include/core/color.h:7-28) ---------------------------------------------------

@@ -80,7 +80,7 @@ class SceneModel {
 public:
     explicit SceneModel(Session* s) : s_(s) {}
 
-    RendererType getRendererType() const { return RendererType::CUDA; }
+    RendererType getRendererType() const { return renderer_; }
     void setRendererType(RendererType t);
     void setColor(float r, float g, float b);
     Vec3 getColor() const;
@@ -124,6 +124,7 @@ private:
     int material_id_ = -1;
     float light_position_ = -0.6f;  // scene.h:17 defaultLightPosition
     int spp_ = 0;
+    RendererType renderer_ = RendererType::CUDA;
 };
 
 class Session {
@@ -153,8 +154,11 @@ public:
     RenderState renderAsync() {
         require_init();
         if (in_flight_) throw std::runtime_error("a frame is already in flight");
-        frame_spp_ = optimizer_.estimate();
-        check(s_, pt_render_async(s_, frame_spp_));
+        const int spp = optimizer_.estimate();
+        check(s_, pt_render_async(s_, spp));
+        // the optimizer tracks the samples the frame rendered (RenderRecord::spp): one for
+        // the normals G-buffer (g_buffer.cu:116)
+        frame_spp_ = model_.getRendererType() == RendererType::Normals ? 1 : spp;
         in_flight_ = true;
         return RenderState{true, 0u};
     }
@@ -348,9 +352,14 @@ void SceneModel::set_camera(const float c[11]) {
     s_->edited();
 }
 
+// The renderer switch (render_session.cu:82-87, applied after the frame in flight,
+// render_session.h:102-112): the CUDA path tracer or the normals G-buffer; no OptiX backend.
 void SceneModel::setRendererType(RendererType t) {
-    if (t != RendererType::CUDA)
-        throw std::runtime_error("only the CUDA path-tracer backend is provided (no OptiX, no normals renderer)");
+    if (t == RendererType::Optix)
+        throw std::runtime_error("no OptiX backend: the CUDA path tracer and the normals renderer are provided");
+    s_->finish();
+    check(s_->handle(), pt_set_renderer(s_->handle(), t == RendererType::Normals ? 1 : 0));
+    renderer_ = t;
     s_->edited();
 }
 

@@ -521,6 +521,14 @@ int Session::set_max_depth(int d) {
     return PT_OK;
 }
 
+int Session::set_renderer(int kind) {
+    if (kind != 0 && kind != 1) return fail(PT_ERR_ARG, "renderer must be 0 (path tracer) or 1 (normals)");
+    if (kind == 1 && batch_mode()) return fail(PT_ERR_STATE, "the normals renderer takes a single scene");
+    if (kind != renderer_) reset();
+    renderer_ = kind;
+    return PT_OK;
+}
+
 int Session::set_nee(int on) {
     nee_ = on ? 1 : 0;
     reset();
@@ -702,6 +710,8 @@ int Session::render_async(int spp) {
     if (in_flight_) return fail(PT_ERR_STATE, "a frame is already in flight");
     const bool batch = batch_mode();
     if (batch) spp = 1;  // each scene of a batch renders its own spp
+    const bool normals = renderer_ == 1;
+    if (normals) spp = 1;  // GBuffer::renderAsync: one sample per frame (g_buffer.cu:97-116)
     if (spp < 1) return fail(PT_ERR_ARG, "spp must be >= 1");
     int r;
     if ((r = ensure_device())) return r;
@@ -761,11 +771,12 @@ int Session::render_async(int spp) {
     p.stack_depth = stack_depth;
     p.num_sms = num_sms_;
     p.count_work = work_counters_;
+    p.renderer = renderer_;
     p.shape = shape_;
     p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 3 ? 1 : 0);
     last_wave_paths_ = p.wave_pixels * spp;
     p.consistent_mis = consistent_mis_ || guiding_;
-    if (guiding_) {
+    if (guiding_ && !normals) {
         if ((r = ensure_guide())) return r;
         const size_t mix_bytes = (size_t)queue_cap_ * kGuideOut * sizeof(float);
         if ((r = check_cuda(d_gmix_.alloc(mix_bytes), "guide mixtures"))) return r;

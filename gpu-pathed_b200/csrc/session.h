@@ -73,6 +73,10 @@ public:
     int set_nee(int on);
     void set_seed(uint64_t s) { seed_ = s; reset(); }
     void reset() { reset_pending_ = true; }
+    // 0 path tracer, 1 normals G-buffer (one pixel-centre ray per pixel and frame); a change
+    // restarts accumulation, as RenderSession's renderer switch does
+    int set_renderer(int kind);
+    int renderer() const { return renderer_; }
     int set_launch(const ::pt_launch_config* c);
     void get_launch(::pt_launch_config* c) const;
 
@@ -156,6 +160,7 @@ private:
     // profiling
     int stage_timing_ = 0;
     int work_counters_ = 0;
+    int renderer_ = 0;
     std::vector<cudaEvent_t> mark_events_;
     std::vector<int> mark_stage_;
     StageMarks marks_{};

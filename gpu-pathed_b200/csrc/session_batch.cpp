@@ -25,6 +25,7 @@ void Session::clear_batch() {
 
 int Session::load_batch(const std::vector<BatchSpec>& specs) {
     if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    if (renderer_ != 0) return fail(PT_ERR_STATE, "batches render with the path tracer only");
     const int n = (int)specs.size();
     if (n < 1 || n > kMaxBatchScenes) return fail(PT_ERR_ARG, "a batch holds 1 to 64 scenes");
     long long paths = 0, pixels = 0;

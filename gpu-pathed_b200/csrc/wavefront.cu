@@ -798,6 +798,77 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
     return cudaSuccess;
 }
 
+// The hit record's normal (Triangle::hit's interpolated (1 - b1 - b2) n0 + b1 n1 + b2 n2,
+// triangle.h:51-56; Sphere::hit's normalized((point - center) / radius), sphere.cu:19-24)
+// with every operation rounded on its own, as the reference's arithmetic reads.
+__device__ __forceinline__ V hit_normal_rn(const SceneDevice& sc, V o, V d, const Hit& h) {
+    if (h.prim >= 0) {
+        const float w0 = __fsub_rn(__fsub_rn(1.f, h.b1), h.b2);
+        const V n0 = mkv(__ldg(sc.tri_n + 3 * h.prim + 0));
+        const V n1 = mkv(__ldg(sc.tri_n + 3 * h.prim + 1));
+        const V n2 = mkv(__ldg(sc.tri_n + 3 * h.prim + 2));
+        return V{__fadd_rn(__fadd_rn(__fmul_rn(w0, n0.x), __fmul_rn(h.b1, n1.x)), __fmul_rn(h.b2, n2.x)),
+                 __fadd_rn(__fadd_rn(__fmul_rn(w0, n0.y), __fmul_rn(h.b1, n1.y)), __fmul_rn(h.b2, n2.y)),
+                 __fadd_rn(__fadd_rn(__fmul_rn(w0, n0.z), __fmul_rn(h.b1, n1.z)), __fmul_rn(h.b2, n2.z))};
+    }
+    const float4 s = __ldg(sc.sph + ~h.prim);
+    const V q{__fdiv_rn(__fsub_rn(__fadd_rn(o.x, __fmul_rn(h.t, d.x)), s.x), s.w),
+              __fdiv_rn(__fsub_rn(__fadd_rn(o.y, __fmul_rn(h.t, d.y)), s.y), s.w),
+              __fdiv_rn(__fsub_rn(__fadd_rn(o.z, __fmul_rn(h.t, d.z)), s.z), s.w)};
+    const float len = __fsqrt_rn(xdot(q, q));
+    return V{__fdiv_rn(q.x, len), __fdiv_rn(q.y, len), __fdiv_rn(q.z, len)};
+}
+
+// Normals renderer (GBuffer with BufferType::Normals, src/renderers/g_buffer.cu:27-57): one
+// pixel-centre camera ray per pixel (Camera::generateRay(row, col), camera.cu:24-27), the
+// closest hit's (shading normal + 1) / 2, black on a miss; the accumulate kernel then treats
+// it as a 1-spp frame, as updateFramebuffer does for the reference.
+template <int W>
+__global__ void k_normals(FrameParams p, int first_pixel, int npix) {
+    extern __shared__ int2 stk[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < npix;  // every lane enters the warp-synchronous traversal
+    const int pixel = first_pixel + (valid ? i : 0);
+    const int row = pixel / p.width, col = pixel - row * p.width;
+    V o, d;
+    camera_ray(p.dyn->cam, row, col, 0.5f, 0.5f, o, d);
+    const RayPre r = make_raypre(o, d);
+    Hit h;
+    int of = 0;
+    traverse<W, false>(p.sc, r, kCameraTMin, FLT_MAX, valid, stk + threadIdx.x, blockDim.x, p.stack_depth, h, of);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_camera, (unsigned long long)npix);
+    if (!valid) return;
+    if (of) atomicOr(&p.stats->error, 1);
+    float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (h.prim != kMissPrim) {
+        const V n = hit_normal_rn(p.sc, o, d, h);
+        out = make_float4(__fdiv_rn(__fadd_rn(n.x, 1.f), 2.f), __fdiv_rn(__fadd_rn(n.y, 1.f), 2.f),
+                          __fdiv_rn(__fadd_rn(n.z, 1.f), 2.f), 0.f);
+    }
+    p.L[i] = out;
+}
+
+// Normals frame: waves of whole pixels, one pixel-centre ray each, then the accumulation.
+template <int W>
+cudaError_t enqueue_normals_w(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
+    const int npixels = p.width * p.height;
+    const int bs = p.shape.block_extend;  // the stack size the session configured covers this block
+    const size_t smem = stack_bytes(p.stack_depth, bs);
+    Marker mark{marks, stream};
+    mark(-1);
+    for (int first = 0; first < npixels; first += p.wave_pixels) {
+        const int npix = npixels - first < p.wave_pixels ? npixels - first : p.wave_pixels;
+        k_normals<W><<<(npix + bs - 1) / bs, bs, smem, stream>>>(p, first, npix);
+        mark(kStageExtend);
+        k_accumulate<false><<<(npix + 127) / 128, 128, 0, stream>>>(p, first, npix, (long long)first);
+        mark(kStageAccum);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (mark.err != cudaSuccess) return mark.err;
+    }
+    return cudaSuccess;
+}
+
 // Single-scene frame: waves of whole pixels, p.wave_pixels each.
 template <int W, bool CNT>
 cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
@@ -831,6 +902,7 @@ cudaError_t set_smem_w(size_t bytes) {
     if ((e = cudaFuncSetAttribute(k_extend<W, true, true>, a, b))) return e;
     if ((e = cudaFuncSetAttribute(k_shadow<W, false, true>, a, b))) return e;
     if ((e = cudaFuncSetAttribute(k_shadow<W, true, true>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_normals<W>, a, b))) return e;
     return cudaSuccess;
 }
 
@@ -908,6 +980,15 @@ __global__ void k_hit_test(SceneDevice sc, CameraParams cam, int stack_depth, in
 
 cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
     if (p.max_depth < 0 || p.max_depth > kMaxDepthLimit) return cudaErrorInvalidValue;
+    if (p.renderer == 1) {
+        if (p.spp != 1) return cudaErrorInvalidValue;
+        switch (p.sc.bvh_width) {
+            case 2: return enqueue_normals_w<2>(p, stream, marks);
+            case 4: return enqueue_normals_w<4>(p, stream, marks);
+            case 8: return enqueue_normals_w<8>(p, stream, marks);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     const bool cnt = p.count_work != 0;
     switch (p.sc.bvh_width) {
         case 2: return cnt ? enqueue_frame_w<2, true>(p, stream, marks) : enqueue_frame_w<2, false>(p, stream, marks);

@@ -148,6 +148,7 @@ struct FrameParams {
     int stack_depth;         // traversal stack entries per thread
     int num_sms;
     int count_work;          // 1: traversal kernels count nodes and leaf entries (slower)
+    int renderer;            // 0 path tracer, 1 normals (one pixel-centre ray per pixel, spp 1)
     LaunchShape shape;
     // ---- learned path guiding (guide.cuh) ----
     int guide_mode;          // 0 off, 1 collect training data only, 2 guided sampling + collect

@@ -35,6 +35,7 @@ EXPORTED = [
     "pt_guide_get_params", "pt_guide_set_params", "pt_guide_forward", "pt_guide_gradients", "pt_set_guide_options",
     "pt_batch_generate", "pt_load_batch", "pt_batch_get_info", "pt_batch_readback", "pt_set_guide_inference",
     "pt_set_bvh_builder",
+    "pt_set_renderer",
 ]
 
 GUIDE_PARAMS = 16104
@@ -155,7 +156,8 @@ def _load():
     lib.pt_trace_rays_static.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
     lib.pt_occluded.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
     lib.pt_hit_test.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
-    for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async"):
+    for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async",
+                 "pt_set_bvh_builder", "pt_set_renderer"):
         getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
     lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_set_profiling.argtypes = [C.c_void_p, C.c_int, C.c_int]
@@ -438,6 +440,10 @@ class Session:
     def set_bvh_builder(self, gpu: bool):
         """Build the BVH on the GPU (LBVH collapsed to the wide format) or on the host (SAH)."""
         self._check(lib.pt_set_bvh_builder(self._h, int(bool(gpu))))
+
+    def set_renderer(self, kind: int):
+        """0 the path tracer, 1 the normals G-buffer (one pixel-centre ray per pixel and frame)."""
+        self._check(lib.pt_set_renderer(self._h, int(kind)))
 
     # ---- batched frames (configuration 4)
     def load_batch(self, scenes: list[dict]):

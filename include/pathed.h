@@ -350,6 +350,15 @@ int pt_batch_readback(pt_session* s, int scene, float* rgb, size_t n, int pass_o
  * (src/world.cu:5-41). Batches always use the host builder. */
 int pt_set_bvh_builder(pt_session* s, int gpu);
 
+/* Renderer of the session's frames: 0 the path tracer (default), 1 the normals G-buffer.
+ * Replaces RenderSession's renderer switch (src/render_session.cu:79-87) to a
+ * GBuffer(BufferType::Normals) (src/renderers/g_buffer.cu:27-117): each frame traces one
+ * pixel-centre camera ray per pixel (Camera::generateRay(row, col)) and writes the closest
+ * hit's (normal + 1) / 2, black on a miss, as a 1-spp pass into the running mean, whatever
+ * spp pt_render_async asks for. A change restarts accumulation. Single scenes only
+ * (PT_ERR_STATE for a batch). */
+int pt_set_renderer(pt_session* s, int kind);
+
 /* Library version string. */
 const char* pt_version(void);
 

@@ -945,6 +945,23 @@ void oracle_light_sample(const Scene* s, const float* p, float x1, float x2, flo
                          ls.distance, ls.pdf, ls.emitted.x(), ls.emitted.y(), ls.emitted.z()};
     std::memcpy(out, v, sizeof(v));
 }
+// Normals G-buffer (src/renderers/g_buffer.cu:27-57): per pixel the pixel-centre camera ray
+// (Camera::generateRay(row, col), src/core/camera.cu:24-27), World::hit over [0, FLT_MAX],
+// and (normal + 1) / 2 of the closest hit, zero on a miss. out: width * height * 3 floats,
+// pixel = row * width + col.
+void oracle_normals(const Scene* s, const float* cam, int width, int height, float* out, int threads) {
+    Camera c;
+    c.init(cam, cam + 3, cam + 6, cam[9], cam[10] != 0.f, width, height);
+    parallel_for(width * height, threads, 64, [&](int i, int) {
+        const int row = i / width, col = i % width;
+        const Ray r = c.generate(row, col, 0.5f, 0.5f);
+        HitRecord rec;
+        Vec3 v(0.f, 0.f, 0.f);
+        if (worldHit(*s, r, 0.f, FLT_MAX, rec))
+            v = Vec3((rec.normal.e[0] + 1.f) / 2.f, (rec.normal.e[1] + 1.f) / 2.f, (rec.normal.e[2] + 1.f) / 2.f);
+        for (int k = 0; k < 3; k++) out[3 * (size_t)i + k] = v.e[k];
+    });
+}
 // out: o[3], d[3]
 void oracle_camera_ray(const float* cam, int width, int height, int row, int col, float x1, float x2, float* out) {
     Camera c;

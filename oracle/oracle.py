@@ -99,6 +99,7 @@ class Oracle(_SceneLib):
         L.oracle_light_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_void_p]
         L.oracle_camera_ray.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                         C.c_void_p]
+        L.oracle_normals.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]
         L.oracle_dist1d.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p]
         L.oracle_dist2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
@@ -158,6 +159,13 @@ class Oracle(_SceneLib):
                                var.ctypes.data, counts.ctypes.data, threads)
         return mean, var, counts
 
+    def normals(self, scene, camera, width, height, threads=0):
+        """normals G-buffer image, (height, width, 3), row 0 = camera row 0"""
+        out = np.empty((height, width, 3), np.float32)
+        cam = _f(camera)
+        self.lib.oracle_normals(scene.h, cam.ctypes.data, width, height, out.ctypes.data, threads)
+        return out
+
     def rng(self, seed, sample, pixel, n):
         out = np.empty(n, np.float32)
         self.lib.oracle_rng(seed, sample, pixel, n, out.ctypes.data)
@@ -186,6 +194,13 @@ class RefCPU(_SceneLib):
         L.ref_phitheta_pdf.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_int, C.c_void_p]
         L.ref_env_sample.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p]
+        L.ref_normals.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+
+    def normals(self, scene, camera, width, height):
+        out = np.empty((height, width, 3), np.float32)
+        cam = _f(camera)
+        self.lib.ref_normals(scene.h, cam.ctypes.data, width, height, out.ctypes.data)
+        return out
 
     def trace(self, scene, o, d, tmin, tmax):
         o, d = _f(o).reshape(-1, 3), _f(d).reshape(-1, 3)

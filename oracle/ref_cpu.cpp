@@ -217,6 +217,22 @@ void ref_camera_ray(const float* cam, int width, int height, int row, int col, f
     }
 }
 
+// The normals G-buffer's per-pixel value (g_buffer.cu:27-57) through the reference's own
+// Camera::generateRay(row, col) and World::hit. out: width * height * 3, pixel = row * width + col.
+void ref_normals(void* p, const float* cam, int width, int height, float* out) {
+    RefScene* s = static_cast<RefScene*>(p);
+    Camera c(Vec3(cam[0], cam[1], cam[2]), Vec3(cam[3], cam[4], cam[5]), Vec3(cam[6], cam[7], cam[8]), cam[9],
+             Resolution{width, height}, cam[10] != 0.f);
+    for (int row = 0; row < height; row++) {
+        for (int col = 0; col < width; col++) {
+            const Ray r = c.generateRay(row, col);
+            HitRecord rec;
+            const Vec3 v = s->world->hit(r, 0.f, FLT_MAX, rec) ? (rec.normal + 1.f) / 2.f : Vec3(0.f);
+            for (int k = 0; k < 3; k++) out[3 * ((size_t)row * width + col) + k] = v[k];
+        }
+    }
+}
+
 // DistributionParams / Distribution (distribution.h:11-65, distribution.cu:19-55)
 void ref_dist1d(const float* values, int n, const float* xis, int nxi, float* pmf_out, float* total_out, int* idx_out,
                 float* spmf_out) {

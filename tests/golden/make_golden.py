@@ -138,6 +138,8 @@ def main():
             L.ref_camera_ray(cam.ctypes.data, 64, 48, int(rc[k, 0]), int(rc[k, 1]), float(cx[k, 0]), float(cx[k, 1]),
                              cr[k].ctypes.data)
         out.update({f"s{cfg}_cam": cam, f"s{cfg}_cam_rc": rc, f"s{cfg}_cam_xi": cx, f"s{cfg}_cam_ray": cr})
+        # the normals G-buffer image (g_buffer.cu:27-57) at 64 x 48
+        out[f"s{cfg}_normals"] = ref.normals(rs, cam, 64, 48)
     # environment light on a small synthetic map (sample, pdf, emit)
     env = small_env()
     scene_env = {"tri_vertices": np.zeros((1, 9), np.float32), "tri_normals": np.zeros((1, 9), np.float32),

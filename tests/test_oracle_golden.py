@@ -119,6 +119,15 @@ def test_camera_rays(O, cfg):
     assert same(out, G[f"s{cfg}_cam_ray"])
 
 
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_normals_gbuffer(O, cfg):
+    """the normals renderer's image (g_buffer.cu:27-57): pixel-centre rays, (n + 1) / 2"""
+    sc, osc = _scene_from_golden(O, cfg)
+    img = O.normals(osc, G[f"s{cfg}_cam"], 64, 48)
+    assert same(img, G[f"s{cfg}_normals"])
+    assert (img == 0).all(-1).sum() < img.shape[0] * img.shape[1]  # not all misses
+
+
 def test_environment_samples(O):
     env = G["env_map"]
     sc = {"tri_vertices": np.zeros((1, 9), np.float32), "tri_normals": np.zeros((1, 9), np.float32),

@@ -54,6 +54,10 @@ def test_scene_model_host_state():
     ref.close()
     with pytest.raises(RuntimeError):
         m.setRendererType(ptm.RendererType.Optix)
+    m.setRendererType(ptm.RendererType.Normals)  # the G-buffer (g_buffer.cu)
+    assert m.getRendererType() == ptm.RendererType.Normals
+    m.setRendererType(ptm.RendererType.CUDA)
+    assert m.getRendererType() == ptm.RendererType.CUDA
     with pytest.raises(RuntimeError):
         s.renderAsync()  # init() first
     # scene selection beyond the reference's hard-coded scene 0
