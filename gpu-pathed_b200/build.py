@@ -24,7 +24,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["wavefront.cu", "guide.cu", "bvh_gpu.cu"]
-CPP_SOURCES = ["host_scene.cpp", "bvh_build.cpp", "host_util.cpp", "session.cpp", "session_batch.cpp", "capi.cpp"]
+CPP_SOURCES = ["host_scene.cpp", "bvh_build.cpp", "host_util.cpp", "assets.cpp", "session.cpp", "session_batch.cpp",
+               "capi.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] if os.path.isdir(CSRC) else []
 
 
@@ -77,7 +78,7 @@ def build(verbose: bool = False, clean: bool = False, ptxas_info: bool = False) 
                   "-I", os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o], verbose)
             relink = True
     if relink:
-        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs, "-lpthread"], verbose)
+        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs, "-lpthread", "-lz"], verbose)
     build_module(verbose, relink)
     return LIB
 

@@ -3,8 +3,10 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/pathed.h"
+#include "assets.h"
 #include "session.h"
 
 struct pt_session {
@@ -24,6 +26,23 @@ int guarded(pt_session* s, F&& f) {
     } catch (const std::exception& e) {
         return s ? s->impl.fail(PT_ERR_ARG, e.what()) : PT_ERR_ARG;
     }
+}
+// Material arrays of pt_scene_desc / pt_scene_request (absent arrays take defaults)
+std::vector<pt::Material> materials_of(int n, const int* types, const float* albedo, const float* emit,
+                                       const float* ior, const float* alpha) {
+    std::vector<pt::Material> mats((size_t)n);
+    for (int i = 0; i < n; i++) {
+        pt::Material& m = mats[i];
+        std::memset(&m, 0, sizeof(m));
+        m.type = types[i];
+        for (int k = 0; k < 3; k++) {
+            m.albedo[k] = albedo ? albedo[3 * i + k] : 0.f;
+            m.emit[k] = emit ? emit[3 * i + k] : 0.f;
+        }
+        m.ior = ior ? ior[i] : 1.f;
+        m.alpha = alpha ? alpha[i] : 0.1f;
+    }
+    return mats;
 }
 }  // namespace
 
@@ -108,18 +127,8 @@ int pt_load_arrays(pt_session* s, const pt_scene_desc* d) {
             sc.sph.assign(d->spheres, d->spheres + ns * 4);
             sc.sph_mat.assign(d->sphere_materials, d->sphere_materials + ns);
         }
-        sc.mats.resize(d->num_materials);
-        for (int i = 0; i < d->num_materials; i++) {
-            pt::Material& m = sc.mats[i];
-            std::memset(&m, 0, sizeof(m));
-            m.type = d->material_types[i];
-            for (int k = 0; k < 3; k++) {
-                m.albedo[k] = d->material_albedo ? d->material_albedo[3 * i + k] : 0.f;
-                m.emit[k] = d->material_emit ? d->material_emit[3 * i + k] : 0.f;
-            }
-            m.ior = d->material_ior ? d->material_ior[i] : 1.f;
-            m.alpha = d->material_alpha ? d->material_alpha[i] : 0.1f;
-        }
+        sc.mats = materials_of(d->num_materials, d->material_types, d->material_albedo, d->material_emit,
+                               d->material_ior, d->material_alpha);
         if (d->env_rgba) {
             if (d->env_width <= 0 || d->env_height <= 0)
                 return s->impl.fail(PT_ERR_ARG, "environment map size must be positive");
@@ -130,6 +139,71 @@ int pt_load_arrays(pt_session* s, const pt_scene_desc* d) {
         sc.name = "arrays";
         return s->impl.load_scene(std::move(sc));
     });
+}
+
+int pt_load_request(pt_session* s, const pt_scene_request* r) {
+    if (!s) return PT_ERR_ARG;
+    if (!r) return s->impl.fail(PT_ERR_ARG, "null scene request");
+    return guarded(s, [&]() -> int {
+        if (r->num_files < 0 || r->num_spheres < 0 || r->num_materials <= 0 || !r->material_types)
+            return s->impl.fail(PT_ERR_ARG, "negative counts or no materials");
+        if ((r->num_files > 0 && !r->files) || (r->num_spheres > 0 && (!r->spheres || !r->sphere_materials)))
+            return s->impl.fail(PT_ERR_ARG, "request arrays missing");
+        if (!r->camera) return s->impl.fail(PT_ERR_ARG, "a camera is required");
+        pt::SceneRequest q;
+        for (int i = 0; i < r->num_files; i++) {
+            if (!r->files[i].path) return s->impl.fail(PT_ERR_ARG, "mesh file without a path");
+            q.files.push_back({r->files[i].path, r->files[i].format, r->files[i].default_material});
+        }
+        q.mats = materials_of(r->num_materials, r->material_types, r->material_albedo, r->material_emit,
+                              r->material_ior, r->material_alpha);
+        q.sph.assign(r->spheres, r->spheres + 4 * (size_t)r->num_spheres);
+        q.sph_mat.assign(r->sphere_materials, r->sphere_materials + (size_t)r->num_spheres);
+        if (r->env_exr) q.env_path = r->env_exr;
+        pt::CameraSpec cam{};
+        for (int k = 0; k < 3; k++) {
+            cam.origin[k] = r->camera[k];
+            cam.target[k] = r->camera[3 + k];
+            cam.up[k] = r->camera[6 + k];
+        }
+        cam.vfov = r->camera[9];
+        cam.flip = r->camera[10] != 0.f;
+        return s->impl.load_request(q, cam);
+    });
+}
+
+int pt_load_reference_scene(pt_session* s, int index, const char* scenes_dir) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.load_reference_scene(index, scenes_dir ? scenes_dir : ""); });
+}
+
+int pt_read_exr(const char* path, int* width, int* height, float* rgba, size_t n) {
+    if (!path || !width || !height) {
+        g_create_error = "pt_read_exr: null argument";
+        return PT_ERR_ARG;
+    }
+    try {
+        std::vector<float> img;
+        std::string err;
+        int w = 0, h = 0;
+        if (!pt::read_exr(path, w, h, img, err)) {
+            g_create_error = err;
+            return PT_ERR_ARG;
+        }
+        *width = w;
+        *height = h;
+        if (rgba) {
+            if (n < img.size()) {
+                g_create_error = "pt_read_exr: destination holds fewer than width * height * 4 floats";
+                return PT_ERR_ARG;
+            }
+            std::memcpy(rgba, img.data(), img.size() * sizeof(float));
+        }
+        return PT_OK;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return PT_ERR_ARG;
+    }
 }
 
 int pt_scene_counts_get(const pt_session* s, pt_scene_counts* out) {

@@ -212,6 +212,13 @@ public:
         check(s_, pt_load_config(s_, config, seed));
         loaded();
     }
+    // SceneParameters::getSceneData(index) / getCamera(index) (scene.cu:14-218), which the
+    // reference's RenderSession constructor loads for index 0 from ../scenes
+    void loadReferenceScene(int index, const std::string& scenes_dir) {
+        finish();
+        check(s_, pt_load_reference_scene(s_, index, scenes_dir.c_str()));
+        loaded();
+    }
     void loadSceneArrays(py::array_t<float, py::array::c_style | py::array::forcecast> tri_vertices,
                          py::object tri_normals,
                          py::array_t<int, py::array::c_style | py::array::forcecast> tri_materials,
@@ -549,6 +556,8 @@ PYBIND11_MODULE(path_tracer, m) {
         .def("readback_rgba8", &Session::readbackRGBA8, "Display bytes, H x W x 4 (sRGB)")
         .def("load_scene", &Session::loadScene, py::arg("config_id"), py::arg("seed") = 0x5EEDULL,
              "Load generated configuration 0-3")
+        .def("load_reference_scene", &Session::loadReferenceScene, py::arg("index"), py::arg("scenes_dir"),
+             "Load the reference's built-in scene 0-3 (OBJ/MTL, PLY and EXR files of its scenes/ directory)")
         .def("load_scene_arrays", &Session::loadSceneArrays, py::arg("tri_vertices"), py::arg("tri_normals"),
              py::arg("tri_materials"), py::arg("spheres"), py::arg("sphere_materials"), py::arg("material_types"),
              py::arg("material_albedo"), py::arg("material_emit"), py::arg("material_ior"),

@@ -108,6 +108,33 @@ int Session::load_config(int config, uint64_t seed, int level) {
     return PT_OK;
 }
 
+int Session::load_request(const SceneRequest& r, const CameraSpec& cam) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    HostScene s;
+    std::string err;
+    if (!build_request(r, s, err)) return fail(PT_ERR_SCENE, err);
+    s.name = "request";
+    const int rc = load_scene(std::move(s));
+    if (rc) return rc;
+    camspec_ = cam;
+    return PT_OK;
+}
+
+int Session::load_reference_scene(int index, const std::string& scenes_dir) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    HostScene s;
+    std::string err;
+    if (index < 0 || index > 3) return fail(PT_ERR_ARG, "reference scene index must be 0-3");
+    if (!reference_scene(index, scenes_dir, s, err)) return fail(PT_ERR_SCENE, err);
+    const CameraSpec cam = s.camera;
+    const int rc = load_scene(std::move(s));
+    if (rc) return rc;
+    camspec_ = cam;
+    max_depth_ = scene_.default_depth;
+    nee_ = scene_.default_nee ? 1 : 0;
+    return PT_OK;
+}
+
 int Session::load_scene(HostScene&& s) {
     if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
     std::string err;

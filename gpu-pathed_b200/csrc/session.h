@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/pathed.h"
+#include "assets.h"
 #include "bvh_build.h"
 #include "bvh_gpu.h"
 #include "devbuf.h"
@@ -59,6 +60,11 @@ public:
     int set_device(int dev);
     int load_config(int config, uint64_t seed, int level);
     int load_scene(HostScene&& s);
+    // scene files (OBJ/MTL, PLY, EXR environment) with the given camera
+    int load_request(const SceneRequest& r, const CameraSpec& cam);
+    // the reference's built-in scene 0-3 from its scenes directory, with its camera and the
+    // reference's defaults (max depth 3, NEE on)
+    int load_reference_scene(int index, const std::string& scenes_dir);
     int set_bvh(int width, int max_leaf);
     int check_bvh();
     // 1: build the BVH on the GPU (Morton-order LBVH collapsed to the wide format) at the next

@@ -36,7 +36,12 @@ EXPORTED = [
     "pt_batch_generate", "pt_load_batch", "pt_batch_get_info", "pt_batch_readback", "pt_set_guide_inference",
     "pt_set_bvh_builder",
     "pt_set_renderer",
+    "pt_load_request",
+    "pt_load_reference_scene",
+    "pt_read_exr",
 ]
+
+MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
 
 GUIDE_PARAMS = 16104
 
@@ -59,6 +64,19 @@ class SceneDesc(C.Structure):
         ("material_albedo", C.c_void_p), ("material_emit", C.c_void_p), ("material_ior", C.c_void_p),
         ("material_alpha", C.c_void_p), ("env_width", C.c_int), ("env_height", C.c_int),
         ("env_rgba", C.c_void_p),
+    ]
+
+
+class MeshFile(C.Structure):
+    _fields_ = [("path", C.c_char_p), ("format", C.c_int), ("default_material", C.c_int)]
+
+
+class SceneRequest(C.Structure):
+    _fields_ = [
+        ("num_files", C.c_int), ("files", C.c_void_p), ("num_materials", C.c_int), ("material_types", C.c_void_p),
+        ("material_albedo", C.c_void_p), ("material_emit", C.c_void_p), ("material_ior", C.c_void_p),
+        ("material_alpha", C.c_void_p), ("num_spheres", C.c_int), ("spheres", C.c_void_p),
+        ("sphere_materials", C.c_void_p), ("env_exr", C.c_char_p), ("camera", C.c_void_p),
     ]
 
 
@@ -113,6 +131,20 @@ class BatchInfo(C.Structure):
 BATCH_FIELDS = ("config", "level", "seed", "width", "height", "spp", "max_depth", "guided")
 
 
+def read_exr(path) -> np.ndarray:
+    """OpenEXR image as (height, width, 4) float32 RGBA, rows top first (LoadEXR's layout)."""
+    w, h = C.c_int(), C.c_int()
+    p = os.fsencode(path)
+    rc = lib.pt_read_exr(p, C.byref(w), C.byref(h), None, 0)
+    if rc != 0:
+        raise PathedError(rc, lib.pt_last_error(None).decode())
+    out = np.empty((h.value, w.value, 4), np.float32)
+    rc = lib.pt_read_exr(p, C.byref(w), C.byref(h), out.ctypes.data, out.size)
+    if rc != 0:
+        raise PathedError(rc, lib.pt_last_error(None).decode())
+    return out
+
+
 def batch_generate(seed: int, n: int) -> list[dict]:
     """Configuration 4's seeded draw of n scenes (dicts of BATCH_FIELDS)."""
     arr = (BatchScene * n)()
@@ -156,6 +188,9 @@ def _load():
     lib.pt_trace_rays_static.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 5
     lib.pt_occluded.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
     lib.pt_hit_test.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
+    lib.pt_load_request.argtypes = [C.c_void_p, C.c_void_p]
+    lib.pt_load_reference_scene.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+    lib.pt_read_exr.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
     for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async",
                  "pt_set_bvh_builder", "pt_set_renderer"):
         getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
@@ -271,6 +306,44 @@ class Session:
             d.env_height, d.env_width = e.shape[0], e.shape[1]
             d.env_rgba = ep
         self._check(lib.pt_load_arrays(self._h, C.byref(d)))
+
+    def load_request(self, files, material_types, camera, material_albedo=None, material_emit=None,
+                     material_ior=None, material_alpha=None, spheres=None, sphere_materials=None, env_exr=None):
+        """Scene files (SceneAdapter::ParseRequest): `files` is a list of (path, MESH_OBJ |
+        MESH_PLY, default material id); camera = origin, target, up, vfov (radians), flip."""
+        keep = []
+
+        def f(a, dt=np.float32):
+            if a is None:
+                return None
+            arr = np.ascontiguousarray(np.asarray(a, dtype=dt))
+            keep.append(arr)
+            return arr
+
+        mf = (MeshFile * max(1, len(files)))()
+        for m, (path, fmt, mat) in zip(mf, files):
+            m.path, m.format, m.default_material = os.fsencode(path), int(fmt), int(mat)
+        r = SceneRequest()
+        r.num_files, r.files = len(files), C.cast(mf, C.c_void_p)
+        mt = f(material_types, np.int32)
+        r.num_materials, r.material_types = mt.size, mt.ctypes.data
+        for name, a in (("material_albedo", material_albedo), ("material_emit", material_emit),
+                        ("material_ior", material_ior), ("material_alpha", material_alpha)):
+            arr = f(a)
+            setattr(r, name, None if arr is None else arr.ctypes.data)
+        if spheres is not None:
+            sp, sm = f(spheres), f(sphere_materials, np.int32)
+            r.num_spheres, r.spheres, r.sphere_materials = sp.size // 4, sp.ctypes.data, sm.ctypes.data
+        r.env_exr = None if env_exr is None else os.fsencode(env_exr)
+        cam = f(camera)
+        if cam is None or cam.size != 11:
+            raise ValueError("camera needs 11 floats")
+        r.camera = cam.ctypes.data
+        self._check(lib.pt_load_request(self._h, C.byref(r)))
+
+    def load_reference_scene(self, index: int, scenes_dir: str):
+        """The reference's built-in scene 0-3, read from its scenes/ directory."""
+        self._check(lib.pt_load_reference_scene(self._h, int(index), os.fsencode(scenes_dir)))
 
     def counts(self) -> SceneCounts:
         c = SceneCounts()

@@ -173,6 +173,56 @@ int pt_load_config(pt_session* s, int config, uint64_t seed);
 /* Same with an explicit icosphere level for configurations 2 and 3 (smaller test scenes). */
 int pt_load_config_level(pt_session* s, int config, uint64_t seed, int icosphere_level);
 int pt_load_arrays(pt_session* s, const pt_scene_desc* desc);
+
+/* Mesh files of a scene request (ObjParser / PLYParser, src/parsers/). */
+#define PT_MESH_OBJ 0 /* OBJ with an optional MTL library: faces "a b c d" (two triangles,
+                         geometric normal), "v/t/n v/t/n v/t/n" and "v//n v//n v//n"; other face
+                         forms are skipped, as by the reference's parser */
+#define PT_MESH_PLY 1 /* binary little-endian PLY, float x y z, a vertex_indices list */
+typedef struct pt_mesh_file {
+    const char* path;
+    int format;            /* PT_MESH_OBJ or PT_MESH_PLY */
+    int default_material;  /* material of faces without MTL materials */
+} pt_mesh_file;
+
+/* SceneAdapter::ParseRequest (include/scene_data.h) plus the camera. Triangles of OBJ files
+ * come first, then PLY files', in request order; an OBJ's MTL materials are appended as
+ * Lambertians (Kd albedo, Ke emission) after the request's own materials, ordered by name. */
+typedef struct pt_scene_request {
+    int num_files;
+    const pt_mesh_file* files;
+    int num_materials;           /* material arrays as in pt_scene_desc */
+    const int* material_types;
+    const float* material_albedo;
+    const float* material_emit;
+    const float* material_ior;
+    const float* material_alpha;
+    int num_spheres;
+    const float* spheres;        /* 4 floats per sphere: cx, cy, cz, radius */
+    const int* sphere_materials;
+    const char* env_exr;         /* OpenEXR environment map (EnvironmentLightParams), or NULL */
+    const float* camera;         /* 11 floats: origin[3], target[3], up[3], vfov (radians), flip */
+} pt_scene_request;
+
+/* Replaces SceneAdapter::createSceneData (src/scene_data.cu:9-118) fed by the reference's
+ * parsers: loads the request's files into the session. PT_ERR_SCENE with pt_last_error naming
+ * the file and line for a file that cannot be read or parsed. */
+int pt_load_request(pt_session* s, const pt_scene_request* request);
+
+/* The reference's built-in scene `index` (SceneParameters::getSceneData / getCamera,
+ * src/scene.cu:14-218; RenderSession loads index 0, render_session.cu:68-72): 0 Cornell box,
+ * 1 glossy Cornell box with a mirror box and a glass ball, 2 plane under the 1-pixel test
+ * environment, 3 the MIS plates under an HDR environment. `scenes_dir` is the reference's
+ * scenes/ directory (its files are read from there); max depth 3 and NEE on, as Scene's
+ * defaults (include/scene.h:17-29). */
+int pt_load_reference_scene(pt_session* s, int index, const char* scenes_dir);
+
+/* LoadEXR (the reference's environment-map reader, src/lights/environment_light.cu:20-31):
+ * width x height RGBA floats, rows top first. Single-part scanline files with NONE, RLE,
+ * ZIPS, ZIP or PIZ compression and HALF or FLOAT channels; R, G and B are required (A defaults
+ * to 1), a single channel fills all four. rgba NULL returns only the size; otherwise n must be
+ * at least width * height * 4. Errors are reported through pt_last_error(NULL). */
+int pt_read_exr(const char* path, int* width, int* height, float* rgba, size_t n);
 int pt_scene_counts_get(const pt_session* s, pt_scene_counts* out);
 int pt_export_scene(const pt_session* s, pt_scene_export* out);
 /* Rebuild the BVH with a given width (2, 4, 8) and maximum leaf size (1..16). */

@@ -24,7 +24,8 @@ def build(ref: bool = True) -> None:
     exists (on a machine without it, the prebuilt _ref/ libraries are used as they are)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref and os.path.isdir(REF_TREE):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "refbench", f"REF={REF_TREE}"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "refbench", "refassets", f"REF={REF_TREE}"],
+                       check=True)
 
 
 def _f(a):
@@ -213,6 +214,48 @@ class RefCPU(_SceneLib):
                            out["prim_type"].ctypes.data, out["prim_id"].ctypes.data, out["mat_id"].ctypes.data,
                            out["t"].ctypes.data)
         return out
+
+
+REF_ASSETS_LIB = os.path.join(HERE, "_ref", "libref_assets.so")
+
+
+class RefAssets:
+    """The reference's OBJ/MTL/PLY parsers and its vendored LoadEXR, compiled for the host."""
+
+    def __init__(self, path=REF_ASSETS_LIB):
+        self.lib = L = C.CDLL(path)
+        L.ref_mesh_parse.restype = C.c_void_p
+        L.ref_mesh_parse.argtypes = [C.c_char_p, C.c_int]
+        for name in ("ref_mesh_faces", "ref_mesh_mtls"):
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.ref_mesh_copy.argtypes = [C.c_void_p] * 5
+        L.ref_mesh_free.argtypes = [C.c_void_p]
+        L.ref_exr_load.restype = C.c_void_p
+        L.ref_exr_load.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.ref_exr_free.argtypes = [C.c_void_p]
+
+    def mesh(self, path, ply=False) -> dict:
+        """faces as p (n, 9), n (n, 9), per-face MTL index, MTL table (m, 6: Kd, Ke)"""
+        h = self.lib.ref_mesh_parse(os.fsencode(path), int(ply))
+        try:
+            nf, nm = self.lib.ref_mesh_faces(h), self.lib.ref_mesh_mtls(h)
+            out = {"p": np.empty((nf, 9), np.float32), "n": np.empty((nf, 9), np.float32),
+                   "mtl": np.empty(nf, np.int32), "mtls": np.empty((nm, 6), np.float32)}
+            self.lib.ref_mesh_copy(h, out["p"].ctypes.data, out["n"].ctypes.data, out["mtl"].ctypes.data,
+                                   out["mtls"].ctypes.data)
+            return out
+        finally:
+            self.lib.ref_mesh_free(h)
+
+    def exr(self, path) -> np.ndarray:
+        w, h, code = C.c_int(), C.c_int(), C.c_int()
+        p = self.lib.ref_exr_load(os.fsencode(path), C.byref(w), C.byref(h), C.byref(code))
+        if not p:
+            raise RuntimeError(f"LoadEXR failed with {code.value}")
+        try:
+            return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_float)), (h.value, w.value, 4)).copy()
+        finally:
+            self.lib.ref_exr_free(p)
 
 
 REFBENCH_LIB = os.path.join(HERE, "_ref", "librefbench.so")
