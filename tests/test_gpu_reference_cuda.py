@@ -129,3 +129,54 @@ def test_image_means_vs_reference_cuda(case):
     assert abs(ma.mean() - mb.mean()) <= 4 * se + 1e-6
     rb.close()
     s.close()
+
+
+REF_SCENES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "_reference_scenes.npz")
+SCENE_FIELDS = ("tri_vertices", "tri_normals", "tri_materials", "spheres", "sphere_materials", "material_types",
+                "material_albedo", "material_emit", "material_ior", "material_alpha", "env_rgba")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF_SCENES), reason="tests/golden/make_reference_scenes.py not run")
+@pytest.mark.parametrize("idx", [0, 1, 2, 3])
+def test_reference_scenes_vs_reference_cuda(idx):
+    """The reference's own scenes 0-3 (its OBJ/MTL, PLY and EXR files through the asset loaders),
+    ours against the reference's CUDA integrator: per-pixel means within 3 combined SE."""
+    g = np.load(REF_SCENES)
+    sc = {k: g[f"s{idx}_{k}"] for k in SCENE_FIELDS + ("camera",)}
+    if sc["env_rgba"].size == 0:
+        sc["env_rgba"] = None
+    depth = int(g[f"s{idx}_depth"])
+    w, h = 96, 72
+    frames, spp = 12, 64
+    s = pathed.Session(w, h)
+    s.load_arrays(**{k: sc[k] for k in SCENE_FIELDS})
+    cam = sc["camera"]
+    s.set_camera(cam[0:3], cam[3:6], cam[6:9], float(cam[9]), bool(cam[10]))
+    s.set_max_depth(depth)
+    ours = []
+    for _ in range(frames):
+        s.render(spp)
+        ours.append(s.readback(pass_only=True).reshape(-1, 3).astype(np.float64))
+    ours = np.stack(ours)
+    rb = orc.RefBench()
+    rb.load(sc, w, h)
+    ref, prev = [], np.zeros((w * h, 3))
+    for k in range(frames):
+        rb.render(spp, depth, True)
+        m = rb.readback().reshape(-1, 3).astype(np.float64)
+        ref.append(m * (k + 1) - prev * k)
+        prev = m
+    ref = np.stack(ref)
+    se_a = ours.std(0, ddof=1) / np.sqrt(frames)
+    se_b = ref.std(0, ddof=1) / np.sqrt(frames)
+    frac = three_se_pass(ours.mean(0), se_a, ref.mean(0), se_b, floor=1e-5)
+    ma, mb = ours.mean(axis=(1, 2)), ref.mean(axis=(1, 2))
+    se = np.sqrt(ma.var(ddof=1) / frames + mb.var(ddof=1) / frames)
+    print(f"reference scene {idx}: 3-SE pass {frac:.4f}, image mean ours {ma.mean():.5f} "
+          f"reference {mb.mean():.5f} (SE {se:.5f})")
+    assert ma.mean() > 0
+    assert frac >= 0.95
+    assert abs(ma.mean() - mb.mean()) <= 4 * se + 1e-6
+    rb.close()
+    s.close()
