@@ -990,6 +990,119 @@ bool read_exr(const std::string& path, int& width, int& height, std::vector<floa
     return true;
 }
 
+namespace {
+
+// FP32 -> FP16: mantissa truncated to 10 bits, plus one when the first dropped bit is set;
+// FP32 denormals become zero, exponents past the half range infinity, NaN a quiet NaN.
+uint16_t half_of(float f) {
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    const uint32_t sign = x >> 31, ex = (x >> 23) & 0xff, man = x & 0x7fffff;
+    uint32_t o = 0;
+    if (ex == 0) {
+        o = 0;
+    } else if (ex == 0xff) {
+        o = (31u << 10) | (man ? 0x200u : 0u);
+    } else {
+        const int ne = (int)ex - 127 + 15;
+        if (ne >= 31) {
+            o = 31u << 10;
+        } else if (ne <= 0) {
+            if (14 - ne <= 24) {
+                const uint32_t m = man | 0x800000u;
+                o = m >> (14 - ne);
+                if ((m >> (13 - ne)) & 1u) o++;
+            }
+        } else {
+            o = ((uint32_t)ne << 10) | (man >> 13);
+            if (man & 0x1000u) o++;
+        }
+    }
+    return (uint16_t)((sign << 15) | o);
+}
+
+void put32(std::string& s, uint32_t v) {
+    for (int k = 0; k < 4; k++) s.push_back((char)((v >> (8 * k)) & 0xff));
+}
+
+void attribute(std::string& s, const char* name, const char* type, const std::string& value) {
+    s.append(name).push_back('\0');
+    s.append(type).push_back('\0');
+    put32(s, (uint32_t)value.size());
+    s.append(value);
+}
+
+}  // namespace
+
+bool write_exr(const std::string& path, int width, int height, const float* rgb, std::string& err) {
+    if (width <= 0 || height <= 0 || !rgb) {
+        err = "write_exr: empty image";
+        return false;
+    }
+    std::string head;
+    put32(head, 20000630u);
+    put32(head, 2u);
+    std::string chl;
+    for (const char* c : {"B", "G", "R"}) {
+        chl.append(c).push_back('\0');
+        put32(chl, 1u);  // HALF
+        put32(chl, 0u);  // pLinear + reserved
+        put32(chl, 1u);
+        put32(chl, 1u);
+    }
+    chl.push_back('\0');
+    std::string box;
+    for (uint32_t v : {0u, 0u, (uint32_t)(width - 1), (uint32_t)(height - 1)}) put32(box, v);
+    // pixelAspectRatio 1; screenWindowWidth holds the image width, as the vendored writer does
+    const float one = 1.f, fw = (float)width;
+    uint32_t onebits, wbits;
+    std::memcpy(&onebits, &one, 4);
+    std::memcpy(&wbits, &fw, 4);
+    std::string f1, v2, sww;
+    put32(f1, onebits);
+    put32(sww, wbits);
+    put32(v2, 0u);
+    put32(v2, 0u);
+    attribute(head, "channels", "chlist", chl);
+    attribute(head, "compression", "compression", std::string(1, '\0'));
+    attribute(head, "dataWindow", "box2i", box);
+    attribute(head, "displayWindow", "box2i", box);
+    attribute(head, "lineOrder", "lineOrder", std::string(1, '\0'));
+    attribute(head, "pixelAspectRatio", "float", f1);
+    attribute(head, "screenWindowCenter", "v2f", v2);
+    attribute(head, "screenWindowWidth", "float", sww);
+    head.push_back('\0');
+    const size_t row_bytes = (size_t)width * 2 * 3;
+    const size_t chunk = 8 + row_bytes;
+    std::string out = head;
+    uint64_t off = head.size() + 8ull * height;
+    for (int y = 0; y < height; y++, off += chunk) {
+        put32(out, (uint32_t)(off & 0xffffffffu));
+        put32(out, (uint32_t)(off >> 32));
+    }
+    std::string line(row_bytes, '\0');
+    for (int y = 0; y < height; y++) {
+        put32(out, (uint32_t)y);
+        put32(out, (uint32_t)row_bytes);
+        const int row = height - 1 - y;  // file row y holds image row height - 1 - y
+        for (int c = 0; c < 3; c++) {      // B, G, R
+            const int k = 2 - c;
+            for (int x = 0; x < width; x++) {
+                const uint16_t h = half_of(rgb[3 * ((size_t)row * width + x) + k]);
+                line[((size_t)c * width + x) * 2] = (char)(h & 0xff);
+                line[((size_t)c * width + x) * 2 + 1] = (char)(h >> 8);
+            }
+        }
+        out += line;
+    }
+    std::ofstream f(path, std::ios::binary);
+    if (!f || !f.write(out.data(), (std::streamsize)out.size())) {
+        err = "cannot write " + path;
+        return false;
+    }
+    return true;
+}
+
 // ---- scenes ----------------------------------------------------------------------------
 
 bool build_request(const SceneRequest& req, HostScene& out, std::string& err) {

@@ -44,6 +44,11 @@ bool parse_ply(const std::string& path, MeshFaces& out, std::string& err);
 // channels are required (A defaults to 1); a single-channel image is replicated into all four.
 bool read_exr(const std::string& path, int& width, int& height, std::vector<float>& rgba, std::string& err);
 
+// Image::save (src/io/image.cpp:9-78): an uncompressed scanline EXR of HALF channels B, G, R
+// from `rgb` (3 floats per pixel, row 0 = the image bottom, written last). Halves round as
+// the writer the reference vendors does: to nearest, ties away from zero, overflow to inf.
+bool write_exr(const std::string& path, int width, int height, const float* rgb, std::string& err);
+
 constexpr int kMeshObj = 0;
 constexpr int kMeshPly = 1;
 

@@ -206,6 +206,38 @@ int pt_read_exr(const char* path, int* width, int* height, float* rgba, size_t n
     }
 }
 
+int pt_save_exr(pt_session* s, const char* path) {
+    if (!s) return PT_ERR_ARG;
+    if (!path) return s->impl.fail(PT_ERR_ARG, "null path");
+    return guarded(s, [&]() -> int {
+        const int w = s->impl.width(), h = s->impl.height();
+        std::vector<float> rgb((size_t)w * h * 3);
+        const int r = s->impl.readback(rgb.data(), rgb.size(), false);
+        if (r) return r;
+        std::string err;
+        if (!pt::write_exr(path, w, h, rgb.data(), err)) return s->impl.fail(PT_ERR_ARG, err);
+        return PT_OK;
+    });
+}
+
+int pt_write_exr(const char* path, int width, int height, const float* rgb) {
+    if (!path || !rgb || width <= 0 || height <= 0) {
+        g_create_error = "pt_write_exr: bad argument";
+        return PT_ERR_ARG;
+    }
+    try {
+        std::string err;
+        if (!pt::write_exr(path, width, height, rgb, err)) {
+            g_create_error = err;
+            return PT_ERR_ARG;
+        }
+        return PT_OK;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return PT_ERR_ARG;
+    }
+}
+
 int pt_scene_counts_get(const pt_session* s, pt_scene_counts* out) {
     if (!s || !out) return PT_ERR_ARG;
     return s->impl.counts(out);

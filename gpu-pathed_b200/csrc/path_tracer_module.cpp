@@ -176,9 +176,16 @@ public:
             int spp = 0;
             check(s_, pt_get_spp(s_, &spp));
             model_.updateSpp(spp);
+            snapshot(spp);
         }
         return RenderState{!done, 0u};
     }
+
+    // pollRender's snapshot (render_session.h:87-101): the radiance buffer as EXR whenever
+    // the accumulated spp crosses a power of two from 2 to 2^20. The reference always writes
+    // out.exr in its working directory; here it is off until a path is set ("" turns it off).
+    void setSnapshotPath(const std::string& path) { snapshot_ = path; }
+    std::string getSnapshotPath() const { return snapshot_; }
 
     // RenderSession::hitTest (render_session.h:54-56, hit_test.cu:25-82)
     void hitTest(int x, int y) {
@@ -289,6 +296,17 @@ public:
             model_.updateSpp(spp);
         }
     }
+    void snapshot(int spp) {
+        if (snapshot_.empty()) return;
+        for (int t = 2; t <= (1 << 20); t <<= 1)
+            if (spp >= t && spp - frame_spp_ < t) {
+                check(s_, pt_save_exr(s_, snapshot_.c_str()));
+                snapshots_++;
+                break;
+            }
+    }
+    int snapshots_ = 0;
+    std::string snapshot_;
     int max_depth_ = 5;
     bool nee_ = true;
     int num_materials_ = 0;
@@ -365,7 +383,7 @@ void SceneModel::setRendererType(RendererType t) {
     if (t == RendererType::Optix)
         throw std::runtime_error("no OptiX backend: the CUDA path tracer and the normals renderer are provided");
     s_->finish();
-    check(s_->handle(), pt_set_renderer(s_->handle(), t == RendererType::Normals ? 1 : 0));
+    check(s_->handle(), pt_set_renderer(s_->handle(), t == RendererType::Normals ? PT_RENDERER_NORMALS : PT_RENDERER_CUDA));
     renderer_ = t;
     s_->edited();
 }
@@ -556,6 +574,10 @@ PYBIND11_MODULE(path_tracer, m) {
         .def("readback_rgba8", &Session::readbackRGBA8, "Display bytes, H x W x 4 (sRGB)")
         .def("load_scene", &Session::loadScene, py::arg("config_id"), py::arg("seed") = 0x5EEDULL,
              "Load generated configuration 0-3")
+        .def("setSnapshotPath", &Session::setSnapshotPath, py::arg("path"),
+             "Write the radiance buffer as EXR at every power-of-two spp (render_session.h:87-101); '' = off")
+        .def("getSnapshotPath", &Session::getSnapshotPath)
+        .def_readonly("snapshots", &Session::snapshots_)
         .def("load_reference_scene", &Session::loadReferenceScene, py::arg("index"), py::arg("scenes_dir"),
              "Load the reference's built-in scene 0-3 (OBJ/MTL, PLY and EXR files of its scenes/ directory)")
         .def("load_scene_arrays", &Session::loadSceneArrays, py::arg("tri_vertices"), py::arg("tri_normals"),

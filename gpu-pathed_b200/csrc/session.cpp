@@ -548,8 +548,10 @@ int Session::set_max_depth(int d) {
     return PT_OK;
 }
 
-int Session::set_renderer(int kind) {
-    if (kind != 0 && kind != 1) return fail(PT_ERR_ARG, "renderer must be 0 (path tracer) or 1 (normals)");
+int Session::set_renderer(int type) {
+    if (type != PT_RENDERER_CUDA && type != PT_RENDERER_NORMALS)
+        return fail(PT_ERR_ARG, "renderer must be PT_RENDERER_CUDA or PT_RENDERER_NORMALS (no OptiX backend)");
+    const int kind = type == PT_RENDERER_NORMALS ? 1 : 0;
     if (kind == 1 && batch_mode()) return fail(PT_ERR_STATE, "the normals renderer takes a single scene");
     if (kind != renderer_) reset();
     renderer_ = kind;

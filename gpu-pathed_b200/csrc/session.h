@@ -79,9 +79,9 @@ public:
     int set_nee(int on);
     void set_seed(uint64_t s) { seed_ = s; reset(); }
     void reset() { reset_pending_ = true; }
-    // 0 path tracer, 1 normals G-buffer (one pixel-centre ray per pixel and frame); a change
-    // restarts accumulation, as RenderSession's renderer switch does
-    int set_renderer(int kind);
+    // PT_RENDERER_CUDA (path tracer) or PT_RENDERER_NORMALS (G-buffer: one pixel-centre ray
+    // per pixel and frame); a change restarts accumulation, as RenderSession's switch does
+    int set_renderer(int type);
     int renderer() const { return renderer_; }
     int set_launch(const ::pt_launch_config* c);
     void get_launch(::pt_launch_config* c) const;

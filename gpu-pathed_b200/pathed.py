@@ -39,9 +39,12 @@ EXPORTED = [
     "pt_load_request",
     "pt_load_reference_scene",
     "pt_read_exr",
+    "pt_save_exr",
+    "pt_write_exr",
 ]
 
 MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
+RENDERER_CUDA, RENDERER_OPTIX, RENDERER_NORMALS = 0, 1, 2  # PT_RENDERER_*
 
 GUIDE_PARAMS = 16104
 
@@ -145,6 +148,15 @@ def read_exr(path) -> np.ndarray:
     return out
 
 
+def write_exr(path, rgb: np.ndarray):
+    """(height, width, 3) radiances, row 0 = image bottom, written as the reference's
+    Image::save writes them (HALF B, G, R, top row first)."""
+    a = np.ascontiguousarray(rgb, np.float32)
+    rc = lib.pt_write_exr(os.fsencode(path), a.shape[1], a.shape[0], a.ctypes.data)
+    if rc != 0:
+        raise PathedError(rc, lib.pt_last_error(None).decode())
+
+
 def batch_generate(seed: int, n: int) -> list[dict]:
     """Configuration 4's seeded draw of n scenes (dicts of BATCH_FIELDS)."""
     arr = (BatchScene * n)()
@@ -190,6 +202,8 @@ def _load():
     lib.pt_hit_test.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
     lib.pt_load_request.argtypes = [C.c_void_p, C.c_void_p]
     lib.pt_load_reference_scene.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+    lib.pt_save_exr.argtypes = [C.c_void_p, C.c_char_p]
+    lib.pt_write_exr.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
     lib.pt_read_exr.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
     for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async",
                  "pt_set_bvh_builder", "pt_set_renderer"):
@@ -340,6 +354,10 @@ class Session:
             raise ValueError("camera needs 11 floats")
         r.camera = cam.ctypes.data
         self._check(lib.pt_load_request(self._h, C.byref(r)))
+
+    def save_exr(self, path):
+        """The accumulated radiance as the reference's Image::save writes it (HALF B, G, R)."""
+        self._check(lib.pt_save_exr(self._h, os.fsencode(path)))
 
     def load_reference_scene(self, index: int, scenes_dir: str):
         """The reference's built-in scene 0-3, read from its scenes/ directory."""
@@ -515,7 +533,8 @@ class Session:
         self._check(lib.pt_set_bvh_builder(self._h, int(bool(gpu))))
 
     def set_renderer(self, kind: int):
-        """0 the path tracer, 1 the normals G-buffer (one pixel-centre ray per pixel and frame)."""
+        """RENDERER_CUDA (the path tracer) or RENDERER_NORMALS (the normals G-buffer: one
+        pixel-centre ray per pixel and frame)."""
         self._check(lib.pt_set_renderer(self._h, int(kind)))
 
     # ---- batched frames (configuration 4)

@@ -42,7 +42,8 @@ extern "C" {
 #define PT_GLASS 2
 #define PT_MICROFACET 3
 
-/* Renderer types (include/scene_model.h:16-20). Only PT_RENDERER_CUDA is built. */
+/* Renderer types (include/scene_model.h:16-20) for pt_set_renderer. CUDA (the path tracer)
+ * and NORMALS (the G-buffer) are built; there is no OptiX backend. */
 #define PT_RENDERER_CUDA 0
 #define PT_RENDERER_OPTIX 1
 #define PT_RENDERER_NORMALS 2
@@ -223,6 +224,14 @@ int pt_load_reference_scene(pt_session* s, int index, const char* scenes_dir);
  * to 1), a single channel fills all four. rgba NULL returns only the size; otherwise n must be
  * at least width * height * 4. Errors are reported through pt_last_error(NULL). */
 int pt_read_exr(const char* path, int* width, int* height, float* rgba, size_t n);
+
+/* Image::save (src/io/image.cpp:9-78) of the accumulated radiance, as RenderSession::pollRender
+ * writes out.exr at every power-of-two spp (include/render_session.h:87-101): an uncompressed
+ * EXR of HALF channels B, G, R with the image's top row first. Waits for a frame in flight. */
+int pt_save_exr(pt_session* s, const char* path);
+/* The same file from caller radiances: rgb holds width * height * 3 floats, row 0 = the image
+ * bottom (the layout of pt_readback). Errors through pt_last_error(NULL). */
+int pt_write_exr(const char* path, int width, int height, const float* rgb);
 int pt_scene_counts_get(const pt_session* s, pt_scene_counts* out);
 int pt_export_scene(const pt_session* s, pt_scene_export* out);
 /* Rebuild the BVH with a given width (2, 4, 8) and maximum leaf size (1..16). */
@@ -400,7 +409,8 @@ int pt_batch_readback(pt_session* s, int scene, float* rgb, size_t n, int pass_o
  * (src/world.cu:5-41). Batches always use the host builder. */
 int pt_set_bvh_builder(pt_session* s, int gpu);
 
-/* Renderer of the session's frames: 0 the path tracer (default), 1 the normals G-buffer.
+/* Renderer of the session's frames: PT_RENDERER_CUDA, the path tracer (default), or
+ * PT_RENDERER_NORMALS, the normals G-buffer (PT_ERR_ARG for PT_RENDERER_OPTIX).
  * Replaces RenderSession's renderer switch (src/render_session.cu:79-87) to a
  * GBuffer(BufferType::Normals) (src/renderers/g_buffer.cu:27-117): each frame traces one
  * pixel-centre camera ray per pixel (Camera::generateRay(row, col)) and writes the closest

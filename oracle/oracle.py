@@ -233,6 +233,12 @@ class RefAssets:
         L.ref_exr_load.restype = C.c_void_p
         L.ref_exr_load.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.ref_exr_free.argtypes = [C.c_void_p]
+        L.ref_image_save.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_char_p]
+
+    def image_save(self, path, rgb):
+        """Image::save of (height, width, 3) radiances, row 0 = image bottom"""
+        a = np.ascontiguousarray(rgb, np.float32)
+        self.lib.ref_image_save(a.shape[1], a.shape[0], a.ctypes.data, os.fsencode(path))
 
     def mesh(self, path, ply=False) -> dict:
         """faces as p (n, 9), n (n, 9), per-face MTL index, MTL table (m, 6: Kd, Ke)"""

@@ -2,18 +2,17 @@
 //
 // C entry points over the reference's own scene-file readers, compiled for the host from the
 // reference sources in place (oracle/Makefile, target refassets): ObjParser + MtlParser
-// (src/parsers/obj_parser.cpp, mtl_parser.cpp), PLYParser (src/parsers/ply_parser.cpp) and
-// LoadEXR from the reference's vendored tinyexr (vendor/tinyexr.h, as src/io/image.cpp
-// instantiates it). Tests compare the product's loaders with these, file by file.
+// (src/parsers/obj_parser.cpp, mtl_parser.cpp), PLYParser (src/parsers/ply_parser.cpp),
+// Image::save (src/io/image.cpp, which instantiates the vendored tinyexr) and tinyexr's
+// LoadEXR. Tests compare the product's loaders and writer with these, file by file.
 #include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
+#include "io/image.h"
 #include "parsers/obj_parser.h"
 #include "parsers/ply_parser.h"
-
-#define TINYEXR_IMPLEMENTATION
 #include "tinyexr.h"
 
 using namespace rays;
@@ -93,5 +92,11 @@ float* ref_exr_load(const char* path, int* width, int* height, int* code) {
 }
 
 void ref_exr_free(float* p) { std::free(p); }
+
+// Image::save(width, height, radiances, filename): rgb row 0 = image bottom
+void ref_image_save(int width, int height, const float* rgb, const char* path) {
+    const std::vector<float> r(rgb, rgb + (size_t)width * height * 3);
+    Image::save(width, height, r, path);
+}
 
 }  // extern "C"

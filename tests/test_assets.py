@@ -341,3 +341,71 @@ def test_module_loads_reference_scene():
     assert (o.x(), o.y(), o.z()) == (0.0, 1.0, np.float32(6.8))
     with pytest.raises(RuntimeError):
         s.load_reference_scene(4, SCENES)
+
+
+def _exr_specials():
+    # rounding ties (away from zero in the vendored writer), half subnormals, overflow, inf, NaN
+    return np.array([0, -0.0, 1e-8, 6e-8, 3e-5, 65504, 65519, 65520, 1e6, -2.5, np.inf, np.nan,
+                     1 + 2 ** -11, 1 + 3 * 2 ** -11, 2 ** -24 * 1.5, 2 ** -14 * (1 + 2 ** -11)], np.float32)
+
+
+@needs_ref
+@pytest.mark.parametrize("shape", [(7, 11), (64, 96), (1, 1), (300, 17)])
+def test_exr_writer_matches_image_save(tmp_path, shape):
+    """pt_write_exr writes the same bytes as the reference's Image::save (src/io/image.cpp)"""
+    rng = np.random.default_rng(shape[0])
+    rgb = rng.lognormal(0, 3, shape + (3,)).astype(np.float32)
+    sp = _exr_specials()
+    rgb.reshape(-1)[:min(sp.size, rgb.size)] = sp[:rgb.size]
+    pathed.write_exr(tmp_path / "ours.exr", rgb)
+    orc.RefAssets().image_save(tmp_path / "ref.exr", rgb)
+    assert (tmp_path / "ours.exr").read_bytes() == (tmp_path / "ref.exr").read_bytes()
+
+
+def test_exr_writer_round_trip(tmp_path):
+    rng = np.random.default_rng(5)
+    rgb = rng.lognormal(0, 2, (13, 9, 3)).astype(np.float32)
+    # move exact half-way values off the tie (the writer rounds ties away from zero, numpy to
+    # even; ties are pinned byte for byte against Image::save above)
+    tie = (rgb.view(np.uint32) & 0x1FFF) == 0x1000
+    rgb[tie] = np.nextafter(rgb[tie], np.float32(np.inf))
+    pathed.write_exr(tmp_path / "a.exr", rgb)
+    img = pathed.read_exr(tmp_path / "a.exr")
+    assert img.shape == (13, 9, 4) and np.all(img[..., 3] == 1)
+    # HALF channels, top row first: the buffer's row 0 (image bottom) is the file's last row
+    assert np.array_equal(img[::-1, :, :3], rgb.astype(np.float16).astype(np.float32))
+    with pytest.raises(pathed.PathedError):
+        pathed.write_exr(tmp_path / "missing_dir" / "a.exr", rgb)
+
+
+@pytest.mark.gpu
+def test_snapshots_at_powers_of_two(tmp_path):
+    """RenderSession's out.exr at every power-of-two spp (render_session.h:87-101)"""
+    import path_tracer as ptm
+
+    rs = ptm.RenderSession(48, 32)
+    rs.init()
+    path = str(tmp_path / "out.exr")
+    rs.setSnapshotPath(path)
+    spp, written = [], []
+    for _ in range(6):
+        rs.renderAsync()
+        while rs.pollRender().isRendering:
+            pass
+        spp.append(rs.getSceneModel().getSpp())
+        written.append(rs.snapshots)
+    crossings = sum(any(s >= t > p for t in (2 ** k for k in range(1, 21))) for p, s in zip([0] + spp, spp))
+    assert written[-1] == crossings and crossings >= 1
+    # the last snapshot holds the radiance buffer of the frame that crossed a threshold
+    last = max(i for i in range(len(spp)) if written[i] > (written[i - 1] if i else 0))
+    if last == len(spp) - 1:
+        img = pathed.read_exr(path)
+        want = rs.getRadianceBuffer().astype(np.float16).astype(np.float32)
+        assert np.allclose(img[::-1, :, :3], want, rtol=1e-3, atol=0)
+    rs.setSnapshotPath("")
+    s = pathed.Session(32, 24)
+    s.load_config(0)
+    s.render(4)
+    s.save_exr(tmp_path / "s.exr")
+    assert np.allclose(pathed.read_exr(tmp_path / "s.exr")[::-1, :, :3], s.readback(), rtol=1e-3)
+    s.close()

@@ -26,14 +26,14 @@ def _session(config, level, w, h, width=4, leaf=4):
 def test_renderer_switch_host_rules():
     s = _session(0, None, 32, 32)
     with pytest.raises(pathed.PathedError):
-        s.set_renderer(2)
-    s.set_renderer(1)
+        s.set_renderer(pathed.RENDERER_OPTIX)
+    s.set_renderer(pathed.RENDERER_NORMALS)
     with pytest.raises(pathed.PathedError):  # batches render with the path tracer only
         s.load_batch([dict(config=0, level=-1, seed=1, width=32, height=32, spp=1, max_depth=3, guided=0)])
-    s.set_renderer(0)
+    s.set_renderer(pathed.RENDERER_CUDA)
     s.load_batch([dict(config=0, level=-1, seed=1, width=32, height=32, spp=1, max_depth=3, guided=0)])
     with pytest.raises(pathed.PathedError):
-        s.set_renderer(1)
+        s.set_renderer(pathed.RENDERER_NORMALS)
     s.close()
 
 
@@ -54,7 +54,7 @@ def test_normals_match_golden_image(cfg):
     g = np.load(os.path.join(HERE, "golden", "reference_vectors.npz"))
     s = _session(cfg, None, 64, 48)
     assert np.array_equal(s.export_scene()["camera"], g[f"s{cfg}_cam"])
-    s.set_renderer(1)
+    s.set_renderer(pathed.RENDERER_NORMALS)
     s.render(1)
     _compare(s.readback(), g[f"s{cfg}_normals"])
     s.close()
@@ -68,7 +68,7 @@ def test_normals_match_oracle_on_meshes(config, level, width, leaf):
     sc = s.export_scene()
     O = orc.Oracle()
     ref = O.normals(O.scene(sc), sc["camera"], w, h)
-    s.set_renderer(1)
+    s.set_renderer(pathed.RENDERER_NORMALS)
     s.render(1)
     err = _compare(s.readback(), ref)
     print(f"config {config} level {level}: max |GPU - oracle| {err:.2e}")
@@ -78,7 +78,7 @@ def test_normals_match_oracle_on_meshes(config, level, width, leaf):
 @pytest.mark.gpu
 def test_normals_frames_accumulate_one_sample_each():
     s = _session(3, 3, 128, 128)
-    s.set_renderer(1)
+    s.set_renderer(pathed.RENDERER_NORMALS)
     s.render(16)  # the G-buffer renders one sample whatever is asked
     first = s.readback().copy()
     assert s.spp() == 1
@@ -89,7 +89,7 @@ def test_normals_frames_accumulate_one_sample_each():
     st = s.stats()
     assert st["rays_camera"] == 128 * 128 and st["rays_shadow"] == 0
     # back to the path tracer: accumulation restarts
-    s.set_renderer(0)
+    s.set_renderer(pathed.RENDERER_CUDA)
     s.render(4)
     assert s.spp() == 4
     img = s.readback()
@@ -113,7 +113,7 @@ def test_module_normals_renderer():
             pass
         assert m.getSpp() == k + 1
     ref = _session(0, None, w, h)
-    ref.set_renderer(1)
+    ref.set_renderer(pathed.RENDERER_NORMALS)
     ref.render(1)
     assert float(np.abs(rs.getRadianceBuffer() - ref.readback()).max()) <= 1e-6
     ref.close()
