@@ -418,50 +418,74 @@ def run_ours(args):
     return 0
 
 
-def guided_time_to_relmse(budget_spp=256, ref_spp=2048, res=1024):
-    """Plain vs guided on the slit room: device ms for the plain render to reach `budget_spp`
-    and for the guided render (trained online from scratch) to reach the same relMSE,
-    relMSE = mean((I - I_ref)^2 / (I_ref^2 + 1e-2)) against a `ref_spp` plain render."""
-    import numpy as np
-
+def _slit_session(res):
     import pathed
 
-    def session():
-        s = pathed.Session(res, res)
-        s.load_config(3)
-        s.set_consistent_mis(True)
-        return s
+    s = pathed.Session(res, res)
+    s.load_config(3)
+    s.set_consistent_mis(True)
+    return s
 
-    r = session()
+
+def _relmse(s, ref, den):
+    import numpy as np
+
+    return float(np.mean((s.readback().astype(np.float64) - ref) ** 2 / den))
+
+
+def slit_reference(ref_spp=2048, res=1024):
+    """Plain render of the slit room at `ref_spp` (seed 12345): the relMSE reference."""
+    import numpy as np
+
+    r = _slit_session(res)
     r.set_seed(12345)
     for _ in range(ref_spp // 64):
         r.render(64)
     ref = r.readback().astype(np.float64)
     r.close()
+    return ref
+
+
+def plain_to_budget(ref, budget_spp=256, res=1024):
+    """Device ms of `budget_spp` 1-spp plain frames and the relMSE they reach."""
     den = ref ** 2 + 1e-2
-
-    def relmse(s):
-        return float(np.mean((s.readback().astype(np.float64) - ref) ** 2 / den))
-
-    p = session()
+    p = _slit_session(res)
     p.set_seed(77)
     p.render(1)
     p.reset()
     t_plain = sum(p.render(1) for _ in range(budget_spp))
-    target = relmse(p)
+    target = _relmse(p, ref, den)
     p.close()
+    return t_plain, target
 
-    g = session()
-    g.set_seed(77)
+
+def guided_to_target(ref, t_plain, target, res=1024, fraction=None, steps=None, warmup=None, lr=None,
+                     schedule=None, seed=77):
+    """Device ms for the guided render, trained online from scratch inside the timed 1-spp
+    frames, to reach `target` relMSE (crossing interpolated in log relMSE between checks).
+    `schedule(frame)`, when given, sets the Adam steps of each frame."""
+    import numpy as np
+
+    den = ref ** 2 + 1e-2
+    g = _slit_session(res)
+    g.set_seed(seed)
     g.set_guiding(True)
+    if fraction is not None:
+        g.set_guide_fraction(fraction)
+    if steps is not None or warmup is not None or lr is not None:
+        g.set_guide_options(steps_per_frame=-1 if steps is None else steps, lr=0.0 if lr is None else lr,
+                            warmup_steps=-1 if warmup is None else warmup)
     t_guided, spp, prev, crossed = 0.0, 0, None, None
     while t_guided < 3 * t_plain:
+        if schedule is not None:
+            st = schedule(spp)
+            st, rate = st if isinstance(st, tuple) else (st, 0.0)
+            g.set_guide_options(steps_per_frame=int(st), lr=float(rate))
         t_guided += g.render(1)
         spp += 1
         if spp >= 16 and spp % 4 == 0:
-            e = relmse(g)
+            e = _relmse(g, ref, den)
             if e <= target:
-                # interpolate the crossing in log relMSE between the last two checks
                 if prev is not None:
                     (t0, e0) = prev
                     f = (np.log(e0) - np.log(target)) / max(1e-12, np.log(e0) - np.log(e))
@@ -472,11 +496,20 @@ def guided_time_to_relmse(budget_spp=256, ref_spp=2048, res=1024):
             prev = (t_guided, e)
     info = g.guide_info()
     g.close()
+    return crossed, (spp if crossed is not None else None), info["steps"]
+
+
+def guided_time_to_relmse(budget_spp=256, ref_spp=2048, res=1024):
+    """Plain vs guided on the slit room: device ms for the plain render to reach `budget_spp`
+    and for the guided render (trained online from scratch) to reach the same relMSE,
+    relMSE = mean((I - I_ref)^2 / (I_ref^2 + 1e-2)) against a `ref_spp` plain render."""
+    ref = slit_reference(ref_spp, res)
+    t_plain, target = plain_to_budget(ref, budget_spp, res)
+    crossed, spp, steps = guided_to_target(ref, t_plain, target, res)
     return {"workload": f"slit-room {res}x{res} depth 10 (2002 + 1310720 triangles, env through a 0.05 slit)",
             "reference": f"plain render, {ref_spp} spp, consistent MIS", "plain_spp": budget_spp,
             "plain_ms": t_plain, "target_relmse": target, "guided_ms": crossed,
-            "guided_spp": spp if crossed is not None else None,
-            "speedup": (t_plain / crossed) if crossed else None, "guide_steps": info["steps"],
+            "guided_spp": spp, "speedup": (t_plain / crossed) if crossed else None, "guide_steps": steps,
             "training": "online from scratch inside the timed frames (automatic Adam schedule)"}
 
 

@@ -319,6 +319,11 @@ int pt_guide_forward(pt_session* s, const float* x, int n, float* raw) {
     if (!s || (n > 0 && (!x || !raw))) return PT_ERR_ARG;
     return guarded(s, [&] { return s->impl.guide_forward(x, n, raw); });
 }
+int pt_set_guide_fraction(pt_session* s, float fraction) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.set_guide_fraction(fraction);
+}
+
 int pt_set_guide_inference(pt_session* s, int tc) {
     if (!s) return PT_ERR_ARG;
     return s->impl.set_guide_inference(tc);

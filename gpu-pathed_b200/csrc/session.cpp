@@ -819,6 +819,7 @@ int Session::render_async(int spp) {
         if ((r = check_cuda(d_grec_.alloc(rec_cap * sizeof(GuideRecord)), "guide records"))) return r;
         p.guide_mode = guide_iters_ >= guide_warmup_ ? 2 : 1;
         p.guide_tc = guide_infer_tc_ ? 1 : 0;
+        p.gfrac = guide_frac_;
         p.gwpack = d_gwpack_.as<uint32_t>();
         p.gmix = d_gmix_.as<float>();
         p.gframe = gframe_;
@@ -833,7 +834,7 @@ int Session::render_async(int spp) {
         p.gnets = guide_nets_;
         // Adam steps this frame: automatic schedule (many while the network is young) unless set
         p.gtrain_steps = guide_steps_per_frame_ > 0 ? guide_steps_per_frame_
-                         : guide_iters_ < 256      ? 8
+                         : guide_iters_ < 512      ? 16
                          : guide_iters_ < 1024     ? 4
                                                    : 2;
         p.gtrain_batch = guide_batch_;

@@ -198,7 +198,7 @@ private:
     int guide_warmup_ = 4;      // steps before the guide is used for sampling
     int guide_batch_ = 1 << 16;      // samples per Adam step
     int guide_steps_per_frame_ = 0;  // 0: automatic schedule
-    float guide_lr_ = 1e-3f;
+    float guide_lr_ = 3e-3f;
     uint64_t guide_seed_ = 0x9e11deULL;
     GuideFrame gframe_{};
     int ensure_guide();
@@ -249,6 +249,13 @@ public:
         return PT_OK;
     }
     bool guide_infer_tc_ = false;
+    // probability of sampling the guide at a non-delta vertex (one-sample MIS), in (0, 1)
+    int set_guide_fraction(float f) {
+        if (!(f > 0.f && f < 1.f)) return fail(PT_ERR_ARG, "guide fraction must lie in (0, 1)");
+        guide_frac_ = f;
+        return PT_OK;
+    }
+    float guide_frac_ = 0.7f;
 
     // ---- batched frames (configuration 4): every scene rendered by one launch per stage ----
     int load_batch(const std::vector<BatchSpec>& specs);

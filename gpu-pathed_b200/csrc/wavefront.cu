@@ -352,7 +352,8 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                     const bool use_guide = guided && !delta_mat;
                     const float* mix = use_guide ? p.gmix + (size_t)slot * kGuideOut : nullptr;
                     bool from_guide = false;
-                    if (use_guide) from_guide = pcg_uniform(st, inc) >= 0.5f;  // one-sample MIS, fraction 0.5
+                    // one-sample MIS: the guide with probability gfrac (u in (0, 1])
+                    if (use_guide) from_guide = pcg_uniform(st, inc) >= 1.f - p.gfrac;
                     BsdfSample bs;
                     V wworld;
                     if (from_guide) {
@@ -384,7 +385,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                         const float pb = bsdf_sampling_pdf(m, wo, bs.wi);
                         float pg = guide_pdf(mix, normalized(wworld));
                         if (!isfinite(pg)) pg = 0.f;
-                        bs.pdf = 0.5f * pb + 0.5f * pg;
+                        bs.pdf = (1.f - p.gfrac) * pb + p.gfrac * pg;
                     }
                     if (do_nee && !bs.delta) {
                         // directSampleLights (path_tracer.cu:83-126)
@@ -397,7 +398,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                             float bpdf = p.consistent_mis ? bsdf_sampling_pdf(m, wo, wil) : bsdf_pdf(m, wo, wil);
                             if (use_guide) {
                                 const float pg = guide_pdf(mix, ls.wi);
-                                bpdf = 0.5f * bpdf + 0.5f * (isfinite(pg) ? pg : 0.f);
+                                bpdf = (1.f - p.gfrac) * bpdf + p.gfrac * (isfinite(pg) ? pg : 0.f);
                             }
                             const float wl = balance(ls.pdf, bpdf);
                             const V f = bsdf_f(m, wo, wil);

@@ -152,6 +152,7 @@ struct FrameParams {
     LaunchShape shape;
     // ---- learned path guiding (guide.cuh) ----
     int guide_mode;          // 0 off, 1 collect training data only, 2 guided sampling + collect
+    float gfrac;             // probability of sampling the guide at a non-delta vertex
     int consistent_mis;      // NEE weights use the BSDF's true sampling density (microfacet)
     int guide_tc;            // guide inference on tcgen05 / tensor memory (single-scene frames)
     const uint32_t* gwpack;  // packed inference weights

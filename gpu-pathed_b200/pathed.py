@@ -41,6 +41,7 @@ EXPORTED = [
     "pt_read_exr",
     "pt_save_exr",
     "pt_write_exr",
+    "pt_set_guide_fraction",
 ]
 
 MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
@@ -203,6 +204,7 @@ def _load():
     lib.pt_load_request.argtypes = [C.c_void_p, C.c_void_p]
     lib.pt_load_reference_scene.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
     lib.pt_save_exr.argtypes = [C.c_void_p, C.c_char_p]
+    lib.pt_set_guide_fraction.argtypes = [C.c_void_p, C.c_float]
     lib.pt_write_exr.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
     lib.pt_read_exr.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
     for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async",
@@ -482,6 +484,10 @@ class Session:
     def set_guide_inference(self, tc: bool):
         """Guide inference on tcgen05 / tensor memory (True) or mma.sync (False)."""
         self._check(lib.pt_set_guide_inference(self._h, int(bool(tc))))
+
+    def set_guide_fraction(self, fraction: float):
+        """Probability of sampling the guide at a non-delta vertex (default 0.7)."""
+        self._check(lib.pt_set_guide_fraction(self._h, float(fraction)))
 
     def guide_params(self) -> np.ndarray:
         out = np.empty(GUIDE_PARAMS, np.float32)

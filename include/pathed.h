@@ -254,17 +254,17 @@ int pt_set_seed(pt_session* s, uint64_t seed);
  * A network (80 -> 64 -> 64 -> 64 -> 40, ReLU; 16,104 parameters, BF16 weights on the
  * tensor cores, FP32 master copy) maps a 12-frequency sin/cos encoding of the hit position,
  * the shading normal and the outgoing direction to an 8-lobe von Mises-Fisher mixture. It is
- * trained online (Adam, lr 1e-3, 2^18 samples per step, one step per frame) on radiance
- * samples the integrator produces, and combined with BSDF sampling by one-sample MIS (guide
- * fraction 0.5) so the estimator stays unbiased; MIS weights of emitter sampling then use
+ * trained online (Adam, lr 3e-3, minibatches of 2^16 samples, several steps per frame) on
+ * radiance samples the integrator produces, and combined with BSDF sampling by one-sample MIS
+ * (guide fraction 0.7) so the estimator stays unbiased; MIS weights of emitter sampling then use
  * the mixture density. Before the first steps have been taken, paths are sampled from the
  * BSDF alone while training data is collected. */
 int pt_set_guiding(pt_session* s, int enabled);
 /* Re-initialise the guide network (seeded) and its optimiser state. */
 int pt_guide_reset(pt_session* s);
-/* Training schedule: Adam steps per frame (0, the default: automatic, 8 steps per frame for
- * the first 256 steps, 4 up to 1024, then 2), samples per step (default 2^16), learning rate
- * (default 1e-3), steps before the guide is used for sampling (default 4). Negative values
+/* Training schedule: Adam steps per frame (0, the default: automatic, 16 steps per frame for
+ * the first 512 steps, 4 up to 1024, then 2), samples per step (default 2^16), learning rate
+ * (default 3e-3), steps before the guide is used for sampling (default 4). Negative values
  * (zero for batch and lr) keep the current setting. */
 int pt_set_guide_options(pt_session* s, int steps_per_frame, int batch, float lr, int warmup_steps);
 /* MIS weights of emitter samples use the BSDF's own sampling density (the reference's
@@ -289,6 +289,10 @@ int pt_guide_forward(pt_session* s, const float* x, int n, float* raw);
 /* Guide inference on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor
  * memory; tc = 1) or on warp-level mma.sync (tc = 0, the default and the fallback). */
 int pt_set_guide_inference(pt_session* s, int tc);
+/* Probability (default 0.7) of drawing a non-delta vertex's direction from the guide instead
+ * of the BSDF; the MIS density is (1 - f) p_bsdf + f p_guide, so the estimator is unbiased for
+ * any f in (0, 1) (PT_ERR_ARG outside). */
+int pt_set_guide_fraction(pt_session* s, float fraction);
 /* Gradient (16104 floats) of -sum w_i log q(wi_i | x_i) / sum w_i computed by the training
  * kernel for n explicit samples (x: n x 80, wi: n x 3 unit vectors, w: n weights). */
 int pt_guide_gradients(pt_session* s, const float* x, const float* wi, const float* w, int n, float* grad);

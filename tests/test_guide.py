@@ -142,9 +142,11 @@ def _slit_room(w, h):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tc", [False, True], ids=["mma.sync", "tcgen05"])
-def test_guided_estimator_is_unbiased(tc):
-    """guided frames converge to the plain (consistent-MIS) image: image mean within 4 SE"""
+@pytest.mark.parametrize("tc,fraction", [(False, None), (True, None), (False, 0.3)],
+                         ids=["mma.sync", "tcgen05", "mma.sync-fraction0.3"])
+def test_guided_estimator_is_unbiased(tc, fraction):
+    """guided frames converge to the plain (consistent-MIS) image: image mean within 4 SE, at
+    the default guide fraction and at another one"""
     w = h = 48
     frames, spp = 24, 16
     means = {}
@@ -153,6 +155,8 @@ def test_guided_estimator_is_unbiased(tc):
         s.set_consistent_mis(True)
         if guided:
             s.set_guide_inference(tc)
+            if fraction is not None:
+                s.set_guide_fraction(fraction)
             s.set_guiding(True)
             s.set_guide_options(steps_per_frame=4, warmup_steps=8)
         vals = []
@@ -210,3 +214,12 @@ def test_trained_guide_reduces_error():
           f"steps {info['steps']}, samples {info['samples']}, loss {info['loss']:.3f})")
     assert info["mode"] == 2
     assert e_guided < 0.8 * e_plain
+
+
+def test_guide_fraction_range():
+    s = pathed.Session(16, 16)
+    for bad in (0.0, 1.0, -0.5, float("nan")):
+        with pytest.raises(pathed.PathedError):
+            s.set_guide_fraction(bad)
+    s.set_guide_fraction(0.9)
+    s.close()
