@@ -513,6 +513,122 @@ def guided_time_to_relmse(budget_spp=256, ref_spp=2048, res=1024):
             "training": "online from scratch inside the timed frames (automatic Adam schedule)"}
 
 
+class BatchRelmse:
+    """Configuration 4's time-to-relMSE pieces: the 48-scene draw, relMSE references for its
+    guided scenes (a plain render of those scenes alone at `ref_frames` frames; a scene renders
+    bit-identically inside or outside a batch), the plain budget and guided runs."""
+
+    def __init__(self, ref_frames=128, draw=0x5EED + 4, n=48):
+        import numpy as np
+
+        import pathed
+
+        self.draw, self.n = draw, n
+        self.specs = pathed.batch_generate(draw, n)
+        self.gids = [i for i, d in enumerate(self.specs) if d["guided"]]
+        self.ref_frames = ref_frames
+        r = pathed.Session(16, 16)
+        r.load_batch([self.specs[i] for i in self.gids])
+        r.set_consistent_mis(True)
+        r.set_seed(12345)
+        for _ in range(ref_frames):
+            r.render(0)
+        self.refs = [r.batch_readback(k).astype(np.float64) for k in range(len(self.gids))]
+        r.close()
+        self.dens = [x ** 2 + 1e-2 for x in self.refs]
+
+    def errors(self, sess):
+        import numpy as np
+
+        return [float(np.mean((sess.batch_readback(i).astype(np.float64) - self.refs[k]) ** 2 / self.dens[k]))
+                for k, i in enumerate(self.gids)]
+
+    def plain(self, budget_frames=16):
+        import pathed
+
+        p = pathed.Session(16, 16)
+        p.load_batch(self.specs)
+        p.set_consistent_mis(True)
+        p.set_seed(77)
+        t = 0.0
+        for _ in range(budget_frames):
+            t += p.render(0)
+        target = self.errors(p)
+        p.close()
+        self.budget_frames, self.t_plain, self.target = budget_frames, t, target
+        return t, target
+
+    def guided(self, steps=None, batch=None, fraction=None, per_frame=None):
+        """Guided run (trained online from scratch inside the timed frames) until the mean
+        relMSE over the guided scenes reaches the plain budget's; `per_frame(frame, session)`
+        may change options before each frame."""
+        import numpy as np
+
+        import pathed
+
+        g = pathed.Session(16, 16)
+        g.load_batch(self.specs)
+        g.set_seed(77)
+        g.set_guiding(True)
+        if steps is not None or batch is not None:
+            g.set_guide_options(steps_per_frame=-1 if steps is None else steps, batch=batch or 0)
+        if fraction is not None:
+            g.set_guide_fraction(fraction)
+        t, prev, crossed, frames = 0.0, None, None, 0
+        per_scene = [None] * len(self.gids)
+        mt = float(np.mean(self.target))
+        while t < 3 * self.t_plain:
+            if per_frame is not None:
+                per_frame(frames, g)
+            t += g.render(0)
+            frames += 1
+            e = self.errors(g)
+            for k in range(len(self.gids)):
+                if per_scene[k] is None and e[k] <= self.target[k]:
+                    per_scene[k] = t
+            m = float(np.mean(e))
+            if crossed is None and m <= mt:
+                if prev is not None:
+                    t0, m0 = prev
+                    f = (np.log(m0) - np.log(mt)) / max(1e-12, np.log(m0) - np.log(m))
+                    crossed = t0 + f * (t - t0)
+                else:
+                    crossed = t
+            prev = (t, m)
+            if crossed is not None and all(x is not None for x in per_scene):
+                break
+        info = g.guide_info()
+        g.close()
+        ratios = [self.t_plain / x if x else None for x in per_scene]
+        done = sorted(x for x in ratios if x is not None)
+        return {"guided_ms": crossed, "guided_frames": frames,
+                "speedup": (self.t_plain / crossed) if crossed else None,
+                "per_scene_speedup_median": done[len(done) // 2] if done else None,
+                "per_scene_speedup_min": done[0] if done else None,
+                "per_scene_not_reached": sum(x is None for x in ratios),
+                "per_scene": [{"config": self.specs[i]["config"], "level": self.specs[i]["level"],
+                               "res": self.specs[i]["width"], "spp": self.specs[i]["spp"],
+                               "depth": self.specs[i]["max_depth"], "speedup": ratios[k]}
+                              for k, i in enumerate(self.gids)],
+                "guide_steps": info["steps"]}
+
+
+def batch_time_to_relmse(budget_frames=16, ref_frames=128, draw=0x5EED + 4, n=48):
+    """Configuration 4: the 48-scene batch rendered plain for `budget_frames` frames, then
+    guided (one network per guided scene, trained online from scratch inside the timed frames)
+    until the mean relMSE over the guided scenes reaches plain's. Times are device ms of whole
+    batch frames, every scene included."""
+    import numpy as np
+
+    b = BatchRelmse(ref_frames, draw, n)
+    t_plain, target = b.plain(budget_frames)
+    out = b.guided()
+    return {"workload": f"batch of {n} scenes (pathed.batch_generate({draw:#x}, {n})), {len(b.gids)} guided",
+            "reference": f"plain render of the guided scenes, {ref_frames} frames, consistent MIS",
+            "plain_frames": budget_frames, "plain_ms": t_plain, "target_mean_relmse": float(np.mean(target)),
+            **out}
+
+
 def _ncu_bytes_per_query(workload):
     """DRAM bytes per closest-hit query that ncu measured on this workload
     (profiles/k_extend_traffic.txt, one `<workload> dram_bytes_per_query: B` line each), or None."""
@@ -542,9 +658,16 @@ def main():
     ap.add_argument("--no-guiding", action="store_true")
     ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
     ap.add_argument("--gpu-bvh", action="store_true", help="build the BVH on the GPU instead of the host")
+    ap.add_argument("--time-to-relmse", action="store_true",
+                    help="with --config 4: print the batch's guided-vs-plain time-to-relMSE line and exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.time_to_relmse:
+        if args.config != 4:
+            ap.error("--time-to-relmse takes --config 4 (configuration 3's figure is in every default line)")
+        print(json.dumps({"metric": "time-to-relMSE speed-up, guided vs plain", **batch_time_to_relmse()}))
+        return 0
     return run_ours(args)
 
 

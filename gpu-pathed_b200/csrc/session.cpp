@@ -11,6 +11,9 @@
 #ifndef PT_GUIDE_TRAIN_PATHS
 #define PT_GUIDE_TRAIN_PATHS 524288
 #endif
+#ifndef PT_GUIDE_TRAIN_PATHS_BATCH
+#define PT_GUIDE_TRAIN_PATHS_BATCH 4194304
+#endif
 
 namespace pt {
 
@@ -718,6 +721,20 @@ int Session::ensure_frame_buffers(int spp) {
             }
             px += npx;
         }
+        // guided paths before a global path index (training paths are counted over them)
+        auto guided_before = [&](long long x) {
+            long long g = 0;
+            for (const BatchHost& b : batch_) {
+                if (!b.spec.guided) continue;
+                const long long np = (long long)b.spec.width * b.spec.height * b.spec.spp;
+                g += std::max(0LL, std::min(x - b.path_base, np));
+            }
+            return g;
+        };
+        for (WaveRange& w : batch_waves_) {
+            w.guided_first = guided_before(w.first_path);
+            w.guided_n = (int)(guided_before(w.first_path + w.npaths) - w.guided_first);
+        }
     }
     const size_t f4 = cap * sizeof(float4);
     for (int k = 0; k < 2; k++) {
@@ -810,9 +827,17 @@ int Session::render_async(int spp) {
         const size_t mix_bytes = (size_t)queue_cap_ * kGuideOut * sizeof(float);
         if ((r = check_cuda(d_gmix_.alloc(mix_bytes), "guide mixtures"))) return r;
         // every gstride-th path of a wave records training data: about 2^19 training paths
-        const int gstride = std::max(1, queue_cap_ / PT_GUIDE_TRAIN_PATHS);
-        const size_t tpaths = (size_t)(queue_cap_ + gstride - 1) / gstride;
-        if ((r = check_cuda(d_gacc_.alloc(tpaths * kMaxDepthLimit * 3 * sizeof(float)), "guide accumulators")))
+        // per wave; in a batch, every gstride-th path of the wave's guided scenes, about 2^22
+        long long train_pool = queue_cap_;
+        int gstride = std::max(1, queue_cap_ / PT_GUIDE_TRAIN_PATHS);
+        if (batch) {
+            train_pool = 1;
+            for (const WaveRange& w : batch_waves_) train_pool = std::max<long long>(train_pool, w.guided_n);
+            gstride = (int)std::max<long long>(1, (train_pool + PT_GUIDE_TRAIN_PATHS_BATCH - 1) /
+                                                      PT_GUIDE_TRAIN_PATHS_BATCH);
+        }
+        const size_t tpaths = (size_t)((train_pool + gstride - 1) / gstride);
+        if ((r = check_cuda(d_gacc_.alloc(tpaths * (size_t)p.max_depth * 3 * sizeof(float)), "guide accumulators")))
             return r;
         // one record per scattering vertex of a training path
         const size_t rec_cap = tpaths * (size_t)std::max(1, p.max_depth - 1);

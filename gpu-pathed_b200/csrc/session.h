@@ -29,6 +29,7 @@ struct BatchHost {
     int root = 0, light_first = 0, num_lights = 0;
     int num_tri = 0, num_sph = 0;
     long long path_base = 0, pixel_base = 0;
+    long long guided_base = 0;  // paths of guided scenes before this one
     int env_w = 0, env_h = 0;
     std::vector<float> env_rgba;
     EnvCdf env_cdf;

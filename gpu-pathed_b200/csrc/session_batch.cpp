@@ -65,7 +65,7 @@ int Session::load_batch(const std::vector<BatchSpec>& specs) {
     mb.width = bvh_width_;
     std::vector<LightRef> lights;
     std::vector<BatchHost> hosts(n);
-    long long path_base = 0, pixel_base = 0;
+    long long path_base = 0, pixel_base = 0, guided_base = 0;
     int max_depth = 0;
     for (int i = 0; i < n; i++) {
         HostScene& sc = scenes[i];
@@ -97,6 +97,8 @@ int Session::load_batch(const std::vector<BatchSpec>& specs) {
         h.gframe = guide_frame_of(sc);
         h.path_base = path_base;
         h.pixel_base = pixel_base;
+        h.guided_base = guided_base;
+        if (specs[i].guided) guided_base += (long long)specs[i].width * specs[i].height * specs[i].spp;
         path_base += (long long)specs[i].width * specs[i].height * specs[i].spp;
         pixel_base += (long long)specs[i].width * specs[i].height;
         max_depth = std::max(max_depth, specs[i].max_depth);
@@ -170,6 +172,7 @@ int Session::upload_batch() {
         b.guide_net = -1;
         b.path_base = h.path_base;
         b.pixel_base = h.pixel_base;
+        b.guided_base = h.guided_base;
         if (h.env_w > 0) {
             const DevBuf* e = d_batch_env_[i].get();
             b.env.rgba = e[0].as<float>();

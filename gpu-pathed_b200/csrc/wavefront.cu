@@ -270,11 +270,24 @@ __device__ __forceinline__ float bsdf_sampling_pdf(const Material& m, V wo, V wi
 
 __device__ __forceinline__ float lum(V c) { return (c.x + c.y + c.z) * (1.f / 3.f); }
 
+// Training index of a path: the path records training data when the index is a multiple of
+// gstride, into slot index / gstride. A single scene: the wave-local path index. A batched
+// frame: the path's position among the wave's paths of guided scenes (-1 for the paths of
+// other scenes), so the training budget goes to the scenes that train a network.
+template <bool B>
+__device__ __forceinline__ long long train_index(const FrameParams& p, int sid, int path, long long wave_first,
+                                                 long long gfirst) {
+    if (!B) return path;
+    const BatchScene& b = p.batch[sid];
+    if (b.guide_net < 0) return -1;
+    return b.guided_base + (wave_first + path - b.path_base) - gfirst;
+}
+
 // Per training path and depth: U (unweighted emission), R (NEE + MIS-weighted emission),
 // W (MIS-weighted emission), luminance times throughput.
-__device__ __forceinline__ void guide_account(const FrameParams& p, int path, int depth, float u, float r, float w) {
-    if (p.guide_mode == 0 || path % p.gstride != 0) return;
-    float* a = p.gacc + ((size_t)(path / p.gstride) * p.max_depth + depth) * 3;
+__device__ __forceinline__ void guide_account(const FrameParams& p, long long ti, int depth, float u, float r, float w) {
+    if (p.guide_mode == 0 || ti < 0 || ti % p.gstride != 0) return;
+    float* a = p.gacc + ((size_t)(ti / p.gstride) * p.max_depth + depth) * 3;
     a[0] += u;
     a[1] += r;
     a[2] += w;
@@ -284,7 +297,7 @@ __device__ __forceinline__ void guide_account(const FrameParams& p, int path, in
 // instantiation keeps the reference integrator's register budget. B: batched frame (the
 // scene, its depth, spp and guide come from the path's tag and the scene table).
 template <bool GUIDE, bool B>
-__global__ void k_shade(FrameParams p, int depth, long long wave_first) {
+__global__ void k_shade(FrameParams p, int depth, long long wave_first, long long gfirst) {
     const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
     const PathQueue qn = p.q[(depth + 1) & 1];
@@ -310,6 +323,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
             SceneDevice scb;
             if (B) scb = batch_scene_view(p, sid);
             const SceneDevice& sc = B ? scb : p.sc;
+            const long long ti = GUIDE && p.guide_mode ? train_index<B>(p, sid, path, wave_first, gfirst) : -1;
             const bool last = B ? depth >= p.batch[sid].max_depth - 1 : last_frame;
             const bool guided = B ? GUIDE && p.batch[sid].guide_mode == 2 : guided_frame;
             const bool do_nee = p.nee && sc.num_lights + (sc.env.present ? 1 : 0) > 0;
@@ -324,7 +338,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                 if (!is_zero(Le)) {
                     const float w = nomis ? 1.f : balance(d4.w, pdf_env_light(sc, dir));
                     Ladd = beta * Le * w;
-                    if (GUIDE) guide_account(p, path, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
+                    if (GUIDE) guide_account(p, ti, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
                 }
             } else {
                 V point, n;
@@ -340,7 +354,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                     const V Le = mkv(m.emit[0], m.emit[1], m.emit[2]);
                     const float w = nomis ? 1.f : balance(d4.w, pdf_scene_light(sc, o, point, n, prim));
                     Ladd = beta * Le * w;
-                    if (GUIDE) guide_account(p, path, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
+                    if (GUIDE) guide_account(p, ti, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
                 }
                 if (!last) {
                     const long long gp = wave_first + path;
@@ -421,12 +435,11 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
                             cd = make_float4(wworld.x, wworld.y, wworld.z, bs.pdf);
                             cb = make_float4(nb.x, nb.y, nb.z, __int_as_float(bs.delta ? 1 : 0));
                             crng = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
-                            if (GUIDE && p.guide_mode && !delta_mat && path % p.gstride == 0 &&
-                                (!B || p.batch[sid].guide_net >= 0)) {
+                            if (GUIDE && p.guide_mode && !delta_mat && ti >= 0 && ti % p.gstride == 0) {
                                 const V wn = normalized(wworld);
                                 const V won = normalized(-dir);
                                 rec = GuideRecord{{point.x, point.y, point.z}, {n.x, n.y, n.z}, {won.x, won.y, won.z},
-                                                  {wn.x, wn.y, wn.z}, lum(fc), lum(nb), path / p.gstride,
+                                                  {wn.x, wn.y, wn.z}, lum(fc), lum(nb), (int)(ti / p.gstride),
                                                   depth | (sid << 8)};
                                 record = true;
                             }
@@ -463,7 +476,7 @@ __global__ void k_shade(FrameParams p, int depth, long long wave_first) {
 }
 
 template <int W, bool CNT, bool B>
-__global__ void k_shadow(FrameParams p, int depth) {
+__global__ void k_shadow(FrameParams p, int depth, long long wave_first, long long gfirst) {
     extern __shared__ int2 stk[];
     const int count = p.counters->shadow_count[depth];
     const int lane = threadIdx.x & 31;
@@ -494,7 +507,11 @@ __global__ void k_shadow(FrameParams p, int depth) {
                 l.y += c.y;
                 l.z += c.z;
                 p.L[path] = l;
-                guide_account(p, path, depth, 0.f, (c.x + c.y + c.z) * (1.f / 3.f), 0.f);
+                if (p.guide_mode) {
+                    const int tg = __float_as_int(d.w);
+                    const long long ti = train_index<B>(p, tag_scene(tg), path, wave_first, gfirst);
+                    guide_account(p, ti, depth, 0.f, (c.x + c.y + c.z) * (1.f / 3.f), 0.f);
+                }
             }
         }
     }
@@ -757,7 +774,7 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
         cudaError_t e = cudaMemsetAsync(p.counters, 0, sizeof(WaveCounters), stream);
         if (e != cudaSuccess) return e;
         if (p.guide_mode) {
-            const size_t tpaths = (size_t)(n + p.gstride - 1) / p.gstride;
+            const size_t tpaths = (size_t)(w.guided_n + p.gstride - 1) / p.gstride;
             if ((e = cudaMemsetAsync(p.gacc, 0, tpaths * p.max_depth * 3 * sizeof(float), stream))) return e;
             if ((e = cudaMemsetAsync(p.grec_count, 0, sizeof(int), stream))) return e;
         }
@@ -778,11 +795,13 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                     k_guide_infer<B><<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
                 mark(kStageGuide);
             }
-            if (p.guide_mode) k_shade<true, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
-            else k_shade<false, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first);
+            if (p.guide_mode)
+                k_shade<true, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first, w.guided_first);
+            else
+                k_shade<false, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first, w.guided_first);
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {
-                k_shadow<W, CNT, B><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d);
+                k_shadow<W, CNT, B><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d, wave_first, w.guided_first);
                 mark(kStageShadow);
             }
         }
@@ -885,7 +904,7 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
     for (int k = 0; k < nwaves; k++) {
         const int first = k * p.wave_pixels;
         const int npix = npixels - first < p.wave_pixels ? npixels - first : p.wave_pixels;
-        waves[k] = WaveRange{first, npix, (long long)first * p.spp, npix * p.spp, 0};
+        waves[k] = WaveRange{first, npix, (long long)first * p.spp, npix * p.spp, 0, 0, npix * p.spp, 0};
     }
     return enqueue_waves<W, CNT, false>(p, waves, nwaves, stream, marks);
 }

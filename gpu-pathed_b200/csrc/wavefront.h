@@ -111,6 +111,7 @@ struct BatchScene {
     int pad0;
     long long path_base;     // first path of this scene in the frame's global path order
     long long pixel_base;    // first pixel in the concatenated image buffers
+    long long guided_base;   // paths of guided scenes (spec.guided) before this one, in path order
     EnvDevice env;
     GuideFrame gframe;
     CameraParams cam;
@@ -126,6 +127,10 @@ struct WaveRange {
     int first_pixel, npix;
     long long first_path;
     int npaths, pad;
+    // training paths are counted over guided scenes only: the wave's first guided-path index
+    // and how many guided paths it holds (a single scene: 0 and npaths)
+    long long guided_first;
+    int guided_n, pad2;
 };
 
 struct FrameParams {
