@@ -572,6 +572,7 @@ int Session::set_launch(const pt_launch_config* c) {
     auto ok_block = [](int b) { return b == 0 || (b >= 32 && b <= 1024 && b % 32 == 0); };
     if (!ok_block(c->block_extend) || !ok_block(c->block_shade) || !ok_block(c->block_shadow))
         return fail(PT_ERR_ARG, "block sizes must be multiples of 32 in [32, 1024]");
+    if (c->block_shade > 512) return fail(PT_ERR_ARG, "the shade stage takes at most 512 threads per block");
     if (c->wave_paths < 0 || c->blocks_per_sm < 0 || c->blocks_per_sm > 64)
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2)

@@ -105,7 +105,7 @@ typedef struct pt_scene_export {
 typedef struct pt_launch_config {
     int wave_paths;        /* paths in flight per wave (queue capacity) */
     int block_extend;      /* threads per block of the closest-hit stage */
-    int block_shade;
+    int block_shade;       /* at most 512; guided frames shade with their own 128-thread blocks */
     int block_shadow;
     int blocks_per_sm;     /* persistent grid = SMs * blocks_per_sm */
     int sort_materials;    /* 1: material-sorted shading, 2: off, 3: automatic (on when the
