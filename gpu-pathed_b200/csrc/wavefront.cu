@@ -17,6 +17,7 @@
 // with tMin 1e-3 and the hit serves both.
 #include "wavefront.h"
 
+#include <algorithm>
 #include <cfloat>
 #include <mutex>
 
@@ -212,8 +213,14 @@ __global__ void k_sort(FrameParams p, int depth) {
         off[c] = acc;
         acc += p.counters->sort_count[depth][c];
     }
+    // Slots are reserved per block: warps add their class counts into shared counters, then
+    // one global atomic per class and block reserves the block's range (the grid is capped at
+    // a few blocks per SM and strides over the queue).
+    __shared__ int s_cnt[8], s_base[8];
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < count; base += stride) {
+        if (threadIdx.x < 8) s_cnt[threadIdx.x] = 0;
+        __syncthreads();
         const int i = base + threadIdx.x;
         const bool valid = i < count;
         const int key = valid ? q.key[i] : 7;
@@ -221,15 +228,20 @@ __global__ void k_sort(FrameParams p, int depth) {
         const int lane = threadIdx.x & 31;
         const int leader = __ffs(peers) - 1;
         int b = 0;
-        if (valid && lane == leader) b = atomicAdd(&p.counters->sort_fill[depth][key], __popc(peers));
+        if (valid && lane == leader) b = atomicAdd(&s_cnt[key], __popc(peers));
+        __syncthreads();
+        if (threadIdx.x < 5 && s_cnt[threadIdx.x] > 0)
+            s_base[threadIdx.x] = atomicAdd(&p.counters->sort_fill[depth][threadIdx.x], s_cnt[threadIdx.x]);
+        __syncthreads();
         b = __shfl_sync(0xffffffffu, b, leader);
         if (valid) {
             int ko = 0;
 #pragma unroll
             for (int c = 0; c < 5; c++)
-                if (c == key) ko = off[c];
+                if (c == key) ko = off[c] + s_base[c];
             p.sort_index[ko + b + __popc(peers & lanemask_lt())] = i;
         }
+        __syncthreads();  // s_cnt / s_base are reused by the next chunk
     }
 }
 
@@ -792,7 +804,7 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
             k_extend<W, CNT, B><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
             mark(kStageExtend);
             if (p.shape.sort_materials) {
-                k_sort<<<(n + 255) / 256, 256, 0, stream>>>(p, d);
+                k_sort<<<std::min((n + 255) / 256, p.num_sms * 8), 256, 0, stream>>>(p, d);
                 mark(kStageSort);
             }
             if (p.guide_mode == 2 && d < p.max_depth - 1) {
