@@ -168,6 +168,7 @@ __global__ void k_extend(FrameParams p, int depth) {
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_extend, (unsigned long long)count);
     TraceWork work;
+    int class_count = 0;  // lane c < 5 counts the warp's hits of material class c
     for (;;) {
         const int base = warp_fetch(&p.counters->work_extend[depth]);
         if (base >= count) break;
@@ -196,10 +197,13 @@ __global__ void k_extend(FrameParams p, int depth) {
 #pragma unroll
             for (int c = 0; c < 5; c++) {
                 const unsigned m = __ballot_sync(0xffffffffu, key == c);
-                if (lane == 0 && m) atomicAdd(&p.counters->sort_count[depth][c], __popc(m));
+                if (lane == c) class_count += __popc(m);
             }
         }
     }
+    // one atomic per class and warp for the whole persistent loop
+    if (p.shape.sort_materials && lane < 5 && class_count > 0)
+        atomicAdd(&p.counters->sort_count[depth][lane], class_count);
     if (CNT) flush_work(work, &p.stats->extend_nodes, &p.stats->extend_prims);
 }
 
