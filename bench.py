@@ -263,6 +263,9 @@ def run_ours(args):
     s.set_seed(0x5EED + 7919 * rank)
     if args.wave_paths:
         s.set_launch(wave_paths=args.wave_paths)
+    tuned = None
+    if not args.no_autotune and not batch:  # untimed: frames of this workload under each candidate shape
+        tuned = s.autotune(spp if spp else 1)
     counts = s.counts()
 
     # one untimed frame with work counters for the algorithmic-bytes accounting
@@ -411,6 +414,9 @@ def run_ours(args):
             "clocks": clk,
             "gpu_launches": gpu_launches,
         }
+        if tuned is not None:
+            line["config"]["autotuned"] = {k: tuned[k] for k in ("bvh_width", "sort_materials", "blocks_per_sm",
+                                                               "block", "wave_paths", "best_ms", "default_ms")}
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:
@@ -658,6 +664,8 @@ def main():
     ap.add_argument("--no-guiding", action="store_true")
     ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
     ap.add_argument("--gpu-bvh", action="store_true", help="build the BVH on the GPU instead of the host")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip the autotuner (BVH width, sorting, blocks per SM, block size) that runs before timing")
     ap.add_argument("--time-to-relmse", action="store_true",
                     help="with --config 4: print the batch's guided-vs-plain time-to-relMSE line and exit")
     args = ap.parse_args()

@@ -820,7 +820,7 @@ int Session::render_async(int spp) {
     p.count_work = work_counters_;
     p.renderer = renderer_;
     p.shape = shape_;
-    p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 3 ? 1 : 0);
+    p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0);
     last_wave_paths_ = p.wave_pixels * spp;
     p.consistent_mis = consistent_mis_ || guiding_;
     if (guiding_ && !normals) {
@@ -1121,7 +1121,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         return PT_OK;
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
-    Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 3 ? 1 : 0), shape_.blocks_per_sm,
+    Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
               shape_.block_extend};
     float best_ms;
     int r;

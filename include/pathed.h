@@ -109,7 +109,7 @@ typedef struct pt_launch_config {
     int block_shadow;
     int blocks_per_sm;     /* persistent grid = SMs * blocks_per_sm */
     int sort_materials;    /* 1: material-sorted shading, 2: off, 3: automatic (on when the
-                              scene has 3 or more material classes; default) (0 keeps current) */
+                              scene has 2 or more material types; default) (0 keeps current) */
     int use_graph;         /* 1: capture each frame's launches in a CUDA graph and replay it
                               while the launch parameters are unchanged (default), 2: off */
 } pt_launch_config;
