@@ -263,6 +263,8 @@ def run_ours(args):
     s.set_seed(0x5EED + 7919 * rank)
     if args.wave_paths:
         s.set_launch(wave_paths=args.wave_paths)
+    if args.quantized_bvh:
+        s.set_bvh_quantized(True)
     tuned = None
     if not args.no_autotune and not batch:  # untimed: frames of this workload under each candidate shape
         tuned = s.autotune(spp if spp else 1)
@@ -399,6 +401,7 @@ def run_ours(args):
                         "nee": True, "triangles": counts.num_triangles, "spheres": counts.num_spheres,
                         "bvh_width": counts.bvh_width, "parallelism": f"replicas{world}",
                         "guided": bool(args.guided), "bvh_builder": "gpu-lbvh" if args.gpu_bvh else "host-sah",
+                        "bvh_nodes": "quantized" if args.quantized_bvh else "float",
                         "l2": "flushed between steps (256 MiB write)"} if not batch else
                        {"workload": wl["name"], "scenes": len(specs), "guided_scenes": sum(d["guided"] for d in specs),
                         "paths_per_frame": sum(d["width"] * d["height"] * d["spp"] for d in specs),
@@ -671,6 +674,8 @@ def main():
     ap.add_argument("--no-guiding", action="store_true")
     ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
     ap.add_argument("--gpu-bvh", action="store_true", help="build the BVH on the GPU instead of the host")
+    ap.add_argument("--quantized-bvh", action="store_true",
+                    help="traverse quantized wide nodes (8-bit child planes) instead of float nodes")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner (BVH width, sorting, blocks per SM, block size) that runs before timing")
     ap.add_argument("--time-to-relmse", action="store_true",

@@ -457,3 +457,51 @@ int append_bvh(const BvhBuild& b, int tri_base, int sph_base, BvhBuild& into) {
 }
 
 }  // namespace pt
+
+namespace pt {
+
+bool check_qnodes(const BvhBuild& b, const std::vector<uint8_t>& q, std::string& err) {
+    const int w = b.width;
+    if (w != 4 && w != 8) {
+        err = "quantized nodes exist for widths 4 and 8";
+        return false;
+    }
+    const size_t fb = w == 4 ? sizeof(BvhNode<4>) : sizeof(BvhNode<8>), qb = (size_t)qnode_bytes(w);
+    if (b.nodes.size() != (size_t)b.num_nodes * fb || q.size() != (size_t)b.num_nodes * qb) {
+        err = "node arrays have unexpected sizes";
+        return false;
+    }
+    for (int i = 0; i < b.num_nodes; i++) {
+        const float* f = reinterpret_cast<const float*>(b.nodes.data() + (size_t)i * fb);
+        const uint8_t* n = q.data() + (size_t)i * qb;
+        float org[3];
+        uint32_t e;
+        std::memcpy(org, n, 12);
+        std::memcpy(&e, n + 12, 4);
+        for (int k = 0; k < w; k++) {
+            int fc, qc;
+            std::memcpy(&fc, f + 6 * w + k, 4);
+            std::memcpy(&qc, n + qnode_child_offset(w) + 4 * k, 4);
+            if (fc != qc) {
+                err = "node " + std::to_string(i) + ": child codes differ";
+                return false;
+            }
+            if (fc == kEmptyChild) continue;
+            for (int a = 0; a < 3; a++) {
+                float sc;
+                const uint32_t bits = ((e >> (8 * a)) & 0xFFu) << 23;
+                std::memcpy(&sc, &bits, 4);
+                const float lo = std::fmaf((float)n[16 + (2 * a) * w + k], sc, org[a]);
+                const float hi = std::fmaf((float)n[16 + (2 * a + 1) * w + k], sc, org[a]);
+                if (!(lo <= f[(2 * a) * w + k]) || !(hi >= f[(2 * a + 1) * w + k])) {
+                    err = "node " + std::to_string(i) + " child " + std::to_string(k) + ": quantized box does not "
+                          "contain the float box";
+                    return false;
+                }
+            }
+        }
+    }
+    return true;
+}
+
+}  // namespace pt

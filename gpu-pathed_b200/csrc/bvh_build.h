@@ -36,6 +36,11 @@ bool build_bvh(const HostScene& s, int width, int max_leaf, BvhBuild& out, std::
 // primitive contained in the padded boxes of all its ancestors, child codes in range.
 bool check_bvh(const HostScene& s, const BvhBuild& b, std::string& err);
 
+// Quantized nodes (qnode_bytes(b.width) each) against the float nodes they replace: the same
+// child codes, and every decoded child box, fmaf(q, scale, origin) per plane, containing the
+// float child box.
+bool check_qnodes(const BvhBuild& b, const std::vector<uint8_t>& q, std::string& err);
+
 // Append a scene's BVH to the shared BVH of a batch (node, leaf-entry and primitive-id
 // offsets applied; the scene's primitives start at tri_base / sph_base). Returns its root.
 int append_bvh(const BvhBuild& b, int tri_base, int sph_base, BvhBuild& into);

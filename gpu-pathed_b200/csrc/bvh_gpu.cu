@@ -412,4 +412,98 @@ cudaError_t gpu_build_bvh(const float4* tri_p, int nt, const float4* sph, int ns
     return cudaGetLastError();
 }
 
+namespace {
+
+// One node per thread: per axis the origin is the smallest child lower plane, the scale the
+// smallest power of two whose 255 steps reach the largest upper plane; each plane's q is then
+// stepped until fmaf(q, scale, origin) lies outside the float plane (down for lower planes,
+// up for upper planes). A larger scale is tried when an upper plane does not fit.
+template <int W>
+__global__ void k_quantize_nodes(const BvhNode<W>* __restrict__ in, int n, uint32_t* __restrict__ out, int* fail) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BvhNode<W> nd = in[i];
+    uint32_t qb[6 * W / 4];
+    for (int j = 0; j < 6 * W / 4; j++) qb[j] = 0u;
+    float org[3] = {0.f, 0.f, 0.f};
+    uint32_t ex[3] = {1u, 1u, 1u};
+    bool all_ok = true;
+    for (int a = 0; a < 3; a++) {
+        const float* lo = a == 0 ? nd.lo_x : a == 1 ? nd.lo_y : nd.lo_z;
+        const float* hi = a == 0 ? nd.hi_x : a == 1 ? nd.hi_y : nd.hi_z;
+        float o = __int_as_float(0x7f800000), m = -__int_as_float(0x7f800000);
+        bool any = false;
+        for (int k = 0; k < W; k++)
+            if (nd.child[k] != kEmptyChild) {
+                o = fminf(o, lo[k]);
+                m = fmaxf(m, hi[k]);
+                any = true;
+            }
+        if (!any) o = m = 0.f;
+        const double ext = (double)m - (double)o;
+        int e = ext > 0.0 ? (int)ceil(log2(ext / 255.0)) + 127 : 1;
+        e = e < 1 ? 1 : e > 254 ? 254 : e;
+        bool ok = false;
+        uint8_t ql[W], qh[W];
+        for (; e <= 254 && !ok; e++) {
+            const float sc = __uint_as_float((uint32_t)e << 23);
+            ok = true;
+            for (int k = 0; k < W; k++) {
+                ql[k] = qh[k] = 0;
+                if (nd.child[k] == kEmptyChild) continue;
+                int l = (int)floor(((double)lo[k] - (double)o) / (double)sc);
+                l = l < 0 ? 0 : l > 255 ? 255 : l;
+                while (l > 0 && __fmaf_rn((float)l, sc, o) > lo[k]) l--;
+                int h = (int)ceil(((double)hi[k] - (double)o) / (double)sc);
+                h = h < 0 ? 0 : h;
+                if (h > 255) {
+                    ok = false;
+                    break;
+                }
+                while (h < 255 && __fmaf_rn((float)h, sc, o) < hi[k]) h++;
+                if (__fmaf_rn((float)l, sc, o) > lo[k] || __fmaf_rn((float)h, sc, o) < hi[k]) {
+                    ok = false;
+                    break;
+                }
+                ql[k] = (uint8_t)l;
+                qh[k] = (uint8_t)h;
+            }
+            if (ok) ex[a] = (uint32_t)e;
+        }
+        if (!ok) all_ok = false;
+        org[a] = o;
+        for (int k = 0; k < W; k++) {
+            const int bl = (2 * a) * W + k, bh = (2 * a + 1) * W + k;
+            qb[bl / 4] |= (uint32_t)ql[k] << (8 * (bl & 3));
+            qb[bh / 4] |= (uint32_t)qh[k] << (8 * (bh & 3));
+        }
+    }
+    if (!all_ok) atomicOr(fail, 1);
+    uint32_t* w = out + (size_t)i * (qnode_bytes(W) / 4);
+    w[0] = __float_as_uint(org[0]);
+    w[1] = __float_as_uint(org[1]);
+    w[2] = __float_as_uint(org[2]);
+    w[3] = ex[0] | (ex[1] << 8) | (ex[2] << 16);
+    for (int j = 0; j < 6 * W / 4; j++) w[4 + j] = qb[j];
+    for (int k = 0; k < W; k++) w[qnode_child_offset(W) / 4 + k] = (uint32_t)nd.child[k];
+    for (int j = qnode_child_offset(W) / 4 + W; j < qnode_bytes(W) / 4; j++) w[j] = 0u;
+}
+
+}  // namespace
+
+cudaError_t quantize_bvh_nodes(const void* nodes, int num_nodes, int width, void* out, int* fail,
+                               cudaStream_t stream) {
+    if (num_nodes <= 0) return cudaSuccess;
+    const int blocks = (num_nodes + 127) / 128;
+    if (width == 4)
+        k_quantize_nodes<4><<<blocks, 128, 0, stream>>>(static_cast<const BvhNode<4>*>(nodes), num_nodes,
+                                                       static_cast<uint32_t*>(out), fail);
+    else if (width == 8)
+        k_quantize_nodes<8><<<blocks, 128, 0, stream>>>(static_cast<const BvhNode<8>*>(nodes), num_nodes,
+                                                       static_cast<uint32_t*>(out), fail);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
 }  // namespace pt

@@ -21,6 +21,12 @@ struct GpuBvhInfo {
 // Build over nt triangles (3 float4 each: p0 p1 p2) and ns spheres (centre, radius) already on
 // the device: wide nodes into nodes_out, leaf entries (3 float4 each, Morton order) into
 // prims_out. Synchronises `st` once per tree level.
+// Quantized copy (qnode_bytes(width) per node, width 4 or 8) of `num_nodes` BvhNode<width>
+// nodes on the device. `fail` (device int) is set when a node cannot be quantized
+// conservatively (it cannot happen for finite boxes; the check is kept).
+cudaError_t quantize_bvh_nodes(const void* nodes, int num_nodes, int width, void* out, int* fail,
+                               cudaStream_t stream);
+
 cudaError_t gpu_build_bvh(const float4* tri_p, int nt, const float4* sph, int ns, int width, int max_leaf,
                           GpuBvhScratch& scratch, DevBuf& nodes_out, DevBuf& prims_out, GpuBvhInfo& info,
                           cudaStream_t st);

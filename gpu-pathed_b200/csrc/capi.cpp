@@ -416,6 +416,11 @@ int pt_set_bvh_builder(pt_session* s, int gpu) {
     return guarded(s, [&] { return s->impl.set_bvh_builder(gpu); });
 }
 
+int pt_set_bvh_nodes(pt_session* s, int quantized) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.set_bvh_nodes(quantized); });
+}
+
 int pt_set_renderer(pt_session* s, int kind) {
     if (!s) return PT_ERR_ARG;
     return guarded(s, [&] { return s->impl.set_renderer(kind); });

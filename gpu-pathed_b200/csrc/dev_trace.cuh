@@ -185,6 +185,35 @@ __device__ __forceinline__ void load_node(const float4* __restrict__ p, NodeView
     }
 }
 
+// Scale of a quantized node's axis: the FP32 power of two with biased exponent e.
+__device__ __forceinline__ float qscale(uint32_t e) { return __uint_as_float((e & 0xFFu) << 23); }
+
+
+// A quantized node (qnode_bytes(W) bytes, W = 4 or 8) decoded into the float view: each plane
+// is fmaf(q, scale, origin), which contains the float box the build quantized.
+template <int W>
+__device__ __forceinline__ void load_qnode(const float4* __restrict__ p, NodeView<W>& nv) {
+    constexpr int kF4 = qnode_bytes(W) / 16;
+    float4 raw[kF4];
+#pragma unroll
+    for (int i = 0; i < kF4; i++) raw[i] = __ldg(p + i);
+    const uint32_t e = __float_as_uint(raw[0].w);
+    const float ox = raw[0].x, oy = raw[0].y, oz = raw[0].z;
+    const float sx = qscale(e), sy = qscale(e >> 8), sz = qscale(e >> 16);
+    const uint32_t* u = reinterpret_cast<const uint32_t*>(raw);
+    auto q = [&](int a, int k) { return (float)((u[4 + (a * W + k) / 4] >> (8 * ((a * W + k) & 3))) & 0xFFu); };
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        nv.lo_x[k] = __fmaf_rn(q(0, k), sx, ox);
+        nv.hi_x[k] = __fmaf_rn(q(1, k), sx, ox);
+        nv.lo_y[k] = __fmaf_rn(q(2, k), sy, oy);
+        nv.hi_y[k] = __fmaf_rn(q(3, k), sy, oy);
+        nv.lo_z[k] = __fmaf_rn(q(4, k), sz, oz);
+        nv.hi_z[k] = __fmaf_rn(q(5, k), sz, oz);
+        nv.child[k] = (int)u[qnode_child_offset(W) / 4 + k];
+    }
+}
+
 // Per-query work counters (only maintained when the CNT template flag is set).
 struct TraceWork {
     unsigned nodes = 0;  // wide nodes loaded
@@ -197,8 +226,8 @@ struct TraceWork {
 // is re-tested against the current hit distance; when it is culled, the siblings behind it
 // (sorted farther) are dropped with it.
 template <int W, bool ANY>
-__device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, const RayPre& r, float tmin, float tmax,
-                                         const Hit& best, int2* __restrict__ stk, int stride, int& sp) {
+__device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, bool quant, const RayPre& r, float tmin,
+                                         float tmax, const Hit& best, int2* __restrict__ stk, int stride, int& sp) {
     constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
     while (sp > 0) {
         const int2 ent = stk[(sp - 1) * stride];
@@ -209,6 +238,28 @@ __device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, const
         const int sl = (int)(list & 7u);
         if (cnt > 1) stk[(sp - 1) * stride] = make_int2(parent, (int)(((uint32_t)(cnt - 1) << 24) | (list >> 3)));
         else sp--;
+        if (W >= 4 && quant) {
+            const float4* pq = nodes + (size_t)parent * (qnode_bytes(W) / 16);
+            const unsigned char* b = reinterpret_cast<const unsigned char*>(pq);
+            if (!ANY) {
+                const float4 h = __ldg(pq);
+                const uint32_t e = __float_as_uint(h.w);
+                const float sx = qscale(e), sy = qscale(e >> 8), sz = qscale(e >> 16);
+                const float tc = best.prim == kMissPrim ? tmax : best.t;
+                const float te = box_entry(
+                    r, __fmaf_rn((float)__ldg(b + 16 + 0 * W + sl), sx, h.x),
+                    __fmaf_rn((float)__ldg(b + 16 + 1 * W + sl), sx, h.x),
+                    __fmaf_rn((float)__ldg(b + 16 + 2 * W + sl), sy, h.y),
+                    __fmaf_rn((float)__ldg(b + 16 + 3 * W + sl), sy, h.y),
+                    __fmaf_rn((float)__ldg(b + 16 + 4 * W + sl), sz, h.z),
+                    __fmaf_rn((float)__ldg(b + 16 + 5 * W + sl), sz, h.z), tmin, tc * kBoxSlack);
+                if (te == __int_as_float(0x7f800000)) {
+                    if (cnt > 1) sp--;
+                    continue;
+                }
+            }
+            return __ldg(reinterpret_cast<const int*>(b + qnode_child_offset(W)) + sl);
+        }
         const float* pf = reinterpret_cast<const float*>(nodes + (size_t)parent * kNF4);
         if (!ANY) {
             const float tc = best.prim == kMissPrim ? tmax : best.t;
@@ -229,14 +280,16 @@ __device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, const
 // lanes that carry a query). Lanes advance through internal nodes in one phase and test
 // leaves in the next, re-converging at each phase boundary (the while-while organisation of
 // Aila and Laine, HPG 2009), so leaf tests and node visits execute as coherent SIMT
-// instructions instead of drifting apart. Returns whether the query hit.
-template <int W, bool ANY, bool CNT = false>
+// instructions instead of drifting apart. Returns whether the query hit. Q: node format, 0 float
+// nodes, 1 quantized nodes (W >= 4), -1 read from the scene at run time.
+template <int W, bool ANY, bool CNT = false, int Q = -1>
 __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r, float tmin, float tmax, bool active,
                                          int2* __restrict__ stk, int stride, int max_depth, Hit& best,
                                          int& overflow, TraceWork* work = nullptr) {
     constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
     const float4* __restrict__ nodes = sc.nodes;
     const float4* __restrict__ prims = sc.prims;
+    const bool quant = Q < 0 ? (W >= 4 && sc.node_q != 0) : (W >= 4 && Q == 1);  // warp-uniform
     best.prim = kMissPrim;
     best.t = tmax;
     int sp = 0;
@@ -248,7 +301,8 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
         while (__any_sync(0xffffffffu, alive && cur >= 0)) {
             if (alive && cur >= 0) {
                 NodeView<W> nv;
-                load_node<W>(nodes + (size_t)cur * kNF4, nv);
+                if (quant) load_qnode<W>(nodes + (size_t)cur * (qnode_bytes(W) / 16), nv);
+                else load_node<W>(nodes + (size_t)cur * kNF4, nv);
                 if (CNT) work->nodes++;
                 const float tcur = best.prim == kMissPrim ? tmax : best.t;
                 const float tlim = tcur * kBoxSlack;
@@ -298,7 +352,7 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
                     for (int k = 0; k < W; k++)
                         if (k == sel) next = nv.child[k];
                 }
-                if (alive && next == kEmptyChild) next = stack_pop<W, ANY>(nodes, r, tmin, tmax, best, stk, stride, sp);
+                if (alive && next == kEmptyChild) next = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
                 cur = next;
                 if (cur == kEmptyChild) alive = false;
             }
@@ -319,7 +373,7 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
                 for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
             }
             if (alive) {
-                cur = stack_pop<W, ANY>(nodes, r, tmin, tmax, best, stk, stride, sp);
+                cur = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
                 if (cur == kEmptyChild) alive = false;
             }
         }

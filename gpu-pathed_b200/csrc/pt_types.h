@@ -83,6 +83,17 @@ static_assert(sizeof(BvhNode<2>) == 64, "BVH2 node");
 static_assert(sizeof(BvhNode<4>) == 128, "BVH4 node");
 static_assert(sizeof(BvhNode<8>) == 256, "BVH8 node");
 
+// Quantized wide node (W = 4 or 8; 64 / 96 B against 128 / 256 B): per axis an origin (the
+// smallest child lower bound, FP32) and a power-of-two scale (its biased FP32 exponent), the
+// child planes as 8-bit multiples of the scale, the child codes unchanged. A plane decodes as
+// fmaf(q, scale, origin), correctly rounded on host and device alike; the builder chooses q so
+// that every decoded box contains the float child box it replaces (lower planes rounded down,
+// upper planes up), so traversal still never culls a hit.
+//   bytes 0-11 origin xyz, 12-14 exponents xyz, 16.. q[6][W] (lo_x, hi_x, lo_y, hi_y, lo_z,
+//   hi_z), then child[W] at 16 + 6W
+PT_HD constexpr int qnode_bytes(int w) { return w == 8 ? 96 : 64; }
+PT_HD constexpr int qnode_child_offset(int w) { return 16 + 6 * w; }
+
 // Environment light (include/lights/environment_light.h:26-99): RGBA texels, y-up lat-long,
 // row 0 = theta 0 (+y). CDFs: marginal over rows (H floats) and one conditional per row
 // (H x W floats), both clamped to 1.0 from the last non-zero entry (src/math/distribution.cu:37-42).
@@ -119,7 +130,8 @@ struct SceneDevice {
     int num_tri, num_sph, num_mat, num_lights;
     int bvh_width;             // 2, 4 or 8
     int root;                  // root node index (always an internal node)
-    int pad[2];
+    int node_q;                // 1: `nodes` holds quantized nodes (widths 4 and 8)
+    int pad;
 };
 
 // Ray-query kinds and their [tMin, tMax] conventions (src/renderers/path_tracer.cu):

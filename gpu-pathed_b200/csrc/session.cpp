@@ -421,10 +421,36 @@ int Session::set_bvh_builder(int gpu) {
     return PT_OK;
 }
 
+int Session::set_bvh_nodes(int quantized) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    const int q = quantized ? 1 : 0;
+    if (q == bvh_quant_) return PT_OK;
+    bvh_quant_ = q;
+    if (have_scene_) scene_dirty_ = true;  // the next device call uploads the chosen node format
+    reset();
+    return PT_OK;
+}
+
+// The quantized node copy on the device against the float nodes (host copy `b`).
+int Session::check_quantized(const BvhBuild& b) {
+    if (!bvh_nodes_quantized()) return PT_OK;
+    int r;
+    if ((r = ensure_device())) return r;
+    if (scene_dirty_ && (r = upload_scene())) return r;
+    std::vector<uint8_t> q((size_t)b.num_nodes * qnode_bytes(b.width));
+    if ((r = check_cuda(cudaMemcpy(q.data(), d_qnodes_.p, q.size(), cudaMemcpyDeviceToHost), "BVH download")))
+        return r;
+    std::string err;
+    return pt::check_qnodes(b, q, err) ? PT_OK : fail(PT_ERR_SCENE, err);
+}
+
 int Session::check_bvh() {
     if (!have_scene_) return PT_ERR_STATE;
     std::string err;
-    if (!bvh_gpu_ || batch_mode()) return pt::check_bvh(scene_, bvh_, err) ? PT_OK : fail(PT_ERR_SCENE, err);
+    if (!bvh_gpu_ || batch_mode()) {
+        if (!pt::check_bvh(scene_, bvh_, err)) return fail(PT_ERR_SCENE, err);
+        return check_quantized(bvh_);
+    }
     // GPU-built tree: build it if still pending, bring it to the host, run the same check
     int r;
     if ((r = ensure_device())) return r;
@@ -440,7 +466,8 @@ int Session::check_bvh() {
         return r;
     h.prim_order.resize(ne);
     for (int e = 0; e < ne; e++) std::memcpy(&h.prim_order[e], &h.prims[(size_t)e * 12 + 3], 4);
-    return pt::check_bvh(scene_, h, err) ? PT_OK : fail(PT_ERR_SCENE, err);
+    if (!pt::check_bvh(scene_, h, err)) return fail(PT_ERR_SCENE, err);
+    return check_quantized(h);
 }
 
 int Session::counts(pt_scene_counts* out) const {
@@ -655,8 +682,24 @@ int Session::upload_scene() {
         bvh_.max_leaf = info.max_leaf;
         bvh_.build_ms = ms;
     }
+    if (bvh_nodes_quantized()) {  // the quantized copy the traversal reads instead
+        if ((r = check_cuda(d_qnodes_.alloc((size_t)bvh_.num_nodes * qnode_bytes(bvh_.width)), "quantized BVH")))
+            return r;
+        if ((r = check_cuda(d_qfail_.alloc(sizeof(int)), "quantized BVH"))) return r;
+        if ((r = check_cuda(cudaMemsetAsync(d_qfail_.p, 0, sizeof(int), stream_), "quantized BVH"))) return r;
+        if ((r = check_cuda(quantize_bvh_nodes(d_nodes_.p, bvh_.num_nodes, bvh_.width, d_qnodes_.p,
+                                               d_qfail_.as<int>(), stream_),
+                            "BVH quantization")))
+            return r;
+    }
     // host vectors above must outlive the async copies
     if ((r = check_cuda(cudaStreamSynchronize(stream_), "scene upload"))) return r;
+    if (bvh_nodes_quantized()) {
+        int qf = 0;
+        if ((r = check_cuda(cudaMemcpy(&qf, d_qfail_.p, sizeof(int), cudaMemcpyDeviceToHost), "BVH quantization")))
+            return r;
+        if (qf) return fail(PT_ERR_SCENE, "a BVH node could not be quantized conservatively");
+    }
     if (batch_mode() && (r = upload_batch())) return r;
     scene_dirty_ = false;
     return upload_materials();
@@ -664,7 +707,8 @@ int Session::upload_scene() {
 
 SceneDevice Session::scene_view() const {
     SceneDevice v{};
-    v.nodes = d_nodes_.as<float4>();
+    v.nodes = bvh_nodes_quantized() ? d_qnodes_.as<float4>() : d_nodes_.as<float4>();
+    v.node_q = bvh_nodes_quantized();
     v.prims = d_prims_.as<float4>();
     v.tri_p = d_tri_p_.as<float4>();
     v.tri_n = d_tri_n_.as<float4>();
@@ -1205,7 +1249,7 @@ int Session::profile(pt_profile* out) const {
     out->shadow_nodes = last_stats_.shadow_nodes;
     out->shadow_prims = last_stats_.shadow_prims;
     out->bvh_width = bvh_.width;
-    out->node_bytes = bvh_.width == 2 ? 64 : bvh_.width == 4 ? 128 : 256;
+    out->node_bytes = bvh_nodes_quantized() ? qnode_bytes(bvh_.width) : bvh_.width == 2 ? 64 : bvh_.width == 4 ? 128 : 256;
     out->prim_bytes = 48;
     out->wave_paths = last_wave_paths_;
     return PT_OK;

@@ -71,6 +71,10 @@ public:
     // 1: build the BVH on the GPU (Morton-order LBVH collapsed to the wide format) at the next
     // upload; 0: the host's binned-SAH builder (default)
     int set_bvh_builder(int gpu);
+    // 1: traverse quantized nodes (widths 4 and 8; 64 / 96 B per node), 0: float nodes
+    int set_bvh_nodes(int quantized);
+    int check_quantized(const BvhBuild& b);
+    int bvh_nodes_quantized() const { return bvh_quant_ && (bvh_.width == 4 || bvh_.width == 8) ? 1 : 0; }
     int counts(::pt_scene_counts* out) const;
     int export_scene(::pt_scene_export* out) const;
 
@@ -143,6 +147,8 @@ private:
     cudaStream_t stream_ = nullptr;
     int num_sms_ = 0;
     size_t max_smem_ = 0;
+    DevBuf d_qnodes_, d_qfail_;
+    int bvh_quant_ = 0;
     DevBuf d_nodes_, d_prims_, d_tri_p_, d_tri_n_, d_tri_mat_, d_sph_, d_sph_mat_, d_mats_, d_lights_;
     DevBuf d_env_rgba_, d_env_marg_, d_env_cond_, d_env_row_;
     // frame state

@@ -159,7 +159,7 @@ __device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long lon
     }
 }
 
-template <int W, bool CNT, bool B>
+template <int W, bool CNT, bool B, int Q>
 __global__ void k_extend(FrameParams p, int depth) {
     extern __shared__ int2 stk[];
     const int count = p.counters->ray_count[depth];
@@ -183,8 +183,8 @@ __global__ void k_extend(FrameParams p, int depth) {
         SceneDevice scb;
         if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(o.w)));
         const SceneDevice& sc = B ? scb : p.sc;
-        traverse<W, false, CNT>(sc, r, tmin, FLT_MAX, valid, stk + threadIdx.x, blockDim.x, p.stack_depth, h, of,
-                                &work);
+        traverse<W, false, CNT, Q>(sc, r, tmin, FLT_MAX, valid, stk + threadIdx.x, blockDim.x, p.stack_depth, h,
+                                   of, &work);
         if (valid) {
             if (of) atomicOr(&p.stats->error, 1);
             q.hit[i] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
     }
 }
 
-template <int W, bool CNT, bool B>
+template <int W, bool CNT, bool B, int Q>
 __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long long gfirst) {
     extern __shared__ int2 stk[];
     const int count = p.counters->shadow_count[depth];
@@ -518,8 +518,8 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
         SceneDevice scb;
         if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(d.w)));
         const SceneDevice& sc = B ? scb : p.sc;
-        const bool occ = traverse<W, true, CNT>(sc, r, kShadowTMin, o.w, valid, stk + threadIdx.x, blockDim.x,
-                                                p.stack_depth, h, of, &work);
+        const bool occ = traverse<W, true, CNT, Q>(sc, r, kShadowTMin, o.w, valid, stk + threadIdx.x, blockDim.x,
+                                                   p.stack_depth, h, of, &work);
         if (valid) {
             if (of) atomicOr(&p.stats->error, 1);
             if (!occ) {
@@ -805,7 +805,12 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
         k_camera<B><<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
         mark(kStageCamera);
         for (int d = 0; d < p.max_depth; d++) {
-            k_extend<W, CNT, B><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+            if constexpr (W >= 4) {
+                if (p.sc.node_q) k_extend<W, CNT, B, 1><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+                else k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+            } else {
+                k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+            }
             mark(kStageExtend);
             if (p.shape.sort_materials) {
                 k_sort<<<std::min((n + 255) / 256, p.num_sms * 8), 256, 0, stream>>>(p, d);
@@ -825,7 +830,12 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                 k_shade<false, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first, w.guided_first);
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {
-                k_shadow<W, CNT, B><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d, wave_first, w.guided_first);
+                if (W >= 4 && p.sc.node_q)
+                    k_shadow<W, CNT, B, (W >= 4 ? 1 : 0)><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(
+                        p, d, wave_first, w.guided_first);
+                else
+                    k_shadow<W, CNT, B, 0><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d, wave_first,
+                                                                                           w.guided_first);
                 mark(kStageShadow);
             }
         }
@@ -938,14 +948,23 @@ cudaError_t set_smem_w(size_t bytes) {
     const int b = (int)bytes;
     cudaError_t e;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if ((e = cudaFuncSetAttribute(k_extend<W, false, false>, a, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_extend<W, true, false>, a, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_shadow<W, false, false>, a, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_shadow<W, true, false>, a, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_extend<W, false, true>, a, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_extend<W, true, true>, a, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_shadow<W, false, true>, a, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_shadow<W, true, true>, a, b))) return e;
+    constexpr int kQ = W >= 4 ? 1 : 0;  // the quantized-node variants (W >= 4)
+    if ((e = cudaFuncSetAttribute(k_extend<W, false, false, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, true, false, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, false, false, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, true, false, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, false, true, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, true, true, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, false, true, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, true, true, 0>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, false, false, kQ>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, true, false, kQ>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, false, false, kQ>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, true, false, kQ>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, false, true, kQ>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_extend<W, true, true, kQ>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, false, true, kQ>, a, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_shadow<W, true, true, kQ>, a, b))) return e;
     if ((e = cudaFuncSetAttribute(k_normals<W>, a, b))) return e;
     return cudaSuccess;
 }

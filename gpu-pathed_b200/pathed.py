@@ -42,6 +42,7 @@ EXPORTED = [
     "pt_save_exr",
     "pt_write_exr",
     "pt_set_guide_fraction",
+    "pt_set_bvh_nodes",
 ]
 
 MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
@@ -208,7 +209,7 @@ def _load():
     lib.pt_write_exr.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
     lib.pt_read_exr.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
     for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async",
-                 "pt_set_bvh_builder", "pt_set_renderer"):
+                 "pt_set_bvh_builder", "pt_set_renderer", "pt_set_bvh_nodes"):
         getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
     lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_set_profiling.argtypes = [C.c_void_p, C.c_int, C.c_int]
@@ -537,6 +538,10 @@ class Session:
     def set_bvh_builder(self, gpu: bool):
         """Build the BVH on the GPU (LBVH collapsed to the wide format) or on the host (SAH)."""
         self._check(lib.pt_set_bvh_builder(self._h, int(bool(gpu))))
+
+    def set_bvh_quantized(self, on: bool):
+        """Traverse quantized wide nodes (widths 4 and 8) instead of float nodes."""
+        self._check(lib.pt_set_bvh_nodes(self._h, int(bool(on))))
 
     def set_renderer(self, kind: int):
         """RENDERER_CUDA (the path tracer) or RENDERER_NORMALS (the normals G-buffer: one

@@ -413,6 +413,15 @@ int pt_batch_readback(pt_session* s, int scene, float* rgb, size_t n, int pass_o
  * (src/world.cu:5-41). Batches always use the host builder. */
 int pt_set_bvh_builder(pt_session* s, int gpu);
 
+/* quantized = 1: traversal reads quantized copies of the wide nodes (widths 4 and 8: 64 and
+ * 96 bytes against 128 and 256). Each node stores per axis an FP32 origin and a power-of-two
+ * scale, and every child plane as an 8-bit multiple of the scale, rounded outward so that the
+ * decoded box contains the float box; closest hits stay identical. quantized = 0 (default):
+ * float nodes. Width 2 always uses float nodes. It trades the node memory (2.7x smaller for
+ * width 8) for decode work: on a B200 it traced 16-28% slower on the generated
+ * configurations, whose nodes mostly stay in L2. No counterpart in the reference. */
+int pt_set_bvh_nodes(pt_session* s, int quantized);
+
 /* Renderer of the session's frames: PT_RENDERER_CUDA, the path tracer (default), or
  * PT_RENDERER_NORMALS, the normals G-buffer (PT_ERR_ARG for PT_RENDERER_OPTIX).
  * Replaces RenderSession's renderer switch (src/render_session.cu:79-87) to a
