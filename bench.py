@@ -112,6 +112,26 @@ def _dist_init():
     return world, rank, local
 
 
+def replica_seed(rank):
+    """Seed of replica `rank`: every rank renders its own samples."""
+    return 0x5EED + 7919 * rank
+
+
+def reduce_over_ranks(t, counts, world, device="cuda"):
+    """Replicas: the job's time is the slowest rank's, its work the sum over ranks. Returns
+    (max over ranks of t, [sum over ranks of each count]); one rank returns its own values."""
+    if world <= 1:
+        return float(t), [float(c) for c in counts]
+    import torch
+    import torch.distributed as dist
+
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    rr = torch.tensor([float(c) for c in counts], dtype=torch.float64, device=device)
+    dist.all_reduce(rr, op=dist.ReduceOp.SUM)
+    return float(tt.item()), [float(x) for x in rr.tolist()]
+
+
 def cpu_reference_run(cfg, seconds_target, threads=0, seed=0x5EED):
     """Oracle restatement of the reference integrator (reference trace convention, linear scan)
     on a bounded pixel sample. Returns (Mrays/s, Mpaths/s, sample description, threads)."""
@@ -260,7 +280,7 @@ def run_ours(args):
         s.load_config(args.config)
         if args.guided:  # learned guiding on the main workload (trained online during warm-up)
             s.set_guiding(True)
-    s.set_seed(0x5EED + 7919 * rank)
+    s.set_seed(replica_seed(rank))
     if args.wave_paths:
         s.set_launch(wave_paths=args.wave_paths)
     if args.quantized_bvh:
@@ -306,17 +326,7 @@ def run_ours(args):
             stage_launches[k] += p["stage_launches"][k]
     barrier()
     clk = clocks.stop()
-    t_max = dev_ms
-    rays_all, paths_all = float(rays), float(paths)
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        rr = torch.tensor([rays_all, paths_all], dtype=torch.float64, device="cuda")
-        dist.all_reduce(rr, op=dist.ReduceOp.SUM)
-        rays_all, paths_all = float(rr[0].item()), float(rr[1].item())
+    t_max, (rays_all, paths_all) = reduce_over_ranks(dev_ms, [rays, paths], world)
     value = rays_all / (t_max / 1e3) / 1e6
 
     # ---- end to end through the C ABI with host buffers
@@ -341,16 +351,7 @@ def run_ours(args):
         st = s.stats()
         e2e_rays += st["rays_extend"] + st["rays_shadow"]
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-        rr = torch.tensor([float(e2e_rays)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(rr, op=dist.ReduceOp.SUM)
-        e2e_rays = float(rr.item())
+    e2e_s, (e2e_rays,) = reduce_over_ranks(time.perf_counter() - t0, [e2e_rays], world)
     e2e_value = e2e_rays / e2e_s / 1e6
 
     # ---- roofline of the extend stage (closest hit): algorithmic bytes per launch
