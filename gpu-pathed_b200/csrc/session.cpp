@@ -602,7 +602,8 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->block_shade > 512) return fail(PT_ERR_ARG, "the shade stage takes at most 512 threads per block");
     if (c->wave_paths < 0 || c->blocks_per_sm < 0 || c->blocks_per_sm > 64)
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
-    if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2)
+    if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
+        c->sort_rays < 0 || c->sort_rays > 2)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
     if (c->block_extend) shape_.block_extend = c->block_extend;
@@ -611,6 +612,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->blocks_per_sm) shape_.blocks_per_sm = c->blocks_per_sm;
     if (c->sort_materials) sort_mode_ = c->sort_materials == 1 ? 1 : c->sort_materials == 2 ? 0 : -1;
     if (c->use_graph) use_graph_ = c->use_graph == 1 ? 1 : 0;
+    if (c->sort_rays) shape_.sort_rays = c->sort_rays == 1 ? 1 : 0;
     return PT_OK;
 }
 
@@ -622,6 +624,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->blocks_per_sm = shape_.blocks_per_sm;
     c->sort_materials = sort_mode_ == 1 ? 1 : sort_mode_ == 0 ? 2 : 3;
     c->use_graph = use_graph_ ? 1 : 2;
+    c->sort_rays = shape_.sort_rays ? 1 : 2;
 }
 
 int Session::upload_materials() {
@@ -792,6 +795,9 @@ int Session::ensure_frame_buffers(int spp) {
         if ((r = check_cuda(d_sq_[a].alloc(f4), "shadow queue"))) return r;
     if ((r = check_cuda(d_L_.alloc(f4), "path radiance"))) return r;
     if ((r = check_cuda(d_sort_.alloc(cap * sizeof(int)), "sort index"))) return r;
+    if ((r = check_cuda(d_rindex_.alloc(cap * sizeof(int)), "ray-sort index"))) return r;
+    if ((r = check_cuda(d_rhist_.alloc(2 * (kMaxDepthLimit + 1) * kRayBuckets * sizeof(int)), "ray-sort buckets")))
+        return r;
     queue_cap_ = (int)cap;
     return PT_OK;
 }
@@ -841,6 +847,8 @@ int Session::render_async(int spp) {
     p.sq.c = d_sq_[2].as<float4>();
     p.L = d_L_.as<float4>();
     p.sort_index = d_sort_.as<int>();
+    p.ray_index = d_rindex_.as<int>();
+    p.ray_hist = d_rhist_.as<int>();
     p.counters = d_counters_.as<WaveCounters>();
     p.stats = d_stats_.as<FrameStats>();
     p.pass_rgb = d_pass_.as<float>();
@@ -865,6 +873,7 @@ int Session::render_async(int spp) {
     p.renderer = renderer_;
     p.shape = shape_;
     p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0);
+    p.gframe = gframe_;  // scene bounds: guide encoding and ray-sort cells
     last_wave_paths_ = p.wave_pixels * spp;
     p.consistent_mis = consistent_mis_ || guiding_;
     if (guiding_ && !normals) {
@@ -930,7 +939,7 @@ int Session::render_async(int spp) {
     marks_active_ = false;
     if (stage_timing_) {
         const int waves = batch ? (int)batch_waves_.size() : (w_ * h_ + p.wave_pixels - 1) / p.wave_pixels;
-        const size_t need = (size_t)waves * (p.max_depth * 5 + 4) + 8;
+        const size_t need = (size_t)waves * (p.max_depth * 7 + 4) + 8;
         while (mark_events_.size() < need) {
             cudaEvent_t e;
             if ((r = check_cuda(cudaEventCreate(&e), "cudaEventCreate"))) return r;
@@ -1109,7 +1118,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     std::memset(&res, 0, sizeof(res));
     const std::string key = tune_key(scene_, material_classes_, w_, h_, spp, max_depth_, nee_);
     struct Cand {
-        int width, sort, bps, block;
+        int width, sort, bps, block, rays;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
@@ -1117,7 +1126,16 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         sort_mode_ = c.sort;
         shape_.blocks_per_sm = c.bps;
         shape_.block_extend = shape_.block_shadow = c.block;
+        shape_.sort_rays = c.rays;
         return PT_OK;
+    };
+    auto report = [&](const Cand& c) {
+        res.bvh_width = c.width;
+        res.sort_materials = c.sort == 1 ? 1 : 2;
+        res.blocks_per_sm = c.bps;
+        res.block = c.block;
+        res.sort_rays = c.rays ? 1 : 2;
+        res.wave_paths = wave_paths_;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1128,15 +1146,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 const std::string line(buf);
                 if (line.find(want) == std::string::npos) continue;
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
-                       json_int(line, "block", 128)};
+                       json_int(line, "block", 128), json_int(line, "sort_rays", 0)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
-                res.bvh_width = c.width;
-                res.sort_materials = c.sort == 1 ? 1 : 2;
-                res.blocks_per_sm = c.bps;
-                res.block = c.block;
-                res.wave_paths = wave_paths_;
+                report(c);
                 res.best_ms = (float)json_num(line, "ms", 0.0);
                 res.from_cache = 1;
                 reset();
@@ -1166,7 +1180,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
-              shape_.block_extend};
+              shape_.block_extend, shape_.sort_rays};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1197,6 +1211,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         c.sort = best.sort ? 0 : 1;
         if ((r = consider(c))) return r;
     }
+    if (max_depth_ > 1) {
+        Cand c = best;
+        c.rays = best.rays ? 0 : 1;
+        if ((r = consider(c))) return r;
+    }
     for (int bps : {8, 24}) {
         Cand c = best;
         c.bps = bps;
@@ -1210,11 +1229,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     if ((r = apply(best))) return r;
     stage_timing_ = saved_timing;
     reset();
-    res.bvh_width = best.width;
-    res.sort_materials = best.sort == 1 ? 1 : 2;
-    res.blocks_per_sm = best.bps;
-    res.block = best.block;
-    res.wave_paths = wave_paths_;
+    report(best);
     res.best_ms = best_ms;
     res.trials = trials;
     if (cache_path) {
@@ -1222,8 +1237,9 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         if (f) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
-                         "\"wave_paths\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
-                         key.c_str(), best.width, best.sort, best.bps, best.block, wave_paths_, best_ms, res.default_ms);
+                         "\"sort_rays\": %d, \"wave_paths\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
+                         key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, wave_paths_, best_ms,
+                         res.default_ms);
             std::fclose(f);
         }
     }

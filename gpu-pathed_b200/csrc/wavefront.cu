@@ -159,6 +159,77 @@ __device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long lon
     }
 }
 
+// Ray sorting (no counterpart in the reference, which traces each path's rays in pixel order,
+// src/renderers/path_tracer.cu:140-190): continuation rays leave a shading point in all
+// directions, so neighbouring queue slots traverse unrelated parts of the BVH. Grouping them
+// by origin cell and direction octant before the closest-hit stage gives a warp's rays
+// similar node sequences. Only the order in which the closest-hit stage visits the slots
+// changes (it writes every hit back to the ray's own slot), so images are unchanged.
+//
+// Key: a 4x4x4 grid over the scene bounds (clamped, so any origin maps to a cell) times the
+// octant. Pass 1 writes the keys and a device histogram (block histograms in shared memory,
+// one global atomic per non-empty bucket and block).
+__global__ void __launch_bounds__(kRaySortBlock) k_ray_key(FrameParams p, int depth) {
+    __shared__ int hist[kRayBuckets];
+    for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x) hist[j] = 0;
+    __syncthreads();
+    const int count = p.counters->ray_count[depth];
+    const PathQueue q = p.q[depth & 1];
+    const GuideFrame gf = p.gframe;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float4 o = q.o[i], d = q.d[i];
+        const float ov[3] = {o.x, o.y, o.z};
+        int cell = 0;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            // inv_ext = 2 / extent: u in [0, 4] inside the bounds; NaN clamps to 0
+            const float u = fminf(fmaxf((ov[a] - gf.lo[a]) * gf.inv_ext[a] * 2.f, 0.f), 3.f);
+            cell = cell * 4 + (int)u;
+        }
+        const int key = (cell << 3) | (d.x < 0.f ? 1 : 0) | (d.y < 0.f ? 2 : 0) | (d.z < 0.f ? 4 : 0);
+        q.key[i] = key;
+        atomicAdd(&hist[key], 1);
+    }
+    __syncthreads();
+    int* cnt = p.ray_hist + 2 * depth * kRayBuckets;
+    for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x)
+        if (hist[j]) atomicAdd(&cnt[j], hist[j]);
+}
+
+// Pass 2: every block scans the histogram (bucket offsets), counts its contiguous chunk of
+// slots per bucket, reserves their ranges with one global atomic per bucket, and writes the
+// slot indices into `ray_index`. Order within a bucket is unspecified.
+__global__ void __launch_bounds__(kRaySortBlock) k_ray_scatter(FrameParams p, int depth) {
+    __shared__ int off[kRayBuckets], loc[kRayBuckets], wsum[kRaySortBlock / 32];
+    const int count = p.counters->ray_count[depth];
+    const PathQueue q = p.q[depth & 1];
+    const int* cnt = p.ray_hist + 2 * depth * kRayBuckets;
+    int* fill = p.ray_hist + (2 * depth + 1) * kRayBuckets;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int c0 = cnt[2 * t], c1 = cnt[2 * t + 1];
+    int x = c0 + c1;  // inclusive scan over the block's pairs
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, k);
+        if (lane >= k) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    loc[2 * t] = loc[2 * t + 1] = 0;
+    __syncthreads();
+    int excl = x - c0 - c1;
+    for (int w = 0; w < warp; w++) excl += wsum[w];
+    off[2 * t] = excl;
+    off[2 * t + 1] = excl + c0;
+    const int per = (count + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * per, b1 = min(count, b0 + per);
+    for (int i = b0 + t; i < b1; i += blockDim.x) atomicAdd(&loc[q.key[i]], 1);
+    __syncthreads();
+    for (int j = t; j < kRayBuckets; j += blockDim.x)
+        if (loc[j]) loc[j] = off[j] + atomicAdd(&fill[j], loc[j]);
+    __syncthreads();
+    for (int i = b0 + t; i < b1; i += blockDim.x) p.ray_index[atomicAdd(&loc[q.key[i]], 1)] = i;
+}
+
 template <int W, bool CNT, bool B, int Q>
 __global__ void k_extend(FrameParams p, int depth) {
     extern __shared__ int2 stk[];
@@ -172,8 +243,8 @@ __global__ void k_extend(FrameParams p, int depth) {
     for (;;) {
         const int base = warp_fetch(&p.counters->work_extend[depth]);
         if (base >= count) break;
-        const int i = base + lane;
-        const bool valid = i < count;
+        const bool valid = base + lane < count;
+        const int i = !B && valid && depth > 0 && p.shape.sort_rays ? p.ray_index[base + lane] : base + lane;
         int key = -1;
         const float4 o = valid ? q.o[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 d = valid ? q.d[i] : make_float4(0.f, 0.f, 1.f, 0.f);
@@ -796,6 +867,9 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
         const long long wave_first = w.first_path;
         cudaError_t e = cudaMemsetAsync(p.counters, 0, sizeof(WaveCounters), stream);
         if (e != cudaSuccess) return e;
+        const bool sort_rays = !B && p.shape.sort_rays;
+        if (sort_rays && (e = cudaMemsetAsync(p.ray_hist, 0, 2 * p.max_depth * kRayBuckets * sizeof(int), stream)))
+            return e;
         if (p.guide_mode) {
             const size_t tpaths = (size_t)(w.guided_n + p.gstride - 1) / p.gstride;
             if ((e = cudaMemsetAsync(p.gacc, 0, tpaths * p.max_depth * 3 * sizeof(float), stream))) return e;
@@ -805,6 +879,13 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
         k_camera<B><<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
         mark(kStageCamera);
         for (int d = 0; d < p.max_depth; d++) {
+            if (sort_rays && d > 0) {
+                k_ray_key<<<std::min((n + kRaySortBlock - 1) / kRaySortBlock, p.num_sms * 4), kRaySortBlock, 0,
+                            stream>>>(p, d);
+                mark(kStageSort);
+                k_ray_scatter<<<p.num_sms * 4, kRaySortBlock, 0, stream>>>(p, d);
+                mark(kStageSort);
+            }
             if constexpr (W >= 4) {
                 if (p.sc.node_q) k_extend<W, CNT, B, 1><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
                 else k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);

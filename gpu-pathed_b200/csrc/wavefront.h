@@ -77,7 +77,14 @@ struct LaunchShape {
     int block_shadow = 128;
     int blocks_per_sm = 16;   // persistent grid = SMs * blocks_per_sm
     int sort_materials = 1;   // material-sorted shading
+    int sort_rays = 0;        // continuation rays extended in (origin cell, direction octant) order
 };
+
+// Ray sorting ahead of the closest-hit stage (single-scene frames, depth >= 1): the key of a
+// ray is its origin's cell in a 4x4x4 grid over the scene bounds and its direction octant.
+constexpr int kRaySortBlock = 256;
+constexpr int kRayBuckets = 512;  // 2 per thread of a ray-sort block
+static_assert(kRayBuckets == 2 * kRaySortBlock, "ray-sort scan layout");
 
 // Values that change from frame to frame live in device memory, so a captured CUDA graph
 // of the frame's launches stays valid across frames; the host updates them with one copy
@@ -140,6 +147,8 @@ struct FrameParams {
     ShadowQueue sq;
     float4* L;               // wave-local path radiance
     int* sort_index;         // material-sorted slot order
+    int* ray_index;          // ray-sorted slot order of the closest-hit stage (shape.sort_rays)
+    int* ray_hist;           // per depth: kRayBuckets bucket counts, then kRayBuckets fill cursors
     WaveCounters* counters;
     FrameStats* stats;
     float* pass_rgb;         // W*H*3: this frame's per-pixel mean (passRadiances)

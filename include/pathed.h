@@ -112,6 +112,9 @@ typedef struct pt_launch_config {
                               scene has 2 or more material types; default) (0 keeps current) */
     int use_graph;         /* 1: capture each frame's launches in a CUDA graph and replay it
                               while the launch parameters are unchanged (default), 2: off */
+    int sort_rays;         /* 1: sort continuation rays by origin cell and direction octant
+                              before the closest-hit stage (single-scene frames), 2: off
+                              (default); images are the same either way */
 } pt_launch_config;
 
 /* Result of pt_autotune. */
@@ -125,6 +128,7 @@ typedef struct pt_tune_result {
     float default_ms;       /* frame time of the configuration before tuning */
     int trials;             /* frames measured (0 when taken from the cache) */
     int from_cache;
+    int sort_rays;          /* 1 on, 2 off */
 } pt_tune_result;
 
 typedef struct pt_stats {
@@ -302,7 +306,7 @@ int pt_set_launch(pt_session* s, const pt_launch_config* cfg);
 int pt_get_launch(const pt_session* s, pt_launch_config* out);
 /* Autotuner (no counterpart in the reference, whose only tuning is SppOptimizer's spp
  * budget, src/spp_optimizer.cpp:8-29): times frames of `spp` samples on the loaded scene over
- * BVH width, material sorting, persistent-grid size and block size (coordinate descent),
+ * BVH width, material sorting, ray sorting, persistent-grid size and block size (coordinate descent),
  * applies the fastest and restarts accumulation. With cache_path, results are stored as one
  * JSON object per line keyed by scene size, material classes, resolution, spp, depth and
  * NEE, and a cached key is applied without measuring. */

@@ -160,6 +160,30 @@ def test_launch_shapes_do_not_change_images(sort, width):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", [(0, None), (1, None), (2, 4), (3, 4)], ids=lambda c: f"cfg{c[0]}")
+def test_ray_sorting_does_not_change_images(case):
+    """sorting continuation rays by origin cell and octant reorders the closest-hit stage's
+    visits only: hits land in each ray's own slot, so images and ray counts are identical"""
+    out = []
+    for rays in (2, 1):
+        s = pathed.Session(96, 80)
+        s.load_config(case[0], level=case[1])
+        s.set_launch(sort_rays=rays, wave_paths=20000)  # several waves per frame
+        s.set_seed(9)
+        s.set_profiling(stage_timing=True)
+        for _ in range(2):
+            s.render(4)
+        st = s.stats()
+        out.append((s.readback().copy(), st["rays_extend"], st["rays_shadow"],
+                    s.profile()["stage_launches"]["sort"]))
+        s.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1:3] == out[1][1:3]
+    # two launches (keys, scatter) per wave and depth >= 1
+    assert out[1][3] > out[0][3] and (out[1][3] - out[0][3]) % 2 == 0
+
+
+@pytest.mark.gpu
 def test_stats_count_canonical_queries(oracle_lib):
     w = h = 32
     s = pathed.Session(w, h)
@@ -209,6 +233,8 @@ def test_autotuner_and_cache(tmp_path):
     t = pathed.Session(128, 128)
     t.load_config(0)
     r2 = t.autotune(4, cache)
-    assert r2["from_cache"] == 1 and r2["bvh_width"] == r["bvh_width"]
+    assert r["sort_rays"] in (1, 2)
+    assert r2["from_cache"] == 1 and r2["bvh_width"] == r["bvh_width"] and r2["sort_rays"] == r["sort_rays"]
+    assert t.get_launch()["sort_rays"] == r["sort_rays"]
     s.close()
     t.close()

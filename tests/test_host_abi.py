@@ -114,6 +114,24 @@ def test_invalid_input_is_an_error_not_a_crash():
     s.close()
 
 
+def test_launch_config_host_state():
+    """launch options are host state: ray sorting defaults off, 0 keeps a field, bad modes fail"""
+    s = pathed.Session(16, 16)
+    s.load_config(0)
+    cfg = s.get_launch()
+    assert cfg["sort_rays"] == 2 and cfg["use_graph"] == 1 and cfg["sort_materials"] == 3
+    s.set_launch(sort_rays=1)
+    assert s.get_launch()["sort_rays"] == 1
+    s.set_launch(block_extend=256)  # other fields 0: unchanged
+    assert s.get_launch()["sort_rays"] == 1 and s.get_launch()["block_extend"] == 256
+    for bad in (-1, 3):
+        with pytest.raises(pathed.PathedError):
+            s.set_launch(sort_rays=bad)
+    s.set_launch(sort_rays=2)
+    assert s.get_launch()["sort_rays"] == 2
+    s.close()
+
+
 def test_load_arrays_roundtrip():
     s = pathed.Session(16, 16)
     s.load_config(1)
