@@ -167,38 +167,25 @@ __device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long lon
 // changes (it writes every hit back to the ray's own slot), so images are unchanged.
 //
 // Key: a 4x4x4 grid over the scene bounds (clamped, so any origin maps to a cell) times the
-// octant. Pass 1 writes the keys and a device histogram (block histograms in shared memory,
-// one global atomic per non-empty bucket and block).
-__global__ void __launch_bounds__(kRaySortBlock) k_ray_key(FrameParams p, int depth) {
-    __shared__ int hist[kRayBuckets];
-    for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x) hist[j] = 0;
-    __syncthreads();
-    const int count = p.counters->ray_count[depth];
-    const PathQueue q = p.q[depth & 1];
-    const GuideFrame gf = p.gframe;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const float4 o = q.o[i], d = q.d[i];
-        const float ov[3] = {o.x, o.y, o.z};
-        int cell = 0;
+// octant, in [0, kRayBuckets). The shade stage that emits a continuation ray writes its key
+// next to it and counts it in a block histogram (shared memory, one global atomic per
+// non-empty bucket and block at the end of the persistent loop).
+__device__ __forceinline__ int ray_sort_key(const GuideFrame& gf, float4 o, float4 d) {
+    const float ov[3] = {o.x, o.y, o.z};
+    int cell = 0;
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-            // inv_ext = 2 / extent: u in [0, 4] inside the bounds; NaN clamps to 0
-            const float u = fminf(fmaxf((ov[a] - gf.lo[a]) * gf.inv_ext[a] * 2.f, 0.f), 3.f);
-            cell = cell * 4 + (int)u;
-        }
-        const int key = (cell << 3) | (d.x < 0.f ? 1 : 0) | (d.y < 0.f ? 2 : 0) | (d.z < 0.f ? 4 : 0);
-        q.key[i] = key;
-        atomicAdd(&hist[key], 1);
+    for (int a = 0; a < 3; a++) {
+        // inv_ext = 2 / extent: u in [0, 4] inside the bounds; NaN clamps to 0
+        const float u = fminf(fmaxf((ov[a] - gf.lo[a]) * gf.inv_ext[a] * 2.f, 0.f), 3.f);
+        cell = cell * 4 + (int)u;
     }
-    __syncthreads();
-    int* cnt = p.ray_hist + 2 * depth * kRayBuckets;
-    for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x)
-        if (hist[j]) atomicAdd(&cnt[j], hist[j]);
+    return (cell << 3) | (d.x < 0.f ? 1 : 0) | (d.y < 0.f ? 2 : 0) | (d.z < 0.f ? 4 : 0);
 }
 
-// Pass 2: every block scans the histogram (bucket offsets), counts its contiguous chunk of
-// slots per bucket, reserves their ranges with one global atomic per bucket, and writes the
-// slot indices into `ray_index`. Order within a bucket is unspecified.
+// Then, ahead of the closest-hit stage, every block scans the histogram (bucket offsets),
+// counts its contiguous chunk of slots per bucket, reserves their ranges with one global
+// atomic per bucket, and writes the slot indices into `ray_index`. Order within a bucket is
+// unspecified.
 __global__ void __launch_bounds__(kRaySortBlock) k_ray_scatter(FrameParams p, int depth) {
     __shared__ int off[kRayBuckets], loc[kRayBuckets], wsum[kRaySortBlock / 32];
     const int count = p.counters->ray_count[depth];
@@ -397,6 +384,13 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
     const PathQueue qn = p.q[(depth + 1) & 1];
     const bool last_frame = depth >= p.max_depth - 1;
     const bool guided_frame = GUIDE && p.guide_mode == 2;
+    // ray-sort keys of the continuation rays (uniform over the grid)
+    const bool rsort = !B && p.shape.sort_rays && depth + 1 < p.max_depth;
+    __shared__ int rhist[B ? 1 : kRayBuckets];
+    if (rsort) {
+        for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x) rhist[j] = 0;
+        __syncthreads();
+    }
     for (;;) {
         const int base = warp_fetch(&p.counters->work_shade[depth]);
         if (base >= count) break;
@@ -559,6 +553,11 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
             qn.d[cslot] = cd;
             qn.beta[cslot] = cb;
             qn.rng[cslot] = crng;
+            if (!B && rsort) {
+                const int key = ray_sort_key(p.gframe, co, cd);
+                qn.key[cslot] = key;
+                atomicAdd(&rhist[key], 1);
+            }
         }
         const int sslot = warp_append(&p.counters->shadow_count[depth], shadow);
         if (shadow) {
@@ -566,6 +565,12 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
             p.sq.d[sslot] = sd;
             p.sq.c[sslot] = sc4;
         }
+    }
+    if (!B && rsort) {
+        __syncthreads();
+        int* cnt = p.ray_hist + 2 * (depth + 1) * kRayBuckets;
+        for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x)
+            if (rhist[j]) atomicAdd(&cnt[j], rhist[j]);
     }
 }
 
@@ -879,10 +884,7 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
         k_camera<B><<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
         mark(kStageCamera);
         for (int d = 0; d < p.max_depth; d++) {
-            if (sort_rays && d > 0) {
-                k_ray_key<<<std::min((n + kRaySortBlock - 1) / kRaySortBlock, p.num_sms * 4), kRaySortBlock, 0,
-                            stream>>>(p, d);
-                mark(kStageSort);
+            if (sort_rays && d > 0) {  // keys and counts come from the previous shade launch
                 k_ray_scatter<<<p.num_sms * 4, kRaySortBlock, 0, stream>>>(p, d);
                 mark(kStageSort);
             }

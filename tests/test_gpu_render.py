@@ -179,8 +179,7 @@ def test_ray_sorting_does_not_change_images(case):
         s.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert out[0][1:3] == out[1][1:3]
-    # two launches (keys, scatter) per wave and depth >= 1
-    assert out[1][3] > out[0][3] and (out[1][3] - out[0][3]) % 2 == 0
+    assert out[1][3] > out[0][3]  # one scatter launch per wave and depth >= 1
 
 
 @pytest.mark.gpu
