@@ -287,7 +287,9 @@ def run_ours(args):
         s.set_bvh_quantized(True)
     tuned = None
     if not args.no_autotune and not batch:  # untimed: frames of this workload under each candidate shape
-        tuned = s.autotune(spp if spp else 1)
+        tuned = s.autotune(spp if spp else 1, args.tune_cache)
+    if args.sort_rays:
+        s.set_launch(sort_rays=1 if args.sort_rays == "on" else 2)
     counts = s.counts()
 
     # one untimed frame with work counters for the algorithmic-bytes accounting
@@ -403,6 +405,7 @@ def run_ours(args):
                         "bvh_width": counts.bvh_width, "parallelism": f"replicas{world}",
                         "guided": bool(args.guided), "bvh_builder": "gpu-lbvh" if args.gpu_bvh else "host-sah",
                         "bvh_nodes": "quantized" if args.quantized_bvh else "float",
+                        "sort_rays": s.get_launch()["sort_rays"] == 1,
                         "l2": "flushed between steps (256 MiB write)"} if not batch else
                        {"workload": wl["name"], "scenes": len(specs), "guided_scenes": sum(d["guided"] for d in specs),
                         "paths_per_frame": sum(d["width"] * d["height"] * d["spp"] for d in specs),
@@ -680,6 +683,11 @@ def main():
                     help="traverse quantized wide nodes (8-bit child planes) instead of float nodes")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner (BVH width, sorting, blocks per SM, block size) that runs before timing")
+    ap.add_argument("--sort-rays", choices=("on", "off"), default=None,
+                    help="force ray sorting before the closest-hit stage on or off (applied after the autotuner)")
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON-lines autotuner cache: a run stores its choice, a later run of the same workload "
+                         "applies it without measuring (a profiled run then times what the plain run chose)")
     ap.add_argument("--time-to-relmse", action="store_true",
                     help="with --config 4: print the batch's guided-vs-plain time-to-relMSE line and exit")
     args = ap.parse_args()
