@@ -276,6 +276,97 @@ __device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, bool 
     return kEmptyChild;
 }
 
+// One internal-node visit of a live query (`cur` >= 0): test the node's children, push the
+// farther hits (nearest first for closest hit, hits first for any hit), descend into the
+// first, or pop the stack when none was hit. The query ends (`alive` false) when the stack
+// runs empty, or gives up with `overflow` set when it would exceed `max_depth` entries.
+template <int W, bool ANY, bool CNT>
+__device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool quant, const RayPre& r, float tmin,
+                                          float tmax, int2* __restrict__ stk, int stride, int max_depth,
+                                          const Hit& best, int& cur, int& sp, bool& alive, int& overflow,
+                                          TraceWork* work) {
+    constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
+    NodeView<W> nv;
+    if (quant) load_qnode<W>(nodes + (size_t)cur * (qnode_bytes(W) / 16), nv);
+    else load_node<W>(nodes + (size_t)cur * kNF4, nv);
+    if (CNT) work->nodes++;
+    const float tcur = best.prim == kMissPrim ? tmax : best.t;
+    const float tlim = tcur * kBoxSlack;
+    float key[W];
+    int slot[W];
+    int nhit = 0;
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k], tmin, tlim);
+        if (nv.child[k] == kEmptyChild) te = __int_as_float(0x7f800000);
+        key[k] = te;
+        slot[k] = k;
+        nhit += te != __int_as_float(0x7f800000) ? 1 : 0;
+    }
+    // odd-even transposition network: nearest first (closest hit) or hits first
+#pragma unroll
+    for (int pass = 0; pass < W; pass++) {
+#pragma unroll
+        for (int k = (pass & 1); k + 1 < W; k += 2) {
+            const bool swap = ANY ? (key[k] == __int_as_float(0x7f800000) && key[k + 1] != __int_as_float(0x7f800000))
+                                  : (key[k + 1] < key[k]);
+            if (swap) {
+                const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
+                const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
+            }
+        }
+    }
+    int next = kEmptyChild;
+    if (nhit > 0) {
+        if (nhit > 1) {
+            uint32_t list = 0;
+#pragma unroll
+            for (int k = W - 1; k >= 1; k--)
+                if (k < nhit) list = (list << 3) | (uint32_t)slot[k];
+            if (sp >= max_depth) {
+                overflow = 1;
+                alive = false;  // reported to the host; the query gives up
+            } else {
+                stk[sp * stride] = make_int2(cur, (int)(((uint32_t)(nhit - 1) << 24) | list));
+                sp++;
+            }
+        }
+        const int sel = slot[0];
+#pragma unroll
+        for (int k = 0; k < W; k++)
+            if (k == sel) next = nv.child[k];
+    }
+    if (alive && next == kEmptyChild) next = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
+    cur = next;
+    if (cur == kEmptyChild) alive = false;
+}
+
+// One leaf visit of a live query (`cur` a leaf code): test its entries, then pop the stack.
+// An any-hit query ends at its first hit (`hit_any`); every query ends on an empty stack.
+template <int W, bool ANY, bool CNT>
+__device__ __forceinline__ void leaf_step(const float4* __restrict__ nodes, const float4* __restrict__ prims,
+                                          bool quant, const RayPre& r, float tmin, float tmax,
+                                          int2* __restrict__ stk, int stride, Hit& best, int& cur, int& sp,
+                                          bool& alive, bool& hit_any, TraceWork* work) {
+    const int first = leaf_first(cur), cnt = leaf_count(cur);
+    if (CNT) work->prims += cnt;
+    if (ANY) {
+        for (int e = first; e < first + cnt; e++) {
+            if (leaf_entry_any(prims, e, r, tmin, tmax)) {
+                hit_any = true;
+                break;
+            }
+        }
+        if (hit_any) alive = false;
+    } else {
+        for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
+    }
+    if (alive) {
+        cur = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
+        if (cur == kEmptyChild) alive = false;
+    }
+}
+
 // Warp-synchronous traversal: every lane of the warp calls this together (`active` marks the
 // lanes that carry a query). Lanes advance through internal nodes in one phase and test
 // leaves in the next, re-converging at each phase boundary (the while-while organisation of
@@ -286,7 +377,6 @@ template <int W, bool ANY, bool CNT = false, int Q = -1>
 __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r, float tmin, float tmax, bool active,
                                          int2* __restrict__ stk, int stride, int max_depth, Hit& best,
                                          int& overflow, TraceWork* work = nullptr) {
-    constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
     const float4* __restrict__ nodes = sc.nodes;
     const float4* __restrict__ prims = sc.prims;
     const bool quant = Q < 0 ? (W >= 4 && sc.node_q != 0) : (W >= 4 && Q == 1);  // warp-uniform
@@ -299,84 +389,12 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
     while (__any_sync(0xffffffffu, alive)) {
         // ---- phase 1: internal nodes, until this lane holds a leaf (or is finished)
         while (__any_sync(0xffffffffu, alive && cur >= 0)) {
-            if (alive && cur >= 0) {
-                NodeView<W> nv;
-                if (quant) load_qnode<W>(nodes + (size_t)cur * (qnode_bytes(W) / 16), nv);
-                else load_node<W>(nodes + (size_t)cur * kNF4, nv);
-                if (CNT) work->nodes++;
-                const float tcur = best.prim == kMissPrim ? tmax : best.t;
-                const float tlim = tcur * kBoxSlack;
-                float key[W];
-                int slot[W];
-                int nhit = 0;
-#pragma unroll
-                for (int k = 0; k < W; k++) {
-                    float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k],
-                                         tmin, tlim);
-                    if (nv.child[k] == kEmptyChild) te = __int_as_float(0x7f800000);
-                    key[k] = te;
-                    slot[k] = k;
-                    nhit += te != __int_as_float(0x7f800000) ? 1 : 0;
-                }
-                // odd-even transposition network: nearest first (closest hit) or hits first
-#pragma unroll
-                for (int pass = 0; pass < W; pass++) {
-#pragma unroll
-                    for (int k = (pass & 1); k + 1 < W; k += 2) {
-                        const bool swap = ANY ? (key[k] == __int_as_float(0x7f800000) &&
-                                                 key[k + 1] != __int_as_float(0x7f800000))
-                                              : (key[k + 1] < key[k]);
-                        if (swap) {
-                            const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
-                            const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
-                        }
-                    }
-                }
-                int next = kEmptyChild;
-                if (nhit > 0) {
-                    if (nhit > 1) {
-                        uint32_t list = 0;
-#pragma unroll
-                        for (int k = W - 1; k >= 1; k--)
-                            if (k < nhit) list = (list << 3) | (uint32_t)slot[k];
-                        if (sp >= max_depth) {
-                            overflow = 1;
-                            alive = false;  // reported to the host; the query gives up
-                        } else {
-                            stk[sp * stride] = make_int2(cur, (int)(((uint32_t)(nhit - 1) << 24) | list));
-                            sp++;
-                        }
-                    }
-                    const int sel = slot[0];
-#pragma unroll
-                    for (int k = 0; k < W; k++)
-                        if (k == sel) next = nv.child[k];
-                }
-                if (alive && next == kEmptyChild) next = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
-                cur = next;
-                if (cur == kEmptyChild) alive = false;
-            }
+            if (alive && cur >= 0)
+                node_step<W, ANY, CNT>(nodes, quant, r, tmin, tmax, stk, stride, max_depth, best, cur, sp, alive,
+                                       overflow, work);
         }
         // ---- phase 2: leaves
-        if (alive) {
-            const int first = leaf_first(cur), cnt = leaf_count(cur);
-            if (CNT) work->prims += cnt;
-            if (ANY) {
-                for (int e = first; e < first + cnt; e++) {
-                    if (leaf_entry_any(prims, e, r, tmin, tmax)) {
-                        hit_any = true;
-                        break;
-                    }
-                }
-                if (hit_any) alive = false;
-            } else {
-                for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
-            }
-            if (alive) {
-                cur = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
-                if (cur == kEmptyChild) alive = false;
-            }
-        }
+        if (alive) leaf_step<W, ANY, CNT>(nodes, prims, quant, r, tmin, tmax, stk, stride, best, cur, sp, alive, hit_any, work);
     }
     if (ANY) {
         if (hit_any) best.prim = 0;

@@ -605,6 +605,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
         c->sort_rays < 0 || c->sort_rays > 2)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
+    if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
     if (c->block_extend) shape_.block_extend = c->block_extend;
     if (c->block_shade) shape_.block_shade = c->block_shade;
@@ -613,6 +614,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->sort_materials) sort_mode_ = c->sort_materials == 1 ? 1 : c->sort_materials == 2 ? 0 : -1;
     if (c->use_graph) use_graph_ = c->use_graph == 1 ? 1 : 0;
     if (c->sort_rays) shape_.sort_rays = c->sort_rays == 1 ? 1 : 0;
+    if (c->refill_idle) shape_.refill_idle = c->refill_idle;
     return PT_OK;
 }
 
@@ -625,6 +627,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->sort_materials = sort_mode_ == 1 ? 1 : sort_mode_ == 0 ? 2 : 3;
     c->use_graph = use_graph_ ? 1 : 2;
     c->sort_rays = shape_.sort_rays ? 1 : 2;
+    c->refill_idle = shape_.refill_idle;
 }
 
 int Session::upload_materials() {

@@ -217,51 +217,89 @@ __global__ void __launch_bounds__(kRaySortBlock) k_ray_scatter(FrameParams p, in
     for (int i = b0 + t; i < b1; i += blockDim.x) p.ray_index[atomicAdd(&loc[q.key[i]], 1)] = i;
 }
 
+// Closest hit for the queue, persistent. Each lane carries one query through the
+// warp-synchronous node and leaf phases (node_step / leaf_step, the while-while loop of
+// Aila and Laine 2009). A lane whose query ends writes its hit at once. When shape.refill_idle
+// or more lanes are idle, they take the next rays of the queue together (one atomic per warp),
+// so a warp does not idle behind its longest query (Aila and Laine's replacement of
+// terminated rays). With refill_idle = 32 a warp takes 32 new rays only after all of its
+// queries ended.
 template <int W, bool CNT, bool B, int Q>
 __global__ void k_extend(FrameParams p, int depth) {
     extern __shared__ int2 stk[];
+    __shared__ int s_class[8];  // the block's hits per material class
     const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
     const float tmin = depth == 0 ? kCameraTMin : kBounceTMin;
     const int lane = threadIdx.x & 31;
+    const bool sorted = !B && depth > 0 && p.shape.sort_rays;
+    const int refill_idle = p.shape.refill_idle;
+    const bool quant = W >= 4 && Q == 1;
+    if (threadIdx.x < 8) s_class[threadIdx.x] = 0;
+    __syncthreads();
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_extend, (unsigned long long)count);
+    int2* const st = stk + threadIdx.x;
+    const int stride = blockDim.x;
     TraceWork work;
-    int class_count = 0;  // lane c < 5 counts the warp's hits of material class c
+    // the lane's query; slot < 0: none (then alive is false as well)
+    int slot = -1, cur = kEmptyChild, sp = 0, of = 0;
+    bool alive = false, hit_any = false;
+    RayPre r = make_raypre(V{0.f, 0.f, 0.f}, V{0.f, 0.f, 1.f});
+    Hit h{FLT_MAX, 0.f, 0.f, kMissPrim};
+    SceneDevice scb;
+    if (B) scb = p.sc;
+    bool more = true;  // warp-uniform: the queue may hold rays not yet taken
     for (;;) {
-        const int base = warp_fetch(&p.counters->work_extend[depth]);
-        if (base >= count) break;
-        const bool valid = base + lane < count;
-        const int i = !B && valid && depth > 0 && p.shape.sort_rays ? p.ray_index[base + lane] : base + lane;
-        int key = -1;
-        const float4 o = valid ? q.o[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 d = valid ? q.d[i] : make_float4(0.f, 0.f, 1.f, 0.f);
-        const RayPre r = make_raypre(mkv(o), mkv(d));
-        Hit h;
-        int of = 0;
-        SceneDevice scb;
-        if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(o.w)));
-        const SceneDevice& sc = B ? scb : p.sc;
-        traverse<W, false, CNT, Q>(sc, r, tmin, FLT_MAX, valid, stk + threadIdx.x, blockDim.x, p.stack_depth, h,
-                                   of, &work);
-        if (valid) {
-            if (of) atomicOr(&p.stats->error, 1);
-            q.hit[i] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
-            if (p.shape.sort_materials) {
-                key = material_class(p.sc, h.prim);
-                q.key[i] = key;
+        if (more) {
+            const unsigned busy = __ballot_sync(0xffffffffu, slot >= 0);
+            const int idle = 32 - __popc(busy);
+            if (idle >= refill_idle) {  // refill_idle is in [1, 32]: an all-idle warp always fetches
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&p.counters->work_extend[depth], idle);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base + idle >= count) more = false;
+                const int k = base + __popc(~busy & lanemask_lt());
+                if (slot < 0 && k < count) {
+                    slot = sorted ? p.ray_index[k] : k;
+                    const float4 o = q.o[slot], d = q.d[slot];
+                    r = make_raypre(mkv(o), mkv(d));
+                    if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(o.w)));
+                    h = Hit{FLT_MAX, 0.f, 0.f, kMissPrim};
+                    cur = B ? scb.root : p.sc.root;
+                    sp = 0;
+                    of = 0;
+                    alive = true;
+                }
             }
         }
-        if (p.shape.sort_materials) {
-#pragma unroll
-            for (int c = 0; c < 5; c++) {
-                const unsigned m = __ballot_sync(0xffffffffu, key == c);
-                if (lane == c) class_count += __popc(m);
+        // with no query left after a fetch, the queue is exhausted (more is false)
+        if (!__any_sync(0xffffffffu, alive)) break;
+        const SceneDevice& sc = B ? scb : p.sc;
+        // ---- phase 1: internal nodes, until every live lane holds a leaf or has finished
+        while (__any_sync(0xffffffffu, alive && cur >= 0)) {
+            if (alive && cur >= 0)
+                node_step<W, false, CNT>(sc.nodes, quant, r, tmin, FLT_MAX, st, stride, p.stack_depth, h, cur, sp,
+                                         alive, of, &work);
+        }
+        // ---- phase 2: leaves
+        if (alive)
+            leaf_step<W, false, CNT>(sc.nodes, sc.prims, quant, r, tmin, FLT_MAX, st, stride, h, cur, sp, alive,
+                                     hit_any, &work);
+        if (slot >= 0 && !alive) {  // the query ended: write its hit to the ray's own slot
+            if (of) atomicOr(&p.stats->error, 1);
+            q.hit[slot] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
+            if (p.shape.sort_materials) {
+                const int key = material_class(p.sc, h.prim);
+                q.key[slot] = key;
+                atomicAdd(&s_class[key], 1);
             }
+            slot = -1;
         }
     }
-    // one atomic per class and warp for the whole persistent loop
-    if (p.shape.sort_materials && lane < 5 && class_count > 0)
-        atomicAdd(&p.counters->sort_count[depth][lane], class_count);
+    __syncthreads();
+    // one atomic per class and block for the whole persistent loop
+    if (p.shape.sort_materials && threadIdx.x < 5 && s_class[threadIdx.x] > 0)
+        atomicAdd(&p.counters->sort_count[depth][threadIdx.x], s_class[threadIdx.x]);
     if (CNT) flush_work(work, &p.stats->extend_nodes, &p.stats->extend_prims);
 }
 
@@ -579,36 +617,70 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
     extern __shared__ int2 stk[];
     const int count = p.counters->shadow_count[depth];
     const int lane = threadIdx.x & 31;
+    const int refill_idle = p.shape.refill_idle;
+    const bool quant = W >= 4 && Q == 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_shadow, (unsigned long long)count);
+    int2* const st = stk + threadIdx.x;
+    const int stride = blockDim.x;
     TraceWork work;
+    // the lane's query, refilled as in k_extend; slot < 0: none
+    int slot = -1, cur = kEmptyChild, sp = 0, of = 0, tag = 0;
+    bool alive = false, occ = false;
+    float tmax = 0.f;
+    RayPre r = make_raypre(V{0.f, 0.f, 0.f}, V{0.f, 0.f, 1.f});
+    Hit h{0.f, 0.f, 0.f, kMissPrim};  // unused by any-hit queries
+    SceneDevice scb;
+    if (B) scb = p.sc;
+    bool more = true;  // warp-uniform
     for (;;) {
-        const int base = warp_fetch(&p.counters->work_shadow[depth]);
-        if (base >= count) break;
-        const int i = base + lane;
-        const bool valid = i < count;
-        const float4 o = valid ? p.sq.o[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 d = valid ? p.sq.d[i] : make_float4(0.f, 0.f, 1.f, 0.f);
-        const RayPre r = make_raypre(mkv(o), mkv(d));
-        Hit h;
-        int of = 0;
-        SceneDevice scb;
-        if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(d.w)));
+        if (more) {
+            const unsigned busy = __ballot_sync(0xffffffffu, slot >= 0);
+            const int idle = 32 - __popc(busy);
+            if (idle >= refill_idle) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&p.counters->work_shadow[depth], idle);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base + idle >= count) more = false;
+                const int k = base + __popc(~busy & lanemask_lt());
+                if (slot < 0 && k < count) {
+                    slot = k;
+                    const float4 o = p.sq.o[k], d = p.sq.d[k];
+                    r = make_raypre(mkv(o), mkv(d));
+                    tmax = o.w;
+                    tag = __float_as_int(d.w);
+                    if (B) scb = batch_scene_view(p, tag_scene(tag));
+                    cur = B ? scb.root : p.sc.root;
+                    sp = 0;
+                    of = 0;
+                    occ = false;
+                    alive = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, alive)) break;
         const SceneDevice& sc = B ? scb : p.sc;
-        const bool occ = traverse<W, true, CNT, Q>(sc, r, kShadowTMin, o.w, valid, stk + threadIdx.x, blockDim.x,
-                                                   p.stack_depth, h, of, &work);
-        if (valid) {
+        while (__any_sync(0xffffffffu, alive && cur >= 0)) {
+            if (alive && cur >= 0)
+                node_step<W, true, CNT>(sc.nodes, quant, r, kShadowTMin, tmax, st, stride, p.stack_depth, h, cur, sp,
+                                        alive, of, &work);
+        }
+        if (alive)
+            leaf_step<W, true, CNT>(sc.nodes, sc.prims, quant, r, kShadowTMin, tmax, st, stride, h, cur, sp, alive,
+                                    occ, &work);
+        if (slot >= 0 && !alive) {  // the query ended: occluded, or the stack ran empty
+            const int i = slot;
+            slot = -1;
             if (of) atomicOr(&p.stats->error, 1);
             if (!occ) {
                 const float4 c = p.sq.c[i];
-                const int path = tag_path(__float_as_int(d.w));
+                const int path = tag_path(tag);
                 float4 l = p.L[path];
                 l.x += c.x;
                 l.y += c.y;
                 l.z += c.z;
                 p.L[path] = l;
                 if (p.guide_mode) {
-                    const int tg = __float_as_int(d.w);
-                    const long long ti = train_index<B>(p, tag_scene(tg), path, wave_first, gfirst);
+                    const long long ti = train_index<B>(p, tag_scene(tag), path, wave_first, gfirst);
                     guide_account(p, ti, depth, 0.f, (c.x + c.y + c.z) * (1.f / 3.f), 0.f);
                 }
             }

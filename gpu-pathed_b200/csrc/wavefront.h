@@ -78,6 +78,7 @@ struct LaunchShape {
     int blocks_per_sm = 16;   // persistent grid = SMs * blocks_per_sm
     int sort_materials = 1;   // material-sorted shading
     int sort_rays = 0;        // continuation rays extended in (origin cell, direction octant) order
+    int refill_idle = 16;     // traversal stages: a warp fetches new rays once this many lanes are idle
 };
 
 // Ray sorting ahead of the closest-hit stage (single-scene frames, depth >= 1): the key of a

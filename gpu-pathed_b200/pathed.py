@@ -102,7 +102,7 @@ class SceneExport(C.Structure):
 class LaunchConfig(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "wave_paths", "block_extend", "block_shade", "block_shadow", "blocks_per_sm", "sort_materials",
-        "use_graph", "sort_rays")]
+        "use_graph", "sort_rays", "refill_idle")]
 
 
 class Stats(C.Structure):

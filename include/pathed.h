@@ -115,6 +115,9 @@ typedef struct pt_launch_config {
     int sort_rays;         /* 1: sort continuation rays by origin cell and direction octant
                               before the closest-hit stage (single-scene frames), 2: off
                               (default); images are the same either way */
+    int refill_idle;       /* closest-hit and shadow stages: a warp takes new rays from its queue
+                              once this many of its 32 lanes are idle (1-32; 32 = only when all
+                              are; default 16) */
 } pt_launch_config;
 
 /* Result of pt_autotune. */

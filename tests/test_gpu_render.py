@@ -183,6 +183,28 @@ def test_ray_sorting_does_not_change_images(case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", [(0, None), (1, None), (2, 4), (3, 4)], ids=lambda c: f"cfg{c[0]}")
+def test_lane_refill_does_not_change_images(case):
+    """idle lanes of the closest-hit stage taking new rays mid-traversal changes which lanes
+    carry which queries, never a hit: images, ray counts and node visits are identical"""
+    out = []
+    for refill in (32, 8, 1):
+        s = pathed.Session(96, 80)
+        s.load_config(case[0], level=case[1])
+        s.set_launch(refill_idle=refill, wave_paths=20000)
+        s.set_seed(9)
+        s.set_profiling(stage_timing=True, work_counters=True)
+        for _ in range(2):
+            s.render(4)
+        st, pr = s.stats(), s.profile()
+        out.append((s.readback().copy(), st["rays_extend"], st["rays_shadow"], pr["extend_nodes"]))
+        s.close()
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0])
+        assert out[0][1:] == o[1:]
+
+
+@pytest.mark.gpu
 def test_stats_count_canonical_queries(oracle_lib):
     w = h = 32
     s = pathed.Session(w, h)

@@ -129,6 +129,12 @@ def test_launch_config_host_state():
             s.set_launch(sort_rays=bad)
     s.set_launch(sort_rays=2)
     assert s.get_launch()["sort_rays"] == 2
+    assert cfg["refill_idle"] == 16
+    s.set_launch(refill_idle=32)
+    assert s.get_launch()["refill_idle"] == 32
+    for bad in (-1, 33):
+        with pytest.raises(pathed.PathedError):
+            s.set_launch(refill_idle=bad)
     s.close()
 
 
