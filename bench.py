@@ -423,8 +423,8 @@ def run_ours(args):
         }
         if tuned is not None:
             line["config"]["autotuned"] = {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays",
-                                                               "blocks_per_sm", "block", "wave_paths", "best_ms",
-                                                               "default_ms")}
+                                                               "speculate", "blocks_per_sm", "block", "wave_paths",
+                                                               "best_ms", "default_ms")}
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:

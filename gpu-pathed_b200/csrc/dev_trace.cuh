@@ -341,14 +341,12 @@ __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool
     if (cur == kEmptyChild) alive = false;
 }
 
-// One leaf visit of a live query (`cur` a leaf code): test its entries, then pop the stack.
-// An any-hit query ends at its first hit (`hit_any`); every query ends on an empty stack.
-template <int W, bool ANY, bool CNT>
-__device__ __forceinline__ void leaf_step(const float4* __restrict__ nodes, const float4* __restrict__ prims,
-                                          bool quant, const RayPre& r, float tmin, float tmax,
-                                          int2* __restrict__ stk, int stride, Hit& best, int& cur, int& sp,
-                                          bool& alive, bool& hit_any, TraceWork* work) {
-    const int first = leaf_first(cur), cnt = leaf_count(cur);
+// Test the entries of one leaf (`leaf` a leaf code) against a query; an any-hit query stops
+// at its first hit.
+template <bool ANY, bool CNT>
+__device__ __forceinline__ void leaf_test(const float4* __restrict__ prims, int leaf, const RayPre& r, float tmin,
+                                          float tmax, Hit& best, bool& hit_any, TraceWork* work) {
+    const int first = leaf_first(leaf), cnt = leaf_count(leaf);
     if (CNT) work->prims += cnt;
     if (ANY) {
         for (int e = first; e < first + cnt; e++) {
@@ -357,14 +355,67 @@ __device__ __forceinline__ void leaf_step(const float4* __restrict__ nodes, cons
                 break;
             }
         }
-        if (hit_any) alive = false;
     } else {
         for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
     }
+}
+
+// One leaf visit of a live query (`cur` a leaf code): test its entries, then pop the stack.
+// An any-hit query ends at its first hit (`hit_any`); every query ends on an empty stack.
+template <int W, bool ANY, bool CNT>
+__device__ __forceinline__ void leaf_step(const float4* __restrict__ nodes, const float4* __restrict__ prims,
+                                          bool quant, const RayPre& r, float tmin, float tmax,
+                                          int2* __restrict__ stk, int stride, Hit& best, int& cur, int& sp,
+                                          bool& alive, bool& hit_any, TraceWork* work) {
+    leaf_test<ANY, CNT>(prims, cur, r, tmin, tmax, best, hit_any, work);
+    if (ANY && hit_any) alive = false;
     if (alive) {
         cur = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
         if (cur == kEmptyChild) alive = false;
     }
+}
+
+// One round of the warp-synchronous traversal; every lane of the warp calls it together.
+// Phase 1 visits internal nodes until each live lane holds a leaf (or its query ended);
+// phase 2 tests the leaves. With `spec` (speculative traversal, Aila and Laine 2009), a lane
+// that reaches its first leaf parks it in `pend` and keeps descending while some lane of the
+// warp has found no leaf yet, so the node phase runs with fuller warps; the parked leaf is
+// tested in phase 2. Closest hits are the minimum of a total order, so the visiting order
+// never changes a result; speculation only visits nodes that a tighter bound might have culled.
+template <int W, bool ANY, bool CNT>
+__device__ __forceinline__ void traverse_round(const float4* __restrict__ nodes, const float4* __restrict__ prims,
+                                               bool quant, bool spec, const RayPre& r, float tmin, float tmax,
+                                               int2* __restrict__ stk, int stride, int max_depth, Hit& best,
+                                               int& cur, int& pend, int& sp, bool& alive, bool& hit_any,
+                                               int& overflow, TraceWork* work) {
+    // ---- phase 1: internal nodes, while some live lane has found no leaf
+    while (__any_sync(0xffffffffu, alive && cur >= 0 && pend == kEmptyChild)) {
+        if (alive && cur >= 0) {
+            node_step<W, ANY, CNT>(nodes, quant, r, tmin, tmax, stk, stride, max_depth, best, cur, sp, alive, overflow,
+                                   work);
+            if (spec) {
+                if (!alive && !overflow && pend != kEmptyChild) {
+                    alive = true;  // the stack ran empty: only the parked leaf is left
+                    cur = pend;
+                    pend = kEmptyChild;
+                } else if (alive && cur < 0 && pend == kEmptyChild) {
+                    pend = cur;  // park the first leaf and keep descending
+                    cur = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
+                    if (cur == kEmptyChild) {
+                        cur = pend;
+                        pend = kEmptyChild;
+                    }
+                }
+            }
+        }
+    }
+    // ---- phase 2: the parked leaf, then the current one (which pops the stack)
+    if (alive && pend != kEmptyChild) {
+        leaf_test<ANY, CNT>(prims, pend, r, tmin, tmax, best, hit_any, work);
+        pend = kEmptyChild;
+        if (ANY && hit_any) alive = false;
+    }
+    if (alive && cur < 0) leaf_step<W, ANY, CNT>(nodes, prims, quant, r, tmin, tmax, stk, stride, best, cur, sp, alive, hit_any, work);
 }
 
 // Warp-synchronous traversal: every lane of the warp calls this together (`active` marks the
@@ -386,16 +437,10 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
     int cur = active ? sc.root : kEmptyChild;
     bool alive = active;
     bool hit_any = false;
-    while (__any_sync(0xffffffffu, alive)) {
-        // ---- phase 1: internal nodes, until this lane holds a leaf (or is finished)
-        while (__any_sync(0xffffffffu, alive && cur >= 0)) {
-            if (alive && cur >= 0)
-                node_step<W, ANY, CNT>(nodes, quant, r, tmin, tmax, stk, stride, max_depth, best, cur, sp, alive,
-                                       overflow, work);
-        }
-        // ---- phase 2: leaves
-        if (alive) leaf_step<W, ANY, CNT>(nodes, prims, quant, r, tmin, tmax, stk, stride, best, cur, sp, alive, hit_any, work);
-    }
+    int pend = kEmptyChild;
+    while (__any_sync(0xffffffffu, alive))
+        traverse_round<W, ANY, CNT>(nodes, prims, quant, false, r, tmin, tmax, stk, stride, max_depth, best, cur, pend,
+                                    sp, alive, hit_any, overflow, work);
     if (ANY) {
         if (hit_any) best.prim = 0;
         return hit_any;

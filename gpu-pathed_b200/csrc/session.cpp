@@ -603,7 +603,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->wave_paths < 0 || c->blocks_per_sm < 0 || c->blocks_per_sm > 64)
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
-        c->sort_rays < 0 || c->sort_rays > 2)
+        c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 2)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
@@ -615,6 +615,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->use_graph) use_graph_ = c->use_graph == 1 ? 1 : 0;
     if (c->sort_rays) shape_.sort_rays = c->sort_rays == 1 ? 1 : 0;
     if (c->refill_idle) shape_.refill_idle = c->refill_idle;
+    if (c->speculate) shape_.speculate = c->speculate == 1 ? 1 : 0;
     return PT_OK;
 }
 
@@ -628,6 +629,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->use_graph = use_graph_ ? 1 : 2;
     c->sort_rays = shape_.sort_rays ? 1 : 2;
     c->refill_idle = shape_.refill_idle;
+    c->speculate = shape_.speculate ? 1 : 2;
 }
 
 int Session::upload_materials() {
@@ -1121,7 +1123,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     std::memset(&res, 0, sizeof(res));
     const std::string key = tune_key(scene_, material_classes_, w_, h_, spp, max_depth_, nee_);
     struct Cand {
-        int width, sort, bps, block, rays;
+        int width, sort, bps, block, rays, spec;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
@@ -1130,6 +1132,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         shape_.blocks_per_sm = c.bps;
         shape_.block_extend = shape_.block_shadow = c.block;
         shape_.sort_rays = c.rays;
+        shape_.speculate = c.spec;
         return PT_OK;
     };
     auto report = [&](const Cand& c) {
@@ -1138,6 +1141,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.blocks_per_sm = c.bps;
         res.block = c.block;
         res.sort_rays = c.rays ? 1 : 2;
+        res.speculate = c.spec ? 1 : 2;
         res.wave_paths = wave_paths_;
     };
     if (cache_path) {
@@ -1149,7 +1153,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 const std::string line(buf);
                 if (line.find(want) == std::string::npos) continue;
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
-                       json_int(line, "block", 128), json_int(line, "sort_rays", 0)};
+                       json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1183,7 +1187,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
-              shape_.block_extend, shape_.sort_rays};
+              shape_.block_extend, shape_.sort_rays, shape_.speculate};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1219,6 +1223,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         c.rays = best.rays ? 0 : 1;
         if ((r = consider(c))) return r;
     }
+    {
+        Cand c = best;
+        c.spec = best.spec ? 0 : 1;
+        if ((r = consider(c))) return r;
+    }
     for (int bps : {8, 24}) {
         Cand c = best;
         c.bps = bps;
@@ -1240,9 +1249,10 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         if (f) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
-                         "\"sort_rays\": %d, \"wave_paths\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
-                         key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, wave_paths_, best_ms,
-                         res.default_ms);
+                         "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"ms\": %.4f, "
+                         "\"default_ms\": %.4f}\n",
+                         key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, wave_paths_,
+                         best_ms, res.default_ms);
             std::fclose(f);
         }
     }

@@ -234,6 +234,7 @@ __global__ void k_extend(FrameParams p, int depth) {
     const int lane = threadIdx.x & 31;
     const bool sorted = !B && depth > 0 && p.shape.sort_rays;
     const int refill_idle = p.shape.refill_idle;
+    const bool spec = p.shape.speculate != 0;
     const bool quant = W >= 4 && Q == 1;
     if (threadIdx.x < 8) s_class[threadIdx.x] = 0;
     __syncthreads();
@@ -242,7 +243,7 @@ __global__ void k_extend(FrameParams p, int depth) {
     const int stride = blockDim.x;
     TraceWork work;
     // the lane's query; slot < 0: none (then alive is false as well)
-    int slot = -1, cur = kEmptyChild, sp = 0, of = 0;
+    int slot = -1, cur = kEmptyChild, pend = kEmptyChild, sp = 0, of = 0;
     bool alive = false, hit_any = false;
     RayPre r = make_raypre(V{0.f, 0.f, 0.f}, V{0.f, 0.f, 1.f});
     Hit h{FLT_MAX, 0.f, 0.f, kMissPrim};
@@ -267,6 +268,7 @@ __global__ void k_extend(FrameParams p, int depth) {
                     h = Hit{FLT_MAX, 0.f, 0.f, kMissPrim};
                     cur = B ? scb.root : p.sc.root;
                     sp = 0;
+                    pend = kEmptyChild;
                     of = 0;
                     alive = true;
                 }
@@ -275,16 +277,8 @@ __global__ void k_extend(FrameParams p, int depth) {
         // with no query left after a fetch, the queue is exhausted (more is false)
         if (!__any_sync(0xffffffffu, alive)) break;
         const SceneDevice& sc = B ? scb : p.sc;
-        // ---- phase 1: internal nodes, until every live lane holds a leaf or has finished
-        while (__any_sync(0xffffffffu, alive && cur >= 0)) {
-            if (alive && cur >= 0)
-                node_step<W, false, CNT>(sc.nodes, quant, r, tmin, FLT_MAX, st, stride, p.stack_depth, h, cur, sp,
-                                         alive, of, &work);
-        }
-        // ---- phase 2: leaves
-        if (alive)
-            leaf_step<W, false, CNT>(sc.nodes, sc.prims, quant, r, tmin, FLT_MAX, st, stride, h, cur, sp, alive,
-                                     hit_any, &work);
+        traverse_round<W, false, CNT>(sc.nodes, sc.prims, quant, spec, r, tmin, FLT_MAX, st, stride, p.stack_depth, h,
+                                      cur, pend, sp, alive, hit_any, of, &work);
         if (slot >= 0 && !alive) {  // the query ended: write its hit to the ray's own slot
             if (of) atomicOr(&p.stats->error, 1);
             q.hit[slot] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
@@ -618,13 +612,14 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
     const int count = p.counters->shadow_count[depth];
     const int lane = threadIdx.x & 31;
     const int refill_idle = p.shape.refill_idle;
+    const bool spec = p.shape.speculate != 0;
     const bool quant = W >= 4 && Q == 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_shadow, (unsigned long long)count);
     int2* const st = stk + threadIdx.x;
     const int stride = blockDim.x;
     TraceWork work;
     // the lane's query, refilled as in k_extend; slot < 0: none
-    int slot = -1, cur = kEmptyChild, sp = 0, of = 0, tag = 0;
+    int slot = -1, cur = kEmptyChild, pend = kEmptyChild, sp = 0, of = 0, tag = 0;
     bool alive = false, occ = false;
     float tmax = 0.f;
     RayPre r = make_raypre(V{0.f, 0.f, 0.f}, V{0.f, 0.f, 1.f});
@@ -651,6 +646,7 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
                     if (B) scb = batch_scene_view(p, tag_scene(tag));
                     cur = B ? scb.root : p.sc.root;
                     sp = 0;
+                    pend = kEmptyChild;
                     of = 0;
                     occ = false;
                     alive = true;
@@ -659,14 +655,8 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
         }
         if (!__any_sync(0xffffffffu, alive)) break;
         const SceneDevice& sc = B ? scb : p.sc;
-        while (__any_sync(0xffffffffu, alive && cur >= 0)) {
-            if (alive && cur >= 0)
-                node_step<W, true, CNT>(sc.nodes, quant, r, kShadowTMin, tmax, st, stride, p.stack_depth, h, cur, sp,
-                                        alive, of, &work);
-        }
-        if (alive)
-            leaf_step<W, true, CNT>(sc.nodes, sc.prims, quant, r, kShadowTMin, tmax, st, stride, h, cur, sp, alive,
-                                    occ, &work);
+        traverse_round<W, true, CNT>(sc.nodes, sc.prims, quant, spec, r, kShadowTMin, tmax, st, stride, p.stack_depth,
+                                     h, cur, pend, sp, alive, occ, of, &work);
         if (slot >= 0 && !alive) {  // the query ended: occluded, or the stack ran empty
             const int i = slot;
             slot = -1;

@@ -79,6 +79,7 @@ struct LaunchShape {
     int sort_materials = 1;   // material-sorted shading
     int sort_rays = 0;        // continuation rays extended in (origin cell, direction octant) order
     int refill_idle = 16;     // traversal stages: a warp fetches new rays once this many lanes are idle
+    int speculate = 0;        // traversal stages: park a lane's first leaf and keep descending
 };
 
 // Ray sorting ahead of the closest-hit stage (single-scene frames, depth >= 1): the key of a

@@ -118,6 +118,9 @@ typedef struct pt_launch_config {
     int refill_idle;       /* closest-hit and shadow stages: a warp takes new rays from its queue
                               once this many of its 32 lanes are idle (1-32; 32 = only when all
                               are; default 16) */
+    int speculate;         /* closest-hit and shadow stages: 1 speculative traversal (a lane
+                              parks its first leaf and keeps descending while other lanes of
+                              its warp search for one), 2 off (default) */
 } pt_launch_config;
 
 /* Result of pt_autotune. */
@@ -132,6 +135,7 @@ typedef struct pt_tune_result {
     int trials;             /* frames measured (0 when taken from the cache) */
     int from_cache;
     int sort_rays;          /* 1 on, 2 off */
+    int speculate;          /* 1 on, 2 off */
 } pt_tune_result;
 
 typedef struct pt_stats {
@@ -309,7 +313,8 @@ int pt_set_launch(pt_session* s, const pt_launch_config* cfg);
 int pt_get_launch(const pt_session* s, pt_launch_config* out);
 /* Autotuner (no counterpart in the reference, whose only tuning is SppOptimizer's spp
  * budget, src/spp_optimizer.cpp:8-29): times frames of `spp` samples on the loaded scene over
- * BVH width, material sorting, ray sorting, persistent-grid size and block size (coordinate descent),
+ * BVH width, material sorting, ray sorting, speculative traversal, persistent-grid size and block
+ * size (coordinate descent),
  * applies the fastest and restarts accumulation. With cache_path, results are stored as one
  * JSON object per line keyed by scene size, material classes, resolution, spp, depth and
  * NEE, and a cached key is applied without measuring. */

@@ -135,6 +135,11 @@ def test_launch_config_host_state():
     for bad in (-1, 33):
         with pytest.raises(pathed.PathedError):
             s.set_launch(refill_idle=bad)
+    assert cfg["speculate"] == 2
+    s.set_launch(speculate=1)
+    assert s.get_launch()["speculate"] == 1
+    with pytest.raises(pathed.PathedError):
+        s.set_launch(speculate=3)
     s.close()
 
 
