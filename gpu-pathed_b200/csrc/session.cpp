@@ -19,7 +19,19 @@ namespace pt {
 
 namespace {
 constexpr int kMaxStackBytesDefault = 48 * 1024;
+
+// pt_launch_config.speculate (1 both stages, 2 off, 3 closest hit, 4 shadow) <-> kSpeculate* bits
+int speculate_bits(int code) {
+    return code == 1 ? kSpeculateExtend | kSpeculateShadow : code == 3 ? kSpeculateExtend
+                                                           : code == 4 ? kSpeculateShadow
+                                                                       : 0;
 }
+int speculate_code(int bits) {
+    return bits == (kSpeculateExtend | kSpeculateShadow) ? 1 : bits == kSpeculateExtend ? 3
+                                                           : bits == kSpeculateShadow   ? 4
+                                                                                        : 2;
+}
+}  // namespace
 
 Session::Session(int w, int h) : w_(w), h_(h) {
     // Reference default camera of scene 0 (src/scene.cu:176-184).
@@ -603,7 +615,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->wave_paths < 0 || c->blocks_per_sm < 0 || c->blocks_per_sm > 64)
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
-        c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 2)
+        c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 4)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
@@ -615,7 +627,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->use_graph) use_graph_ = c->use_graph == 1 ? 1 : 0;
     if (c->sort_rays) shape_.sort_rays = c->sort_rays == 1 ? 1 : 0;
     if (c->refill_idle) shape_.refill_idle = c->refill_idle;
-    if (c->speculate) shape_.speculate = c->speculate == 1 ? 1 : 0;
+    if (c->speculate) shape_.speculate = speculate_bits(c->speculate);
     return PT_OK;
 }
 
@@ -629,7 +641,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->use_graph = use_graph_ ? 1 : 2;
     c->sort_rays = shape_.sort_rays ? 1 : 2;
     c->refill_idle = shape_.refill_idle;
-    c->speculate = shape_.speculate ? 1 : 2;
+    c->speculate = speculate_code(shape_.speculate);
 }
 
 int Session::upload_materials() {
@@ -1141,7 +1153,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.blocks_per_sm = c.bps;
         res.block = c.block;
         res.sort_rays = c.rays ? 1 : 2;
-        res.speculate = c.spec ? 1 : 2;
+        res.speculate = speculate_code(c.spec);
         res.wave_paths = wave_paths_;
     };
     if (cache_path) {
@@ -1224,9 +1236,13 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         if ((r = consider(c))) return r;
     }
     {
-        Cand c = best;
-        c.spec = best.spec ? 0 : 1;
-        if ((r = consider(c))) return r;
+        const Cand base = best;  // speculation per traversal stage: none, either, both
+        for (int bits = 0; bits <= (kSpeculateExtend | kSpeculateShadow); bits++)
+            if (bits != base.spec) {
+                Cand c = base;
+                c.spec = bits;
+                if ((r = consider(c))) return r;
+            }
     }
     for (int bps : {8, 24}) {
         Cand c = best;

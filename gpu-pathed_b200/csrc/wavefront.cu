@@ -234,7 +234,7 @@ __global__ void k_extend(FrameParams p, int depth) {
     const int lane = threadIdx.x & 31;
     const bool sorted = !B && depth > 0 && p.shape.sort_rays;
     const int refill_idle = p.shape.refill_idle;
-    const bool spec = p.shape.speculate != 0;
+    const bool spec = (p.shape.speculate & kSpeculateExtend) != 0;
     const bool quant = W >= 4 && Q == 1;
     if (threadIdx.x < 8) s_class[threadIdx.x] = 0;
     __syncthreads();
@@ -612,7 +612,7 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
     const int count = p.counters->shadow_count[depth];
     const int lane = threadIdx.x & 31;
     const int refill_idle = p.shape.refill_idle;
-    const bool spec = p.shape.speculate != 0;
+    const bool spec = (p.shape.speculate & kSpeculateShadow) != 0;
     const bool quant = W >= 4 && Q == 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_shadow, (unsigned long long)count);
     int2* const st = stk + threadIdx.x;

@@ -79,8 +79,11 @@ struct LaunchShape {
     int sort_materials = 1;   // material-sorted shading
     int sort_rays = 0;        // continuation rays extended in (origin cell, direction octant) order
     int refill_idle = 16;     // traversal stages: a warp fetches new rays once this many lanes are idle
-    int speculate = 0;        // traversal stages: park a lane's first leaf and keep descending
+    int speculate = 0;        // kSpeculate* bits: stages that park a lane's first leaf and descend on
 };
+
+constexpr int kSpeculateExtend = 1;  // closest-hit stage
+constexpr int kSpeculateShadow = 2;  // shadow (any-hit) stage
 
 // Ray sorting ahead of the closest-hit stage (single-scene frames, depth >= 1): the key of a
 // ray is its origin's cell in a 4x4x4 grid over the scene bounds and its direction octant.

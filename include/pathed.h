@@ -118,9 +118,10 @@ typedef struct pt_launch_config {
     int refill_idle;       /* closest-hit and shadow stages: a warp takes new rays from its queue
                               once this many of its 32 lanes are idle (1-32; 32 = only when all
                               are; default 16) */
-    int speculate;         /* closest-hit and shadow stages: 1 speculative traversal (a lane
-                              parks its first leaf and keeps descending while other lanes of
-                              its warp search for one), 2 off (default) */
+    int speculate;         /* speculative traversal (a lane parks its first leaf and keeps
+                              descending while other lanes of its warp search for one):
+                              1 closest-hit and shadow stages, 2 off (default), 3 closest-hit
+                              stage only, 4 shadow stage only */
 } pt_launch_config;
 
 /* Result of pt_autotune. */
@@ -135,7 +136,7 @@ typedef struct pt_tune_result {
     int trials;             /* frames measured (0 when taken from the cache) */
     int from_cache;
     int sort_rays;          /* 1 on, 2 off */
-    int speculate;          /* 1 on, 2 off */
+    int speculate;          /* as pt_launch_config.speculate: 1 both stages, 2 off, 3 closest hit, 4 shadow */
 } pt_tune_result;
 
 typedef struct pt_stats {

@@ -136,10 +136,11 @@ def test_launch_config_host_state():
         with pytest.raises(pathed.PathedError):
             s.set_launch(refill_idle=bad)
     assert cfg["speculate"] == 2
-    s.set_launch(speculate=1)
-    assert s.get_launch()["speculate"] == 1
+    for code in (1, 3, 4, 2):  # both stages, closest hit only, shadow only, off
+        s.set_launch(speculate=code)
+        assert s.get_launch()["speculate"] == code
     with pytest.raises(pathed.PathedError):
-        s.set_launch(speculate=3)
+        s.set_launch(speculate=5)
     s.close()
 
 
