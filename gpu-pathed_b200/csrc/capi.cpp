@@ -378,6 +378,10 @@ int pt_get_profile(const pt_session* s, pt_profile* out) {
 
 int pt_readback(pt_session* s, float* rgb, size_t n) { return s ? s->impl.readback(rgb, n, false) : PT_ERR_ARG; }
 int pt_readback_pass(pt_session* s, float* rgb, size_t n) { return s ? s->impl.readback(rgb, n, true) : PT_ERR_ARG; }
+int pt_readback_async(pt_session* s, float* rgb, size_t n) {
+    return s ? s->impl.readback_async(rgb, n) : PT_ERR_ARG;
+}
+int pt_readback_wait(pt_session* s) { return s ? s->impl.readback_wait() : PT_ERR_ARG; }
 int pt_readback_rgba8(pt_session* s, uint8_t* rgba, size_t n) {
     return s ? s->impl.readback_rgba8(rgba, n) : PT_ERR_ARG;
 }

@@ -42,6 +42,12 @@ Session::~Session() {
     if (dev_ready_) {
         cudaSetDevice(device_);
         if (stream_) cudaStreamSynchronize(stream_);
+        if (copy_stream_) {
+            cudaStreamSynchronize(copy_stream_);
+            cudaStreamDestroy(copy_stream_);
+        }
+        if (rb_snap_) cudaEventDestroy(rb_snap_);
+        if (rb_done_) cudaEventDestroy(rb_done_);
         if (ev_begin_) cudaEventDestroy(ev_begin_);
         if (ev_end_) cudaEventDestroy(ev_end_);
         for (cudaEvent_t e : mark_events_) cudaEventDestroy(e);
@@ -1309,6 +1315,39 @@ int Session::readback(float* rgb, size_t n, bool pass) {
     DevBuf& src = pass ? d_pass_ : d_accum_;
     if ((r = check_cuda(cudaMemcpyAsync(rgb, src.p, need * 4, cudaMemcpyDeviceToHost, stream_), "readback"))) return r;
     return check_cuda(cudaStreamSynchronize(stream_), "readback");
+}
+
+int Session::readback_async(float* rgb, size_t n) {
+    const size_t need = (size_t)w_ * h_ * 3;
+    if (!rgb || n < need) return fail(PT_ERR_ARG, "readback buffer too small");
+    if (!dev_ready_ || (frames_ == 0 && !in_flight_)) return fail(PT_ERR_STATE, "nothing rendered yet");
+    int r;
+    if ((r = readback_wait())) return r;  // the staging buffer holds one image at a time
+    if (!copy_stream_) {
+        if ((r = check_cuda(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate")))
+            return r;
+        if ((r = check_cuda(cudaEventCreateWithFlags(&rb_snap_, cudaEventDisableTiming), "cudaEventCreate"))) return r;
+        if ((r = check_cuda(cudaEventCreateWithFlags(&rb_done_, cudaEventDisableTiming), "cudaEventCreate"))) return r;
+    }
+    if ((r = check_cuda(d_rb_stage_.alloc(need * 4), "readback staging"))) return r;
+    // snapshot behind the last enqueued frame (device to device), then copy out on the side
+    if ((r = check_cuda(cudaMemcpyAsync(d_rb_stage_.p, d_accum_.p, need * 4, cudaMemcpyDeviceToDevice, stream_),
+                        "readback snapshot")))
+        return r;
+    if ((r = check_cuda(cudaEventRecord(rb_snap_, stream_), "cudaEventRecord"))) return r;
+    if ((r = check_cuda(cudaStreamWaitEvent(copy_stream_, rb_snap_, 0), "cudaStreamWaitEvent"))) return r;
+    if ((r = check_cuda(cudaMemcpyAsync(rgb, d_rb_stage_.p, need * 4, cudaMemcpyDeviceToHost, copy_stream_),
+                        "readback")))
+        return r;
+    if ((r = check_cuda(cudaEventRecord(rb_done_, copy_stream_), "cudaEventRecord"))) return r;
+    rb_pending_ = true;
+    return PT_OK;
+}
+
+int Session::readback_wait() {
+    if (!rb_pending_) return PT_OK;
+    rb_pending_ = false;
+    return check_cuda(cudaEventSynchronize(rb_done_), "readback");
 }
 
 int Session::readback_rgba8(uint8_t* out, size_t n) {

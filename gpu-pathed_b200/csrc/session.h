@@ -100,6 +100,8 @@ public:
     int profile(::pt_profile* out) const;
 
     int readback(float* rgb, size_t n, bool pass);
+    int readback_async(float* rgb, size_t n);
+    int readback_wait();
     int readback_rgba8(uint8_t* out, size_t n);
     int hit_test(int x, int y, int* mat);
     int trace_rays(const float* o, const float* d, const float* tmin, const float* tmax, int n, int* pt,
@@ -166,6 +168,11 @@ private:
     bool in_flight_ = false;
     int inflight_spp_ = 0;
     cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
+    // asynchronous readback: snapshot on stream_, device-to-host copy on copy_stream_
+    cudaStream_t copy_stream_ = nullptr;
+    cudaEvent_t rb_snap_ = nullptr, rb_done_ = nullptr;
+    DevBuf d_rb_stage_;
+    bool rb_pending_ = false;
     float last_ms_ = 0.f;
     int last_spp_ = 0;
     int frames_ = 0;

@@ -43,6 +43,8 @@ EXPORTED = [
     "pt_write_exr",
     "pt_set_guide_fraction",
     "pt_set_bvh_nodes",
+    "pt_readback_async",
+    "pt_readback_wait",
 ]
 
 MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
@@ -192,6 +194,8 @@ def _load():
     lib.pt_poll.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     lib.pt_wait.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
     lib.pt_readback.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.pt_readback_async.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.pt_readback_wait.argtypes = [C.c_void_p]
     lib.pt_readback_pass.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.pt_readback_rgba8.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.pt_batch_generate.argtypes = [C.c_ulonglong, C.c_int, C.c_void_p]
@@ -534,6 +538,19 @@ class Session:
             out = np.empty((self.height, self.width, 3), np.float32)
         fn = lib.pt_readback_pass if pass_only else lib.pt_readback
         self._check(fn(self._h, out.ctypes.data, out.size))
+        return out
+
+    def readback_async(self, out: np.ndarray):
+        """Start copying the running mean as of the last enqueued frame into `out` (float32
+        H x W x 3, ideally page-locked); it overlaps the next frame. readback_wait() finishes it."""
+        if out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float32 array")
+        self._check(lib.pt_readback_async(self._h, out.ctypes.data, out.size))
+        self._pending_out = out  # keep the buffer alive until the copy is waited for
+
+    def readback_wait(self) -> np.ndarray | None:
+        self._check(lib.pt_readback_wait(self._h))
+        out, self._pending_out = getattr(self, "_pending_out", None), None
         return out
 
     def set_bvh_builder(self, gpu: bool):

@@ -343,6 +343,15 @@ int pt_readback(pt_session* s, float* rgb, size_t n);
 int pt_readback_pass(pt_session* s, float* rgb, size_t n);
 /* sRGB-encoded, clamped RGBA8 display buffer (framebuffer.cu:35-40); n bytes >= 4*W*H. */
 int pt_readback_rgba8(pt_session* s, uint8_t* rgba, size_t n);
+/* Asynchronous pt_readback: the running mean as of the last enqueued frame is snapshotted
+ * behind that frame, then copied into `rgb` on a separate copy stream, so the copy overlaps
+ * the next frame. Returns at once; the next pt_render_async may follow immediately.
+ * pt_readback_wait blocks until `rgb` holds the image (a no-op with none pending). `rgb`
+ * should be page-locked for the copy to run asynchronously, and must stay valid until the
+ * wait. A second pt_readback_async first waits for the pending copy. (The reference reads
+ * its display buffer synchronously each frame, renderer.cpp:20-42.) */
+int pt_readback_async(pt_session* s, float* rgb, size_t n);
+int pt_readback_wait(pt_session* s);
 
 /* ---- queries --------------------------------------------------------------------------- */
 /* Material id under pixel (x = column, y = row) through its centre, -1 on a miss

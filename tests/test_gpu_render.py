@@ -244,6 +244,28 @@ def test_graph_replay_matches_direct_launches():
 
 
 @pytest.mark.gpu
+def test_async_readback_overlaps_the_next_frame():
+    """pt_readback_async snapshots the image behind the last enqueued frame: the copy equals
+    a synchronous readback of that frame even when the next frame is already enqueued"""
+    import torch
+
+    s = pathed.Session(128, 96)
+    s.load_config(1)
+    s.render(4)
+    ref = s.readback().copy()
+    host = torch.empty((96, 128, 3), dtype=torch.float32).pin_memory().numpy()
+    s.readback_async(host)
+    s.render_async(4)  # next frame enqueued behind the snapshot
+    got = s.readback_wait()
+    assert got is host and np.array_equal(host, ref)
+    s.wait()
+    s.readback_async(host)  # after the second frame: the two-frame mean
+    s.readback_wait()
+    assert np.array_equal(host, s.readback())
+    s.close()
+
+
+@pytest.mark.gpu
 def test_autotuner_and_cache(tmp_path):
     cache = str(tmp_path / "tune.jsonl")
     s = pathed.Session(128, 128)

@@ -172,4 +172,7 @@ def test_device_calls_fail_cleanly_without_gpu():
     with pytest.raises(pathed.PathedError) as e:
         s.render(1)
     assert e.value.code == pathed.PT_ERR_CUDA
+    with pytest.raises(pathed.PathedError):  # nothing rendered: no image to copy out
+        s.readback_async(np.empty((16, 16, 3), np.float32))
+    assert s.readback_wait() is None  # nothing pending: returns at once
     s.close()
