@@ -27,6 +27,7 @@ contributing shadow rays); Mpaths/s is reported beside it.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import subprocess
@@ -67,9 +68,9 @@ class ClockSampler:
 
     def start(self):
         cmd = ["nvidia-smi", "-i", str(self.index),
-               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+               "--query-gpu=timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-               "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"]
+               "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "50"]
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
@@ -80,31 +81,45 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
-    def stop(self):
+    def wait_first(self, timeout=5.0):
+        """Block until the sampler delivered its first sample (it takes a moment to start)."""
+        t_end = time.time() + timeout
+        while self.proc is not None and not self.lines and time.time() < t_end:
+            time.sleep(0.02)
+
+    def stop(self, t0=None, t1=None):
+        """Median SM clock and the throttle reasons seen in the wall-clock window [t0, t1]
+        (time.time()); by nvidia-smi's own sample timestamps. A window shorter than the
+        sampling interval may hold no sample: then the samples nearest to it stand in."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.12)  # one more sample after the window
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, smax, reasons = [], None, set()
+        rows = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
+            if len(parts) < 8:
                 continue
             try:
-                sm.append(float(parts[0]))
-                smax = float(parts[1])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[1]), float(parts[2]), parts[4:8]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[3:7]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        sm.sort()
-        med = sm[len(sm) // 2] if sm else None
-        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if t0 is None or t0 <= r[0] <= t1]
+        used, where = inside, "inside the timed region"
+        if not inside and rows and t0 is not None:
+            before = [r for r in rows if r[0] < t0][-1:]
+            after = [r for r in rows if r[0] > t1][:1]
+            used, where = before + after, "nearest before and after the timed region (shorter than the 50 ms interval)"
+        sm = sorted(r[1] for r in used)
+        reasons = {nm for r in used for nm, v in zip(names, r[3]) if v.lower() == "active"}
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": used[-1][2] if used else None,
+                "reasons": sorted(reasons), "samples": len(inside), "from": where}
 
 
 def _dist_init():
@@ -311,7 +326,9 @@ def run_ours(args):
 
     clocks = ClockSampler(local)
     clocks.start()
+    clocks.wait_first()
     barrier()
+    t_clk0 = time.time()
     dev_ms = 0.0
     rays = paths = 0
     stage_ms = {k: 0.0 for k in pathed.STAGES}
@@ -329,7 +346,7 @@ def run_ours(args):
             stage_ms[k] += p["stage_ms"][k]
             stage_launches[k] += p["stage_launches"][k]
     barrier()
-    clk = clocks.stop()
+    clk = clocks.stop(t_clk0, time.time())
     t_max, (rays_all, paths_all) = reduce_over_ranks(dev_ms, [rays, paths], world)
     value = rays_all / (t_max / 1e3) / 1e6
 
@@ -343,6 +360,10 @@ def run_ours(args):
         host = torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
         cam_host = torch.from_numpy(cam.copy()).pin_memory().numpy()
     s.render(0 if batch else spp)
+    if not batch:  # the side stream and staging buffer of the asynchronous readback
+        s.readback_async(host)
+        s.readback_wait()
+    captures0 = s.profile()["graph_captures"]
     barrier()
     e2e_rays = 0
     t0 = time.perf_counter()
@@ -365,6 +386,7 @@ def run_ours(args):
     barrier()
     e2e_s, (e2e_rays,) = reduce_over_ranks(time.perf_counter() - t0, [e2e_rays], world)
     e2e_value = e2e_rays / e2e_s / 1e6
+    e2e_captures = s.profile()["graph_captures"] - captures0  # 0: every timed frame replayed its graph
 
     # ---- roofline of the extend stage (closest hit): algorithmic bytes per launch
     hbm, peak_kind = _peaks()
@@ -424,7 +446,8 @@ def run_ours(args):
                         "draw": "pathed.batch_generate(0x5EED + 4, 48)", "parallelism": f"replicas{world}",
                         "l2": "flushed between steps (256 MiB write)"}),
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0 if batch else 44,
-                    "d2h_bytes_per_step": (sum(d["width"] * d["height"] for d in specs) if batch else w * h) * 3 * 4},
+                    "d2h_bytes_per_step": (sum(d["width"] * d["height"] for d in specs) if batch else w * h) * 3 * 4,
+                    "graph_captures": e2e_captures},
             "roofline": roof,
             "cpu_baseline": cpu,
             "guiding": guiding,

@@ -1303,6 +1303,7 @@ int Session::profile(pt_profile* out) const {
     out->node_bytes = bvh_nodes_quantized() ? qnode_bytes(bvh_.width) : bvh_.width == 2 ? 64 : bvh_.width == 4 ? 128 : 256;
     out->prim_bytes = 48;
     out->wave_paths = last_wave_paths_;
+    out->graph_captures = graph_captures_;
     return PT_OK;
 }
 

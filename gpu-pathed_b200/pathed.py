@@ -174,7 +174,8 @@ def batch_generate(seed: int, n: int) -> list[dict]:
 class Profile(C.Structure):
     _fields_ = [("stage_ms", C.c_float * 7), ("stage_launches", C.c_int * 7), ("extend_nodes", C.c_ulonglong),
                 ("extend_prims", C.c_ulonglong), ("shadow_nodes", C.c_ulonglong), ("shadow_prims", C.c_ulonglong),
-                ("bvh_width", C.c_int), ("node_bytes", C.c_int), ("prim_bytes", C.c_int), ("wave_paths", C.c_int)]
+                ("bvh_width", C.c_int), ("node_bytes", C.c_int), ("prim_bytes", C.c_int), ("wave_paths", C.c_int),
+                ("graph_captures", C.c_int)]
 
 
 def _load():

@@ -166,6 +166,7 @@ typedef struct pt_profile {
     int node_bytes;                   /* bytes per wide node */
     int prim_bytes;                   /* bytes per leaf entry */
     int wave_paths;                   /* paths per wave of the last frame */
+    int graph_captures;               /* frame CUDA graphs captured by this session so far */
 } pt_profile;
 
 /* ---- session lifetime (RenderSession ctor, render_session.cu:55-117) ------------------ */

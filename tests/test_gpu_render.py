@@ -239,6 +239,7 @@ def test_graph_replay_matches_direct_launches():
         s.set_camera((1.0, 5.0, 15.0), (0, 0.5, 0), (0, 1, 0), 0.7)  # constants change, launches do not
         s.render(4)
         imgs.append(s.readback().copy())
+        assert s.profile()["graph_captures"] == (1 if graph == 1 else 0)  # one capture, replayed
         s.close()
     assert np.array_equal(imgs[0], imgs[1])
 
