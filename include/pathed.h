@@ -346,7 +346,8 @@ int pt_readback_pass(pt_session* s, float* rgb, size_t n);
 int pt_readback_rgba8(pt_session* s, uint8_t* rgba, size_t n);
 /* Asynchronous pt_readback: the running mean as of the last enqueued frame is snapshotted
  * behind that frame, then copied into `rgb` on a separate copy stream, so the copy overlaps
- * the next frame. Returns at once; the next pt_render_async may follow immediately.
+ * the next frame. Returns at once; once the frame is done (pt_poll / pt_wait), the next
+ * pt_render_async may start while the copy runs.
  * pt_readback_wait blocks until `rgb` holds the image (a no-op with none pending). `rgb`
  * should be page-locked for the copy to run asynchronously, and must stay valid until the
  * wait. A second pt_readback_async first waits for the pending copy. (The reference reads
