@@ -223,7 +223,8 @@ __global__ void __launch_bounds__(kRaySortBlock) k_ray_scatter(FrameParams p, in
 // or more lanes are idle, they take the next rays of the queue together (one atomic per warp),
 // so a warp does not idle behind its longest query (Aila and Laine's replacement of
 // terminated rays). With refill_idle = 32 a warp takes 32 new rays only after all of its
-// queries ended.
+// queries ended. With kSpeculateExtend set, traverse_round parks each lane's first leaf and
+// keeps descending while another lane of the warp still searches for one.
 template <int W, bool CNT, bool B, int Q>
 __global__ void k_extend(FrameParams p, int depth) {
     extern __shared__ int2 stk[];
@@ -244,7 +245,7 @@ __global__ void k_extend(FrameParams p, int depth) {
     TraceWork work;
     // the lane's query; slot < 0: none (then alive is false as well)
     int slot = -1, cur = kEmptyChild, pend = kEmptyChild, sp = 0, of = 0;
-    bool alive = false, hit_any = false;
+    bool alive = false, hit_any = false;  // hit_any: any-hit output, never set for closest hit
     RayPre r = make_raypre(V{0.f, 0.f, 0.f}, V{0.f, 0.f, 1.f});
     Hit h{FLT_MAX, 0.f, 0.f, kMissPrim};
     SceneDevice scb;
