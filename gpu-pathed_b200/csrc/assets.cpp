@@ -661,69 +661,48 @@ bool huf_decode(const uint8_t* in, size_t nin, uint16_t* out, size_t nout, std::
     return true;
 }
 
-// one inverse step of the 14-bit (lossless, no modulo) and 16-bit (modulo) wavelets
-inline void wdec14(uint16_t l, uint16_t h, uint16_t& a, uint16_t& b) {
-    const int ls = (int16_t)l, hs = (int16_t)h;
-    const int ai = ls + (hs & 1) + (hs >> 1);
-    a = (uint16_t)(int16_t)ai;
-    b = (uint16_t)(int16_t)(ai - hs);
-}
-inline void wdec16(uint16_t l, uint16_t h, uint16_t& a, uint16_t& b) {
-    const int m = l, d = h;
-    const int bb = (m - (d >> 1)) & 0xffff;
-    const int aa = (d + bb - 0x8000) & 0xffff;
-    b = (uint16_t)bb;
-    a = (uint16_t)aa;
-}
+// Inverse of PIZ's lossless 2-D Haar wavelet (OpenEXR file format, PIZ compression). A
+// forward step maps a pair (a, b) to a low word l and a high word h, h = a - b. Two pair
+// rules exist, and a block uses the first when every word value it holds is below 2^14:
+//   exact:  l = floor((a + b) / 2), words as signed 16-bit integers; so a = l + ceil(h / 2);
+//   modulo: words as unsigned 16-bit integers mod 2^16, with b = l - floor(h / 2) and
+//           a = b + h - 2^15 (the forward rule's 2^15 offset keeps h in range).
+struct PizPair {
+    bool exact;
+    void inverse(uint16_t& lo_then_a, uint16_t& hi_then_b) const {
+        if (exact) {
+            const int l = (int16_t)lo_then_a, h = (int16_t)hi_then_b;
+            const int a = l + ((h + 1) >> 1);  // arithmetic shift: ceil(h / 2)
+            lo_then_a = (uint16_t)a;
+            hi_then_b = (uint16_t)(a - h);
+        } else {
+            const unsigned l = lo_then_a, h = hi_then_b;
+            const unsigned b = (l - (h >> 1)) & 0xffffu;
+            lo_then_a = (uint16_t)((b + h - 0x8000u) & 0xffffu);
+            hi_then_b = (uint16_t)b;
+        }
+    }
+};
 
-// Inverse 2-D wavelet over an nx x ny plane (element stride ox, row stride oy), from the
-// coarsest level to the finest; odd trailing columns and rows take 1-D steps.
-void wav2_decode(uint16_t* in, int nx, int ox, int ny, int oy, uint16_t mx) {
-    const bool w14 = mx < (1 << 14);
-    auto dec = [w14](uint16_t l, uint16_t h, uint16_t& a, uint16_t& b) {
-        if (w14) wdec14(l, h, a, b); else wdec16(l, h, a, b);
-    };
-    const int n = nx > ny ? ny : nx;
-    int p = 1;
-    while (p <= n) p <<= 1;
-    p >>= 1;
-    int p2 = p;
-    p >>= 1;
-    while (p >= 1) {
-        uint16_t* py = in;
-        uint16_t* ey = in + (ptrdiff_t)oy * (ny - p2);
-        const ptrdiff_t oy1 = (ptrdiff_t)oy * p, oy2 = (ptrdiff_t)oy * p2;
-        const ptrdiff_t ox1 = (ptrdiff_t)ox * p, ox2 = (ptrdiff_t)ox * p2;
-        uint16_t i00, i01, i10, i11;
-        for (; py <= ey; py += oy2) {
-            uint16_t* px = py;
-            uint16_t* ex = py + (ptrdiff_t)ox * (nx - p2);
-            for (; px <= ex; px += ox2) {
-                uint16_t* p01 = px + ox1;
-                uint16_t* p10 = px + oy1;
-                uint16_t* p11 = p10 + ox1;
-                dec(*px, *p10, i00, i10);
-                dec(*p01, *p11, i01, i11);
-                dec(i00, i01, *px, *p01);
-                dec(i10, i11, *p10, *p11);
-            }
-            if (nx & p) {  // odd column
-                uint16_t* p10 = px + oy1;
-                dec(*px, *p10, i00, *p10);
-                *px = i00;
-            }
-        }
-        if (ny & p) {  // odd row
-            uint16_t* px = py;
-            uint16_t* ex = py + (ptrdiff_t)ox * (nx - p2);
-            for (; px <= ex; px += ox2) {
-                uint16_t* p01 = px + ox1;
-                dec(*px, *p01, i00, *p01);
-                *px = i00;
-            }
-        }
-        p2 = p;
-        p >>= 1;
+// Inverse 2-D wavelet over an nx x ny plane of words at element stride sx, row stride sy.
+// Level `step` pairs samples `step` apart. At each level, the samples on the step grid are
+// first inverted in vertical pairs (rows 2j*step and (2j+1)*step, every column of the
+// grid, the unpaired last column of an odd count included), then in horizontal pairs (every
+// row of the grid, the unpaired last row included); an unpaired last row or column keeps its
+// value in the other direction. Levels run from the coarsest step (half the largest power
+// of two not above min(nx, ny)) down to 1.
+void wav2_decode(uint16_t* plane, int nx, int sx, int ny, int sy, uint16_t max_word) {
+    const PizPair pair{max_word < (1 << 14)};
+    const int n = std::min(nx, ny);
+    int top = 1;
+    while (top * 2 <= n) top *= 2;
+    auto at = [&](int x, int y) -> uint16_t& { return plane[(ptrdiff_t)y * sy + (ptrdiff_t)x * sx]; };
+    for (int step = top / 2; step >= 1; step /= 2) {
+        const int cols = nx / step, rows = ny / step;  // grid samples in each direction
+        for (int j = 0; j + 1 < rows; j += 2)          // vertical pairs
+            for (int i = 0; i < cols; i++) pair.inverse(at(i * step, j * step), at(i * step, (j + 1) * step));
+        for (int j = 0; j < rows; j++)                 // horizontal pairs
+            for (int i = 0; i + 1 < cols; i += 2) pair.inverse(at(i * step, j * step), at((i + 1) * step, j * step));
     }
 }
 
@@ -994,6 +973,10 @@ namespace {
 
 // FP32 -> FP16: mantissa truncated to 10 bits, plus one when the first dropped bit is set;
 // FP32 denormals become zero, exponents past the half range infinity, NaN a quiet NaN.
+// This is the rounding rule of the conversion the reference's Image::save goes through:
+// tinyexr's float_to_half_full (vendor/tinyexr.h:7164-7197, which takes it from the ISPC
+// reference code). It is restated case for case because the snapshot files must be
+// byte-identical to the reference's.
 uint16_t half_of(float f) {
     uint32_t x;
     std::memcpy(&x, &f, 4);

@@ -400,13 +400,13 @@ int pt_trace_rays(pt_session* s, const float* o, const float* d, const float* tm
 int pt_trace_rays_device(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax, int n,
                          int* prim_type, int* prim_id, int* mat_id, float* t, float* bary) {
     if (!s) return PT_ERR_ARG;
-    return s->impl.trace_rays(o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary, true);
+    return guarded(s, [&] { return s->impl.trace_rays(o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary, true); });
 }
 
 int pt_trace_rays_static(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax, int n,
                          int* prim_type, int* prim_id, int* mat_id, float* t, float* bary) {
     if (!s) return PT_ERR_ARG;
-    return s->impl.trace_rays_static(o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary);
+    return guarded(s, [&] { return s->impl.trace_rays_static(o, d, tmin, tmax, n, prim_type, prim_id, mat_id, t, bary); });
 }
 
 int pt_occluded(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax, int n,

@@ -55,6 +55,10 @@ Session::~Session() {
         if (h_dyn_) cudaFreeHost(h_dyn_);
         if (h_batch_) cudaFreeHost(h_batch_);
         if (stream_) cudaStreamDestroy(stream_);
+        if (query_stream_) {
+            cudaStreamSynchronize(query_stream_);
+            cudaStreamDestroy(query_stream_);
+        }
         if (h_stats_) cudaFreeHost(h_stats_);
     }
 }
@@ -94,6 +98,8 @@ int Session::ensure_device() {
     num_sms_ = prop.multiProcessorCount;
     max_smem_ = prop.sharedMemPerBlockOptin;
     if ((r = check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return r;
+    if ((r = check_cuda(cudaStreamCreateWithFlags(&query_stream_, cudaStreamNonBlocking), "cudaStreamCreate")))
+        return r;
     if ((r = check_cuda(cudaEventCreate(&ev_begin_), "cudaEventCreate"))) return r;
     if ((r = check_cuda(cudaEventCreate(&ev_end_), "cudaEventCreate"))) return r;
     if ((r = check_cuda(cudaMallocHost((void**)&h_stats_, sizeof(FrameStats)), "cudaMallocHost"))) return r;
@@ -1472,8 +1478,9 @@ int Session::trace_rays_static(const float* o, const float* d, const float* tmin
     int r;
     if ((r = check_cuda(cudaSetDevice(device_), "cudaSetDevice"))) return r;
     int of = 0;
+    // on the session's query stream: a frame in flight on the render stream keeps running
     if ((r = check_cuda(pt::trace_rays_static(scene_view(), sd, o, d, tmin, tmax, n, pty, pid, mid, t, bary, &of,
-                                              stream_),
+                                              query_stream_),
                         "static trace rays")))
         return r;
     if (of) return fail(PT_ERR_DEVICE, "traversal stack overflow reported by a kernel");

@@ -147,6 +147,10 @@ private:
     bool scene_dirty_ = true;
     bool mats_dirty_ = true;
     cudaStream_t stream_ = nullptr;
+    // allocation-free queries (trace_rays_static): their own stream, so a query does not wait
+    // behind a frame in flight on stream_ (the scene buffers it reads are written only by
+    // uploads, which complete before the call that made them returns)
+    cudaStream_t query_stream_ = nullptr;
     int num_sms_ = 0;
     size_t max_smem_ = 0;
     DevBuf d_qnodes_, d_qfail_;

@@ -1319,22 +1319,30 @@ cudaError_t trace_rays_static(const SceneDevice& sc, int stack_depth, const floa
     float* sT = reinterpret_cast<float*>(sMat + N);
     float* sBary = sT + N;
     int* sFlag = reinterpret_cast<int*>(sBary + 2 * N);
-    if ((e = cudaMemsetAsync(sFlag, 0, sizeof(int), stream))) return e;
-    if (n == 0) return cudaSuccess;
     const size_t b = (size_t)n * sizeof(float);
-    if ((e = cudaMemcpyAsync(sO, o, 3 * b, cudaMemcpyHostToDevice, stream))) return e;
-    if ((e = cudaMemcpyAsync(sD, d, 3 * b, cudaMemcpyHostToDevice, stream))) return e;
-    if ((e = cudaMemcpyAsync(sTmin, tmin, b, cudaMemcpyHostToDevice, stream))) return e;
-    if ((e = cudaMemcpyAsync(sTmax, tmax, b, cudaMemcpyHostToDevice, stream))) return e;
-    if ((e = enqueue_trace_rays(sc, stack_depth, sO, sD, sTmin, sTmax, n, sType, sId, sMat, sT, sBary, sFlag, stream)))
-        return e;
-    if ((e = cudaMemcpyAsync(prim_type, sType, b, cudaMemcpyDeviceToHost, stream))) return e;
-    if ((e = cudaMemcpyAsync(prim_id, sId, b, cudaMemcpyDeviceToHost, stream))) return e;
-    if ((e = cudaMemcpyAsync(mat_id, sMat, b, cudaMemcpyDeviceToHost, stream))) return e;
-    if ((e = cudaMemcpyAsync(t, sT, b, cudaMemcpyDeviceToHost, stream))) return e;
-    if (bary && (e = cudaMemcpyAsync(bary, sBary, 2 * b, cudaMemcpyDeviceToHost, stream))) return e;
-    if ((e = cudaMemcpyAsync(overflow, sFlag, sizeof(int), cudaMemcpyDeviceToHost, stream))) return e;
-    return cudaStreamSynchronize(stream);
+    // Once a copy is queued, an error returns only after the stream has drained, so no copy
+    // into the caller's arrays lands after the call has returned.
+    auto enqueue = [&]() -> cudaError_t {
+        cudaError_t x;
+        if ((x = cudaMemsetAsync(sFlag, 0, sizeof(int), stream))) return x;
+        if (n == 0) return cudaSuccess;
+        if ((x = cudaMemcpyAsync(sO, o, 3 * b, cudaMemcpyHostToDevice, stream))) return x;
+        if ((x = cudaMemcpyAsync(sD, d, 3 * b, cudaMemcpyHostToDevice, stream))) return x;
+        if ((x = cudaMemcpyAsync(sTmin, tmin, b, cudaMemcpyHostToDevice, stream))) return x;
+        if ((x = cudaMemcpyAsync(sTmax, tmax, b, cudaMemcpyHostToDevice, stream))) return x;
+        if ((x = enqueue_trace_rays(sc, stack_depth, sO, sD, sTmin, sTmax, n, sType, sId, sMat, sT, sBary, sFlag,
+                                    stream)))
+            return x;
+        if ((x = cudaMemcpyAsync(prim_type, sType, b, cudaMemcpyDeviceToHost, stream))) return x;
+        if ((x = cudaMemcpyAsync(prim_id, sId, b, cudaMemcpyDeviceToHost, stream))) return x;
+        if ((x = cudaMemcpyAsync(mat_id, sMat, b, cudaMemcpyDeviceToHost, stream))) return x;
+        if ((x = cudaMemcpyAsync(t, sT, b, cudaMemcpyDeviceToHost, stream))) return x;
+        if (bary && (x = cudaMemcpyAsync(bary, sBary, 2 * b, cudaMemcpyDeviceToHost, stream))) return x;
+        return cudaMemcpyAsync(overflow, sFlag, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    };
+    e = enqueue();
+    const cudaError_t s = cudaStreamSynchronize(stream);
+    return e != cudaSuccess ? e : s;
 }
 
 cudaError_t enqueue_hit_test(const SceneDevice& sc, const CameraParams& cam, int stack_depth, int x, int y,

@@ -378,10 +378,12 @@ int pt_trace_rays_device(pt_session* s, const float* o, const float* d, const fl
  * PT_STATIC_MAX_RAYS entries (about 3.7 MB, reserved on every GPU that loads the library
  * until the process exits) and allocates nothing; n above PT_STATIC_MAX_RAYS is rejected
  * with PT_ERR_ARG. The scene must already be on the device: after loading or editing it,
- * make one ordinary device call first (otherwise PT_ERR_STATE). The first call on a device
- * looks the array's address up; make that first call before any stream capture. All calls
- * share the array and it keeps the last call's contents; calls whose work overlaps on the
- * GPU (other sessions, streams or host threads) race on it. */
+ * make one ordinary device call first (otherwise PT_ERR_STATE). The query runs on a stream
+ * of the session's own, not the render stream, so a call made while a frame is in flight
+ * returns without waiting for that frame. The first call on a device looks the array's
+ * address up; make that first call before any stream capture. All calls share the array and
+ * it keeps the last call's contents; calls whose work overlaps on the GPU (other sessions,
+ * streams or host threads) race on it. */
 #define PT_STATIC_MAX_RAYS 65536
 int pt_trace_rays_static(pt_session* s, const float* o, const float* d, const float* tmin, const float* tmax,
                          int n, int* prim_type, int* prim_id, int* mat_id, float* t, float* bary);

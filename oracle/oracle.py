@@ -16,16 +16,35 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_cpu.so")
-REF_TREE = os.environ.get("PATHED_REFERENCE", "/root/reference")
+# Where the reference tree lies: $PATHED_REFERENCE, else the path the last build() was
+# given (recorded in _ref/REFERENCE_TREE), else None (tests that read it then skip).
+_TREE_NOTE = os.path.join(HERE, "_ref", "REFERENCE_TREE")
 
 
-def build(ref: bool = True) -> None:
-    """Compile liboracle.so, and the reference's CPU and GPU builds when the reference tree
-    exists (on a machine without it, the prebuilt _ref/ libraries are used as they are)."""
+def _reference_tree():
+    t = os.environ.get("PATHED_REFERENCE")
+    if not t and os.path.exists(_TREE_NOTE):
+        with open(_TREE_NOTE) as f:
+            t = f.read().strip()
+    return t or None
+
+
+REF_TREE = _reference_tree()
+
+
+def build(ref_tree=None) -> None:
+    """Compile liboracle.so and, when `ref_tree` names an existing reference tree, the
+    reference's CPU and GPU builds from its sources (on a machine without it, the prebuilt
+    _ref/ libraries are used as they are). The tree's path is recorded for the tests."""
+    global REF_TREE
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if ref and os.path.isdir(REF_TREE):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "refbench", "refassets", f"REF={REF_TREE}"],
+    if ref_tree and os.path.isdir(ref_tree):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "refbench", "refassets", f"REF={ref_tree}"],
                        check=True)
+        os.makedirs(os.path.dirname(_TREE_NOTE), exist_ok=True)
+        with open(_TREE_NOTE, "w") as f:
+            f.write(os.path.abspath(ref_tree) + "\n")
+        REF_TREE = os.path.abspath(ref_tree)
 
 
 def _f(a):
@@ -234,6 +253,16 @@ class RefAssets:
         L.ref_exr_load.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.ref_exr_free.argtypes = [C.c_void_p]
         L.ref_image_save.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_char_p]
+        L.ref_exr_save_piz.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_char_p]
+
+    def exr_save_piz(self, path, planes, names=b"BGRA"[:3], half=False):
+        """tinyexr's SaveEXRImageToFile with PIZ compression of (channels, height, width)
+        FP32 planes, stored as HALF or FLOAT"""
+        a = np.ascontiguousarray(planes, np.float32)
+        code = self.lib.ref_exr_save_piz(a.shape[2], a.shape[1], a.shape[0], names, 1 if half else 2, a.ctypes.data,
+                                         os.fsencode(path))
+        if code != 0:
+            raise RuntimeError(f"SaveEXRImageToFile failed with {code}")
 
     def image_save(self, path, rgb):
         """Image::save of (height, width, 3) radiances, row 0 = image bottom"""

@@ -93,6 +93,38 @@ float* ref_exr_load(const char* path, int* width, int* height, int* code) {
 
 void ref_exr_free(float* p) { std::free(p); }
 
+// tinyexr's SaveEXRImageToFile with PIZ compression: nch channel planes of width x height
+// FLOAT values (names from `names`, one char each), stored as pixel_type (1 HALF, 2 FLOAT).
+// Used to write multi-level PIZ files for the product's reader; returns tinyexr's code.
+int ref_exr_save_piz(int width, int height, int nch, const char* names, int pixel_type, const float* planes,
+                     const char* path) {
+    EXRHeader header;
+    InitEXRHeader(&header);
+    EXRImage image;
+    InitEXRImage(&image);
+    std::vector<const float*> ptrs((size_t)nch);
+    for (int c = 0; c < nch; c++) ptrs[c] = planes + (size_t)c * width * height;
+    image.num_channels = nch;
+    image.images = reinterpret_cast<unsigned char**>(const_cast<float**>(ptrs.data()));
+    image.width = width;
+    image.height = height;
+    std::vector<EXRChannelInfo> ch((size_t)nch);
+    std::vector<int> in_types((size_t)nch, TINYEXR_PIXELTYPE_FLOAT), out_types((size_t)nch, pixel_type);
+    for (int c = 0; c < nch; c++) {
+        std::memset(&ch[c], 0, sizeof(EXRChannelInfo));
+        ch[c].name[0] = names[c];
+    }
+    header.num_channels = nch;
+    header.channels = ch.data();
+    header.pixel_types = in_types.data();
+    header.requested_pixel_types = out_types.data();
+    header.compression_type = TINYEXR_COMPRESSIONTYPE_PIZ;
+    const char* err = nullptr;
+    const int code = SaveEXRImageToFile(&image, &header, path, &err);
+    if (err) FreeEXRErrorMessage(err);
+    return code;
+}
+
 // Image::save(width, height, radiances, filename): rgb row 0 = image bottom
 void ref_image_save(int width, int height, const float* rgb, const char* path) {
     const std::vector<float> r(rgb, rgb + (size_t)width * height * 3);

@@ -5,7 +5,7 @@ against the reference's CUDA integrator (tests/test_gpu_reference_cuda.py).
 The file holds the reference's scene data (meshes, materials, environment maps), so it is
 kept out of version control; it is written on a machine that has the reference tree:
 
-    python tests/golden/make_reference_scenes.py [path/to/reference]
+    python tests/golden/make_reference_scenes.py path/to/reference
 """
 import os
 import sys
@@ -22,8 +22,10 @@ FIELDS = ("tri_vertices", "tri_normals", "tri_materials", "spheres", "sphere_mat
           "material_albedo", "material_emit", "material_ior", "material_alpha", "env_rgba", "camera")
 
 
-def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PATHED_REFERENCE", "/root/reference")
+def main(ref=None):
+    ref = ref or (sys.argv[1] if len(sys.argv) > 1 else None)
+    if not ref or not os.path.isdir(os.path.join(ref, "scenes")):
+        sys.exit("usage: make_reference_scenes.py path/to/reference (the tree holding scenes/)")
     out = {}
     for idx in range(4):
         s = pathed.Session(64, 48)

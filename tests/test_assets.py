@@ -57,6 +57,31 @@ def test_exr_matches_reference_loader(name):
     assert ours.shape == ref.shape and np.array_equal(ours, ref)
 
 
+@pytest.mark.skipif(not os.path.exists(orc.REF_ASSETS_LIB), reason="libref_assets.so absent")
+@pytest.mark.parametrize("w,h,half,smooth", [(37, 23, True, True), (203, 70, False, False), (64, 33, True, False),
+                                              (5, 130, False, True)])
+def test_piz_files_written_by_tinyexr(tmp_path, w, h, half, smooth):
+    """PIZ blocks of every wavelet depth: odd and even sizes, HALF and FLOAT words, smooth
+    data (few distinct words: the exact 14-bit pair rule) and noise (more than 2^14 distinct
+    words in a block: the modulo rule), written by the reference's tinyexr and read back by
+    both loaders"""
+    rng = np.random.default_rng(w * 1000 + h)
+    if smooth:
+        y, x = np.mgrid[0:h, 0:w]
+        planes = np.stack([np.sin(x / 7.0 + c) * np.cos(y / 5.0) + 1.5 for c in range(3)]).astype(np.float32)
+    else:
+        planes = rng.lognormal(0.0, 2.0, (3, h, w)).astype(np.float32)
+    f = str(tmp_path / "piz.exr")
+    R = orc.RefAssets()
+    R.exr_save_piz(f, planes, b"BGR", half=half)
+    ref = R.exr(f)
+    ours = pathed.read_exr(f)
+    assert ours.shape == ref.shape == (h, w, 4)
+    assert np.array_equal(ours, ref)
+    if not half:
+        assert np.array_equal(ours[..., 2], planes[0]) and np.array_equal(ours[..., 0], planes[2])
+
+
 @needs_ref
 def test_reference_scenes_assemble_as_scene_cu():
     """SceneParameters::getSceneData / getCamera (src/scene.cu:14-218) over the reference's parsers"""

@@ -137,7 +137,7 @@ SCENE_FIELDS = ("tri_vertices", "tri_normals", "tri_materials", "spheres", "sphe
 
 
 @pytest.mark.gpu
-@pytest.mark.skipif(not os.path.exists(REF_SCENES), reason="tests/golden/make_reference_scenes.py not run")
+@pytest.mark.skipif(not os.path.exists(REF_SCENES), reason="FIXTURE MISSING: tests/golden/_reference_scenes.npz is written by __graft_entry__.build() where the reference tree is present")
 @pytest.mark.parametrize("idx", [0, 1, 2, 3])
 def test_reference_scenes_vs_reference_cuda(idx):
     """The reference's own scenes 0-3 (its OBJ/MTL, PLY and EXR files through the asset loaders),
