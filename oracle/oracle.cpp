@@ -19,6 +19,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -283,12 +284,34 @@ struct Env {
 
 struct LightIndex { int type, index; };
 
+// Parity accelerator (not part of the reference): a binary BVH over the scene's triangles
+// and spheres, used only where the linear scan is too slow for a parity run (the
+// 1.31M-triangle meshes). It returns World::hit's own answer, because that answer is the
+// minimum of a total order over the candidates that the per-primitive tests accept
+// (src/world.cu:14-38): smaller t first; at equal t a triangle before a sphere, the higher
+// triangle index first (triangle.cu:34 accepts t <= tNear, so a later equal one replaces the
+// earlier), the lower sphere index first (sphere.cu:16,29 need t < tNear). Each candidate is
+// tested with the query's own [tMin, tMax], exactly as the scan tests it. Boxes are built in
+// double and padded by 1e-5 of the scene diagonal plus 1e-6 of the coordinate, and a subtree
+// is skipped only when its box lies wholly beyond the best t found so far (with the same
+// relative slack), so the traversal never skips a candidate that the float tests accept
+// within that distance of its primitive.
+struct AccelNode {
+    double lo[3], hi[3];
+    int first, count;  // count > 0: leaf over order[first, first + count); else children first, first + 1
+};
+struct Accel {
+    std::vector<AccelNode> nodes;
+    std::vector<int> order;  // >= 0 triangle index, < 0 ~sphere index
+};
+
 struct Scene {
     std::vector<Triangle> tris;
     std::vector<Sphere> sphs;
     std::vector<Material> mats;
     std::vector<LightIndex> lights;
     Env env;
+    Accel accel;  // empty: World::hit's linear scan
 };
 
 struct HitRecord {
@@ -353,8 +376,172 @@ inline bool sphereHit(const Sphere& sp, const Ray& ray, float tMin, float tMax, 
     return false;
 }
 
-// World::hit (src/world.cu:5-41): all triangles, then all spheres
-inline bool worldHit(const Scene& sc, const Ray& ray, float tMin, float tMax, HitRecord& rec) {
+// The linear scan's preference between two accepted candidates (a: t ta, primitive code
+// a; b likewise; code >= 0 triangle index, < 0 ~sphere index): true if the scan ends on a
+// rather than b. Same class at equal t: the larger code wins (a later triangle, or an
+// earlier sphere, whose ~index is larger).
+inline bool scanPrefers(float ta, int a, float tb, int b) {
+    if (ta != tb) return ta < tb;
+    if ((a >= 0) != (b >= 0)) return a >= 0;
+    return a > b;
+}
+
+void buildAccel(Scene& s) {
+    const int nt = (int)s.tris.size(), ns = (int)s.sphs.size(), n = nt + ns;
+    s.accel = Accel{};
+    if (n == 0) return;
+    std::vector<double> lo(3 * (size_t)n), hi(3 * (size_t)n), cen(3 * (size_t)n);
+    double slo[3] = {INFINITY, INFINITY, INFINITY}, shi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < n; i++) {
+        for (int a = 0; a < 3; a++) {
+            double l, h;
+            if (i < nt) {
+                const Triangle& t = s.tris[i];
+                l = std::min({(double)t.p0.e[a], (double)t.p1.e[a], (double)t.p2.e[a]});
+                h = std::max({(double)t.p0.e[a], (double)t.p1.e[a], (double)t.p2.e[a]});
+            } else {
+                const Sphere& sp = s.sphs[i - nt];
+                l = (double)sp.c.e[a] - std::fabs((double)sp.r);
+                h = (double)sp.c.e[a] + std::fabs((double)sp.r);
+            }
+            lo[3 * (size_t)i + a] = l;
+            hi[3 * (size_t)i + a] = h;
+            cen[3 * (size_t)i + a] = 0.5 * (l + h);
+            slo[a] = std::min(slo[a], l);
+            shi[a] = std::max(shi[a], h);
+        }
+    }
+    const double diag = std::sqrt((shi[0] - slo[0]) * (shi[0] - slo[0]) + (shi[1] - slo[1]) * (shi[1] - slo[1]) +
+                                  (shi[2] - slo[2]) * (shi[2] - slo[2]));
+    for (size_t k = 0; k < 3 * (size_t)n; k++) {
+        const double pad = 1e-5 * diag + 1e-6 * std::max(std::fabs(lo[k]), std::fabs(hi[k])) + 1e-30;
+        lo[k] -= pad;
+        hi[k] += pad;
+    }
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; i++) idx[i] = i;
+    Accel& A = s.accel;
+    A.nodes.reserve(2 * (size_t)n / 3 + 2);
+    struct Job { int node, first, count; };
+    std::vector<Job> jobs;
+    A.nodes.push_back(AccelNode{});
+    jobs.push_back({0, 0, n});
+    while (!jobs.empty()) {
+        const Job j = jobs.back();
+        jobs.pop_back();
+        AccelNode nd;
+        double clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int a = 0; a < 3; a++) { nd.lo[a] = INFINITY; nd.hi[a] = -INFINITY; }
+        for (int k = j.first; k < j.first + j.count; k++) {
+            const size_t p = (size_t)idx[k];
+            for (int a = 0; a < 3; a++) {
+                nd.lo[a] = std::min(nd.lo[a], lo[3 * p + a]);
+                nd.hi[a] = std::max(nd.hi[a], hi[3 * p + a]);
+                clo[a] = std::min(clo[a], cen[3 * p + a]);
+                chi[a] = std::max(chi[a], cen[3 * p + a]);
+            }
+        }
+        if (j.count <= 4) {
+            nd.first = j.first;
+            nd.count = j.count;
+            A.nodes[j.node] = nd;
+            continue;
+        }
+        int axis = 0;
+        for (int a = 1; a < 3; a++) if (chi[a] - clo[a] > chi[axis] - clo[axis]) axis = a;
+        const int half = j.count / 2;
+        std::nth_element(idx.begin() + j.first, idx.begin() + j.first + half, idx.begin() + j.first + j.count,
+                         [&](int x, int y) { return cen[3 * (size_t)x + axis] < cen[3 * (size_t)y + axis]; });
+        nd.first = (int)A.nodes.size();
+        nd.count = 0;
+        A.nodes[j.node] = nd;
+        A.nodes.push_back(AccelNode{});
+        A.nodes.push_back(AccelNode{});
+        jobs.push_back({nd.first, j.first, half});
+        jobs.push_back({nd.first + 1, j.first + half, j.count - half});
+    }
+    A.order.resize(n);
+    for (int k = 0; k < n; k++) A.order[k] = idx[k] < nt ? idx[k] : ~(idx[k] - nt);
+}
+
+// Ray against a padded box over the parameter range [t0, t1] (double); entry parameter out.
+inline bool accelSlab(const AccelNode& nd, const double o[3], const double d[3], double t0, double t1, double& entry) {
+    for (int a = 0; a < 3; a++) {
+        if (d[a] == 0.0) {
+            if (o[a] < nd.lo[a] || o[a] > nd.hi[a]) return false;
+            continue;
+        }
+        double ta = (nd.lo[a] - o[a]) / d[a], tb = (nd.hi[a] - o[a]) / d[a];
+        if (ta > tb) std::swap(ta, tb);
+        t0 = std::max(t0, ta);
+        t1 = std::min(t1, tb);
+        if (t0 > t1) return false;
+    }
+    entry = t0;
+    return true;
+}
+
+// World::hit through the accelerator: the same result as the scan (see scanPrefers). With
+// `any`, returns at the first accepted candidate (occlusion queries need only the flag).
+bool accelHit(const Scene& sc, const Ray& ray, float tMin, float tMax, HitRecord& rec, bool any) {
+    const Accel& A = sc.accel;
+    const double o[3] = {ray.o.e[0], ray.o.e[1], ray.o.e[2]}, d[3] = {ray.d.e[0], ray.d.e[1], ray.d.e[2]};
+    const double dl = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (!(dl > 0.0)) return false;
+    // slack in ray-parameter units: the boxes' padding is already in space units
+    const auto upper = [&](float t) { return (double)t * (1.0 + 1e-5) + 1e-9 / dl; };
+    const double lower = (double)tMin - 1e-3 * (std::fabs((double)tMin) + 1.0 / dl);
+    bool found = false;
+    float bestT = tMax;
+    int bestCode = 0;
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const AccelNode& nd = A.nodes[stack[--sp]];
+        double e;
+        // re-tested at pop time: the best hit may have moved closer since the push
+        if (!accelSlab(nd, o, d, lower, upper(bestT), e)) continue;
+        if (nd.count > 0) {
+            for (int k = nd.first; k < nd.first + nd.count; k++) {
+                const int code = A.order[k];
+                HitRecord tmp;
+                const bool h = code >= 0 ? triangleHit(sc.tris[code], ray, tMin, tMax, tmp)
+                                         : sphereHit(sc.sphs[~code], ray, tMin, tMax, tmp);
+                if (!h) continue;
+                if (any) return true;
+                if (!found || scanPrefers(tmp.t, code, bestT, bestCode)) {
+                    found = true;
+                    bestT = tmp.t;
+                    bestCode = code;
+                    rec = tmp;
+                    rec.primType = code >= 0 ? TRIANGLE : SPHERE;
+                    rec.primIndex = code >= 0 ? code : ~code;
+                }
+            }
+            continue;
+        }
+        const double lim = upper(bestT);
+        double ea, eb;
+        const bool ha = accelSlab(A.nodes[nd.first], o, d, lower, lim, ea);
+        const bool hb = accelSlab(A.nodes[nd.first + 1], o, d, lower, lim, eb);
+        if (sp + 2 > 128) std::abort();  // a median-split tree is far shallower than this
+        if (ha && hb) {  // nearer child on top
+            stack[sp++] = ea <= eb ? nd.first + 1 : nd.first;
+            stack[sp++] = ea <= eb ? nd.first : nd.first + 1;
+        } else if (ha) {
+            stack[sp++] = nd.first;
+        } else if (hb) {
+            stack[sp++] = nd.first + 1;
+        }
+    }
+    return found;
+}
+
+// World::hit (src/world.cu:5-41): all triangles, then all spheres. Scenes with an accelerator
+// answer through it (same result; `any` lets an occlusion query stop at its first hit).
+inline bool worldHit(const Scene& sc, const Ray& ray, float tMin, float tMax, HitRecord& rec, bool any = false) {
+    if (!sc.accel.nodes.empty()) return accelHit(sc, ray, tMin, tMax, rec, any);
     bool isHit = false;
     double tNear = tMax;
     const int nt = (int)sc.tris.size();
@@ -684,8 +871,20 @@ struct Camera {
 // `duplicate` counts the reference's second trace of each BSDF direction (compat mode only).
 struct Counters { uint64_t queries = 0, shadow = 0, duplicate = 0; };
 
+// The BSDF sampler's own density of a direction: Microfacet::sample draws with alpha(wo)
+// (microfacet.h:148-158) while Microfacet::pdf evaluates D with alpha(wi) (:124-134).
+inline float bsdfSamplingPdf(const Material& m, const Vec3& wo, const Vec3& wi) {
+    if (m.type != MICROFACET) return bsdfPdf(m, wo, wi);
+    if (wo.z() < 0.f || wi.z() < 0.f) return 0.f;
+    const Beckmann d{m.alpha};
+    const Vec3 wh = normalized(wo + wi);
+    return d.pdf(wo, wh) / (4.f * absDot(wo, wh));
+}
+
+// consistent: the light sample's MIS weight uses the BSDF's sampling density (an unbiased
+// combination) instead of the reference's Microfacet::pdf.
 Vec3 directLight(const Scene& sc, const HitRecord& rec, const BSDFSample& bs, Rng& rng, Counters& cnt,
-                 int traceOnce) {
+                 int traceOnce, bool consistent = false) {
     // directSampleLights (:83-126)
     if (bs.isDelta) return Vec3(0.f);
     if (traceOnce && sc.lights.empty() && !sc.env.present) return Vec3(0.f);  // no emitter to sample
@@ -697,14 +896,14 @@ Vec3 directLight(const Scene& sc, const HitRecord& rec, const BSDFSample& bs, Rn
     // order, :115-124); a shadow ray that cannot contribute is neither traced nor counted.
     const Vec3 wiLocal = Frame(rec.normal).toLocal(ls.wi);
     const Material& m = sc.mats[rec.materialID];
-    const float bsdfPDF = bsdfPdf(m, rec.wo, wiLocal);
+    const float bsdfPDF = consistent ? bsdfSamplingPdf(m, rec.wo, wiLocal) : bsdfPdf(m, rec.wo, wiLocal);
     const float lw = balance(ls.pdf, bsdfPDF);
     const Vec3 c = Vec3(1.f) * ls.emitted * lw * bsdfF(m, rec.wo, wiLocal) * fabsf(dot(rec.normal, ls.wi)) / ls.pdf;
     if (c.isZero()) return c;
     Ray shadow{rec.point, ls.wi};
     HitRecord occ;
     cnt.shadow++;
-    if (worldHit(sc, shadow, 1e-4, ls.distance - 2e-4, occ)) return Vec3(0.f);
+    if (worldHit(sc, shadow, 1e-4, ls.distance - 2e-4, occ, true)) return Vec3(0.f);
     return c;
 }
 
@@ -724,7 +923,8 @@ Vec3 bsdfDirectFromHit(const Scene& sc, const HitRecord& rec, const BSDFSample& 
     return sc.env.emit(dir) * w * bs.f * fabsf(bs.wiLocal.z()) / bs.pdf;
 }
 
-Vec3 LiNEE(const Scene& sc, const Ray& ray, int maxDepth, Rng& rng, int traceOnce, Counters& cnt) {
+Vec3 LiNEE(const Scene& sc, const Ray& ray, int maxDepth, Rng& rng, int traceOnce, Counters& cnt,
+           bool consistent = false) {
     if (maxDepth == 0) return Vec3(0.f);
     Vec3 beta(1.f), result(0.f);
     HitRecord rec;
@@ -739,7 +939,7 @@ Vec3 LiNEE(const Scene& sc, const Ray& ray, int maxDepth, Rng& rng, int traceOnc
     for (int path = 1; path < maxDepth; path++) {
         const Frame fr(rec.normal);
         const BSDFSample bs = bsdfSample(sc.mats[rec.materialID], rec.wo, rng);
-        Vec3 direct = directLight(sc, rec, bs, rng, cnt, traceOnce);
+        Vec3 direct = directLight(sc, rec, bs, rng, cnt, traceOnce, consistent);
         const Vec3 bounceDir = fr.toWorld(bs.wiLocal);
         const Ray bounce{rec.point, bounceDir};
         HitRecord next;
@@ -847,6 +1047,9 @@ Scene* oracle_scene_create(int ntri, const float* tri_p, const float* tri_n, con
 }
 
 void oracle_scene_destroy(Scene* s) { delete s; }
+// Build the parity accelerator: later queries on the scene give the linear scan's results
+// through a BVH (buildAccel).
+void oracle_scene_accel(Scene* s) { buildAccel(*s); }
 int oracle_num_lights(const Scene* s) { return (int)s->lights.size(); }
 
 // Closest hit of n rays by the reference's linear scan. prim_type -1 on a miss.
@@ -875,7 +1078,7 @@ void oracle_trace(const Scene* s, const float* o, const float* d, const float* t
 // non-canonical extra traces of the reference's convention.
 void oracle_render(const Scene* s, const float* cam, int width, int height, const int* pixels, int npix, int spp,
                    int max_depth, int nee, uint64_t seed, uint64_t sample_base, int trace_once, double* mean,
-                   double* var, uint64_t* counts, int threads) {
+                   double* var, uint64_t* counts, int threads, int consistent_mis) {
     Camera c;
     c.init(cam, cam + 3, cam + 6, cam[9], cam[10] != 0.f, width, height);
     std::atomic<uint64_t> q{0}, sh{0}, dup{0};
@@ -888,7 +1091,8 @@ void oracle_render(const Scene* s, const float* cam, int width, int height, cons
             Rng rng = Rng::seeded(seed, sample_base + (uint64_t)sIdx, (uint32_t)pixel);
             const float x1 = rng.uniform(), x2 = rng.uniform();  // camera.cu:29-34
             const Ray r = c.generate(row, col, x1, x2);
-            const Vec3 L = nee ? LiNEE(*s, r, max_depth, rng, trace_once, cnt) : LiNaive(*s, r, max_depth, rng, cnt);
+            const Vec3 L = nee ? LiNEE(*s, r, max_depth, rng, trace_once, cnt, consistent_mis != 0)
+                               : LiNaive(*s, r, max_depth, rng, cnt);
             for (int ch = 0; ch < 3; ch++) {  // Welford
                 const double v = L.e[ch];
                 const double dlt = v - m[ch];

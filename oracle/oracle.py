@@ -71,8 +71,10 @@ class _SceneLib:
             + [C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_void_p])
         getattr(self.lib, p + "scene_destroy").argtypes = [C.c_void_p]
 
-    def scene(self, sc: dict):
-        """Create a scene from an export dict (pathed.Session.export_scene layout)."""
+    def scene(self, sc: dict, accel: bool = False):
+        """Create a scene from an export dict (pathed.Session.export_scene layout). With
+        `accel` (oracle only), queries run through the parity accelerator, which gives the
+        linear scan's results on meshes the scan is too slow for."""
         keep = [
             _f(sc["tri_vertices"]), _f(sc["tri_normals"]), _i(sc["tri_materials"]), _f(sc["spheres"]),
             _i(sc["sphere_materials"]), _i(sc["material_types"]), _f(sc["material_albedo"]),
@@ -88,6 +90,8 @@ class _SceneLib:
             keep[4].ctypes.data if keep[4].size else None,
             keep[5].size, keep[5].ctypes.data, keep[6].ctypes.data, keep[7].ctypes.data, keep[8].ctypes.data,
             keep[9].ctypes.data, ew, eh, None if env is None else env.ctypes.data)
+        if accel:
+            getattr(self.lib, self.prefix + "scene_accel")(h)
         return _SceneHandle(self, h, keep + [env])
 
 
@@ -108,10 +112,11 @@ class Oracle(_SceneLib):
     def __init__(self, path=ORACLE_LIB):
         super().__init__(path)
         L = self.lib
+        L.oracle_scene_accel.argtypes = [C.c_void_p]
         L.oracle_trace.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_int]
         L.oracle_render.argtypes = ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                      C.c_int, C.c_uint64, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
-                                     C.c_int])
+                                     C.c_int, C.c_int])
         L.oracle_bsdf_sample.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_float,
                                          C.c_float, C.c_void_p]
         L.oracle_bsdf_eval.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p,
@@ -167,7 +172,7 @@ class Oracle(_SceneLib):
         return out
 
     def render(self, scene, camera, width, height, pixels, spp, max_depth, nee=True, seed=0x5EED, sample_base=0,
-               trace_once=True, threads=0):
+               trace_once=True, threads=0, consistent_mis=False):
         pixels = _i(pixels)
         n = pixels.size
         mean = np.zeros((n, 3), np.float64)
@@ -176,7 +181,7 @@ class Oracle(_SceneLib):
         cam = _f(camera)
         self.lib.oracle_render(scene.h, cam.ctypes.data, width, height, pixels.ctypes.data, n, spp, max_depth,
                                int(bool(nee)), seed, sample_base, int(bool(trace_once)), mean.ctypes.data,
-                               var.ctypes.data, counts.ctypes.data, threads)
+                               var.ctypes.data, counts.ctypes.data, threads, int(bool(consistent_mis)))
         return mean, var, counts
 
     def normals(self, scene, camera, width, height, threads=0):

@@ -1,0 +1,132 @@
+"""Parity at the configurations' full sizes, with relMSE stated.
+
+  * configurations 2 and 3 at full size (the 1,310,720-triangle displaced icosphere under
+    the 2048x1024 environment with three suns, 1920x1080, depth 6; the slit room holding it,
+    1024x1024, depth 10): the GPU and the oracle on the same random streams, per pixel;
+  * configurations 0-3 at full size: the GPU's accumulated image against the converged
+    FP64 oracle (reference trace convention, independent samples) on a seeded 4096-pixel
+    subset, per pixel within 3 combined standard errors, and relMSE against the oracle
+    bounded by what the two estimators' variances alone give (no bias beyond noise);
+  * the slit room's time-to-relMSE reference (the plain 2048-spp render, consistent MIS,
+    passes accumulated in FP64) against the FP64 oracle in the same MIS convention.
+
+relMSE = mean over pixel channels of (I - I_ref)^2 / (I_ref^2 + 1e-2), I_ref the oracle.
+The oracle traces through its parity accelerator (bit-identical to the linear scan,
+tests/test_oracle_accel.py), so the million-triangle cases finish in seconds.
+"""
+import numpy as np
+import pytest
+
+import pathed
+from _util import pixel_subset, three_se_pass
+
+# width, height, depth of each configuration at full size
+FULL = {0: (512, 512, 5), 1: (1024, 1024, 8), 2: (1920, 1080, 6), 3: (1024, 1024, 10)}
+# oracle samples per pixel of the converged FP64 reference (the slit room's paths are 15x longer)
+ORACLE_SPP = {0: 1024, 1: 1024, 2: 1024, 3: 256}
+
+
+def rel_mse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def expected_rel_mse(se_a, se_b, ref):
+    """relMSE two unbiased estimators with these standard errors reach in expectation"""
+    return float(np.mean((se_a ** 2 + se_b ** 2) / (ref ** 2 + 1e-2)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg", [2, 3])
+def test_full_size_same_stream_agreement(oracle_lib, cfg):
+    w, h, depth = FULL[cfg]
+    spp = 2
+    s = pathed.Session(w, h)
+    s.load_config(cfg)
+    assert s.counts().num_triangles >= 1310720 and s.counts().default_depth == depth
+    s.render(spp)
+    img = s.readback().reshape(-1, 3).astype(np.float64)
+    sc = s.export_scene()
+    s.close()
+    osc = oracle_lib.scene(sc, accel=True)
+    pix = pixel_subset(w, h, 3000, seed=20 + cfg)
+    mean, var, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, spp, depth, nee=True, trace_once=True)
+    g = img[pix]
+    tight = np.all(np.abs(g - mean) <= 1e-3 * np.abs(mean) + 1e-5, axis=1).mean()
+    loose = np.all(np.abs(g - mean) <= 5e-2 * np.abs(mean) + 1e-4, axis=1).mean()
+    e_same = rel_mse(g, mean)
+    e_noise = float(np.mean(var * spp / (mean ** 2 + 1e-2)))  # one sample's relMSE, for scale
+    print(f"cfg{cfg} full size: {tight:.4f} of pixels agree to 1e-3, {loose:.4f} to 5e-2; same-stream relMSE "
+          f"{e_same:.3e} (one-sample noise relMSE {e_noise:.3e})")
+    assert tight >= 0.97 and loose >= 0.99
+    assert e_same <= 0.02 * e_noise
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3])
+def test_full_size_statistical_parity_vs_fp64_oracle(oracle_lib, cfg):
+    w, h, depth = FULL[cfg]
+    frames, spp = 16, 8
+    pix = pixel_subset(w, h, 4096, seed=30 + cfg)
+    s = pathed.Session(w, h)
+    s.load_config(cfg)
+    s.set_seed(4321)
+    passes = []
+    for _ in range(frames):
+        s.render(spp)
+        passes.append(s.readback(pass_only=True).reshape(-1, 3)[pix].astype(np.float64))
+    sc = s.export_scene()
+    s.close()
+    passes = np.stack(passes)
+    g_mean = passes.mean(0)
+    g_se = passes.std(0, ddof=1) / np.sqrt(frames)
+    osc = oracle_lib.scene(sc, accel=True)
+    o_mean, o_var, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, ORACLE_SPP[cfg], depth, nee=True, seed=99,
+                                         trace_once=False)
+    o_se = np.sqrt(o_var)
+    frac = three_se_pass(g_mean, g_se, o_mean, o_se, floor=1e-6)
+    e = rel_mse(g_mean, o_mean)
+    e_exp = expected_rel_mse(g_se, o_se, o_mean)
+    print(f"cfg{cfg} {w}x{h}: GPU {frames * spp} spp vs FP64 oracle {ORACLE_SPP[cfg]} spp on 4096 pixels: 3-SE pass "
+          f"{frac:.4f}; relMSE {e:.3e} (expected from the variances alone {e_exp:.3e}); image mean GPU "
+          f"{g_mean.mean():.5f} oracle {o_mean.mean():.5f}")
+    assert frac >= 0.97, f"3-SE pass fraction {frac:.4f}"
+    assert e <= 2.0 * e_exp + 1e-8, f"relMSE {e:.3e} beyond the noise level {e_exp:.3e}"
+
+
+@pytest.mark.gpu
+def test_time_to_relmse_reference_vs_fp64_oracle(oracle_lib):
+    """bench.py's guiding block measures relMSE against a plain 2048-spp render of the slit
+    room (seed 12345, consistent MIS, 32 passes of 64 spp summed in FP64). Recomputed here
+    pass by pass, it must agree with the FP64 oracle in the same MIS convention, and its own
+    noise must stay small against the relMSE target it defines."""
+    import bench
+
+    w, h, depth = FULL[3]
+    pix = pixel_subset(w, h, 4096, seed=77)
+    r = bench._slit_session(w)
+    r.set_seed(12345)
+    passes = []
+    for _ in range(2048 // 64):
+        r.render(64)
+        passes.append(r.readback(pass_only=True).reshape(-1, 3)[pix].astype(np.float64))
+    sc = r.export_scene()
+    r.close()
+    passes = np.stack(passes)
+    ref = passes.mean(0)
+    ref_se = passes.std(0, ddof=1) / np.sqrt(len(passes))
+    osc = oracle_lib.scene(sc, accel=True)
+    o_mean, o_var, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, 256, depth, nee=True, seed=5,
+                                         trace_once=False, consistent_mis=True)
+    o_se = np.sqrt(o_var)
+    frac = three_se_pass(ref, ref_se, o_mean, o_se, floor=1e-6)
+    e = rel_mse(ref, o_mean)
+    e_exp = expected_rel_mse(ref_se, o_se, o_mean)
+    ref_noise = float(np.mean(ref_se ** 2 / (o_mean ** 2 + 1e-2)))
+    print(f"slit-room 2048-spp reference vs FP64 oracle (256 spp, consistent MIS) on 4096 pixels: 3-SE pass "
+          f"{frac:.4f}; relMSE {e:.3e} (expected from the variances {e_exp:.3e}); the reference's own noise "
+          f"relMSE {ref_noise:.3e}")
+    assert frac >= 0.97
+    assert e <= 2.0 * e_exp + 1e-8
+    # bench's plain 256-spp target relMSE is about 1.7e-3: the reference's own noise must be
+    # well below it for the crossing to measure the renders, not the reference
+    assert ref_noise <= 2.5e-4

@@ -22,6 +22,8 @@ from _util import pixel_subset, seeded_rays, three_se_pass
 pytestmark = pytest.mark.skipif(not os.path.exists(orc.REFBENCH_LIB), reason="reference GPU build not available")
 
 CASES = [(0, None), (1, None), (2, 4), (3, 4)]
+# the full 1,310,720-triangle mesh: the reference's linear scan costs about 1 s per ray batch
+FULL_MESH = [(2, None), (3, None)]
 
 
 def _ours(cfg, level, w=64, h=64):
@@ -31,12 +33,12 @@ def _ours(cfg, level, w=64, h=64):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", CASES, ids=lambda c: f"cfg{c[0]}")
+@pytest.mark.parametrize("case", CASES + FULL_MESH, ids=lambda c: f"cfg{c[0]}" + ("-full" if c in FULL_MESH else ""))
 def test_hit_ids_bitexact_vs_reference_nofma(case):
     s, sc = _ours(*case)
     rb = orc.RefBench(nofma=True)
     rb.load(sc, 16, 16)
-    o, d, tmin, tmax = seeded_rays(sc, 20000, seed=31)
+    o, d, tmin, tmax = seeded_rays(sc, 6000 if case in FULL_MESH else 20000, seed=31)
     g = s.trace_rays(o, d, tmin, tmax)
     r = rb.trace(o, d, tmin, tmax)
     for k in ("prim_type", "prim_id", "mat_id", "t"):
@@ -95,10 +97,13 @@ def test_hit_ids_vs_reference_default_build(case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", [(0, None), (1, None), (3, 4)], ids=lambda c: f"cfg{c[0]}")
+@pytest.mark.parametrize("case", [(0, None), (1, None), (2, 4), (3, 4)], ids=lambda c: f"cfg{c[0]}")
 def test_image_means_vs_reference_cuda(case):
+    """configuration 2 keeps its 2048x1024 environment with the three suns at every mesh
+    level: this is the reference's environment sampling (PhiThetaDistribution, the
+    pixel-centre directions) on that map, at the configuration's 16:9 aspect"""
     cfg, level = case
-    w = h = 64
+    w, h = (96, 54) if cfg == 2 else (64, 64)
     frames, spp = 8, 32
     s, sc = _ours(cfg, level, w, h)
     depth = s.counts().default_depth
@@ -129,6 +134,42 @@ def test_image_means_vs_reference_cuda(case):
     assert abs(ma.mean() - mb.mean()) <= 4 * se + 1e-6
     rb.close()
     s.close()
+
+
+@pytest.mark.gpu
+def test_image_mean_vs_reference_cuda_full_mesh():
+    """configuration 2 with its full 1,310,720-triangle mesh: the reference's linear scan
+    takes seconds per sample of a small image, so this compares the image mean (and reports
+    the per-pixel pass fraction) at 32x18 over 6 frames of 2 samples"""
+    w, h, frames, spp = 32, 18, 6, 2
+    s, sc = _ours(2, None, w, h)
+    assert s.counts().num_triangles == 1310720
+    depth = s.counts().default_depth
+    ours = []
+    for _ in range(frames * 8):  # more of our frames: the combined SE is the reference's
+        s.render(spp)
+        ours.append(s.readback(pass_only=True).reshape(-1, 3).astype(np.float64))
+    ours = np.stack(ours)
+    rb = orc.RefBench()
+    rb.load(sc, w, h)
+    ref, prev, ms = [], np.zeros((w * h, 3)), 0.0
+    for k in range(frames):
+        ms += rb.render(spp, depth, True)
+        m = rb.readback().reshape(-1, 3).astype(np.float64)
+        ref.append(m * (k + 1) - prev * k)
+        prev = m
+    ref = np.stack(ref)
+    rb.close()
+    s.close()
+    se_a = ours.std(0, ddof=1) / np.sqrt(len(ours))
+    se_b = ref.std(0, ddof=1) / np.sqrt(frames)
+    frac = three_se_pass(ours.mean(0), se_a, ref.mean(0), se_b, floor=1e-5)
+    ma, mb = ours.mean(axis=(1, 2)), ref.mean(axis=(1, 2))
+    se = np.sqrt(ma.var(ddof=1) / len(ma) + mb.var(ddof=1) / frames)
+    print(f"cfg2 full mesh {w}x{h}: reference {ms / frames:.0f} ms per {spp}-spp frame; 3-SE pass {frac:.4f}; "
+          f"image mean ours {ma.mean():.5f} reference {mb.mean():.5f} (SE {se:.5f})")
+    assert abs(ma.mean() - mb.mean()) <= 4 * se + 1e-6
+    assert frac >= 0.9
 
 
 REF_SCENES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "_reference_scenes.npz")
