@@ -58,6 +58,23 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+L2_BYTES = 126 * 1024 * 1024  # B200 L2
+L1_RESIDENT_BYTES = 1 << 20   # nodes + leaf entries this small stay in the SMs' L1 caches
+ISSUE_SLOTS_PER_CYCLE = 4 * 148  # one warp instruction per cycle per SM sub-partition, 148 SMs
+L2_PROBE_BYTES = 32 << 20     # pt_measure_l2_read buffer: well inside either die's L2 half
+
+
+def traversal_bound(counts, prof):
+    """The resource that bounds closest-hit traversal on this scene (nodes + leaf entries
+    footprint): 'issue' when it fits in L1, 'l2' when it fits in L2, else 'hbm'."""
+    footprint = counts.bvh_nodes * prof["node_bytes"] + (counts.num_triangles + counts.num_spheres) * prof["prim_bytes"]
+    if footprint <= L1_RESIDENT_BYTES:
+        return "issue", footprint
+    if footprint <= L2_BYTES:
+        return "l2", footprint
+    return "hbm", footprint
+
+
 class ClockSampler:
     """nvidia-smi SM clock / throttle sampling during the timed region."""
 
@@ -263,8 +280,173 @@ def _reference_cuda(args, rays_per_path):
         return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
+def _time_frames(s, spp, steps, flush, barrier=None):
+    """Device time (CUDA events on the session's stream, summed) of `steps` frames with L2
+    flushed before each, the canonical rays and paths they traced, per-stage ms and launches."""
+    import torch
+
+    import pathed
+
+    dev_ms = 0.0
+    rays = paths = 0
+    stage_ms = {k: 0.0 for k in pathed.STAGES}
+    stage_launches = {k: 0 for k in pathed.STAGES}
+    for _ in range(steps):
+        flush.zero_()  # L2 flush between steps (outside the frame's events)
+        torch.cuda.synchronize()
+        ms = s.render(spp)
+        dev_ms += ms
+        st = s.stats()
+        rays += st["rays_extend"] + st["rays_shadow"]
+        paths += st["rays_camera"]
+        p = s.profile()
+        for k in pathed.STAGES:
+            stage_ms[k] += p["stage_ms"][k]
+            stage_launches[k] += p["stage_launches"][k]
+    return dev_ms, rays, paths, stage_ms, stage_launches
+
+
+def _count_frame(s, spp):
+    """One untimed frame with work counters: node visits and leaf entries of the closest-hit
+    stage, for the algorithmic-bytes accounting."""
+    s.set_profiling(stage_timing=True, work_counters=True)
+    s.render(spp)
+    prof, st = s.profile(), s.stats()
+    s.set_profiling(stage_timing=True, work_counters=False)
+    return prof, st
+
+
+def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs, sm_mhz):
+    """Roofline of the closest-hit stage (k_extend) on the bound its scene sets:
+      issue  nodes + leaf entries fit in L1 (a few KB): warp instructions issued per second
+             (ncu's instructions per query x queries per launch / live launch time) against
+             4 x 148 issue slots per cycle at the SM clock seen in the timed region;
+      l2     they fit in L2: algorithmic bytes per launch / live launch time against the L2
+             read bandwidth measured in this run (pt_measure_l2_read);
+      hbm    otherwise: the same bytes against the measured HBM copy bandwidth.
+    Algorithmic bytes = nodes x node bytes + leaf entries x 48 B + 48 B queue I/O per query."""
+    hbm, peak_kind = _peaks()
+    bound, footprint = traversal_bound(counts, prof_count)
+    ext_launches = max(1, prof_count["stage_launches"]["extend"])
+    q_ext = st_count["rays_extend"]
+    nodes, prims = prof_count["extend_nodes"], prof_count["extend_prims"]
+    algo_bytes_frame = nodes * prof_count["node_bytes"] + prims * prof_count["prim_bytes"] + q_ext * 48
+    per_launch_bytes = algo_bytes_frame / ext_launches
+    queries_per_launch = q_ext / ext_launches
+    ext_ms = stage_ms["extend"] / max(1, stage_launches["extend"])
+    bytes_gbs = per_launch_bytes / (ext_ms / 1e3) / 1e9
+    bpq = _ncu_bytes_per_query(workload)
+    roof = {"kernel": "k_extend (closest-hit traversal)", "bound": bound, "footprint_bytes": footprint,
+            "traffic": None if bpq is None else bpq * queries_per_launch,
+            "traffic_source": "ncu dram bytes per query x queries per launch (profiles/k_extend_traffic.txt)",
+            "algorithmic_bytes_per_launch": per_launch_bytes, "algorithmic_gbs": bytes_gbs,
+            "avg_launch_ms": ext_ms, "queries_per_launch": queries_per_launch,
+            "nodes_per_query": nodes / max(1, q_ext), "prims_per_query": prims / max(1, q_ext),
+            "hbm_frac": bytes_gbs / hbm}
+    if bound == "issue":
+        ipq = _ncu_per_query(workload, "warp_inst_per_query", "k_extend_issue.txt")
+        fpq = _ncu_per_query(workload, "fp32_flop_per_query", "k_extend_issue.txt")
+        clk = sm_mhz or 1965.0
+        peak = ISSUE_SLOTS_PER_CYCLE * clk * 1e6 / 1e9  # G warp instructions / s
+        achieved = None if ipq is None else ipq * queries_per_launch / (ext_ms / 1e3) / 1e9
+        roof.update({"achieved": achieved, "peak": peak, "unit": "G warp-inst/s",
+                     "frac": None if achieved is None else achieved / peak,
+                     "peak_source": f"4 x 148 issue slots per cycle at {clk:.0f} MHz (median SM clock, timed region)",
+                     "inst_source": "ncu smsp__inst_executed.sum per query (profiles/k_extend_issue.txt)"})
+        if fpq is not None:
+            tflops = fpq * queries_per_launch / (ext_ms / 1e3) / 1e12
+            fp_peak = 148 * 128 * 2 * clk * 1e6 / 1e12
+            roof["fp32"] = {"achieved_tflops": tflops, "peak_tflops": fp_peak, "frac": tflops / fp_peak,
+                            "flop_per_query": fpq}
+    elif bound == "l2":
+        roof.update({"achieved": bytes_gbs, "peak": l2_gbs, "unit": "GB/s",
+                     "frac": bytes_gbs / l2_gbs if l2_gbs else None,
+                     "peak_source": f"measured L2 read bandwidth of a {L2_PROBE_BYTES >> 20} MiB buffer in this run"})
+    else:
+        roof.update({"achieved": bytes_gbs, "peak": hbm, "unit": "GB/s", "frac": bytes_gbs / hbm,
+                     "peak_source": peak_kind + " hbm_gbs (burst copy)"})
+    roof["stage_ms_per_step"] = {k: v / steps for k, v in stage_ms.items()}
+    roof["stage_share"] = {k: v / max(1e-9, sum(stage_ms.values())) for k, v in stage_ms.items()}
+    return roof
+
+
+def _reference_cuda_config(cfg, rays_per_path):
+    """The reference's own CUDA integrator on configuration `cfg`, on this GPU. Configurations
+    0 and 1 at their full size and spp; configurations 2 and 3 (a linear scan of 1.31M
+    triangles per query) on a reduced frame that still fills the GPU (one resident wave of the
+    reference's 16x16 blocks), 1 spp, its per-path time extrapolated to the full frame."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import pathed
+
+    if not os.path.exists(orc.REFBENCH_LIB):
+        return {"unavailable": "reference GPU build (oracle/_ref/librefbench.so) not built"}
+    wl = WORKLOADS[cfg]
+    fw, fh = wl["res"]
+    w, h, spp = (fw, fh, wl["spp"]) if cfg in (0, 1) else ((384, 216) if cfg == 2 else (288, 288)) + (1,)
+    s = pathed.Session(w, h)
+    s.load_config(cfg)
+    sc = s.export_scene()
+    s.close()
+    rb = orc.RefBench()
+    rb.load(sc, w, h)
+    if cfg in (0, 1):
+        rb.render(1, wl["depth"], True)  # warm-up
+        ms = [rb.render(spp, wl["depth"], True) for _ in range(2)]
+    else:
+        ms = [rb.render(spp, wl["depth"], True)]
+    rb.close()
+    mean_ms = sum(ms) / len(ms)
+    paths = w * h * spp
+    mpaths = paths / (mean_ms / 1e3) / 1e6
+    out = {"mpaths_per_s": mpaths, "ms_measured": mean_ms, "measured": f"{w}x{h}, {spp} spp, {len(ms)} frame(s)",
+           "ms_per_frame": mean_ms * (fw * fh * wl["spp"]) / paths,
+           "extrapolated": cfg not in (0, 1),
+           "build": "reference sources (src/renderers/path_tracer.cu et al.), nvcc -O3 sm_100a, FMA on"}
+    if rays_per_path:
+        out["value"] = mpaths * rays_per_path
+        out["unit"] = "Mrays/s"
+        out["rays_per_path"] = rays_per_path
+        out["rays_per_path_source"] = "canonical rays per path of our frames (same estimator, same path lengths)"
+    return out
+
+
+def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
+    """Configuration `cfg` at its full size on rank 0: our Mrays/s and Mpaths/s (autotuned,
+    device time), the closest-hit roofline on its bound and the reference CUDA backend."""
+    import pathed
+
+    wl = WORKLOADS[cfg]
+    w, h = wl["res"]
+    s = pathed.Session(w, h)
+    s.load_config(cfg)
+    tuned = s.autotune(wl["spp"], tune_cache)
+    counts = s.counts()
+    prof_count, st_count = _count_frame(s, wl["spp"])
+    for _ in range(warmup):
+        s.render(wl["spp"])
+    dev_ms, rays, paths, stage_ms, stage_launches = _time_frames(s, wl["spp"], steps, flush)
+    s.close()
+    out = {"workload": wl["name"], "resolution": [w, h], "spp": wl["spp"], "max_depth": wl["depth"],
+           "value": rays / (dev_ms / 1e3) / 1e6, "unit": "Mrays/s", "mpaths_per_s": paths / (dev_ms / 1e3) / 1e6,
+           "ms_per_step": dev_ms / steps, "steps": steps, "warmup": warmup, "triangles": counts.num_triangles,
+           "spheres": counts.num_spheres,
+           "autotuned": {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays", "speculate",
+                                                "blocks_per_sm", "block", "wave_paths")},
+           "roofline": _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs,
+                                 None)}
+    if with_reference:
+        try:
+            ref = _reference_cuda_config(cfg, rays / max(1, paths))
+        except Exception as e:  # report, do not fail the line
+            ref = {"unavailable": f"{type(e).__name__}: {e}"}
+        out["reference_cuda"] = ref
+        if ref.get("mpaths_per_s"):
+            out["speedup_vs_reference_cuda"] = out["mpaths_per_s"] / ref["mpaths_per_s"]
+    return out
+
+
 def run_ours(args):
-    import numpy as np
     import torch
 
     import pathed
@@ -283,6 +465,8 @@ def run_ours(args):
     batch = args.config == 4
     if batch:
         w = h = 16
+    # the L2 read bandwidth that bounds traversal on L2-resident scenes, measured on this GPU
+    l2_gbs, l2_ms = pathed.measure_l2_read(local, L2_PROBE_BYTES, 64, 5)
     s = pathed.Session(w, h)
     s.set_device(local)  # the library's CUDA runtime keeps its own current device
     specs = None
@@ -303,18 +487,14 @@ def run_ours(args):
     if args.quantized_bvh:
         s.set_bvh_quantized(True)
     tuned = None
-    if not args.no_autotune and not batch:  # untimed: frames of this workload under each candidate shape
+    if not args.no_autotune:  # untimed: frames of this workload under each candidate shape
         tuned = s.autotune(spp if spp else 1, args.tune_cache)
     if args.sort_rays:
         s.set_launch(sort_rays=1 if args.sort_rays == "on" else 2)
     counts = s.counts()
 
     # one untimed frame with work counters for the algorithmic-bytes accounting
-    s.set_profiling(stage_timing=True, work_counters=True)
-    s.render(spp)
-    prof_count = s.profile()
-    st_count = s.stats()
-    s.set_profiling(stage_timing=True, work_counters=False)
+    prof_count, st_count = _count_frame(s, spp)
     for _ in range(args.warmup):
         s.render(spp)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -329,22 +509,7 @@ def run_ours(args):
     clocks.wait_first()
     barrier()
     t_clk0 = time.time()
-    dev_ms = 0.0
-    rays = paths = 0
-    stage_ms = {k: 0.0 for k in pathed.STAGES}
-    stage_launches = {k: 0 for k in pathed.STAGES}
-    for _ in range(args.steps):
-        flush.zero_()  # L2 flush between steps (outside the frame's events)
-        torch.cuda.synchronize()
-        ms = s.render(spp)
-        dev_ms += ms
-        st = s.stats()
-        rays += st["rays_extend"] + st["rays_shadow"]
-        paths += st["rays_camera"]
-        p = s.profile()
-        for k in pathed.STAGES:
-            stage_ms[k] += p["stage_ms"][k]
-            stage_launches[k] += p["stage_launches"][k]
+    dev_ms, rays, paths, stage_ms, stage_launches = _time_frames(s, spp, args.steps, flush)
     barrier()
     clk = clocks.stop(t_clk0, time.time())
     t_max, (rays_all, paths_all) = reduce_over_ranks(dev_ms, [rays, paths], world)
@@ -388,38 +553,22 @@ def run_ours(args):
     e2e_value = e2e_rays / e2e_s / 1e6
     e2e_captures = s.profile()["graph_captures"] - captures0  # 0: every timed frame replayed its graph
 
-    # ---- roofline of the extend stage (closest hit): algorithmic bytes per launch
-    hbm, peak_kind = _peaks()
-    ext_launches = max(1, prof_count["stage_launches"]["extend"])
-    nodes = prof_count["extend_nodes"]
-    prims = prof_count["extend_prims"]
     roof = None
     if rank == 0:
-        # algorithmic bytes of the counted frame: nodes x node size + leaf entries x 48 B +
-        # queue traffic (ray 32 B read + hit 16 B written per closest-hit query)
-        q_ext = st_count["rays_extend"]
-        algo_bytes_frame = nodes * prof_count["node_bytes"] + prims * prof_count["prim_bytes"] + q_ext * 48
-        per_launch_bytes = algo_bytes_frame / ext_launches
-        ext_ms = stage_ms["extend"] / max(1, stage_launches["extend"])
-        achieved = per_launch_bytes / (ext_ms / 1e3) / 1e9
-        bpq = _ncu_bytes_per_query(wl["name"])
-        # ncu measured one launch's DRAM bytes; scaled to the average launch by its queries
-        traffic = None if bpq is None else bpq * q_ext / ext_launches
-        roof = {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                "traffic_source": "ncu dram bytes per query x queries per launch (profiles/k_extend_traffic.txt)",
-                "peak_source": peak_kind + " hbm_gbs (burst copy)",
-                "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": ext_ms,
-                "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
-                "stage_share": {k: v / max(1e-9, sum(stage_ms.values())) for k, v in stage_ms.items()},
-                "nodes_per_query": nodes / max(1, q_ext),
-                "prims_per_query": prims / max(1, q_ext)}
+        roof = _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, args.steps, l2_gbs,
+                         clk.get("sm_mhz"))
+        roof["l2_probe"] = {"gbs": l2_gbs, "ms": l2_ms, "bytes": L2_PROBE_BYTES}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not batch:
         mr, mp, sample, thr, _ = cpu_reference_run(args.config, args.cpu_seconds)
         cpu = {"value": mr, "unit": "Mrays/s", "cores": thr, "kind": "port", "sample": sample,
                "mpaths_per_s": mp, "algorithm": "reference integrator restated (two traces per bounce, linear scan)"}
+
+    per_config = None
+    if rank == 0 and world == 1 and not args.no_per_config and not batch:
+        per_config = {str(c): _per_config(c, 3, 3, flush, l2_gbs, args.tune_cache, not args.no_reference_cuda)
+                      for c in (0, 1, 2, 3) if c != args.config}
 
     guiding = None
     if rank == 0 and world == 1 and not args.no_guiding and not batch:
@@ -450,6 +599,7 @@ def run_ours(args):
                     "graph_captures": e2e_captures},
             "roofline": roof,
             "cpu_baseline": cpu,
+            "per_config": per_config,
             "guiding": guiding,
             "clocks": clk,
             "gpu_launches": gpu_launches,
@@ -683,19 +833,47 @@ def batch_time_to_relmse(budget_frames=16, ref_frames=128, draw=0x5EED + 4, n=48
             **out}
 
 
-def _ncu_bytes_per_query(workload):
-    """DRAM bytes per closest-hit query that ncu measured on this workload
-    (profiles/k_extend_traffic.txt, one `<workload> dram_bytes_per_query: B` line each), or None."""
-    p = os.path.join(ROOT, "profiles", "k_extend_traffic.txt")
+def _ncu_per_query(workload, field, fname="k_extend_traffic.txt"):
+    """A per-closest-hit-query figure that ncu measured on this workload (profiles/<fname>,
+    one `<workload> <field>: value` line each), or None."""
+    p = os.path.join(ROOT, "profiles", fname)
     try:
         with open(p) as f:
             for line in f:
                 parts = line.split()
-                if len(parts) == 3 and parts[0] == workload and parts[1] == "dram_bytes_per_query:":
+                if len(parts) == 3 and parts[0] == workload and parts[1] == field + ":":
                     return float(parts[2])
     except OSError:
         pass
     return None
+
+
+def _ncu_bytes_per_query(workload):
+    return _ncu_per_query(workload, "dram_bytes_per_query")
+
+
+def ncu_frames(args):
+    """Frames for an ncu capture (ncu times every launch itself; nothing is timed here). Prints
+    one JSON line per frame with its closest-hit and shadow query counts, so per-query figures
+    can be formed from the captured launches."""
+    import pathed
+
+    wl = WORKLOADS[args.config]
+    w, h = args.res or wl["res"]
+    spp = args.spp or wl["spp"]
+    s = pathed.Session(w, h)
+    s.load_config(args.config)
+    if args.sort_rays:
+        s.set_launch(sort_rays=1 if args.sort_rays == "on" else 2)
+    s.set_profiling(stage_timing=True, work_counters=False)  # direct launches, counted per stage
+    for _ in range(args.ncu_frames):
+        s.render(spp)
+        st = s.stats()
+        print(json.dumps({"workload": wl["name"], "resolution": [w, h], "spp": spp,
+                          "rays_extend": st["rays_extend"], "rays_shadow": st["rays_shadow"],
+                          "extend_launches": s.profile()["stage_launches"]["extend"]}), flush=True)
+    s.close()
+    return 0
 
 
 def main():
@@ -710,6 +888,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guiding", action="store_true")
+    ap.add_argument("--no-per-config", action="store_true",
+                    help="skip the per_config block (the other single-scene configurations at full size)")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="per_config without the reference CUDA backend's timings")
     ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
     ap.add_argument("--gpu-bvh", action="store_true", help="build the BVH on the GPU instead of the host")
     ap.add_argument("--quantized-bvh", action="store_true",
@@ -723,7 +905,13 @@ def main():
                          "applies it without measuring (a profiled run then times what the plain run chose)")
     ap.add_argument("--time-to-relmse", action="store_true",
                     help="with --config 4: print the batch's guided-vs-plain time-to-relMSE line and exit")
+    ap.add_argument("--ncu-frames", type=int, default=0,
+                    help="profiling aid: load the configuration (at --res if given), render this many frames "
+                         "with the default launch shape, print their closest-hit query counts and exit")
+    ap.add_argument("--res", type=int, nargs=2, default=None, help="with --ncu-frames: width height")
     args = ap.parse_args()
+    if args.ncu_frames:
+        return ncu_frames(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.time_to_relmse:

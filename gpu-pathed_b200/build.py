@@ -23,7 +23,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["wavefront.cu", "guide.cu", "bvh_gpu.cu"]
+CU_SOURCES = ["wavefront.cu", "guide.cu", "bvh_gpu.cu", "probe.cu"]
 CPP_SOURCES = ["host_scene.cpp", "bvh_build.cpp", "host_util.cpp", "assets.cpp", "session.cpp", "session_batch.cpp",
                "capi.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] if os.path.isdir(CSRC) else []

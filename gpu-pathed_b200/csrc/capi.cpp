@@ -50,6 +50,12 @@ extern "C" {
 
 const char* pt_version(void) { return "pathed-b200 0.1 (sm_100a)"; }
 
+int pt_measure_l2_read(int device, size_t bytes, int reps, int trials, double* gbs, double* ms) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = pt::measure_l2_read(bytes, reps, trials, gbs, ms);
+    return e == cudaSuccess ? PT_OK : (e == cudaErrorInvalidValue ? PT_ERR_ARG : PT_ERR_CUDA);
+}
+
 int pt_create(int width, int height, pt_session** out) {
     if (!out) return PT_ERR_ARG;
     *out = nullptr;

@@ -139,6 +139,7 @@ struct SceneDevice {
 //   shadow [1e-4, distance - 2e-4] (:104-108).
 constexpr float kCameraTMin = 0.0f;
 constexpr float kBounceTMin = 1e-3f;
+constexpr float kDirectTMin = 1e-4f;  // directSampleBSDF's trace of the sampled direction (:51)
 constexpr float kShadowTMin = 1e-4f;
 
 }  // namespace pt

@@ -823,6 +823,7 @@ int Session::ensure_frame_buffers(int spp) {
     for (int a = 0; a < 3; a++)
         if ((r = check_cuda(d_sq_[a].alloc(f4), "shadow queue"))) return r;
     if ((r = check_cuda(d_L_.alloc(f4), "path radiance"))) return r;
+    if ((r = check_cuda(d_hitd_.alloc(f4), "BSDF-direct hits"))) return r;
     if ((r = check_cuda(d_sort_.alloc(cap * sizeof(int)), "sort index"))) return r;
     if ((r = check_cuda(d_rindex_.alloc(cap * sizeof(int)), "ray-sort index"))) return r;
     if ((r = check_cuda(d_rhist_.alloc(2 * (kMaxDepthLimit + 1) * kRayBuckets * sizeof(int)), "ray-sort buckets")))
@@ -869,6 +870,7 @@ int Session::render_async(int spp) {
         p.q[k].beta = d_q_[k][2].as<float4>();
         p.q[k].rng = d_q_[k][3].as<uint2>();
         p.q[k].hit = d_q_[k][4].as<float4>();
+        p.q[k].hitd = d_hitd_.as<float4>();
         p.q[k].key = d_q_[k][5].as<int>();
     }
     p.sq.o = d_sq_[0].as<float4>();
@@ -1127,6 +1129,30 @@ std::string tune_key(const HostScene& s, int classes, int w, int h, int spp, int
            "_e" + std::to_string(s.env_w) + "_" + std::to_string(w) + "x" + std::to_string(h) + "_spp" +
            std::to_string(spp) + "_d" + std::to_string(depth) + "_n" + std::to_string(nee);
 }
+// A batch's key: its scene count and an FNV-1a hash over every scene's draw (configuration,
+// seed, level, size, spp, depth, guided), so a different draw never reuses another's choice.
+std::string batch_tune_key(const std::vector<BatchSpec>& specs, int nee) {
+    uint64_t h = 1469598103934665603ULL;
+    auto mix = [&](uint64_t v) {
+        for (int k = 0; k < 8; k++) {
+            h ^= (v >> (8 * k)) & 0xff;
+            h *= 1099511628211ULL;
+        }
+    };
+    for (const BatchSpec& b : specs) {
+        mix((uint64_t)b.config);
+        mix(b.seed);
+        mix((uint64_t)(int64_t)b.level);
+        mix((uint64_t)b.width);
+        mix((uint64_t)b.height);
+        mix((uint64_t)b.spp);
+        mix((uint64_t)b.max_depth);
+        mix((uint64_t)b.guided);
+    }
+    char buf[32];
+    std::snprintf(buf, sizeof(buf), "%016llx", (unsigned long long)h);
+    return "batch" + std::to_string(specs.size()) + "_" + buf + "_n" + std::to_string(nee);
+}
 int json_int(const std::string& line, const char* field, int dflt) {
     const std::string k = std::string("\"") + field + "\": ";
     const size_t p = line.find(k);
@@ -1145,9 +1171,13 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     if (spp < 1) return fail(PT_ERR_ARG, "spp must be >= 1");
     pt_tune_result res;
     std::memset(&res, 0, sizeof(res));
-    const std::string key = tune_key(scene_, material_classes_, w_, h_, spp, max_depth_, nee_);
+    const bool batch = batch_mode();
+    const std::string key =
+        batch ? batch_tune_key(batch_specs_, nee_) : tune_key(scene_, material_classes_, w_, h_, spp, max_depth_, nee_);
+    // paths of one frame: waves smaller than this split the frame
+    const long long frame_paths = batch ? batch_paths_ : (long long)w_ * h_ * spp;
     struct Cand {
-        int width, sort, bps, block, rays, spec;
+        int width, sort, bps, block, rays, spec, wave;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
@@ -1157,6 +1187,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         shape_.block_extend = shape_.block_shadow = c.block;
         shape_.sort_rays = c.rays;
         shape_.speculate = c.spec;
+        wave_paths_ = c.wave;
         return PT_OK;
     };
     auto report = [&](const Cand& c) {
@@ -1166,7 +1197,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.block = c.block;
         res.sort_rays = c.rays ? 1 : 2;
         res.speculate = speculate_code(c.spec);
-        res.wave_paths = wave_paths_;
+        res.wave_paths = c.wave;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1177,7 +1208,8 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 const std::string line(buf);
                 if (line.find(want) == std::string::npos) continue;
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
-                       json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0)};
+                       json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0),
+                       json_int(line, "wave_paths", wave_paths_)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1211,7 +1243,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
-              shape_.block_extend, shape_.sort_rays, shape_.speculate};
+              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1226,10 +1258,12 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         }
         return PT_OK;
     };
-    // coordinate descent: BVH width, then material sorting, then grid and block size
+    // coordinate descent: BVH width, then material sorting, ray sorting, speculation, grid and
+    // block size, then the wave size (the queues' capacity). A batch keeps its BVH width (a
+    // change rebuilds every scene of the batch) and its queue order (no ray sorting).
     const int widths_small[3] = {2, 4, 8}, widths_large[2] = {4, 8};
     const int* widths = prims < 100000 ? widths_small : widths_large;
-    const int nw = prims < 100000 ? 3 : 2;
+    const int nw = batch ? 0 : (prims < 100000 ? 3 : 2);
     const Cand start = best;
     for (int i = 0; i < nw; i++)
         if (widths[i] != start.width) {
@@ -1242,7 +1276,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         c.sort = best.sort ? 0 : 1;
         if ((r = consider(c))) return r;
     }
-    if (max_depth_ > 1) {
+    if (!batch && max_depth_ > 1) {
         Cand c = best;
         c.rays = best.rays ? 0 : 1;
         if ((r = consider(c))) return r;
@@ -1266,6 +1300,17 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         c.block = best.block == 128 ? 256 : 128;
         if ((r = consider(c))) return r;
     }
+    {
+        // a wave holds at most kMaxWavePaths paths; halving it only matters where it splits
+        // the frame into more waves (shallower queues, shorter deep-depth tails)
+        const int base_wave = best.wave;
+        for (int wv : {kMaxWavePaths, kMaxWavePaths / 2, kMaxWavePaths / 4})
+            if (wv != base_wave && (long long)wv < frame_paths) {
+                Cand c = best;
+                c.wave = wv;
+                if ((r = consider(c))) return r;
+            }
+    }
     if ((r = apply(best))) return r;
     stage_timing_ = saved_timing;
     reset();
@@ -1279,7 +1324,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
                          "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"ms\": %.4f, "
                          "\"default_ms\": %.4f}\n",
-                         key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, wave_paths_,
+                         key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, best.wave,
                          best_ms, res.default_ms);
             std::fclose(f);
         }

@@ -161,7 +161,7 @@ private:
     DevBuf d_pass_, d_accum_, d_rgba8_;
     DevBuf d_q_[2][6];
     DevBuf d_sq_[3];
-    DevBuf d_L_, d_sort_, d_counters_, d_stats_, d_scratch_;
+    DevBuf d_L_, d_hitd_, d_sort_, d_counters_, d_stats_, d_scratch_;
     DevBuf d_rindex_, d_rhist_;  // ray sorting: slot order and bucket counts/cursors
     int queue_cap_ = 0;
     LaunchShape shape_;

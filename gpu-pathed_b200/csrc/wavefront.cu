@@ -12,9 +12,13 @@
 //   accumulate  per pixel: mean over the frame's samples and the running mean across frames
 //            (src/framebuffer.cu:7-41)
 //
-// Per bounce the reference traces the BSDF direction twice (path_tracer.cu:51 with tMin 1e-4
-// for the MIS emission term and :177 with 1e-3 for the continuation); here it is traced once
-// with tMin 1e-3 and the hit serves both.
+// Per bounce the reference traces the BSDF direction twice: directSampleBSDF with tMin 1e-4
+// for the MIS emission term (path_tracer.cu:51) and the continuation with tMin 1e-3 (:177).
+// Here the extend stage traces it once with tMin 1e-4. That hit serves both unless it lies
+// closer than 1e-3: the closest hit at or beyond 1e-4 that is also at or beyond 1e-3 is the
+// closest hit beyond 1e-3. Only then is the direction traced again from 1e-3, and the shade
+// stage takes the emission term from the first hit and the next vertex from the second, as
+// the reference does. With NEE off (calculateLiNaive, :186-233) there is one trace at 1e-3.
 #include "wavefront.h"
 
 #include <algorithm>
@@ -231,7 +235,11 @@ __global__ void k_extend(FrameParams p, int depth) {
     __shared__ int s_class[8];  // the block's hits per material class
     const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
-    const float tmin = depth == 0 ? kCameraTMin : kBounceTMin;
+    // NEE frames trace bounce rays from the BSDF-direct tMin and re-trace the rare ones whose
+    // hit lies closer than the continuation's (see the file comment); at a path's last depth
+    // only the emission term is needed, so no re-trace
+    const bool two = depth > 0 && p.nee;
+    const float tmin0 = depth == 0 ? kCameraTMin : (two ? kDirectTMin : kBounceTMin);
     const int lane = threadIdx.x & 31;
     const bool sorted = !B && depth > 0 && p.shape.sort_rays;
     const int refill_idle = p.shape.refill_idle;
@@ -246,6 +254,9 @@ __global__ void k_extend(FrameParams p, int depth) {
     // the lane's query; slot < 0: none (then alive is false as well)
     int slot = -1, cur = kEmptyChild, pend = kEmptyChild, sp = 0, of = 0;
     bool alive = false, hit_any = false;  // hit_any: any-hit output, never set for closest hit
+    bool retrace = false;  // the query may be traced again from kBounceTMin (two, not the last depth)
+    bool second = false;   // the query is that second trace
+    float tmin = tmin0;
     RayPre r = make_raypre(V{0.f, 0.f, 0.f}, V{0.f, 0.f, 1.f});
     Hit h{FLT_MAX, 0.f, 0.f, kMissPrim};
     SceneDevice scb;
@@ -265,7 +276,15 @@ __global__ void k_extend(FrameParams p, int depth) {
                     slot = sorted ? p.ray_index[k] : k;
                     const float4 o = q.o[slot], d = q.d[slot];
                     r = make_raypre(mkv(o), mkv(d));
-                    if (B) scb = batch_scene_view(p, tag_scene(__float_as_int(o.w)));
+                    int last = p.max_depth - 1;
+                    if (B) {
+                        const int sid = tag_scene(__float_as_int(o.w));
+                        scb = batch_scene_view(p, sid);
+                        last = p.batch[sid].max_depth - 1;
+                    }
+                    retrace = two && depth < last;
+                    second = false;
+                    tmin = tmin0;
                     h = Hit{FLT_MAX, 0.f, 0.f, kMissPrim};
                     cur = B ? scb.root : p.sc.root;
                     sp = 0;
@@ -280,9 +299,26 @@ __global__ void k_extend(FrameParams p, int depth) {
         const SceneDevice& sc = B ? scb : p.sc;
         traverse_round<W, false, CNT>(sc.nodes, sc.prims, quant, spec, r, tmin, FLT_MAX, st, stride, p.stack_depth, h,
                                       cur, pend, sp, alive, hit_any, of, &work);
+        // a triangle at t = tMin is inside the continuation's range, a sphere is not (triangle.cu:34
+        // accepts t >= tMin, sphere.cu:16,29 need t > tMin)
+        if (slot >= 0 && !alive && retrace && !second && h.prim != kMissPrim &&
+            (h.t < kBounceTMin || (h.prim < 0 && h.t == kBounceTMin))) {
+            // the BSDF-direct ray stopped closer than the continuation's tMin: keep its hit for
+            // the emission term and trace the direction again from kBounceTMin
+            if (of) atomicOr(&p.stats->error, 1);
+            q.hitd[slot] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
+            second = true;
+            tmin = kBounceTMin;
+            h = Hit{FLT_MAX, 0.f, 0.f, kMissPrim};
+            cur = B ? scb.root : p.sc.root;
+            sp = 0;
+            pend = kEmptyChild;
+            of = 0;
+            alive = true;
+        }
         if (slot >= 0 && !alive) {  // the query ended: write its hit to the ray's own slot
             if (of) atomicOr(&p.stats->error, 1);
-            q.hit[slot] = make_float4(h.t, h.b1, h.b2, __int_as_float(h.prim));
+            q.hit[slot] = make_float4(second ? -h.t : h.t, h.b1, h.b2, __int_as_float(h.prim));
             if (p.shape.sort_materials) {
                 const int key = material_class(p.sc, h.prim);
                 q.key[slot] = key;
@@ -400,6 +436,27 @@ __device__ __forceinline__ void guide_account(const FrameParams& p, long long ti
     a[2] += w;
 }
 
+// Emission term of a BSDF-direct ray that stopped closer than the continuation's tMin
+// (directSampleBSDF's hit branch, path_tracer.cu:52-68, at the first hit): front-face
+// emission of a Lambertian emitter with the MIS weight against the emitter sampler, else
+// nothing. Rare, so kept out of line to spare the shade stage's registers.
+// Returns the unweighted emission and its weight through `w`.
+__device__ __noinline__ V direct_hit_emission(const SceneDevice& sc, V o, V dir, float4 hd, float bsdf_pdf,
+                                              bool nomis, bool orthonormal, float& w) {
+    V point, n;
+    int mat;
+    w = 0.f;
+    hit_info(sc, o, dir, hd, point, n, mat);
+    if (orthonormal) n = normalized(n);
+    const Material m = sc.mats[mat];
+    if (!m.emitting) return mkv(0.f);
+    const Frame fr = make_frame(n);
+    const V wo = normalized(to_local(fr, -dir));
+    if (wo.z < 0.f) return mkv(0.f);
+    w = nomis ? 1.f : balance(bsdf_pdf, pdf_scene_light(sc, o, point, n, __float_as_int(hd.w)));
+    return mkv(m.emit[0], m.emit[1], m.emit[2]);
+}
+
 // GUIDE: compiled with the path-guiding code (used when guide_mode != 0); the plain
 // instantiation keeps the reference integrator's register budget. B: batched frame (the
 // scene, its depth, spp and guide come from the path's tag and the scene table).
@@ -437,7 +494,10 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
             const float4 o4 = q.o[slot];
             const float4 d4 = q.d[slot];
             const float4 b4 = q.beta[slot];
-            const float4 h4 = q.hit[slot];
+            float4 h4 = q.hit[slot];
+            // a negative t: the BSDF-direct ray stopped closer (hitd), this is the continuation's hit
+            const bool split = __float_as_int(h4.x) < 0;
+            h4.x = fabsf(h4.x);
             const int tag = __float_as_int(o4.w);
             const int path = tag_path(tag);
             const int sid = B ? tag_scene(tag) : 0;
@@ -453,9 +513,19 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
             const int prim = __float_as_int(h4.w);
             const bool nomis = (flags & 1) || !p.nee;
             V Ladd = mkv(0.f);
+            if (split) {
+                const bool ortho = GUIDE && (B ? p.batch[sid].guide_mode : p.guide_mode);
+                float w;
+                const V Le = direct_hit_emission(sc, o, dir, q.hitd[slot], d4.w, nomis, ortho, w);
+                if (!is_zero(Le)) {
+                    Ladd = beta * Le * w;
+                    if (GUIDE) guide_account(p, ti, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
+                }
+            }
             if (prim == kMissPrim) {
-                // escaped: environment radiance (path_tracer.cu:68-79, :162, :206, :228)
-                const V Le = env_emit(sc.env, dir);
+                // escaped: environment radiance (path_tracer.cu:68-79, :162, :206, :228); a
+                // continuation that misses after a closer BSDF-direct hit adds nothing (:178-180)
+                const V Le = split ? mkv(0.f) : env_emit(sc.env, dir);
                 if (!is_zero(Le)) {
                     const float w = nomis ? 1.f : balance(d4.w, pdf_env_light(sc, dir));
                     Ladd = beta * Le * w;
@@ -471,7 +541,7 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                 const Frame fr = make_frame(n);
                 const V wo = normalized(to_local(fr, -dir));
                 const Material m = sc.mats[mat];
-                if (m.emitting && wo.z >= 0.f) {  // front-face emission (lambertian.cu:5-11)
+                if (!split && m.emitting && wo.z >= 0.f) {  // front-face emission (lambertian.cu:5-11)
                     const V Le = mkv(m.emit[0], m.emit[1], m.emit[2]);
                     const float w = nomis ? 1.f : balance(d4.w, pdf_scene_light(sc, o, point, n, prim));
                     Ladd = beta * Le * w;
@@ -694,6 +764,7 @@ __device__ __forceinline__ bool guide_features(const FrameParams& p, const Guide
         for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
         return false;
     }
+    h4.x = fabsf(h4.x);  // drop the mark of a split BSDF-direct hit
     V point, n;
     int mat;
     hit_info(p.sc, mkv(o4), mkv(d4), h4, point, n, mat);

@@ -15,7 +15,10 @@ struct PathQueue {
     float4* d;     // direction.xyz, pdf of the BSDF sample that produced the ray
     float4* beta;  // throughput.xyz, flags (int bits): bit 0 = no MIS on the next emission
     uint2* rng;    // PCG32 state
-    float4* hit;   // t, b1, b2, primitive (int bits); written by the extend stage
+    float4* hit;   // t, b1, b2, primitive (int bits); written by the extend stage. A negative t
+                   // (-t) marks a continuation hit whose BSDF-direct ray stopped closer (hitd)
+    float4* hitd;  // the BSDF-direct ray's hit where it lies closer than the continuation's tMin
+                   // (written and read only for marked slots; one array shared by both queues)
     int* key;      // material-sort key of the hit (shade stage order), optional
 };
 
@@ -234,6 +237,10 @@ constexpr int kStaticTraceMaxRays = 65536;
 cudaError_t trace_rays_static(const SceneDevice& sc, int stack_depth, const float* o, const float* d,
                               const float* tmin, const float* tmax, int n, int* prim_type, int* prim_id,
                               int* mat_id, float* t, float* bary, int* overflow, cudaStream_t stream);
+
+// Read bandwidth (GB/s, best of `trials` launches of `reps` passes) of an L2-resident buffer of
+// `bytes` on the current device (probe.cu).
+cudaError_t measure_l2_read(size_t bytes, int reps, int trials, double* gbs, double* ms);
 
 // Size in bytes of the traversal stack per block for `threads` threads.
 inline size_t stack_bytes(int stack_depth, int threads) { return (size_t)stack_depth * threads * sizeof(int2); }

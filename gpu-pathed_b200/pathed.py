@@ -45,6 +45,7 @@ EXPORTED = [
     "pt_set_bvh_nodes",
     "pt_readback_async",
     "pt_readback_wait",
+    "pt_measure_l2_read",
 ]
 
 MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
@@ -218,6 +219,8 @@ def _load():
                  "pt_set_bvh_builder", "pt_set_renderer", "pt_set_bvh_nodes"):
         getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
     lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.pt_measure_l2_read.argtypes = [C.c_int, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]
     lib.pt_set_profiling.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_autotune.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p]
     lib.pt_guide_reset.argtypes = [C.c_void_p]
@@ -630,3 +633,14 @@ class Session:
 
 def version() -> str:
     return lib.pt_version().decode()
+
+
+def measure_l2_read(device: int = 0, nbytes: int = 32 << 20, reps: int = 64, trials: int = 5):
+    """Read bandwidth (GB/s) of an L2-resident buffer of `nbytes` on `device`, and the best
+    launch's ms (pt_measure_l2_read): the roofline denominator of traversal on scenes whose
+    nodes and leaf entries fit in L2."""
+    gbs, ms = C.c_double(), C.c_double()
+    rc = lib.pt_measure_l2_read(int(device), int(nbytes), int(reps), int(trials), C.byref(gbs), C.byref(ms))
+    if rc != 0:
+        raise PathedError(rc, "pt_measure_l2_read failed")
+    return gbs.value, ms.value

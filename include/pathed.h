@@ -458,6 +458,16 @@ int pt_set_bvh_nodes(pt_session* s, int quantized);
  * (PT_ERR_STATE for a batch). */
 int pt_set_renderer(pt_session* s, int kind);
 
+/* Measurement support (no counterpart in the reference): the read bandwidth, in GB/s, of a
+ * buffer of `bytes` (a multiple of 16, at least 1 MiB) that stays in L2, on CUDA device
+ * `device` (made the library's current device).
+ * A full persistent grid reads it `reps` times per launch with 16-byte loads cached in L2
+ * only; the best of `trials` launches timed with CUDA events is returned in *gbs, its
+ * duration in *ms (either may be NULL). Allocates the buffer for the call and frees it. It is
+ * the denominator of the closest-hit roofline on scenes whose nodes and leaf entries fit in
+ * L2 (the 1.31M-triangle mesh: about 100 MB against a 126 MB L2). */
+int pt_measure_l2_read(int device, size_t bytes, int reps, int trials, double* gbs, double* ms);
+
 /* Library version string. */
 const char* pt_version(void);
 

@@ -866,7 +866,10 @@ struct Camera {
 
 // ---- integrator (src/renderers/path_tracer.cu:38-233) -----------------------------------
 // trace_once = 0: the reference's two traces per bounce (BSDF-direct at tMin 1e-4, :51, and
-// continuation at 1e-3, :177). trace_once = 1: one trace at 1e-3 serves both (the CUDA path).
+// continuation at 1e-3, :177). trace_once = 1: the CUDA path's rules: one trace at 1e-4 serves
+// both unless its hit lies closer than 1e-3, when the direction is traced again from 1e-3 for
+// the continuation (the same hits as the two traces), and paths that cannot add anything are
+// dropped instead of traced.
 // Canonical queries: camera + continuation closest hits, and shadow rays that can contribute.
 // `duplicate` counts the reference's second trace of each BSDF direction (compat mode only).
 struct Counters { uint64_t queries = 0, shadow = 0, duplicate = 0; };
@@ -953,8 +956,19 @@ Vec3 LiNEE(const Scene& sc, const Ray& ray, int maxDepth, Rng& rng, int traceOnc
                 return result;
             }
             cnt.queries++;
-            nhit = worldHit(sc, bounce, 1e-3, FLT_MAX, next);
-            direct += bsdfDirectFromHit(sc, rec, bs, nhit, next, bounceDir);
+            HitRecord dh;
+            const bool dhit = worldHit(sc, bounce, 1e-4, FLT_MAX, dh);
+            direct += bsdfDirectFromHit(sc, rec, bs, dhit, dh, bounceDir);
+            // a triangle at t = tMin is inside the continuation's range, a sphere is not
+            // (triangle.cu:34 accepts t >= tMin, sphere.cu:16,29 need t > tMin)
+            const bool closer = dh.t < 1e-3f || (dh.primType == SPHERE && dh.t == 1e-3f);
+            if (dhit && closer && path + 1 < maxDepth) {
+                cnt.duplicate++;  // the continuation's own trace: not a canonical query
+                nhit = worldHit(sc, bounce, 1e-3, FLT_MAX, next);
+            } else {
+                nhit = dhit;
+                next = dh;
+            }
         } else {
             if (!bs.f.isZero()) {
                 HitRecord br;

@@ -8,7 +8,8 @@
     subset, per pixel within 3 combined standard errors, and relMSE against the oracle
     bounded by what the two estimators' variances alone give (no bias beyond noise);
   * the slit room's time-to-relMSE reference (the plain 2048-spp render, consistent MIS,
-    passes accumulated in FP64) against the FP64 oracle in the same MIS convention.
+    passes accumulated in FP64) against the FP64 oracle in the same MIS convention, on a
+    seeded 2048-pixel subset.
 
 relMSE = mean over pixel channels of (I - I_ref)^2 / (I_ref^2 + 1e-2), I_ref the oracle.
 The oracle traces through its parity accelerator (bit-identical to the linear scan,
@@ -102,7 +103,10 @@ def test_time_to_relmse_reference_vs_fp64_oracle(oracle_lib):
     import bench
 
     w, h, depth = FULL[3]
-    pix = pixel_subset(w, h, 4096, seed=77)
+    # few pixels at many oracle samples: the light arrives through the slit, so a pixel's
+    # samples are mostly dark with rare bright ones, and a standard error estimated from a
+    # few hundred of them is too small in most pixels
+    pix = pixel_subset(w, h, 2048, seed=77)
     r = bench._slit_session(w)
     r.set_seed(12345)
     passes = []
@@ -115,14 +119,14 @@ def test_time_to_relmse_reference_vs_fp64_oracle(oracle_lib):
     ref = passes.mean(0)
     ref_se = passes.std(0, ddof=1) / np.sqrt(len(passes))
     osc = oracle_lib.scene(sc, accel=True)
-    o_mean, o_var, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, 256, depth, nee=True, seed=5,
+    o_mean, o_var, _ = oracle_lib.render(osc, sc["camera"], w, h, pix, 1024, depth, nee=True, seed=5,
                                          trace_once=False, consistent_mis=True)
     o_se = np.sqrt(o_var)
     frac = three_se_pass(ref, ref_se, o_mean, o_se, floor=1e-6)
     e = rel_mse(ref, o_mean)
     e_exp = expected_rel_mse(ref_se, o_se, o_mean)
     ref_noise = float(np.mean(ref_se ** 2 / (o_mean ** 2 + 1e-2)))
-    print(f"slit-room 2048-spp reference vs FP64 oracle (256 spp, consistent MIS) on 4096 pixels: 3-SE pass "
+    print(f"slit-room 2048-spp reference vs FP64 oracle (1024 spp, consistent MIS) on 2048 pixels: 3-SE pass "
           f"{frac:.4f}; relMSE {e:.3e} (expected from the variances {e_exp:.3e}); the reference's own noise "
           f"relMSE {ref_noise:.3e}")
     assert frac >= 0.97
