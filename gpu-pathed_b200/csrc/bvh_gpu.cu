@@ -491,6 +491,24 @@ __global__ void k_quantize_nodes(const BvhNode<W>* __restrict__ in, int n, uint3
 
 }  // namespace
 
+// Triangle leaf entries for the watertight test: (p0, id) (p1) (p2), the original vertices
+// (tri_p, 3 float4 per triangle) in place of the edges e1, e2; sphere entries are unchanged.
+// Shared vertices keep their exact values, which the test's watertightness relies on.
+__global__ void k_prims_vertices(float4* __restrict__ prims, int n, const float4* __restrict__ tri_p) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int id = __float_as_int(prims[3 * e].w);
+    if (id < 0) return;
+    prims[3 * e + 1] = tri_p[3 * (size_t)id + 1];
+    prims[3 * e + 2] = tri_p[3 * (size_t)id + 2];
+}
+
+cudaError_t prims_to_vertices(float4* prims, int n, const float4* tri_p, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_prims_vertices<<<(n + 255) / 256, 256, 0, st>>>(prims, n, tri_p);
+    return cudaGetLastError();
+}
+
 cudaError_t quantize_bvh_nodes(const void* nodes, int num_nodes, int width, void* out, int* fail,
                                cudaStream_t stream) {
     if (num_nodes <= 0) return cudaSuccess;

@@ -24,6 +24,8 @@ struct GpuBvhInfo {
 // Quantized copy (qnode_bytes(width) per node, width 4 or 8) of `num_nodes` BvhNode<width>
 // nodes on the device. `fail` (device int) is set when a node cannot be quantized
 // conservatively (it cannot happen for finite boxes; the check is kept).
+// Rewrite the n leaf entries' triangles as (p0, id) (p1) (p2) for the watertight test.
+cudaError_t prims_to_vertices(float4* prims, int n, const float4* tri_p, cudaStream_t st);
 cudaError_t quantize_bvh_nodes(const void* nodes, int num_nodes, int width, void* out, int* fail,
                                cudaStream_t stream);
 

@@ -50,6 +50,16 @@ extern "C" {
 
 const char* pt_version(void) { return "pathed-b200 0.1 (sm_100a)"; }
 
+int pt_set_watertight(pt_session* s, int on) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.set_watertight(on); });
+}
+
+int pt_set_test_limits(pt_session* s, int stack_entries, int mma_polls) {
+    if (!s) return PT_ERR_ARG;
+    return guarded(s, [&] { return s->impl.set_test_limits(stack_entries, mma_polls); });
+}
+
 int pt_measure_l2_read(int device, size_t bytes, int reps, int trials, double* gbs, double* ms) {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = pt::measure_l2_read(bytes, reps, trials, gbs, ms);

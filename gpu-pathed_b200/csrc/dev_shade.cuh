@@ -134,6 +134,20 @@ __device__ __forceinline__ V mf_f(float alpha, V wo, V wi) {
     const float G = mf_G(alpha, wi, wo, wh);
     return mkv(D * G * F / (4.f * ci * co));
 }
+// kMetal: the same D and G with a per-channel Schlick Fresnel, F = F0 + (1 - F0)(1 - c)^5 at
+// c = wi . wh, F0 the material's albedo (Schlick 1994).
+__device__ __forceinline__ V mf_metal_f(const Material& m, V wo, V wi) {
+    if (wo.z < 0.f || wi.z < 0.f) return mkv(0.f);
+    const float co = fabsf(wo.z), ci = fabsf(wi.z);
+    const V wh = normalized(wo + wi);
+    if (co == 0.f || ci == 0.f) return mkv(0.f);
+    if (is_zero(wh)) return mkv(0.f);
+    const float cinc = fminf(1.f, fmaxf(dot(wi, wh), 0.f));
+    const float q = 1.f - cinc, q2 = q * q, q5 = q2 * q2 * q;
+    const float s = mf_D(m.alpha, wi, wh) * mf_G(m.alpha, wi, wo, wh) / (4.f * ci * co);
+    return mkv((m.albedo[0] + (1.f - m.albedo[0]) * q5) * s, (m.albedo[1] + (1.f - m.albedo[1]) * q5) * s,
+               (m.albedo[2] + (1.f - m.albedo[2]) * q5) * s);
+}
 __device__ __forceinline__ float mf_pdf(float alpha, V wo, V wi) {
     if (wo.z < 0.f || wi.z < 0.f) return 0.f;
     const V wh = normalized(wo + wi);
@@ -159,13 +173,15 @@ __device__ __forceinline__ V bsdf_f(const Material& m, V wo, V wi) {
     switch (m.type) {
         case kLambertian: return lambert_f(m, wo, wi);
         case kMicrofacet: return mf_f(m.alpha, wo, wi);
+        case kMetal: return mf_metal_f(m, wo, wi);
         default: return mkv(0.f);  // mirror, glass: f = 0
     }
 }
 __device__ __forceinline__ float bsdf_pdf(const Material& m, V wo, V wi) {
     switch (m.type) {
         case kLambertian: return lambert_pdf(wi);
-        case kMicrofacet: return mf_pdf(m.alpha, wo, wi);
+        case kMicrofacet:
+        case kMetal: return mf_pdf(m.alpha, wo, wi);
         default: return 0.f;
     }
 }

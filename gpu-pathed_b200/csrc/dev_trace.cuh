@@ -60,6 +60,64 @@ __device__ __forceinline__ bool tri_test(V p0, V e1, V e2, V o, V d, float tmin,
     return true;
 }
 
+// Component k (0, 1, 2) of a vector, by selects (no local memory).
+__device__ __forceinline__ float vcomp(V v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Watertight ray/triangle test (Woop, Benthin and Wald, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1), 2013), the opt-in alternative to Triangle::hit: no ray that
+// passes through a shared edge or vertex of a closed mesh slips between its triangles.
+// - Axes: kz is the largest component of |d| (first of x, y, z on ties), kx and ky the next two
+//   cyclically, swapped when d[kz] < 0 so the winding is kept.
+// - Shear: sz = 1 / d[kz], sx = d[kx] * sz, sy = d[ky] * sz (every operation rounded once).
+// - Vertices relative to the origin, sheared so the ray runs along +z: ax = A[kx] - sx A[kz],
+//   ay = A[ky] - sy A[kz] (likewise B, C).
+// - Edge functions U = cx by - cy bx, V = ax cy - ay cx, W = bx ay - by ax; any that is exactly 0
+//   is recomputed in FP64 from the same FP32 inputs (products exact, one rounding each).
+// - Mixed signs miss; det = U + V + W, det = 0 misses; T = U sz A[kz] + V sz B[kz] + W sz C[kz],
+//   t = T / det within [tmin, tmax] (inclusive, as Triangle::hit), b1 = V / det (weight of p1),
+//   b2 = W / det (weight of p2). No backface culling, as the reference.
+// Every FP32 operation is an explicit round-to-nearest intrinsic (no contraction), so the
+// oracle's host restatement gives the same bits.
+__device__ __forceinline__ bool tri_test_wt(V p0, V p1, V p2, V o, V d, float tmin, float tmax, float& t,
+                                            float& b1, float& b2) {
+    const float adx = fabsf(d.x), ady = fabsf(d.y), adz = fabsf(d.z);
+    const int kz = adx >= ady ? (adx >= adz ? 0 : 2) : (ady >= adz ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    const float dz = vcomp(d, kz);
+    if (dz < 0.f) {
+        const int k = kx;
+        kx = ky;
+        ky = k;
+    }
+    const float sz = __fdiv_rn(1.f, dz);
+    const float sx = __fmul_rn(vcomp(d, kx), sz), sy = __fmul_rn(vcomp(d, ky), sz);
+    const V A = xsub(p0, o), B = xsub(p1, o), C = xsub(p2, o);
+    const float Az = vcomp(A, kz), Bz = vcomp(B, kz), Cz = vcomp(C, kz);
+    const float ax = __fsub_rn(vcomp(A, kx), __fmul_rn(sx, Az)), ay = __fsub_rn(vcomp(A, ky), __fmul_rn(sy, Az));
+    const float bx = __fsub_rn(vcomp(B, kx), __fmul_rn(sx, Bz)), by = __fsub_rn(vcomp(B, ky), __fmul_rn(sy, Bz));
+    const float cx = __fsub_rn(vcomp(C, kx), __fmul_rn(sx, Cz)), cy = __fsub_rn(vcomp(C, ky), __fmul_rn(sy, Cz));
+    float U = __fsub_rn(__fmul_rn(cx, by), __fmul_rn(cy, bx));
+    float Vv = __fsub_rn(__fmul_rn(ax, cy), __fmul_rn(ay, cx));
+    float Ww = __fsub_rn(__fmul_rn(bx, ay), __fmul_rn(by, ax));
+    if (U == 0.f || Vv == 0.f || Ww == 0.f) {
+        U = __double2float_rn(__dsub_rn(__dmul_rn((double)cx, (double)by), __dmul_rn((double)cy, (double)bx)));
+        Vv = __double2float_rn(__dsub_rn(__dmul_rn((double)ax, (double)cy), __dmul_rn((double)ay, (double)cx)));
+        Ww = __double2float_rn(__dsub_rn(__dmul_rn((double)bx, (double)ay), __dmul_rn((double)by, (double)ax)));
+    }
+    if ((U < 0.f || Vv < 0.f || Ww < 0.f) && (U > 0.f || Vv > 0.f || Ww > 0.f)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, Vv), Ww);
+    if (det == 0.f) return false;
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, __fmul_rn(sz, Az)), __fmul_rn(Vv, __fmul_rn(sz, Bz))),
+                              __fmul_rn(Ww, __fmul_rn(sz, Cz)));
+    const float inv = __fdiv_rn(1.f, det);
+    t = __fmul_rn(T, inv);
+    if (!(t >= tmin && t <= tmax)) return false;
+    b1 = __fmul_rn(Vv, inv);
+    b2 = __fmul_rn(Ww, inv);
+    return true;
+}
+
 // Sphere::hit root selection: the near root when it lies above tmin, else the far root.
 // Returns false when neither root is above tmin (the caller applies the strict upper bound).
 __device__ __forceinline__ bool sphere_candidate(V c, float r, V o, V d, float tmin, float& t) {
@@ -110,8 +168,9 @@ __device__ __forceinline__ float box_entry(const RayPre& r, float lx, float hx, 
 }
 
 // Closest-hit acceptance for one leaf entry (tie rules above). `tcur` is best.t or tmax.
+// `wt`: the scene's triangle entries hold p0, p1, p2 and take the watertight test.
 __device__ __forceinline__ void leaf_entry(const float4* __restrict__ prims, int e, const RayPre& r,
-                                           float tmin, float tmax, Hit& best) {
+                                           float tmin, float tmax, Hit& best, bool wt) {
     const float4 a = __ldg(prims + 3 * e);
     const int id = __float_as_int(a.w);
     const float tcur = best.prim == kMissPrim ? tmax : best.t;
@@ -119,7 +178,9 @@ __device__ __forceinline__ void leaf_entry(const float4* __restrict__ prims, int
         const float4 b = __ldg(prims + 3 * e + 1);
         const float4 c = __ldg(prims + 3 * e + 2);
         float t, b1, b2;
-        if (tri_test(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tcur, t, b1, b2)) {
+        const bool h = wt ? tri_test_wt(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tcur, t, b1, b2)
+                          : tri_test(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tcur, t, b1, b2);
+        if (h) {
             // equal t: the higher triangle index wins; a triangle beats a sphere
             if (t == tcur && best.prim != kMissPrim && best.prim >= 0 && id < best.prim) return;
             best.t = t;
@@ -146,14 +207,15 @@ __device__ __forceinline__ void leaf_entry(const float4* __restrict__ prims, int
 
 // Any-hit acceptance for one leaf entry: true if the entry blocks [tmin, tmax].
 __device__ __forceinline__ bool leaf_entry_any(const float4* __restrict__ prims, int e, const RayPre& r,
-                                               float tmin, float tmax) {
+                                               float tmin, float tmax, bool wt) {
     const float4 a = __ldg(prims + 3 * e);
     const int id = __float_as_int(a.w);
     if (id >= 0) {
         const float4 b = __ldg(prims + 3 * e + 1);
         const float4 c = __ldg(prims + 3 * e + 2);
         float t, b1, b2;
-        return tri_test(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tmax, t, b1, b2);
+        return wt ? tri_test_wt(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tmax, t, b1, b2)
+                  : tri_test(mkv(a), mkv(b), mkv(c), r.o, r.d, tmin, tmax, t, b1, b2);
     }
     const float4 b = __ldg(prims + 3 * e + 1);
     float t;
@@ -345,18 +407,18 @@ __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool
 // at its first hit.
 template <bool ANY, bool CNT>
 __device__ __forceinline__ void leaf_test(const float4* __restrict__ prims, int leaf, const RayPre& r, float tmin,
-                                          float tmax, Hit& best, bool& hit_any, TraceWork* work) {
+                                          float tmax, Hit& best, bool& hit_any, TraceWork* work, bool wt) {
     const int first = leaf_first(leaf), cnt = leaf_count(leaf);
     if (CNT) work->prims += cnt;
     if (ANY) {
         for (int e = first; e < first + cnt; e++) {
-            if (leaf_entry_any(prims, e, r, tmin, tmax)) {
+            if (leaf_entry_any(prims, e, r, tmin, tmax, wt)) {
                 hit_any = true;
                 break;
             }
         }
     } else {
-        for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best);
+        for (int e = first; e < first + cnt; e++) leaf_entry(prims, e, r, tmin, tmax, best, wt);
     }
 }
 
@@ -366,8 +428,8 @@ template <int W, bool ANY, bool CNT>
 __device__ __forceinline__ void leaf_step(const float4* __restrict__ nodes, const float4* __restrict__ prims,
                                           bool quant, const RayPre& r, float tmin, float tmax,
                                           int2* __restrict__ stk, int stride, Hit& best, int& cur, int& sp,
-                                          bool& alive, bool& hit_any, TraceWork* work) {
-    leaf_test<ANY, CNT>(prims, cur, r, tmin, tmax, best, hit_any, work);
+                                          bool& alive, bool& hit_any, TraceWork* work, bool wt) {
+    leaf_test<ANY, CNT>(prims, cur, r, tmin, tmax, best, hit_any, work, wt);
     if (ANY && hit_any) alive = false;
     if (alive) {
         cur = stack_pop<W, ANY>(nodes, quant, r, tmin, tmax, best, stk, stride, sp);
@@ -387,7 +449,7 @@ __device__ __forceinline__ void traverse_round(const float4* __restrict__ nodes,
                                                bool quant, bool spec, const RayPre& r, float tmin, float tmax,
                                                int2* __restrict__ stk, int stride, int max_depth, Hit& best,
                                                int& cur, int& pend, int& sp, bool& alive, bool& hit_any,
-                                               int& overflow, TraceWork* work) {
+                                               int& overflow, TraceWork* work, bool wt = false) {
     // ---- phase 1: internal nodes, while some live lane has found no leaf
     while (__any_sync(0xffffffffu, alive && cur >= 0 && pend == kEmptyChild)) {
         if (alive && cur >= 0) {
@@ -411,11 +473,12 @@ __device__ __forceinline__ void traverse_round(const float4* __restrict__ nodes,
     }
     // ---- phase 2: the parked leaf, then the current one (which pops the stack)
     if (alive && pend != kEmptyChild) {
-        leaf_test<ANY, CNT>(prims, pend, r, tmin, tmax, best, hit_any, work);
+        leaf_test<ANY, CNT>(prims, pend, r, tmin, tmax, best, hit_any, work, wt);
         pend = kEmptyChild;
         if (ANY && hit_any) alive = false;
     }
-    if (alive && cur < 0) leaf_step<W, ANY, CNT>(nodes, prims, quant, r, tmin, tmax, stk, stride, best, cur, sp, alive, hit_any, work);
+    if (alive && cur < 0)
+        leaf_step<W, ANY, CNT>(nodes, prims, quant, r, tmin, tmax, stk, stride, best, cur, sp, alive, hit_any, work, wt);
 }
 
 // Warp-synchronous traversal: every lane of the warp calls this together (`active` marks the
@@ -431,6 +494,7 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
     const float4* __restrict__ nodes = sc.nodes;
     const float4* __restrict__ prims = sc.prims;
     const bool quant = Q < 0 ? (W >= 4 && sc.node_q != 0) : (W >= 4 && Q == 1);  // warp-uniform
+    const bool wt = sc.watertight != 0;
     best.prim = kMissPrim;
     best.t = tmax;
     int sp = 0;
@@ -440,7 +504,7 @@ __device__ __forceinline__ bool traverse(const SceneDevice& sc, const RayPre& r,
     int pend = kEmptyChild;
     while (__any_sync(0xffffffffu, alive))
         traverse_round<W, ANY, CNT>(nodes, prims, quant, false, r, tmin, tmax, stk, stride, max_depth, best, cur, pend,
-                                    sp, alive, hit_any, overflow, work);
+                                    sp, alive, hit_any, overflow, work, wt);
     if (ANY) {
         if (hit_any) best.prim = 0;
         return hit_any;

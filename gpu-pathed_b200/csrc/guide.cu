@@ -114,7 +114,8 @@ __global__ void k_guide_forward_x(const uint32_t* __restrict__ wpack, const floa
 // 128 inputs per tile, one thread each. Raw outputs like k_guide_forward_x.
 __global__ void __launch_bounds__(kTcRows) k_guide_forward_x_tc(const uint32_t* __restrict__ wpack,
                                                                 const float* __restrict__ x, int n,
-                                                                float* __restrict__ raw, int* error) {
+                                                                float* __restrict__ raw, int* error,
+                                                                int test_polls) {
     extern __shared__ __align__(1024) uint8_t tsm[];
     TcSmem& s = *reinterpret_cast<TcSmem*>(tsm);
     const int tiles = (n + kTcRows - 1) / kTcRows;
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(kTcRows) k_guide_forward_x_tc(const uint32_t* 
         tc_fence_before();
         __syncthreads();
         float out[kGuideOut];
-        if (!tc_network(s, tmem, phase, out)) {
+        if (!tc_network(s, tmem, phase, out, test_polls)) {
             if (t == 0) atomicOr(error, 2);
             break;
         }
@@ -592,11 +593,11 @@ cudaError_t guide_configure() {
 }
 
 cudaError_t guide_forward_features_tc(const GuideDevice& g, const float* x, int n, float* raw, int* error,
-                                      cudaStream_t s) {
+                                      cudaStream_t s, int test_polls) {
     if (n <= 0) return cudaSuccess;
     const int tiles = (n + kTcRows - 1) / kTcRows;
     const int grid = tiles < g.num_sms * 4 ? tiles : g.num_sms * 4;
-    k_guide_forward_x_tc<<<grid, kTcRows, sizeof(TcSmem), s>>>(g.wpack, x, n, raw, error);
+    k_guide_forward_x_tc<<<grid, kTcRows, sizeof(TcSmem), s>>>(g.wpack, x, n, raw, error, test_polls);
     return cudaGetLastError();
 }
 

@@ -59,9 +59,9 @@ cudaError_t guide_pack(const GuideDevice& g, cudaStream_t s);
 // Raw network outputs for n explicit input vectors (inference kernel, tensor cores).
 cudaError_t guide_forward_features(const GuideDevice& g, const float* x, int n, float* raw, cudaStream_t s);
 // The same on the 5th-generation tensor cores (tcgen05.mma into tensor memory); a wait that
-// gives up sets bit 1 of *error (device int).
+// gives up sets bit 1 of *error (device int). test_polls > 0: the test hook of tc_network.
 cudaError_t guide_forward_features_tc(const GuideDevice& g, const float* x, int n, float* raw, int* error,
-                                      cudaStream_t s);
+                                      cudaStream_t s, int test_polls = 0);
 // Gradient of the batch loss -sum_i w_i log q(wi_i | x_i) / sum_i w_i with respect to all
 // parameters, for explicit input vectors (training kernel); grad is overwritten.
 cudaError_t guide_gradients_features(const GuideDevice& g, const float* x, const float* wi, const float* w, int n,

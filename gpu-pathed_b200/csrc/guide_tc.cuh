@@ -75,6 +75,21 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 
+// Non-blocking test of the mbarrier's phase `parity`.
+__device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t"
+        "}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
 // Wait for the mbarrier's phase `parity` to complete; gives up after `limit` polls.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int limit) {
     for (int i = 0; i < limit; i++) {
@@ -175,8 +190,11 @@ struct TcSmem {
 
 // The whole network for the CTA's current 128-row tile (inputs already in s.a, fenced and
 // synchronised). Leaves each thread's 40 raw outputs in `raw`. Returns false when a wait
-// gave up (outputs invalid). All 128 threads call it.
-__device__ __forceinline__ bool tc_network(TcSmem& s, uint32_t tmem, uint32_t& phase, float raw[kGuideOut]) {
+// gave up (outputs invalid). All 128 threads call it. test_polls > 0 (a test hook) limits the
+// first wait of each layer to that many non-blocking polls, so it gives up while the layer's
+// MMA is still running; the bounded drain that follows still waits for that MMA to finish.
+__device__ __forceinline__ bool tc_network(TcSmem& s, uint32_t tmem, uint32_t& phase, float raw[kGuideOut],
+                                           int test_polls = 0) {
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t mbar = smem_u32(&s.mbar);
     const uint32_t a_saddr = smem_u32(s.a), w_saddr = smem_u32(s.w);
@@ -190,7 +208,12 @@ __device__ __forceinline__ bool tc_network(TcSmem& s, uint32_t tmem, uint32_t& p
             const int woff = layer == 0 ? kTcW1 : layer == 1 ? kTcW2 : layer == 2 ? kTcW3 : kTcW4;
             tc_layer(tmem, a_saddr, w_saddr + woff, k, n, layer == 3 ? kTcLboW4 : kTcLboW, mbar);
         }
-        const bool done = mbar_wait(mbar, phase, kLimit);
+        bool done = false;
+        if (test_polls > 0) {
+            for (int i = 0; i < test_polls && !done; i++) done = mbar_test(mbar, phase);
+        } else {
+            done = mbar_wait(mbar, phase, kLimit);
+        }
         if (!__syncthreads_and(done ? 1 : 0)) {
             // give up: wait once more (bounded) for the layer in flight before the caller
             // releases tensor memory; the phase bookkeeping is lost, so the caller stops

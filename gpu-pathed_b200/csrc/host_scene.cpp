@@ -301,6 +301,21 @@ void gen_spheres(uint64_t seed, HostScene& s) {
                                    (float)balls[i].r});
         s.sph_mat.push_back((int)s.mats.size() - 1);
     }
+    // F0 0.04 or a metallic RGB: half the Beckmann spheres (drawn from their own stream, so
+    // the rest of the draw is unchanged) become metals with the normal-incidence reflectance of
+    // gold, silver, copper or aluminium (linear RGB, the values tabulated in Hoffman's
+    // physically based shading notes, SIGGRAPH 2010); the others keep the reference's
+    // dielectric Fresnel of eta 1.5
+    static const float kMetalF0[4][3] = {
+        {1.000f, 0.766f, 0.336f}, {0.972f, 0.960f, 0.915f}, {0.955f, 0.638f, 0.538f}, {0.913f, 0.922f, 0.924f}};
+    HostRng mrng(seed ^ 0x3E7A11C0FFEEULL);
+    for (size_t i = 1; i < s.mats.size(); i++) {
+        Material& m = s.mats[i];
+        if (m.type != kMicrofacet || mrng.uniform(0.0, 1.0) >= 0.5) continue;
+        const float* f0 = kMetalF0[mrng.next() % 4];
+        m.type = kMetal;
+        for (int k = 0; k < 3; k++) m.albedo[k] = f0[k];
+    }
     for (int i = 0; i < 4; i++) {  // 4 sphere emitters, radiance 5..50
         const float e = (float)rng.uniform(5.0, 50.0);
         s.mats.push_back(lambert(0.f, 0.f, 0.f, e, e, e));
@@ -486,7 +501,7 @@ bool validate_scene(const HostScene& s, std::string& err) {
         return false;
     }
     for (const Material& m : s.mats) {
-        if (m.type < kLambertian || m.type > kMicrofacet) {
+        if (m.type < kLambertian || m.type > kMetal || m.type == kMaterialNone) {
             err = "unknown material type " + std::to_string(m.type);
             return false;
         }

@@ -26,7 +26,8 @@ namespace py = pybind11;
 namespace {
 
 // materials/types.h:5-11
-enum class MaterialType { Lambertian = 0, Mirror = 1, Glass = 2, Microfacet = 3, None = 4 };
+// Metal (5) is this build's metallic-F0 Beckmann material; the reference's enum stops at None.
+enum class MaterialType { Lambertian = 0, Mirror = 1, Glass = 2, Microfacet = 3, None = 4, Metal = 5 };
 // scene_model.h:15-19
 enum class RendererType { CUDA = 0, Optix = 1, Normals = 2 };
 
@@ -524,6 +525,7 @@ PYBIND11_MODULE(path_tracer, m) {
         .value("Glass", MaterialType::Glass)
         .value("Microfacet", MaterialType::Microfacet)
         .value("None", MaterialType::None)
+        .value("Metal", MaterialType::Metal)
         .export_values();
 
     py::class_<MaterialIndex>(m, "MaterialIndex")

@@ -25,14 +25,20 @@
 
 namespace pt {
 
-// Material types: same enumerators and values as the reference (include/materials/types.h:5-11).
+// Material types: same enumerators and values as the reference (include/materials/types.h:5-11),
+// plus kMetal, which the reference lacks: its Beckmann microfacet with a Schlick Fresnel term of
+// RGB reflectance F0 (the material's albedo) at normal incidence, for metals; the reference's
+// Microfacet uses a dielectric Fresnel of fixed eta 1.5 (F0 = 0.04, microfacet.h:111).
 enum MaterialType : int {
     kLambertian = 0,
     kMirror = 1,
     kGlass = 2,
     kMicrofacet = 3,
     kMaterialNone = 4,
+    kMetal = 5,
 };
+// Material classes of sorted shading: miss, then one per type (type + 1)
+constexpr int kMaterialClasses = kMetal + 2;
 
 // Primitive types (include/primitives/types.h:5-8).
 enum PrimType : int { kTriangle = 0, kSphere = 1 };
@@ -131,7 +137,7 @@ struct SceneDevice {
     int bvh_width;             // 2, 4 or 8
     int root;                  // root node index (always an internal node)
     int node_q;                // 1: `nodes` holds quantized nodes (widths 4 and 8)
-    int pad;
+    int watertight;            // 1: triangle leaf entries hold p0, p1, p2 and take the watertight test
 };
 
 // Ray-query kinds and their [tMin, tMax] conventions (src/renderers/path_tracer.cu):

@@ -113,10 +113,11 @@ int Session::ensure_device() {
 }
 
 void Session::update_material_classes() {
-    bool seen[4] = {false, false, false, false};
-    for (int m : scene_.tri_mat) seen[scene_.mats[m].type & 3] = true;
-    for (int m : scene_.sph_mat) seen[scene_.mats[m].type & 3] = true;
-    material_classes_ = (int)seen[0] + (int)seen[1] + (int)seen[2] + (int)seen[3];
+    bool seen[8] = {false};
+    for (int m : scene_.tri_mat) seen[scene_.mats[m].type & 7] = true;
+    for (int m : scene_.sph_mat) seen[scene_.mats[m].type & 7] = true;
+    material_classes_ = 0;
+    for (bool b : seen) material_classes_ += b ? 1 : 0;
 }
 
 int Session::load_config(int config, uint64_t seed, int level) {
@@ -366,6 +367,23 @@ int Session::guide_params(float* out, int n, bool set) {
     return check_cuda(cudaStreamSynchronize(stream_), "guide params");
 }
 
+int Session::set_watertight(int on) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    if ((on != 0) == watertight_) return PT_OK;
+    watertight_ = on != 0;
+    scene_dirty_ = true;     // leaf entries re-uploaded in the test's format
+    reset_pending_ = true;   // another intersection test: a new image
+    return PT_OK;
+}
+
+int Session::set_test_limits(int stack_entries, int mma_polls) {
+    if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+    if (stack_entries < 0 || mma_polls < 0) return fail(PT_ERR_ARG, "limits must be >= 0 (0: none)");
+    test_stack_cap_ = stack_entries;
+    test_mma_polls_ = mma_polls;
+    return PT_OK;
+}
+
 int Session::guide_forward(const float* x, int n, float* raw) {
     if (n < 0) return fail(PT_ERR_ARG, "negative count");
     int r;
@@ -379,7 +397,8 @@ int Session::guide_forward(const float* x, int n, float* raw) {
     if ((r = check_cuda(cudaMemcpyAsync(dx, x, (size_t)n * kGuideIn * 4, cudaMemcpyHostToDevice, stream_), "copy")))
         return r;
     if ((r = check_cuda(cudaMemsetAsync(derr, 0, sizeof(int), stream_), "copy"))) return r;
-    const cudaError_t e = guide_infer_tc_ ? guide_forward_features_tc(guide_view(), dx, n, dy, derr, stream_)
+    const cudaError_t e = guide_infer_tc_ ? guide_forward_features_tc(guide_view(), dx, n, dy, derr, stream_,
+                                                                      test_mma_polls_)
                                           : guide_forward_features(guide_view(), dx, n, dy, stream_);
     if ((r = check_cuda(e, "guide forward"))) return r;
     if ((r = check_cuda(cudaMemcpyAsync(raw, dy, (size_t)n * kGuideOut * 4, cudaMemcpyDeviceToHost, stream_), "copy")))
@@ -565,14 +584,19 @@ int Session::set_material(int id, int type, const float* albedo, const float* em
     if (!have_scene_) return fail(PT_ERR_STATE, "no scene loaded");
     if (batch_mode()) return fail(PT_ERR_STATE, "not available for a batch (one query per scene session)");
     if (id < 0 || id >= (int)scene_.mats.size()) return fail(PT_ERR_ARG, "material id out of range");
-    if (type < kLambertian || type > kMicrofacet) return fail(PT_ERR_ARG, "unknown material type");
+    if (type < kLambertian || type > kMetal || type == kMaterialNone) return fail(PT_ERR_ARG, "unknown material type");
     Material& m = scene_.mats[id];
     if (m.type != type) {
         // Scene::setMaterialType defaults (include/scene.h:36-61)
         Material n{};
         n.type = type;
         if (type == kGlass) n.ior = 1.4f;
-        if (type == kMicrofacet) n.alpha = 0.1f;
+        if (type == kMicrofacet || type == kMetal) n.alpha = 0.1f;
+        if (type == kMetal) {  // copper's F0 until an albedo is given
+            n.albedo[0] = 0.955f;
+            n.albedo[1] = 0.638f;
+            n.albedo[2] = 0.538f;
+        }
         m = n;
     } else {
         // the type's own parameters only (MaterialParams setters, include/materials/params.h)
@@ -584,6 +608,10 @@ int Session::set_material(int id, int type, const float* albedo, const float* em
         } else if (type == kGlass) {
             m.ior = ior;
         } else if (type == kMicrofacet) {
+            m.alpha = alpha;
+        } else if (type == kMetal) {  // F0 in the albedo, and the roughness
+            for (int k = 0; k < 3; k++)
+                if (albedo) m.albedo[k] = albedo[k];
             m.alpha = alpha;
         }
     }
@@ -714,6 +742,12 @@ int Session::upload_scene() {
         bvh_.max_leaf = info.max_leaf;
         bvh_.build_ms = ms;
     }
+    if (watertight_) {  // triangle entries carry their vertices for the watertight test
+        const int entries = gpu_tree ? nt + scene_.num_sph() : (int)(bvh_.prims.size() / 12);
+        if ((r = check_cuda(prims_to_vertices(d_prims_.as<float4>(), entries, d_tri_p_.as<float4>(), stream_),
+                            "watertight leaf entries")))
+            return r;
+    }
     if (bvh_nodes_quantized()) {  // the quantized copy the traversal reads instead
         if ((r = check_cuda(d_qnodes_.alloc((size_t)bvh_.num_nodes * qnode_bytes(bvh_.width)), "quantized BVH")))
             return r;
@@ -739,8 +773,10 @@ int Session::upload_scene() {
 
 SceneDevice Session::scene_view() const {
     SceneDevice v{};
-    v.nodes = bvh_nodes_quantized() ? d_qnodes_.as<float4>() : d_nodes_.as<float4>();
-    v.node_q = bvh_nodes_quantized();
+    // the watertight kernels read float nodes
+    const bool qn = bvh_nodes_quantized() && !watertight_;
+    v.nodes = qn ? d_qnodes_.as<float4>() : d_nodes_.as<float4>();
+    v.node_q = qn;
     v.prims = d_prims_.as<float4>();
     v.tri_p = d_tri_p_.as<float4>();
     v.tri_n = d_tri_n_.as<float4>();
@@ -755,6 +791,7 @@ SceneDevice Session::scene_view() const {
     v.num_lights = (int)lights_.size();
     v.bvh_width = bvh_.width;
     v.root = bvh_.root;
+    v.watertight = watertight_ ? 1 : 0;
     if (scene_.env_w > 0) {
         v.env.rgba = d_env_rgba_.as<float>();
         v.env.marg_cdf = d_env_marg_.as<float>();
@@ -898,7 +935,8 @@ int Session::render_async(int spp) {
         p.batch_pixel_base = d_batch_pixel_base_.as<long long>();
         p.num_scenes = (int)batch_.size();
     }
-    p.stack_depth = stack_depth;
+    p.stack_depth = stack_entries();
+    p.mma_test_polls = test_mma_polls_;
     p.num_sms = num_sms_;
     p.count_work = work_counters_;
     p.renderer = renderer_;
@@ -1452,7 +1490,7 @@ int Session::trace_rays(const float* o, const float* d, const float* tmin, const
     if (in_flight_ && (r = wait(nullptr))) return r;
     if (scene_dirty_ && (r = upload_scene())) return r;
     if (mats_dirty_ && (r = upload_materials())) return r;
-    const int sd = bvh_.depth + 1;
+    const int sd = stack_entries();
     if (stack_bytes(sd, 128) > (size_t)kMaxStackBytesDefault)
         return fail(PT_ERR_SCENE, "BVH too deep for the traversal stack in shared memory");
     if (device_ptrs) {
@@ -1543,7 +1581,7 @@ int Session::occluded(const float* o, const float* d, const float* tmin, const f
     if (in_flight_ && (r = wait(nullptr))) return r;
     if (scene_dirty_ && (r = upload_scene())) return r;
     if (mats_dirty_ && (r = upload_materials())) return r;
-    const int sd = bvh_.depth + 1;
+    const int sd = stack_entries();
     const size_t N = (size_t)n;
     if ((r = check_cuda(d_scratch_.alloc(N * 4 * 9 + 256), "scratch"))) return r;
     float* dO = d_scratch_.as<float>();

@@ -285,6 +285,19 @@ public:
     int guide_params(float* out, int n, bool set);
     int guide_forward(const float* x, int n, float* raw);
     int guide_gradients(const float* x, const float* wi, const float* w, int n, float* grad);
+    int set_test_limits(int stack_entries, int mma_polls);
+    int set_watertight(int on);
+
+private:
+    bool watertight_ = false;  // triangles take the watertight test (leaf entries hold vertices)
+    // test hooks for the device-error paths (0: off): traversal stack entries per query, and
+    // non-blocking polls of the first wait of each tensor-core inference layer
+    int test_stack_cap_ = 0;
+    int test_mma_polls_ = 0;
+    int stack_entries() const {
+        const int sd = bvh_.depth + 1;
+        return test_stack_cap_ > 0 && test_stack_cap_ < sd ? test_stack_cap_ : sd;
+    }
 };
 
 }  // namespace pt

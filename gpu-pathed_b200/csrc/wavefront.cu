@@ -298,7 +298,7 @@ __global__ void k_extend(FrameParams p, int depth) {
         if (!__any_sync(0xffffffffu, alive)) break;
         const SceneDevice& sc = B ? scb : p.sc;
         traverse_round<W, false, CNT>(sc.nodes, sc.prims, quant, spec, r, tmin, FLT_MAX, st, stride, p.stack_depth, h,
-                                      cur, pend, sp, alive, hit_any, of, &work);
+                                      cur, pend, sp, alive, hit_any, of, &work, Q == 2);
         // a triangle at t = tMin is inside the continuation's range, a sphere is not (triangle.cu:34
         // accepts t >= tMin, sphere.cu:16,29 need t > tMin)
         if (slot >= 0 && !alive && retrace && !second && h.prim != kMissPrim &&
@@ -329,7 +329,7 @@ __global__ void k_extend(FrameParams p, int depth) {
     }
     __syncthreads();
     // one atomic per class and block for the whole persistent loop
-    if (p.shape.sort_materials && threadIdx.x < 5 && s_class[threadIdx.x] > 0)
+    if (p.shape.sort_materials && threadIdx.x < kMaterialClasses && s_class[threadIdx.x] > 0)
         atomicAdd(&p.counters->sort_count[depth][threadIdx.x], s_class[threadIdx.x]);
     if (CNT) flush_work(work, &p.stats->extend_nodes, &p.stats->extend_prims);
 }
@@ -337,10 +337,10 @@ __global__ void k_extend(FrameParams p, int depth) {
 __global__ void k_sort(FrameParams p, int depth) {
     const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
-    int off[5];
+    int off[kMaterialClasses];
     int acc = 0;
 #pragma unroll
-    for (int c = 0; c < 5; c++) {
+    for (int c = 0; c < kMaterialClasses; c++) {
         off[c] = acc;
         acc += p.counters->sort_count[depth][c];
     }
@@ -361,14 +361,14 @@ __global__ void k_sort(FrameParams p, int depth) {
         int b = 0;
         if (valid && lane == leader) b = atomicAdd(&s_cnt[key], __popc(peers));
         __syncthreads();
-        if (threadIdx.x < 5 && s_cnt[threadIdx.x] > 0)
+        if (threadIdx.x < kMaterialClasses && s_cnt[threadIdx.x] > 0)
             s_base[threadIdx.x] = atomicAdd(&p.counters->sort_fill[depth][threadIdx.x], s_cnt[threadIdx.x]);
         __syncthreads();
         b = __shfl_sync(0xffffffffu, b, leader);
         if (valid) {
             int ko = 0;
 #pragma unroll
-            for (int c = 0; c < 5; c++)
+            for (int c = 0; c < kMaterialClasses; c++)
                 if (c == key) ko = off[c] + s_base[c];
             p.sort_index[ko + b + __popc(peers & lanemask_lt())] = i;
         }
@@ -404,7 +404,7 @@ __device__ __forceinline__ void hit_info(const SceneDevice& sc, V o, V dir, floa
 // with alpha(wi), microfacet.h:124-134, while sampling uses alpha(wo), :148-158).
 __device__ __forceinline__ float bsdf_sampling_pdf(const Material& m, V wo, V wi) {
     if (m.type == kLambertian) return lambert_pdf(wi);
-    if (m.type == kMicrofacet) {
+    if (m.type == kMicrofacet || m.type == kMetal) {
         const V wh = normalized(wo + wi);
         return mf_D(m.alpha, wo, wh) * fabsf(wh.z) / (4.f * fabsf(dot(wo, wh)));
     }
@@ -577,10 +577,11 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                             }
                             case kMirror: bs = mirror_sample(wo); break;
                             case kGlass: bs = glass_sample(m, wo, pcg_uniform(st, inc)); break;
-                            default: {
+                            default: {  // Beckmann: kMicrofacet, kMetal
                                 const float x1 = pcg_uniform(st, inc);
                                 const float x2 = pcg_uniform(st, inc);
                                 bs = mf_sample(m.alpha, wo, x1, x2);
+                                if (m.type == kMetal) bs.f = mf_metal_f(m, wo, bs.wi);
                             }
                         }
                         wworld = to_world(fr, bs.wi);
@@ -727,7 +728,7 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
         if (!__any_sync(0xffffffffu, alive)) break;
         const SceneDevice& sc = B ? scb : p.sc;
         traverse_round<W, true, CNT>(sc.nodes, sc.prims, quant, spec, r, kShadowTMin, tmax, st, stride, p.stack_depth,
-                                     h, cur, pend, sp, alive, occ, of, &work);
+                                     h, cur, pend, sp, alive, occ, of, &work, Q == 2);
         if (slot >= 0 && !alive) {  // the query ended: occluded, or the stack ran empty
             const int i = slot;
             slot = -1;
@@ -884,7 +885,7 @@ __global__ void __launch_bounds__(kTcRows, 4) k_guide_infer_tc(FrameParams p, in
         tc_fence_before();
         __syncthreads();
         float raw[kGuideOut];
-        if (!tc_network(s, tmem, phase, raw)) {
+        if (!tc_network(s, tmem, phase, raw, p.mma_test_polls)) {
             if (t == 0) atomicOr(&p.stats->error, 2);
             break;
         }
@@ -1022,7 +1023,9 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                 k_ray_scatter<<<p.num_sms * 4, kRaySortBlock, 0, stream>>>(p, d);
                 mark(kStageSort);
             }
-            if constexpr (W >= 4) {
+            if (p.sc.watertight) {
+                k_extend<W, CNT, B, 2><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+            } else if constexpr (W >= 4) {
                 if (p.sc.node_q) k_extend<W, CNT, B, 1><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
                 else k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
             } else {
@@ -1047,7 +1050,10 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                 k_shade<false, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first, w.guided_first);
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {
-                if (W >= 4 && p.sc.node_q)
+                if (p.sc.watertight)
+                    k_shadow<W, CNT, B, 2><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d, wave_first,
+                                                                                           w.guided_first);
+                else if (W >= 4 && p.sc.node_q)
                     k_shadow<W, CNT, B, (W >= 4 ? 1 : 0)><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(
                         p, d, wave_first, w.guided_first);
                 else
@@ -1182,6 +1188,15 @@ cudaError_t set_smem_w(size_t bytes) {
     if ((e = cudaFuncSetAttribute(k_extend<W, true, true, kQ>, a, b))) return e;
     if ((e = cudaFuncSetAttribute(k_shadow<W, false, true, kQ>, a, b))) return e;
     if ((e = cudaFuncSetAttribute(k_shadow<W, true, true, kQ>, a, b))) return e;
+    for (int cnt = 0; cnt < 2; cnt++)  // the watertight variants (Q = 2)
+        for (int bt = 0; bt < 2; bt++) {
+            const void* ke = cnt ? (bt ? (const void*)k_extend<W, true, true, 2> : (const void*)k_extend<W, true, false, 2>)
+                                 : (bt ? (const void*)k_extend<W, false, true, 2> : (const void*)k_extend<W, false, false, 2>);
+            const void* ks = cnt ? (bt ? (const void*)k_shadow<W, true, true, 2> : (const void*)k_shadow<W, true, false, 2>)
+                                 : (bt ? (const void*)k_shadow<W, false, true, 2> : (const void*)k_shadow<W, false, false, 2>);
+            if ((e = cudaFuncSetAttribute(ke, a, b))) return e;
+            if ((e = cudaFuncSetAttribute(ks, a, b))) return e;
+        }
     if ((e = cudaFuncSetAttribute(k_normals<W>, a, b))) return e;
     return cudaSuccess;
 }

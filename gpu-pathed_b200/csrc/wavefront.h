@@ -177,6 +177,7 @@ struct FrameParams {
     float gfrac;             // probability of sampling the guide at a non-delta vertex
     int consistent_mis;      // NEE weights use the BSDF's true sampling density (microfacet)
     int guide_tc;            // guide inference on tcgen05 / tensor memory (single-scene frames)
+    int mma_test_polls;      // test hook: > 0 limits the first wait of each tcgen05 layer (tc_network)
     const uint32_t* gwpack;  // packed inference weights
     GuideFrame gframe;       // scene bounds for the position encoding
     float* gmix;             // per queue slot: mixture (40 floats)

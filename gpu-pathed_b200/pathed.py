@@ -22,6 +22,7 @@ PT_ERR_SCENE = -4
 PT_ERR_DEVICE = -5
 
 LAMBERTIAN, MIRROR, GLASS, MICROFACET = 0, 1, 2, 3
+METAL = 5  # Beckmann microfacet with a Schlick Fresnel of RGB F0 = albedo (no reference counterpart)
 
 # every symbol declared in include/pathed.h
 EXPORTED = [
@@ -46,6 +47,8 @@ EXPORTED = [
     "pt_readback_async",
     "pt_readback_wait",
     "pt_measure_l2_read",
+    "pt_set_test_limits",
+    "pt_set_watertight",
 ]
 
 MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
@@ -216,9 +219,10 @@ def _load():
     lib.pt_write_exr.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
     lib.pt_read_exr.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
     for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async",
-                 "pt_set_bvh_builder", "pt_set_renderer", "pt_set_bvh_nodes"):
+                 "pt_set_bvh_builder", "pt_set_renderer", "pt_set_bvh_nodes", "pt_set_watertight"):
         getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
     lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.pt_set_test_limits.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_measure_l2_read.argtypes = [C.c_int, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_double),
                                        C.POINTER(C.c_double)]
     lib.pt_set_profiling.argtypes = [C.c_void_p, C.c_int, C.c_int]
@@ -564,6 +568,16 @@ class Session:
     def set_bvh_quantized(self, on: bool):
         """Traverse quantized wide nodes (widths 4 and 8) instead of float nodes."""
         self._check(lib.pt_set_bvh_nodes(self._h, int(bool(on))))
+
+    def set_watertight(self, on: bool):
+        """Watertight ray/triangle test (Woop, Benthin and Wald 2013) instead of the
+        reference's Triangle::hit arithmetic (the default)."""
+        self._check(lib.pt_set_watertight(self._h, int(bool(on))))
+
+    def set_test_limits(self, stack_entries: int = 0, mma_polls: int = 0):
+        """Test hook for the device-error paths: cap the traversal stack and the tensor-core
+        inference waits (0: off); calls that hit a limit raise PathedError(PT_ERR_DEVICE)."""
+        self._check(lib.pt_set_test_limits(self._h, int(stack_entries), int(mma_polls)))
 
     def set_renderer(self, kind: int):
         """RENDERER_CUDA (the path tracer) or RENDERER_NORMALS (the normals G-buffer: one

@@ -458,6 +458,23 @@ int pt_set_bvh_nodes(pt_session* s, int quantized);
  * (PT_ERR_STATE for a batch). */
 int pt_set_renderer(pt_session* s, int kind);
 
+/* on = 1: triangles take a watertight ray/triangle test (Woop, Benthin and Wald 2013) in every
+ * query and frame, in place of Triangle::hit's arithmetic (src/primitives/triangle.cu:7-48),
+ * which a ray through a shared edge or vertex can slip between. The leaf entries then hold the
+ * triangles' own vertices (re-uploaded on the next device call) and accumulation restarts.
+ * on = 0 (default): the reference's test, bit for bit. Spheres keep Sphere::hit's test. */
+int pt_set_watertight(pt_session* s, int on);
+
+/* Test hook for the device-error paths (no counterpart in the reference, whose gpuAssert exits
+ * the process, include/macro_helper.h:10-19). stack_entries > 0 caps the traversal stack of
+ * every query of the frames, pt_trace_rays and pt_occluded at that many entries (below the BVH
+ * depth a query that needs more gives up); mma_polls > 0 limits the first wait of each
+ * tensor-core inference layer (pt_set_guide_inference(1)) to that many non-blocking polls, so
+ * it gives up while the layer's MMA runs (a bounded drain still waits for that MMA before the
+ * kernel releases tensor memory). Either way the kernel sets its error flag and returns; the
+ * call reports PT_ERR_DEVICE and the session stays usable. 0 and 0 (default) turn both off. */
+int pt_set_test_limits(pt_session* s, int stack_entries, int mma_polls);
+
 /* Measurement support (no counterpart in the reference): the read bandwidth, in GB/s, of a
  * buffer of `bytes` (a multiple of 16, at least 1 MiB) that stays in L2, on CUDA device
  * `device` (made the library's current device).

@@ -140,7 +140,7 @@ struct Rng {
 };
 
 // ---- scene -------------------------------------------------------------------------------
-enum { LAMBERTIAN = 0, MIRROR = 1, GLASS = 2, MICROFACET = 3 };
+enum { LAMBERTIAN = 0, MIRROR = 1, GLASS = 2, MICROFACET = 3, METAL = 5 };  // METAL: the CUDA path's metallic Beckmann
 enum { TRIANGLE = 0, SPHERE = 1 };
 
 struct Triangle { Vec3 p0, p1, p2, n0, n1, n2; int mat; };
@@ -312,6 +312,7 @@ struct Scene {
     std::vector<LightIndex> lights;
     Env env;
     Accel accel;  // empty: World::hit's linear scan
+    bool watertight = false;  // triangles take the watertight test (the CUDA path's opt-in)
 };
 
 struct HitRecord {
@@ -347,6 +348,57 @@ inline bool triangleHit(const Triangle& tr, const Ray& ray, float tMin, float tM
     rec.wo = normalized(frame.toLocal(-ray.d));
     rec.materialID = tr.mat;
     return true;
+}
+
+// Watertight ray/triangle test (Woop, Benthin and Wald, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1), 2013): the CUDA path's opt-in alternative to Triangle::hit, in the
+// same steps and FP32 roundings (this file is built without contraction):
+// kz = the largest |d| component (first of x, y, z on ties), kx, ky the next two cyclically,
+// swapped when d[kz] < 0; sz = 1 / d[kz], sx = d[kx] sz, sy = d[ky] sz; vertices relative to
+// the origin and sheared; edge functions U, V, W, each recomputed in FP64 when exactly zero;
+// mixed signs or det = U + V + W = 0 miss; t = T / det in [tMin, tMax]; b1 = V / det,
+// b2 = W / det. The hit record is Triangle::hit's from those barycentrics.
+inline bool triangleHitWT(const Triangle& tr, const Ray& ray, float tMin, float tMax, HitRecord& rec) {
+    const Vec3& d = ray.d;
+    const float adx = fabsf(d.x()), ady = fabsf(d.y()), adz = fabsf(d.z());
+    const int kz = adx >= ady ? (adx >= adz ? 0 : 2) : (ady >= adz ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    if (d.e[kz] < 0.f) std::swap(kx, ky);
+    const float sz = 1.f / d.e[kz];
+    const float sx = d.e[kx] * sz, sy = d.e[ky] * sz;
+    const Vec3 A = tr.p0 - ray.o, B = tr.p1 - ray.o, C = tr.p2 - ray.o;
+    const float ax = A.e[kx] - sx * A.e[kz], ay = A.e[ky] - sy * A.e[kz];
+    const float bx = B.e[kx] - sx * B.e[kz], by = B.e[ky] - sy * B.e[kz];
+    const float cx = C.e[kx] - sx * C.e[kz], cy = C.e[ky] - sy * C.e[kz];
+    float U = cx * by - cy * bx;
+    float V = ax * cy - ay * cx;
+    float W = bx * ay - by * ax;
+    if (U == 0.f || V == 0.f || W == 0.f) {
+        U = (float)((double)cx * (double)by - (double)cy * (double)bx);
+        V = (float)((double)ax * (double)cy - (double)ay * (double)cx);
+        W = (float)((double)bx * (double)ay - (double)by * (double)ax);
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+    const float det = U + V + W;
+    if (det == 0.f) return false;
+    const float T = U * (sz * A.e[kz]) + V * (sz * B.e[kz]) + W * (sz * C.e[kz]);
+    const float inv = 1.f / det;
+    const float t = T * inv;
+    if (!(t >= tMin && t <= tMax)) return false;
+    const float b1 = V * inv, b2 = W * inv;
+    const Vec3 hitPoint = tr.p0 * (1.f - b1 - b2) + (tr.p1 * b1) + (tr.p2 * b2);
+    const Vec3 shadingNormal = (1.f - b1 - b2) * tr.n0 + b1 * tr.n1 + b2 * tr.n2;
+    const Frame frame(shadingNormal);
+    rec.t = t;
+    rec.point = hitPoint;
+    rec.normal = shadingNormal;
+    rec.wo = normalized(frame.toLocal(-ray.d));
+    rec.materialID = tr.mat;
+    return true;
+}
+inline bool triangleTest(const Scene& sc, const Triangle& tr, const Ray& ray, float tMin, float tMax, HitRecord& rec) {
+    return sc.watertight ? triangleHitWT(tr, ray, tMin, tMax, rec) : triangleHit(tr, ray, tMin, tMax, rec);
 }
 
 // Sphere::hit (src/primitives/sphere.cu:7-43)
@@ -506,7 +558,7 @@ bool accelHit(const Scene& sc, const Ray& ray, float tMin, float tMax, HitRecord
             for (int k = nd.first; k < nd.first + nd.count; k++) {
                 const int code = A.order[k];
                 HitRecord tmp;
-                const bool h = code >= 0 ? triangleHit(sc.tris[code], ray, tMin, tMax, tmp)
+                const bool h = code >= 0 ? triangleTest(sc, sc.tris[code], ray, tMin, tMax, tmp)
                                          : sphereHit(sc.sphs[~code], ray, tMin, tMax, tmp);
                 if (!h) continue;
                 if (any) return true;
@@ -547,7 +599,7 @@ inline bool worldHit(const Scene& sc, const Ray& ray, float tMin, float tMax, Hi
     const int nt = (int)sc.tris.size();
     for (int i = 0; i < nt; i++) {
         HitRecord tmp;
-        if (triangleHit(sc.tris[i], ray, tMin, (float)tNear, tmp)) {
+        if (triangleTest(sc, sc.tris[i], ray, tMin, (float)tNear, tmp)) {
             isHit = true;
             tNear = tmp.t;
             rec = tmp;
@@ -702,6 +754,21 @@ inline Vec3 microfacetF(const Material& m, const Vec3& wo, const Vec3& wi) {
     const float Gv = d.G(wi, wo, wh);
     return Vec3(1.f) * Dv * Gv * F / (4 * cI * cO);
 }
+// METAL (the CUDA path's metallic Beckmann, no counterpart in the reference): the same D and
+// G with a Schlick Fresnel per channel, F = F0 + (1 - F0)(1 - c)^5 at c = wi . wh, F0 = albedo.
+inline Vec3 metalF(const Material& m, const Vec3& wo, const Vec3& wi) {
+    const Beckmann d{m.alpha};
+    if (wo.z() < 0.f || wi.z() < 0.f) return Vec3(0.f);
+    const float cO = fabsf(wo.z()), cI = fabsf(wi.z());
+    const Vec3 wh = normalized(wo + wi);
+    if (cO == 0.f || cI == 0.f) return Vec3(0.f);
+    if (wh.isZero()) return Vec3(0.f);
+    const float cInc = fminf(1.f, fmaxf(dot(wi, wh), 0.f));
+    const float q = 1.f - cInc, q2 = q * q, q5 = q2 * q2 * q;
+    const float s = d.D(wi, wh) * d.G(wi, wo, wh) / (4.f * cI * cO);
+    return Vec3((m.albedo.x() + (1.f - m.albedo.x()) * q5) * s, (m.albedo.y() + (1.f - m.albedo.y()) * q5) * s,
+                (m.albedo.z() + (1.f - m.albedo.z()) * q5) * s);
+}
 inline float microfacetPdf(const Material& m, const Vec3& wo, const Vec3& wi) {
     const Beckmann d{m.alpha};
     if (wo.z() < 0.f || wi.z() < 0.f) return 0.f;
@@ -712,7 +779,8 @@ inline BSDFSample microfacetSample(const Material& m, const Vec3& wo, float xi1,
     const Beckmann d{m.alpha};
     const Vec3 wh = d.sampleWh(wo, xi1, xi2);
     const Vec3 wi = wo.reflect(wh);
-    return BSDFSample{wi, d.pdf(wo, wh) / (4.f * absDot(wi, wh)), microfacetF(m, wo, wi), false};
+    const Vec3 f = m.type == METAL ? metalF(m, wo, wi) : microfacetF(m, wo, wi);
+    return BSDFSample{wi, d.pdf(wo, wh) / (4.f * absDot(wi, wh)), f, false};
 }
 
 // bsdf.h:19-115
@@ -720,13 +788,15 @@ inline Vec3 bsdfF(const Material& m, const Vec3& wo, const Vec3& wi) {
     switch (m.type) {
         case LAMBERTIAN: return lambertF(m, wo, wi);
         case MICROFACET: return microfacetF(m, wo, wi);
+        case METAL: return metalF(m, wo, wi);
         default: return Vec3(0.f);
     }
 }
 inline float bsdfPdf(const Material& m, const Vec3& wo, const Vec3& wi) {
     switch (m.type) {
         case LAMBERTIAN: return uniformHemispherePDF(wi);
-        case MICROFACET: return microfacetPdf(m, wo, wi);
+        case MICROFACET:
+        case METAL: return microfacetPdf(m, wo, wi);
         default: return 0.f;
     }
 }
@@ -877,7 +947,7 @@ struct Counters { uint64_t queries = 0, shadow = 0, duplicate = 0; };
 // The BSDF sampler's own density of a direction: Microfacet::sample draws with alpha(wo)
 // (microfacet.h:148-158) while Microfacet::pdf evaluates D with alpha(wi) (:124-134).
 inline float bsdfSamplingPdf(const Material& m, const Vec3& wo, const Vec3& wi) {
-    if (m.type != MICROFACET) return bsdfPdf(m, wo, wi);
+    if (m.type != MICROFACET && m.type != METAL) return bsdfPdf(m, wo, wi);
     if (wo.z() < 0.f || wi.z() < 0.f) return 0.f;
     const Beckmann d{m.alpha};
     const Vec3 wh = normalized(wo + wi);
@@ -1064,6 +1134,8 @@ void oracle_scene_destroy(Scene* s) { delete s; }
 // Build the parity accelerator: later queries on the scene give the linear scan's results
 // through a BVH (buildAccel).
 void oracle_scene_accel(Scene* s) { buildAccel(*s); }
+// Triangles take the watertight test (1) or Triangle::hit's (0, the default).
+void oracle_scene_watertight(Scene* s, int on) { s->watertight = on != 0; }
 int oracle_num_lights(const Scene* s) { return (int)s->lights.size(); }
 
 // Closest hit of n rays by the reference's linear scan. prim_type -1 on a miss.

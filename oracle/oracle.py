@@ -71,10 +71,11 @@ class _SceneLib:
             + [C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_void_p])
         getattr(self.lib, p + "scene_destroy").argtypes = [C.c_void_p]
 
-    def scene(self, sc: dict, accel: bool = False):
+    def scene(self, sc: dict, accel: bool = False, watertight: bool = False):
         """Create a scene from an export dict (pathed.Session.export_scene layout). With
         `accel` (oracle only), queries run through the parity accelerator, which gives the
-        linear scan's results on meshes the scan is too slow for."""
+        linear scan's results on meshes the scan is too slow for. With `watertight` (oracle
+        only), triangles take the watertight test of the CUDA path's opt-in mode."""
         keep = [
             _f(sc["tri_vertices"]), _f(sc["tri_normals"]), _i(sc["tri_materials"]), _f(sc["spheres"]),
             _i(sc["sphere_materials"]), _i(sc["material_types"]), _f(sc["material_albedo"]),
@@ -90,6 +91,8 @@ class _SceneLib:
             keep[4].ctypes.data if keep[4].size else None,
             keep[5].size, keep[5].ctypes.data, keep[6].ctypes.data, keep[7].ctypes.data, keep[8].ctypes.data,
             keep[9].ctypes.data, ew, eh, None if env is None else env.ctypes.data)
+        if watertight:
+            getattr(self.lib, self.prefix + "scene_watertight")(h, 1)
         if accel:
             getattr(self.lib, self.prefix + "scene_accel")(h)
         return _SceneHandle(self, h, keep + [env])
@@ -113,6 +116,7 @@ class Oracle(_SceneLib):
         super().__init__(path)
         L = self.lib
         L.oracle_scene_accel.argtypes = [C.c_void_p]
+        L.oracle_scene_watertight.argtypes = [C.c_void_p, C.c_int]
         L.oracle_trace.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 + [C.c_int]
         L.oracle_render.argtypes = ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                      C.c_int, C.c_uint64, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -322,8 +326,11 @@ class RefBench:
         self.h = None
 
     def load(self, sc: dict, width: int, height: int):
+        # the reference has no metallic Beckmann (type 5): it renders those materials as its own
+        # Microfacet (type 3, dielectric Fresnel of eta 1.5), the closest material it has
+        types = np.where(_i(sc["material_types"]) == 5, 3, _i(sc["material_types"])).astype(np.int32)
         keep = [_f(sc["tri_vertices"]), _f(sc["tri_normals"]), _i(sc["tri_materials"]), _f(sc["spheres"]),
-                _i(sc["sphere_materials"]), _i(sc["material_types"]), _f(sc["material_albedo"]),
+                _i(sc["sphere_materials"]), types, _f(sc["material_albedo"]),
                 _f(sc["material_emit"]), _f(sc["material_ior"]), _f(sc["material_alpha"])]
         env = sc.get("env_rgba")
         env = None if env is None or env.size == 0 else _f(env)

@@ -150,3 +150,44 @@ def test_guided_batch_one_network_per_guided_scene():
     m1, e1 = np.mean(means), np.std(means, ddof=1) / np.sqrt(len(means))
     print(f"slit room in a guided batch: {m1:.6f} +- {e1:.6f}, alone plain {m0:.6f} +- {e0:.6f}")
     assert abs(m0 - m1) <= 4.5 * np.hypot(e0, e1)
+
+
+@pytest.mark.gpu
+def test_autotuner_on_a_batch(tmp_path):
+    """the autotuner runs on batched frames too (BVH width and ray sorting fixed, wave size
+    tuned), changes scheduling only, and caches its choice under the batch's own key"""
+    cache = str(tmp_path / "tune.jsonl")
+    s = pathed.Session(16, 16)
+    s.load_batch(SMALL)
+    s.set_seed(3)
+    s.render(0)
+    base = [s.batch_readback(k).copy() for k in range(len(SMALL))]
+    r = s.autotune(1, cache)
+    assert r["trials"] > 0 and r["from_cache"] == 0 and r["bvh_width"] == s.counts().bvh_width
+    assert r["wave_paths"] > 0 and r["best_ms"] <= r["default_ms"] * 1.05
+    s.render(0)  # tuning restarts accumulation: this is the first frame again
+    for k in range(len(SMALL)):
+        assert np.allclose(s.batch_readback(k), base[k], rtol=1e-5, atol=1e-6)
+    t = pathed.Session(16, 16)
+    t.load_batch(SMALL)
+    r2 = t.autotune(1, cache)
+    assert r2["from_cache"] == 1 and r2["wave_paths"] == r["wave_paths"] and r2["block"] == r["block"]
+    u = pathed.Session(16, 16)
+    u.load_batch(SMALL[:3])  # another draw: its own key, so it is measured
+    assert u.autotune(1, cache)["from_cache"] == 0
+    for x in (s, t, u):
+        x.close()
+
+
+@pytest.mark.gpu
+def test_wave_size_does_not_change_images():
+    """the autotuner's wave size splits a frame into more waves: same paths, same images"""
+    out = []
+    for wave in (1 << 25, 5000):
+        s = pathed.Session(64, 48)
+        s.load_config(1)
+        s.set_launch(wave_paths=wave)
+        s.render(8)
+        out.append(s.readback().copy())
+        s.close()
+    assert np.allclose(out[0], out[1], rtol=1e-5, atol=1e-6)

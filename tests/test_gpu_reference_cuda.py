@@ -27,8 +27,15 @@ FULL_MESH = [(2, None), (3, None)]
 
 
 def _ours(cfg, level, w=64, h=64):
+    """our session on the configuration, its metallic Beckmann materials (configuration 1;
+    the reference has none) turned into the reference's Microfacet with the same roughness,
+    the material RefBench gives the reference for them"""
     s = pathed.Session(w, h)
     s.load_config(cfg, level=level)
+    sc = s.export_scene()
+    for i in np.nonzero(sc["material_types"] == pathed.METAL)[0]:
+        s.set_material(int(i), pathed.MICROFACET)
+        s.set_material(int(i), pathed.MICROFACET, alpha=float(sc["material_alpha"][i]))
     return s, s.export_scene()
 
 

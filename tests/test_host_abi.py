@@ -48,7 +48,15 @@ def test_config_contents(cfg, ntri, nsph, nlights):
         assert np.all(n[:, 1] < 0)
     if cfg == 1:
         types = sc["material_types"][sc["sphere_materials"][:64]]
-        assert (types == pathed.MICROFACET).sum() == 26 and (types == pathed.MIRROR).sum() == 13
+        # 40% Beckmann: F0 0.04 (the reference's dielectric Fresnel) or a metallic RGB F0
+        beck = (types == pathed.MICROFACET) | (types == pathed.METAL)
+        assert beck.sum() == 26 and (types == pathed.MIRROR).sum() == 13
+        metal = sc["material_types"] == pathed.METAL
+        assert 6 <= metal.sum() <= 20
+        f0 = sc["material_albedo"][metal]
+        assert np.all((f0 > 0.3) & (f0 <= 1.0))
+        alpha = sc["material_alpha"][sc["sphere_materials"][:64]][beck]
+        assert alpha.min() >= 0.05 and alpha.max() <= 0.5
         assert (types == pathed.GLASS).sum() == 13 and (types == pathed.LAMBERTIAN).sum() == 12
         r = sc["spheres"][:64, 3]
         assert r.min() >= 0.2 and r.max() <= 1.0
