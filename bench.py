@@ -432,7 +432,7 @@ def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
            "ms_per_step": dev_ms / steps, "steps": steps, "warmup": warmup, "triangles": counts.num_triangles,
            "spheres": counts.num_spheres,
            "autotuned": {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays", "speculate",
-                                                "blocks_per_sm", "block", "wave_paths")},
+                                                "blocks_per_sm", "block", "wave_paths", "split_shade")},
            "roofline": _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs,
                                  None)}
     if with_reference:
@@ -607,7 +607,7 @@ def run_ours(args):
         if tuned is not None:
             line["config"]["autotuned"] = {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays",
                                                                "speculate", "blocks_per_sm", "block", "wave_paths",
-                                                               "best_ms", "default_ms")}
+                                                               "split_shade", "best_ms", "default_ms")}
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:

@@ -24,6 +24,11 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["wavefront.cu", "guide.cu", "bvh_gpu.cu", "probe.cu"]
+# The integrator's kernels are compiled without FMA contraction: every FP32 operation rounds
+# on its own, as in the oracle (-ffp-contract=off), so the kernels specialised per material
+# class, per batch and per node format compute bit-identical paths (contraction would fuse
+# differently in each instantiation), at about 2% of the shade stage's time.
+CU_FLAGS = {"wavefront.cu": ["-fmad=false"]}
 CPP_SOURCES = ["host_scene.cpp", "bvh_build.cpp", "host_util.cpp", "assets.cpp", "session.cpp", "session_batch.cpp",
                "capi.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] if os.path.isdir(CSRC) else []
@@ -62,7 +67,7 @@ def build(verbose: bool = False, clean: bool = False, ptxas_info: bool = False) 
         objs.append(o)
         if _newer([s] + headers, o):
             cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                   "--expt-relaxed-constexpr", "-c", s, "-o", o]
+                   "--expt-relaxed-constexpr", *CU_FLAGS.get(src, []), "-c", s, "-o", o]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
             out = _run(cmd, verbose)

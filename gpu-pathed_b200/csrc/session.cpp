@@ -117,7 +117,12 @@ void Session::update_material_classes() {
     for (int m : scene_.tri_mat) seen[scene_.mats[m].type & 7] = true;
     for (int m : scene_.sph_mat) seen[scene_.mats[m].type & 7] = true;
     material_classes_ = 0;
-    for (bool b : seen) material_classes_ += b ? 1 : 0;
+    class_mask_ = 1;  // misses
+    for (int t = 0; t < 8; t++)
+        if (seen[t]) {
+            material_classes_++;
+            if (t + 1 < 8) class_mask_ |= 1 << (t + 1);
+        }
 }
 
 int Session::load_config(int config, uint64_t seed, int level) {
@@ -655,7 +660,8 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->wave_paths < 0 || c->blocks_per_sm < 0 || c->blocks_per_sm > 64)
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
-        c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 4)
+        c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 4 || c->split_shade < 0 ||
+        c->split_shade > 2)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
@@ -668,6 +674,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->sort_rays) shape_.sort_rays = c->sort_rays == 1 ? 1 : 0;
     if (c->refill_idle) shape_.refill_idle = c->refill_idle;
     if (c->speculate) shape_.speculate = speculate_bits(c->speculate);
+    if (c->split_shade) shape_.split_shade = c->split_shade == 1 ? 1 : 0;
     return PT_OK;
 }
 
@@ -682,6 +689,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->sort_rays = shape_.sort_rays ? 1 : 2;
     c->refill_idle = shape_.refill_idle;
     c->speculate = speculate_code(shape_.speculate);
+    c->split_shade = shape_.split_shade ? 1 : 2;
 }
 
 int Session::upload_materials() {
@@ -942,6 +950,7 @@ int Session::render_async(int spp) {
     p.renderer = renderer_;
     p.shape = shape_;
     p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0);
+    p.class_mask = shape_.split_shade ? class_mask_ : 0;
     p.gframe = gframe_;  // scene bounds: guide encoding and ray-sort cells
     last_wave_paths_ = p.wave_pixels * spp;
     p.consistent_mis = consistent_mis_ || guiding_;
@@ -1215,7 +1224,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     // paths of one frame: waves smaller than this split the frame
     const long long frame_paths = batch ? batch_paths_ : (long long)w_ * h_ * spp;
     struct Cand {
-        int width, sort, bps, block, rays, spec, wave;
+        int width, sort, bps, block, rays, spec, wave, split;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
@@ -1226,6 +1235,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         shape_.sort_rays = c.rays;
         shape_.speculate = c.spec;
         wave_paths_ = c.wave;
+        shape_.split_shade = c.split;
         return PT_OK;
     };
     auto report = [&](const Cand& c) {
@@ -1236,6 +1246,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.sort_rays = c.rays ? 1 : 2;
         res.speculate = speculate_code(c.spec);
         res.wave_paths = c.wave;
+        res.split_shade = c.split ? 1 : 2;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1247,7 +1258,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 if (line.find(want) == std::string::npos) continue;
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
                        json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0),
-                       json_int(line, "wave_paths", wave_paths_)};
+                       json_int(line, "wave_paths", wave_paths_), json_int(line, "split_shade", 1)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1281,7 +1292,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
-              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_};
+              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.split_shade};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1312,6 +1323,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     if (material_classes_ >= 2) {
         Cand c = best;
         c.sort = best.sort ? 0 : 1;
+        if ((r = consider(c))) return r;
+    }
+    if (best.sort && !guiding_) {  // the sorted shade stage as one kernel per class, or one for all
+        Cand c = best;
+        c.split = best.split ? 0 : 1;
         if ((r = consider(c))) return r;
     }
     if (!batch && max_depth_ > 1) {
@@ -1360,10 +1376,10 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         if (f) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
-                         "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"ms\": %.4f, "
-                         "\"default_ms\": %.4f}\n",
+                         "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"split_shade\": %d, "
+                         "\"ms\": %.4f, \"default_ms\": %.4f}\n",
                          key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, best.wave,
-                         best_ms, res.default_ms);
+                         best.split, best_ms, res.default_ms);
             std::fclose(f);
         }
     }

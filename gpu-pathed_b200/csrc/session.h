@@ -205,6 +205,7 @@ private:
     // material sorting: 1 on, 0 off, -1 automatic (on when >= 3 material classes are present)
     int sort_mode_ = -1;
     int material_classes_ = 1;
+    int class_mask_ = 1;  // material classes present (bit 0 miss, bit type + 1)
     void update_material_classes();
 
     // ---- learned path guiding ----

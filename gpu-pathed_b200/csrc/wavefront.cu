@@ -411,6 +411,33 @@ __device__ __forceinline__ float bsdf_sampling_pdf(const Material& m, V wo, V wi
     return 0.f;
 }
 
+// The material functions with the type fixed at compile time (T >= 0) or read from the
+// material (T < 0): a shade kernel specialised to one material class carries only its BSDF.
+template <int T>
+__device__ __forceinline__ V bsdf_f_t(const Material& m, V wo, V wi) {
+    if constexpr (T == kLambertian) return lambert_f(m, wo, wi);
+    else if constexpr (T == kMicrofacet) return mf_f(m.alpha, wo, wi);
+    else if constexpr (T == kMetal) return mf_metal_f(m, wo, wi);
+    else if constexpr (T == kMirror || T == kGlass) return mkv(0.f);
+    else return bsdf_f(m, wo, wi);
+}
+template <int T>
+__device__ __forceinline__ float bsdf_pdf_t(const Material& m, V wo, V wi) {
+    if constexpr (T == kLambertian) return lambert_pdf(wi);
+    else if constexpr (T == kMicrofacet || T == kMetal) return mf_pdf(m.alpha, wo, wi);
+    else if constexpr (T == kMirror || T == kGlass) return 0.f;
+    else return bsdf_pdf(m, wo, wi);
+}
+template <int T>
+__device__ __forceinline__ float bsdf_sampling_pdf_t(const Material& m, V wo, V wi) {
+    if constexpr (T == kLambertian) return lambert_pdf(wi);
+    else if constexpr (T == kMicrofacet || T == kMetal) {
+        const V wh = normalized(wo + wi);
+        return mf_D(m.alpha, wo, wh) * fabsf(wh.z) / (4.f * fabsf(dot(wo, wh)));
+    } else if constexpr (T == kMirror || T == kGlass) return 0.f;
+    else return bsdf_sampling_pdf(m, wo, wi);
+}
+
 __device__ __forceinline__ float lum(V c) { return (c.x + c.y + c.z) * (1.f / 3.f); }
 
 // Training index of a path: the path records training data when the index is a multiple of
@@ -465,11 +492,26 @@ __device__ __noinline__ V direct_hit_emission(const SceneDevice& sc, V o, V dir,
 // which measured 37% faster on the latency-bound guided shade (slit room, 1024^2).
 constexpr int kShadeGuidedBlock = 128;
 constexpr int kShadeGuidedBlocksPerSm = 8;
+// Register budget of the per-class shade kernels (k_shade_class), measured on a B200 against
+// 64, 80, 96 and 168: 64 for the Lambert, mirror, glass and miss classes (the slit room's
+// Lambert walls shaded 24% faster than in the kernel of all materials), 96 for the two
+// Beckmann classes (their sampling spills at 64; the icosphere shaded 12% faster).
+__host__ __device__ constexpr int shade_class_regs(int cls) { return cls == kMicrofacet + 1 || cls == kMetal + 1 ? 96 : 64; }
 
-template <bool GUIDE, bool B>
-__global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShadeGuidedBlocksPerSm : 1)
-    k_shade(FrameParams p, int depth, long long wave_first, long long gfirst) {
-    const int count = p.counters->ray_count[depth];
+// CLS: -1, every slot of the queue (in material-sorted order when sorting is on); >= 0, only
+// the slots the sort put in material class CLS (0 miss, type + 1 otherwise), with that
+// class's BSDF fixed at compile time, so each class kernel holds only its own registers.
+template <bool GUIDE, bool B, int CLS>
+__device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long long wave_first, long long gfirst) {
+    constexpr int kType = CLS > 0 ? CLS - 1 : -1;  // the material type of a class kernel
+    int count = p.counters->ray_count[depth];
+    int cls_first = 0;
+    if constexpr (CLS >= 0) {  // the class's range of the sorted order
+        for (int c = 0; c < CLS; c++) cls_first += p.counters->sort_count[depth][c];
+        count = p.counters->sort_count[depth][CLS];
+        if (count == 0) return;  // a class absent at this depth: no fetch, no atomics
+    }
+    int* const work = CLS >= 0 ? &p.counters->work_class[depth][CLS < 0 ? 0 : CLS] : &p.counters->work_shade[depth];
     const PathQueue q = p.q[depth & 1];
     const PathQueue qn = p.q[(depth + 1) & 1];
     const bool last_frame = depth >= p.max_depth - 1;
@@ -482,7 +524,7 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
         __syncthreads();
     }
     for (;;) {
-        const int base = warp_fetch(&p.counters->work_shade[depth]);
+        const int base = warp_fetch(work);
         if (base >= count) break;
         const int i = base + (threadIdx.x & 31);
         bool cont = false, shadow = false, record = false;
@@ -490,7 +532,7 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
         uint2 crng;
         GuideRecord rec;
         if (i < count) {
-            const int slot = p.shape.sort_materials ? p.sort_index[i] : i;
+            const int slot = CLS >= 0 ? p.sort_index[cls_first + i] : (p.shape.sort_materials ? p.sort_index[i] : i);
             const float4 o4 = q.o[slot];
             const float4 d4 = q.d[slot];
             const float4 b4 = q.beta[slot];
@@ -522,7 +564,9 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                     if (GUIDE) guide_account(p, ti, depth, lum(beta * Le), lum(Ladd), lum(Ladd));
                 }
             }
-            if (prim == kMissPrim) {
+            // a class kernel knows whether its slots missed
+            const bool miss = CLS == 0 ? true : (CLS > 0 ? false : prim == kMissPrim);
+            if (miss) {
                 // escaped: environment radiance (path_tracer.cu:68-79, :162, :206, :228); a
                 // continuation that misses after a closer BSDF-direct hit adds nothing (:178-180)
                 const V Le = split ? mkv(0.f) : env_emit(sc.env, dir);
@@ -541,7 +585,9 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                 const Frame fr = make_frame(n);
                 const V wo = normalized(to_local(fr, -dir));
                 const Material m = sc.mats[mat];
-                if (!split && m.emitting && wo.z >= 0.f) {  // front-face emission (lambertian.cu:5-11)
+                const int mtype = kType >= 0 ? kType : m.type;
+                // front-face emission (lambertian.cu:5-11); only Lambertian materials emit
+                if ((kType < 0 || kType == kLambertian) && !split && m.emitting && wo.z >= 0.f) {
                     const V Le = mkv(m.emit[0], m.emit[1], m.emit[2]);
                     const float w = nomis ? 1.f : balance(d4.w, pdf_scene_light(sc, o, point, n, prim));
                     Ladd = beta * Le * w;
@@ -553,7 +599,7 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                         B ? (uint32_t)((gp - p.batch[sid].path_base) / p.batch[sid].spp) : (uint32_t)(gp / p.spp);
                     const uint64_t inc = pcg_inc(pixel);
                     uint64_t st = ((uint64_t)q.rng[slot].y << 32) | q.rng[slot].x;
-                    const bool delta_mat = m.type == kMirror || m.type == kGlass;
+                    const bool delta_mat = mtype == kMirror || mtype == kGlass;
                     const bool use_guide = guided && !delta_mat;
                     const float* mix = use_guide ? p.gmix + (size_t)slot * kGuideOut : nullptr;
                     bool from_guide = false;
@@ -565,10 +611,10 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                         const float u0 = pcg_uniform(st, inc), u1 = pcg_uniform(st, inc), u2 = pcg_uniform(st, inc);
                         wworld = normalized(guide_sample(mix, u0, u1, u2));
                         bs.wi = to_local(fr, wworld);
-                        bs.f = bsdf_f(m, wo, bs.wi);
+                        bs.f = bsdf_f_t<kType>(m, wo, bs.wi);
                         bs.delta = false;
                     } else {
-                        switch (m.type) {
+                        switch (mtype) {
                             case kLambertian: {
                                 const float x1 = pcg_uniform(st, inc);
                                 const float x2 = pcg_uniform(st, inc);
@@ -581,19 +627,20 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                                 const float x1 = pcg_uniform(st, inc);
                                 const float x2 = pcg_uniform(st, inc);
                                 bs = mf_sample(m.alpha, wo, x1, x2);
-                                if (m.type == kMetal) bs.f = mf_metal_f(m, wo, bs.wi);
+                                if (mtype == kMetal) bs.f = mf_metal_f(m, wo, bs.wi);
                             }
                         }
                         wworld = to_world(fr, bs.wi);
                     }
                     if (use_guide) {
                         // mixture density of the direction, whichever strategy produced it
-                        const float pb = bsdf_sampling_pdf(m, wo, bs.wi);
+                        const float pb = bsdf_sampling_pdf_t<kType>(m, wo, bs.wi);
                         float pg = guide_pdf(mix, normalized(wworld));
                         if (!isfinite(pg)) pg = 0.f;
                         bs.pdf = (1.f - p.gfrac) * pb + p.gfrac * pg;
                     }
-                    if (do_nee && !bs.delta) {
+                    // mirror and glass samples are delta: no emitter sampling (:84)
+                    if (kType != kMirror && kType != kGlass && do_nee && !bs.delta) {
                         // directSampleLights (path_tracer.cu:83-126)
                         const float x1 = pcg_uniform(st, inc);
                         const float x2 = pcg_uniform(st, inc);
@@ -601,13 +648,14 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
                         const LightSample ls = sample_lights(sc, point, x1, x2, x3);
                         if (dot(ls.normal, ls.wi) < 0.f && ls.pdf > 0.f) {
                             const V wil = to_local(fr, ls.wi);
-                            float bpdf = p.consistent_mis ? bsdf_sampling_pdf(m, wo, wil) : bsdf_pdf(m, wo, wil);
+                            float bpdf = p.consistent_mis ? bsdf_sampling_pdf_t<kType>(m, wo, wil)
+                                                          : bsdf_pdf_t<kType>(m, wo, wil);
                             if (use_guide) {
                                 const float pg = guide_pdf(mix, ls.wi);
                                 bpdf = (1.f - p.gfrac) * bpdf + p.gfrac * (isfinite(pg) ? pg : 0.f);
                             }
                             const float wl = balance(ls.pdf, bpdf);
-                            const V f = bsdf_f(m, wo, wil);
+                            const V f = bsdf_f_t<kType>(m, wo, wil);
                             const V contrib = beta * (ls.emitted * wl * f * fabsf(dot(n, ls.wi)) / ls.pdf);
                             if (!is_zero(contrib)) {
                                 shadow = true;
@@ -676,6 +724,20 @@ __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShad
         for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x)
             if (rhist[j]) atomicAdd(&cnt[j], rhist[j]);
     }
+}
+
+// The shade stage over every slot of the queue (all materials).
+template <bool GUIDE, bool B>
+__global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShadeGuidedBlocksPerSm : 1)
+    k_shade(FrameParams p, int depth, long long wave_first, long long gfirst) {
+    shade_body<GUIDE, B, -1>(p, depth, wave_first, gfirst);
+}
+
+// The shade stage over one material class of a sorted queue (plain frames).
+template <bool B, int CLS>
+__global__ void __maxnreg__(shade_class_regs(CLS)) k_shade_class(FrameParams p, int depth, long long wave_first,
+                                                                long long gfirst) {
+    shade_body<false, B, CLS>(p, depth, wave_first, gfirst);
 }
 
 template <int W, bool CNT, bool B, int Q>
@@ -994,6 +1056,28 @@ struct Marker {
     }
 };
 
+// The plain shade stage of material-sorted frames: one kernel per material class present
+// (p.class_mask), each over its class's range of the sorted order. The class kernels hold
+// fewer registers than the kernel of all materials; each persistent grid is as many blocks
+// as the SMs keep resident at that register budget, and a class absent at a depth returns
+// before its first fetch.
+template <bool B>
+cudaError_t enqueue_class_shades(const FrameParams& p, int d, long long wave_first, long long gfirst,
+                                 cudaStream_t stream) {
+    const int bs = p.shape.block_shade;
+    auto grid = [&](int cls) {
+        const int per_sm = std::max(1, std::min(65536 / (shade_class_regs(cls) * bs), 2048 / bs));
+        return p.num_sms * per_sm;
+    };
+    if (p.class_mask & 1) k_shade_class<B, 0><<<grid(0), bs, 0, stream>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 2) k_shade_class<B, 1><<<grid(1), bs, 0, stream>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 4) k_shade_class<B, 2><<<grid(2), bs, 0, stream>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 8) k_shade_class<B, 3><<<grid(3), bs, 0, stream>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 16) k_shade_class<B, 4><<<grid(4), bs, 0, stream>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 64) k_shade_class<B, 6><<<grid(6), bs, 0, stream>>>(p, d, wave_first, gfirst);
+    return cudaGetLastError();
+}
+
 template <int W, bool CNT, bool B>
 cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
                           StageMarks* marks) {
@@ -1046,8 +1130,11 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
             if (p.guide_mode)
                 k_shade<true, B><<<p.num_sms * kShadeGuidedBlocksPerSm, kShadeGuidedBlock, 0, stream>>>(
                     p, d, wave_first, w.guided_first);
+            else if (p.shape.sort_materials && p.class_mask)
+                e = enqueue_class_shades<B>(p, d, wave_first, w.guided_first, stream);
             else
                 k_shade<false, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first, w.guided_first);
+            if (e != cudaSuccess) return e;
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {
                 if (p.sc.watertight)

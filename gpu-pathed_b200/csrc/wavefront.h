@@ -37,6 +37,7 @@ struct WaveCounters {
     int work_extend[kMaxDepthLimit + 1];   // persistent work-fetch cursors
     int work_shade[kMaxDepthLimit + 1];
     int work_shadow[kMaxDepthLimit + 1];
+    int work_class[kMaxDepthLimit + 1][8];  // fetch cursors of the per-class shade kernels
     int sort_count[kMaxDepthLimit + 1][8]; // per material class hit counts (sorted shading)
     int sort_fill[kMaxDepthLimit + 1][8];
 };
@@ -83,6 +84,7 @@ struct LaunchShape {
     int sort_rays = 0;        // continuation rays extended in (origin cell, direction octant) order
     int refill_idle = 16;     // traversal stages: a warp fetches new rays once this many lanes are idle
     int speculate = 0;        // kSpeculate* bits: stages that park a lane's first leaf and descend on
+    int split_shade = 1;      // material-sorted plain frames: one shade kernel per material class
 };
 
 constexpr int kSpeculateExtend = 1;  // closest-hit stage
@@ -177,6 +179,7 @@ struct FrameParams {
     float gfrac;             // probability of sampling the guide at a non-delta vertex
     int consistent_mis;      // NEE weights use the BSDF's true sampling density (microfacet)
     int guide_tc;            // guide inference on tcgen05 / tensor memory (single-scene frames)
+    int class_mask;          // material classes that can occur (bit 0 miss, bit type + 1); 0: one shade kernel
     int mma_test_polls;      // test hook: > 0 limits the first wait of each tcgen05 layer (tc_network)
     const uint32_t* gwpack;  // packed inference weights
     GuideFrame gframe;       // scene bounds for the position encoding

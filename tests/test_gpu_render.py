@@ -287,3 +287,25 @@ def test_autotuner_and_cache(tmp_path):
     assert t.get_launch()["sort_rays"] == r["sort_rays"]
     s.close()
     t.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [(0, None), (1, None), (2, 4), (3, 4)], ids=lambda c: f"cfg{c[0]}")
+@pytest.mark.parametrize("nee", [True, False])
+def test_class_shade_kernels_do_not_change_images(case, nee):
+    """the material-sorted shade stage as one kernel per material class (each compiled for
+    its own BSDF) gives the images of the single kernel over all materials, bit for bit"""
+    out = []
+    for split in (2, 1):
+        s = pathed.Session(96, 80)
+        s.load_config(case[0], level=case[1])
+        s.set_nee(nee)
+        s.set_launch(sort_materials=1, split_shade=split, wave_paths=20000)
+        s.set_seed(9)
+        for _ in range(2):
+            s.render(4)
+        st = s.stats()
+        out.append((s.readback().copy(), st["rays_extend"], st["rays_shadow"]))
+        s.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1:] == out[1][1:]
