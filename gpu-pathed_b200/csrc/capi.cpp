@@ -344,6 +344,10 @@ int pt_set_guide_inference(pt_session* s, int tc) {
     if (!s) return PT_ERR_ARG;
     return s->impl.set_guide_inference(tc);
 }
+int pt_set_guide_training(pt_session* s, int tc) {
+    if (!s) return PT_ERR_ARG;
+    return s->impl.set_guide_training(tc);
+}
 int pt_guide_gradients(pt_session* s, const float* x, const float* wi, const float* w, int n, float* grad) {
     if (!s || !x || !wi || !w || !grad) return PT_ERR_ARG;
     return guarded(s, [&] { return s->impl.guide_gradients(x, wi, w, n, grad); });

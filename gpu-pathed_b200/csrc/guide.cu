@@ -17,6 +17,7 @@
 
 #include "guide_mlp.cuh"
 #include "guide_tc.cuh"
+#include "guide_train_tc.cuh"
 
 namespace pt {
 
@@ -185,7 +186,15 @@ __device__ __forceinline__ void source_sample(const TrainSource& s, const GuideF
         wi[0] = sm.wi[0]; wi[1] = sm.wi[1]; wi[2] = sm.wi[2];
         w = sm.weight;
     } else {
-        for (int k = 0; k < kGuideIn; k++) xrow[k] = s.x[(size_t)i * kGuideIn + k];
+        const float4* xr = reinterpret_cast<const float4*>(s.x + (size_t)i * kGuideIn);  // 320-byte rows
+#pragma unroll
+        for (int k = 0; k < kGuideIn / 4; k++) {
+            const float4 v = __ldg(xr + k);
+            xrow[4 * k] = v.x;
+            xrow[4 * k + 1] = v.y;
+            xrow[4 * k + 2] = v.z;
+            xrow[4 * k + 3] = v.w;
+        }
         wi[0] = s.wi[3 * i]; wi[1] = s.wi[3 * i + 1]; wi[2] = s.wi[3 * i + 2];
         w = s.w[i];
     }
@@ -537,6 +546,211 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideDevice g,
     if (lane == 0 && loss != 0.f) atomicAdd(g.wsum + 1, loss);  // batch loss, for monitoring
 }
 
+// The training step of k_guide_train on tcgen05 (guide_train_tc.cuh): the same loss,
+// weight cap and gradient layout, every product on the tensor cores with the accumulators in
+// tensor memory.
+__global__ void __launch_bounds__(kTtThreads, 1) k_guide_train_tc(GuideDevice g, TrainSource src0) {
+    extern __shared__ __align__(1024) uint8_t ttsm[];
+    TtSmem& s = *reinterpret_cast<TtSmem*>(ttsm);
+    const int net = blockIdx.y;
+    g.wpack += (size_t)net * kGuidePackWords;
+    g.grad += (size_t)net * kGuideParams;
+    g.wsum += 4 * net;
+    const TrainSource src = source_of_net(src0, net);
+    const int t = threadIdx.x, warp = t >> 5, sub = t / kTcRows, row = t % kTcRows;
+    TtSubTile& my = s.sub[sub];
+    int first, n;
+    source_range(src, first, n);
+    if ((int)blockIdx.x * kTtRows >= n) return;  // no tile for this CTA: no setup, no TMEM
+    // ---- setup: weight images, biases, the ones columns, mbarrier, tensor memory
+    copy_words16(g.wpack + kPackWords, reinterpret_cast<uint32_t*>(s.w), kTcPackWords);
+    for (int i = t; i < 64 * 3 + 48; i += blockDim.x)
+        s.bias[i] = i < 192 + kGuideOut ? __uint_as_float(g.wpack[kSB + i]) : 0.f;
+    {
+        const uint4 ones = make_uint4(pack_bf16(1.f, 0.f), 0u, 0u, 0u), zero = make_uint4(0u, 0u, 0u, 0u);
+        uint8_t* tiles[3] = {my.a1, my.a2, my.a3};
+        for (int k = 0; k < 3; k++) {  // features 64 (one) and 65-79 (zero) of the row
+            *reinterpret_cast<uint4*>(tiles[k] + tc_offset(row, 64, kTcLboA)) = ones;
+            *reinterpret_cast<uint4*>(tiles[k] + tc_offset(row, 72, kTcLboA)) = zero;
+        }
+    }
+    if (t == 0) {
+        mbar_init(smem_u32(&s.mbar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tc_alloc(smem_u32(&s.tmem_slot), kTtTmemCols);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s.tmem_slot;
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;  // this warp's TMEM lanes
+    const uint32_t scratch = tmem + kTtColScratch + 64u * sub;
+    const uint32_t mbar = smem_u32(&s.mbar);
+    const uint32_t w_s = smem_u32(s.w);
+    uint32_t sx[kTtSub], sa1[kTtSub], sa2[kTtSub], sa3[kTtSub], sdy[kTtSub];
+#pragma unroll
+    for (int k = 0; k < kTtSub; k++) {
+        sx[k] = smem_u32(s.sub[k].x);
+        sa1[k] = smem_u32(s.sub[k].a1);
+        sa2[k] = smem_u32(s.sub[k].a2);
+        sa3[k] = smem_u32(s.sub[k].a3);
+        sdy[k] = smem_u32(s.sub[k].dy);
+    }
+    const float wsum = g.wsum[0];
+    const float inv_wsum = wsum > 0.f ? 1.f / wsum : 0.f;
+    uint32_t phase = 0;
+    bool ok = true, first_tile = true;
+    float loss = 0.f;
+    for (int tile = blockIdx.x; tile * kTtRows < n && ok; tile += gridDim.x) {
+        // 1. stage this thread's sample
+        float wi[3] = {0.f, 0.f, 1.f}, w = 0.f;
+        {
+            const int i = tile * kTtRows + t;
+            float x[kGuideIn];
+            if (i < n) {
+                source_sample(src, g.frames ? g.frames[net] : g.frame, first, i, x, wi, w);
+            } else {
+#pragma unroll
+                for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
+            }
+            w = fminf(w * inv_wsum, kWeightCap / (float)n);
+            tc_store_input(my.x, row, x);  // inputs 78, 79 read as zero in the forward pass
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // 2. forward
+        float raw[kGuideOut];
+        for (int layer = 0; layer < 4 && ok; layer++) {
+            if (t == 0) {
+                tc_fence_after();
+                const int k = layer == 0 ? kGuideIn : kGuideHidden;
+                const int nn = layer == 3 ? 48 : 64;
+                const int woff = layer == 0 ? kTcW1 : layer == 1 ? kTcW2 : layer == 2 ? kTcW3 : kTcW4;
+                const int lbo = layer == 3 ? kTcLboW4 : kTcLboW;
+                const uint32_t idesc = tc_idesc(kTcRows, nn);
+                for (int b = 0; b < kTtSub; b++) {
+                    const uint32_t a = layer == 0 ? sx[b] : layer == 1 ? sa1[b] : layer == 2 ? sa2[b] : sa3[b];
+                    for (int st = 0; st < k / 16; st++)
+                        tc_mma(tmem + kTtColScratch + 64u * b, tc_smem_desc(a + st * 2 * kTcLboA, kTcLboA, 128),
+                               tc_smem_desc(w_s + woff + st * 2 * lbo, lbo, 128), idesc, st > 0 ? 1u : 0u);
+                }
+                tc_commit(mbar);
+            }
+            if (!(ok = tt_wait(mbar, phase))) break;
+            if (layer < 3) {
+                uint8_t* dst = layer == 0 ? my.a1 : layer == 1 ? my.a2 : my.a3;
+                tc_epilogue_hidden(scratch + lane_base, s.bias + 64 * layer, dst, row);
+                tc_fence_before();
+                fence_async_smem();
+                __syncthreads();
+            } else {
+#pragma unroll
+                for (int c = 0; c < 48; c += 16) {
+                    float v[16];
+                    tc_ld16(scratch + lane_base + c, v);
+                    tc_wait_ld();
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        if (c + j < kGuideOut) raw[c + j] = v[j] + s.bias[192 + c + j];
+                }
+            }
+        }
+        if (!ok) break;
+        // 3. loss gradient of the raw outputs, BF16 into dY (columns 40-47 zero)
+        {
+            float dy[kGuideOut];
+            loss += loss_grad(raw, wi, w, dy);
+#pragma unroll
+            for (int c = 0; c < 48; c += 8) {
+                uint32_t q[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int k = c + 2 * j;
+                    q[j] = pack_bf16(k < kGuideOut ? dy[k] : 0.f, k + 1 < kGuideOut ? dy[k + 1] : 0.f);
+                }
+                *reinterpret_cast<uint4*>(my.dy + tc_offset(row, c, kTcLboA)) = make_uint4(q[0], q[1], q[2], q[3]);
+            }
+        }
+        tc_fence_before();
+        fence_async_smem();
+        __syncthreads();
+        // 4. backward: layer 4 (W4' += A3^T dY, dZ3 = dY W4), 3, 2, then W1' += X^T dZ1
+        for (int layer = 3; layer >= 1 && ok; layer--) {
+            if (t == 0) {
+                tc_fence_after();
+                const uint32_t gcol = layer == 3 ? kTtColW4 : layer == 2 ? kTtColW3 : kTtColW2;
+                const int nn = layer == 3 ? 48 : 64;
+                const int woff = layer == 3 ? kTcW4 : layer == 2 ? kTcW3 : kTcW2;
+                const uint32_t wchunk = layer == 3 ? kTcLboW4 : kTcLboW;
+                for (int b = 0; b < kTtSub; b++) {
+                    const uint32_t act = layer == 3 ? sa3[b] : layer == 2 ? sa2[b] : sa1[b];  // A_{l-1}
+                    const uint32_t dz = layer == 3 ? sdy[b] : layer == 2 ? sa3[b] : sa2[b];   // dZ_l
+                    tt_wgrad(tmem + gcol, act, dz, nn, first_tile && b == 0);
+                    tt_bdata(tmem + kTtColScratch + 64u * b, dz, w_s + woff, nn, wchunk);
+                }
+                tc_commit(mbar);
+            }
+            if (!(ok = tt_wait(mbar, phase))) break;
+            // dZ_{l-1} = D [A_{l-1} > 0], over A_{l-1}
+            tt_epilogue_mask(scratch + lane_base, layer == 3 ? my.a3 : layer == 2 ? my.a2 : my.a1, row);
+            tc_fence_before();
+            fence_async_smem();
+            __syncthreads();
+        }
+        if (!ok) break;
+        // b1 rides on input 78 of X for the W1 product
+        *reinterpret_cast<uint32_t*>(my.x + tc_offset(row, kGuideIn - 2, kTcLboA)) = pack_bf16(1.f, 0.f);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+            for (int b = 0; b < kTtSub; b++) tt_wgrad(tmem + kTtColW1, sx[b], sa1[b], 64, first_tile && b == 0);
+            tc_commit(mbar);
+        }
+        if (!(ok = tt_wait(mbar, phase))) break;
+        first_tile = false;
+    }
+    if (!ok) {
+        if (t == 0) atomicAdd(g.wsum + 2, 1.f);  // a wait gave up: no partial gradient
+    } else if (!first_tile && t < 2 * kTcRows) {
+        // 5. the accumulators to the global gradient: warps 0-3 add W1 and W2, warps 4-7 W3
+        //    and W4; the thread's TMEM lane is input row i
+        const int i = row;
+        for (int m = 0; m < 2; m++) {
+            const int layer = sub == 0 ? m : 2 + m;  // 0..3 = W1..W4
+            const uint32_t col = layer == 0 ? kTtColW1 : layer == 1 ? kTtColW2 : layer == 2 ? kTtColW3 : kTtColW4;
+            const int nout = layer == 3 ? kGuideOut : 64;
+            const int wbase = layer == 0 ? kGW1 : layer == 1 ? kGW2 : layer == 2 ? kGW3 : kGW4;
+            const int bbase = layer == 0 ? kGB1 : layer == 1 ? kGB2 : layer == 2 ? kGB3 : kGB4;
+            const int ones = layer == 0 ? kGuideIn - 2 : 64;  // the row of the ones input
+            const int nin = layer == 0 ? kGuideIn - 2 : 64;   // real input rows
+            // rows of padding inputs and past the layer's inputs add nothing (every lane of the
+            // warp still takes part in the warp-wide tcgen05.ld)
+            const bool use = i < nin || i == ones;
+            float* dst = i < nin ? g.grad + wbase + i * nout : g.grad + bbase;  // 16-byte aligned rows
+            for (int c = 0; c < 64; c += 16) {
+                if (layer == 3 && c >= 48) break;
+                float v[16];
+                tc_ld16(tmem + lane_base + col + c, v);
+                tc_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 16; j += 4)  // one 16-byte reduction per four outputs
+                    if (use && c + j < nout)
+                        atomicAdd(reinterpret_cast<float4*>(dst + c + j), make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]));
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if ((t & 31) == 0 && loss != 0.f) atomicAdd(g.wsum + 1, loss);  // batch loss, for monitoring
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc_dealloc(tmem, kTtTmemCols);
+}
+
 __global__ void k_guide_adam(GuideDevice g, float lr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kGuideParams) return;
@@ -566,9 +780,10 @@ __global__ void k_guide_step(int* step, int nets) {
 constexpr size_t kTrainSmemBytes = (size_t)kTrainSmemWords * sizeof(uint32_t);
 
 __global__ void k_guide_clear_sums(float* wsum, int nets) {
-    if (threadIdx.x < nets) {  // weight sum, batch loss of each network
+    if (threadIdx.x < nets) {  // weight sum, batch loss, failed waits of each network
         wsum[4 * threadIdx.x] = 0.f;
         wsum[4 * threadIdx.x + 1] = 0.f;
+        wsum[4 * threadIdx.x + 2] = 0.f;
     }
 }
 
@@ -578,7 +793,10 @@ cudaError_t launch_train(const GuideDevice& g, const TrainSource& src, cudaStrea
     // about one block per SM in total, at least 4 per network
     const int per = std::max(4, g.num_sms / nets);
     k_guide_wsum<<<dim3(per, nets), 256, 0, s>>>(src, g.wsum);
-    k_guide_train<<<dim3(per, nets), kTrainThreads, kTrainSmemBytes, s>>>(g, src);
+    if (g.train_tc)
+        k_guide_train_tc<<<dim3(per, nets), kTtThreads, sizeof(TtSmem), s>>>(g, src);
+    else
+        k_guide_train<<<dim3(per, nets), kTrainThreads, kTrainSmemBytes, s>>>(g, src);
     return cudaGetLastError();
 }
 
@@ -587,6 +805,8 @@ cudaError_t launch_train(const GuideDevice& g, const TrainSource& src, cudaStrea
 cudaError_t guide_configure() {
     cudaError_t e =
         cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmemBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TtSmem));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_guide_forward_x_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(TcSmem));

@@ -23,6 +23,7 @@ struct GuideDevice {
     int* step;           // Adam steps taken (device counter, so training launches replay in graphs)
     int num_sms;         // training grid: one block per SM
     int nets;            // networks trained together (1 for a single scene)
+    int train_tc;        // 1: the training kernel on tcgen05 (k_guide_train_tc), 0: on mma.sync
     const GuideFrame* frames;  // per-network encoding frames (nets > 1), else `frame`
     GuideFrame frame;
 };

@@ -225,6 +225,7 @@ GuideDevice Session::guide_view() const {
     g.step = reinterpret_cast<int*>(d_gwsum_.as<float>() + 3);
     g.num_sms = num_sms_;
     g.nets = guide_nets_;
+    g.train_tc = guide_train_tc_ ? 1 : 0;
     g.frame = gframe_;
     g.frames = guide_nets_ > 1 || batch_mode() ? d_gframes_.as<GuideFrame>() : nullptr;
     return g;
@@ -431,8 +432,13 @@ int Session::guide_gradients(const float* x, const float* wi, const float* w, in
     if ((r = check_cuda(guide_gradients_features(guide_view(), dx, dwi, dw, n, stream_), "guide gradients"))) return r;
     if ((r = check_cuda(cudaMemcpyAsync(grad, d_ggrad_.p, kGuideParams * 4, cudaMemcpyDeviceToHost, stream_), "copy")))
         return r;
+    float sums[4] = {0.f, 0.f, 0.f, 0.f};
+    if ((r = check_cuda(cudaMemcpyAsync(sums, d_gwsum_.p, sizeof(sums), cudaMemcpyDeviceToHost, stream_), "copy")))
+        return r;
     if ((r = check_cuda(cudaMemsetAsync(d_ggrad_.p, 0, kGuideParams * 4, stream_), "guide"))) return r;
-    return check_cuda(cudaStreamSynchronize(stream_), "guide gradients");
+    if ((r = check_cuda(cudaStreamSynchronize(stream_), "guide gradients"))) return r;
+    if (sums[2] != 0.f) return fail(PT_ERR_DEVICE, "tensor-core training: a wait for the MMA completion gave up");
+    return PT_OK;
 }
 
 int Session::set_bvh(int width, int max_leaf) {

@@ -269,6 +269,13 @@ public:
         return PT_OK;
     }
     bool guide_infer_tc_ = false;
+    // guide training on tcgen05 / TMEM (1) or on mma.sync (0)
+    int set_guide_training(int tc) {
+        if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
+        guide_train_tc_ = tc != 0;
+        return PT_OK;
+    }
+    bool guide_train_tc_ = true;  // 64 us per 2^16-sample step against 95 us on mma.sync
     // probability of sampling the guide at a non-delta vertex (one-sample MIS), in (0, 1)
     int set_guide_fraction(float f) {
         if (!(f > 0.f && f < 1.f)) return fail(PT_ERR_ARG, "guide fraction must lie in (0, 1)");

@@ -49,6 +49,7 @@ EXPORTED = [
     "pt_measure_l2_read",
     "pt_set_test_limits",
     "pt_set_watertight",
+    "pt_set_guide_training",
 ]
 
 MESH_OBJ, MESH_PLY = 0, 1  # PT_MESH_OBJ, PT_MESH_PLY
@@ -219,7 +220,8 @@ def _load():
     lib.pt_write_exr.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
     lib.pt_read_exr.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
     for name in ("pt_set_device", "pt_set_max_depth", "pt_set_nee", "pt_set_guiding", "pt_render_async",
-                 "pt_set_bvh_builder", "pt_set_renderer", "pt_set_bvh_nodes", "pt_set_watertight"):
+                 "pt_set_bvh_builder", "pt_set_renderer", "pt_set_bvh_nodes", "pt_set_watertight",
+                 "pt_set_guide_training"):
         getattr(lib, name).argtypes = [C.c_void_p, C.c_int]
     lib.pt_set_bvh.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.pt_set_test_limits.argtypes = [C.c_void_p, C.c_int, C.c_int]
@@ -494,6 +496,10 @@ class Session:
         g = GuideInfo()
         self._check(lib.pt_guide_get_info(self._h, C.byref(g)))
         return {k: getattr(g, k) for k, _ in GuideInfo._fields_}
+
+    def set_guide_training(self, tc: bool):
+        """Guide training on tcgen05 / tensor memory (True) or mma.sync (False)."""
+        self._check(lib.pt_set_guide_training(self._h, int(bool(tc))))
 
     def set_guide_inference(self, tc: bool):
         """Guide inference on tcgen05 / tensor memory (True) or mma.sync (False)."""

@@ -306,6 +306,11 @@ int pt_guide_forward(pt_session* s, const float* x, int n, float* raw);
 /* Guide inference on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor
  * memory; tc = 1) or on warp-level mma.sync (tc = 0, the default and the fallback). */
 int pt_set_guide_inference(pt_session* s, int tc);
+/* Guide training on the 5th-generation tensor cores (tc = 1, the default): forward,
+ * backward-data and weight-gradient products as tcgen05.mma with the gradient accumulators in
+ * tensor memory across all of a CTA's samples; or on warp-level mma.sync (tc = 0). Same loss,
+ * weight cap and BF16 operands either way. */
+int pt_set_guide_training(pt_session* s, int tc);
 /* Probability (default 0.7) of drawing a non-delta vertex's direction from the guide instead
  * of the BSDF; the MIS density is (1 - f) p_bsdf + f p_guide, so the estimator is unbiased for
  * any f in (0, 1) (PT_ERR_ARG outside). */

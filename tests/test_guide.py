@@ -110,11 +110,14 @@ def test_bf16_operand_rounding_is_a_small_perturbation(oracle_lib):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("tc", [False, True], ids=["mma.sync", "tcgen05"])
 @pytest.mark.parametrize("n", [3000, 40000])
-def test_training_gradients_match_oracle(oracle_lib, n):
-    """tensor-core training kernel (BF16 operands, FP32 accumulation) against the FP64 oracle
-    that rounds the same operands to BF16; n = 40000 gives blocks several sample tiles"""
+def test_training_gradients_match_oracle(oracle_lib, n, tc):
+    """tensor-core training kernels (BF16 operands, FP32 accumulation; mma.sync, or tcgen05
+    with the weight-gradient accumulators in tensor memory) against the FP64 oracle that
+    rounds the same operands to BF16; n = 40000 gives blocks several sample tiles"""
     s = pathed.Session(8, 8)
+    s.set_guide_training(tc)
     p = random_params(9)
     s.set_guide_params(p)
     x, wi, w = random_batch(n, seed=10)
@@ -223,3 +226,28 @@ def test_guide_fraction_range():
             s.set_guide_fraction(bad)
     s.set_guide_fraction(0.9)
     s.close()
+
+
+@pytest.mark.gpu
+def test_tcgen05_training_in_frames():
+    """guided frames whose online training runs on tcgen05: the loss falls and the image stays
+    finite; the same frames trained on mma.sync reach a loss of the same size"""
+    losses = {}
+    for tc in (True, False):
+        s = _slit_room(48, 48)
+        s.set_seed(21)
+        s.set_guide_training(tc)
+        s.set_guiding(True)
+        s.set_guide_options(steps_per_frame=4, warmup_steps=8)
+        trace = []
+        for f in range(32):
+            s.render(4)
+            trace.append(s.guide_info()["loss"])
+        early, late = float(np.mean(trace[2:6])), float(np.mean(trace[-6:]))
+        losses[tc] = (early, late, s.guide_info()["steps"])
+        assert np.all(np.isfinite(s.readback())) and np.all(np.isfinite(trace))
+        s.close()
+    print("loss early / late / steps:", losses)
+    e_tc, l_tc, steps = losses[True]
+    assert steps >= 96 and l_tc < e_tc
+    assert abs(l_tc - losses[False][1]) <= 0.5 * abs(losses[False][1]) + 0.5
