@@ -481,6 +481,8 @@ def run_ours(args):
         s.load_config(args.config)
         if args.guided:  # learned guiding on the main workload (trained online during warm-up)
             s.set_guiding(True)
+            if args.guide_inference:
+                s.set_guide_inference(args.guide_inference == "tc")
     s.set_seed(replica_seed(rank))
     if args.wave_paths:
         s.set_launch(wave_paths=args.wave_paths)
@@ -660,7 +662,7 @@ def plain_to_budget(ref, budget_spp=256, res=1024):
 
 
 def guided_to_target(ref, t_plain, target, res=1024, fraction=None, steps=None, warmup=None, lr=None,
-                     schedule=None, seed=77):
+                     schedule=None, seed=77, batch=None):
     """Device ms for the guided render, trained online from scratch inside the timed 1-spp
     frames, to reach `target` relMSE (crossing interpolated in log relMSE between checks).
     `schedule(frame)`, when given, sets the Adam steps of each frame."""
@@ -672,9 +674,9 @@ def guided_to_target(ref, t_plain, target, res=1024, fraction=None, steps=None, 
     g.set_guiding(True)
     if fraction is not None:
         g.set_guide_fraction(fraction)
-    if steps is not None or warmup is not None or lr is not None:
+    if steps is not None or warmup is not None or lr is not None or batch is not None:
         g.set_guide_options(steps_per_frame=-1 if steps is None else steps, lr=0.0 if lr is None else lr,
-                            warmup_steps=-1 if warmup is None else warmup)
+                            warmup_steps=-1 if warmup is None else warmup, batch=batch or 0)
     t_guided, spp, prev, crossed = 0.0, 0, None, None
     while t_guided < 3 * t_plain:
         if schedule is not None:
@@ -706,12 +708,20 @@ def guided_time_to_relmse(budget_spp=256, ref_spp=2048, res=1024):
     ref = slit_reference(ref_spp, res)
     t_plain, target = plain_to_budget(ref, budget_spp, res)
     crossed, spp, steps = guided_to_target(ref, t_plain, target, res)
+    # the configuration as written: guide fraction 0.5, Adam lr 1e-3, one 2^18-sample step per frame
+    aw_crossed, aw_spp, aw_steps = guided_to_target(ref, t_plain, target, res, fraction=0.5, steps=1, lr=1e-3,
+                                                    batch=1 << 18)
+    as_written = {"fraction": 0.5, "lr": 1e-3, "samples_per_step": 1 << 18, "steps_per_frame": 1,
+                  "guided_ms": aw_crossed, "guided_spp": aw_spp, "guide_steps": aw_steps,
+                  "speedup": (t_plain / aw_crossed) if aw_crossed else None}
     return {"workload": f"slit-room {res}x{res} depth 10 (2002 + 1310720 triangles, env through a 0.05 slit)",
             "reference": f"plain render, {ref_spp} spp, consistent MIS, passes accumulated in FP64",
             "plain_spp": budget_spp,
             "plain_ms": t_plain, "target_relmse": target, "guided_ms": crossed,
             "guided_spp": spp, "speedup": (t_plain / crossed) if crossed else None, "guide_steps": steps,
-            "training": "online from scratch inside the timed frames (automatic Adam schedule)"}
+            "training": "online from scratch inside the timed frames (automatic Adam schedule: fraction 0.7, "
+                        "lr 3e-3, 16 steps of 2^16 samples per frame early, fewer later), tcgen05 training kernel",
+            "as_written": as_written}
 
 
 class BatchRelmse:
@@ -876,6 +886,33 @@ def ncu_frames(args):
     return 0
 
 
+def ncu_train(calls, n=1 << 16):
+    """Guide-gradient calls (pt_guide_gradients) of n seeded samples on each training kernel,
+    for an ncu capture of the training launches: `calls` on mma.sync, then `calls` on tcgen05."""
+    import numpy as np
+
+    import pathed
+
+    rng = np.random.default_rng(10)
+    s = pathed.Session(8, 8)
+    p = (rng.normal(0, 1, pathed.GUIDE_PARAMS) * 0.1).astype(np.float32)
+    s.set_guide_params(p)
+    x = rng.uniform(-1, 1, (n, 80)).astype(np.float32)
+    wi = rng.normal(0, 1, (n, 3)).astype(np.float32)
+    wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+    w = rng.exponential(1.0, n).astype(np.float32)
+    out = {}
+    for tc in (False, True):
+        s.set_guide_training(tc)
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            s.guide_gradients(x, wi, w)
+        out["tcgen05" if tc else "mma.sync"] = (time.perf_counter() - t0) / calls * 1e3
+    s.close()
+    print(json.dumps({"guide_gradient_calls": calls, "samples": n, "wall_ms_per_call": out}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -893,6 +930,8 @@ def main():
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="per_config without the reference CUDA backend's timings")
     ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
+    ap.add_argument("--guide-inference", choices=("mma", "tc"), default=None,
+                    help="with --guided: guide inference on mma.sync or on tcgen05 (default: the library's)")
     ap.add_argument("--gpu-bvh", action="store_true", help="build the BVH on the GPU instead of the host")
     ap.add_argument("--quantized-bvh", action="store_true",
                     help="traverse quantized wide nodes (8-bit child planes) instead of float nodes")
@@ -909,9 +948,14 @@ def main():
                     help="profiling aid: load the configuration (at --res if given), render this many frames "
                          "with the default launch shape, print their closest-hit query counts and exit")
     ap.add_argument("--res", type=int, nargs=2, default=None, help="with --ncu-frames: width height")
+    ap.add_argument("--ncu-train", type=int, default=0,
+                    help="profiling aid: this many guide-gradient calls of 2^16 seeded samples on the mma.sync "
+                         "training kernel, then as many on the tcgen05 kernel; prints their wall ms and exits")
     args = ap.parse_args()
     if args.ncu_frames:
         return ncu_frames(args)
+    if args.ncu_train:
+        return ncu_train(args.ncu_train)
     if args.impl == "reference":
         return run_reference(args)
     if args.time_to_relmse:

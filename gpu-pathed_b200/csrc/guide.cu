@@ -112,23 +112,23 @@ __global__ void k_guide_forward_x(const uint32_t* __restrict__ wpack, const floa
 }
 
 // Inference on explicit input vectors on the tensor cores (tcgen05, TMEM accumulators):
-// 128 inputs per tile, one thread each. Raw outputs like k_guide_forward_x.
-__global__ void __launch_bounds__(kTcRows) k_guide_forward_x_tc(const uint32_t* __restrict__ wpack,
+// kTcThreads inputs per tile, one thread each. Raw outputs like k_guide_forward_x.
+__global__ void __launch_bounds__(kTcThreads) k_guide_forward_x_tc(const uint32_t* __restrict__ wpack,
                                                                 const float* __restrict__ x, int n,
                                                                 float* __restrict__ raw, int* error,
                                                                 int test_polls) {
     extern __shared__ __align__(1024) uint8_t tsm[];
     TcSmem& s = *reinterpret_cast<TcSmem*>(tsm);
-    const int tiles = (n + kTcRows - 1) / kTcRows;
+    const int tiles = (n + kTcThreads - 1) / kTcThreads;
     if ((int)blockIdx.x >= tiles) return;
     const uint32_t tmem = tc_setup(s, wpack, wpack + kPackWords);
     uint32_t phase = 0;
     const int t = threadIdx.x;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int row = tile * kTcRows + t;
+        const int row = tile * kTcThreads + t;
         float xi[kGuideIn];
         for (int k = 0; k < kGuideIn; k++) xi[k] = row < n ? x[(size_t)row * kGuideIn + k] : 0.f;
-        tc_store_input(s.a, t, xi);
+        tc_store_input(s.a[tc_sub()], tc_row(), xi);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -815,9 +815,9 @@ cudaError_t guide_configure() {
 cudaError_t guide_forward_features_tc(const GuideDevice& g, const float* x, int n, float* raw, int* error,
                                       cudaStream_t s, int test_polls) {
     if (n <= 0) return cudaSuccess;
-    const int tiles = (n + kTcRows - 1) / kTcRows;
-    const int grid = tiles < g.num_sms * 4 ? tiles : g.num_sms * 4;
-    k_guide_forward_x_tc<<<grid, kTcRows, sizeof(TcSmem), s>>>(g.wpack, x, n, raw, error, test_polls);
+    const int tiles = (n + kTcThreads - 1) / kTcThreads;
+    const int grid = tiles < g.num_sms * 2 ? tiles : g.num_sms * 2;
+    k_guide_forward_x_tc<<<grid, kTcThreads, sizeof(TcSmem), s>>>(g.wpack, x, n, raw, error, test_polls);
     return cudaGetLastError();
 }
 

@@ -1,5 +1,7 @@
 // Guide network inference on the 5th-generation tensor cores (tcgen05, sm_100a): one CTA of
-// 128 threads evaluates tiles of 128 samples (the MMA's M), one thread per sample.
+// 256 threads evaluates tiles of 256 samples, two sub-tiles of 128 (the MMA's M), one thread
+// per sample; one thread issues both sub-tiles' MMAs of a layer before a single commit, so
+// each commit-and-wait round serves 256 samples and one weight copy serves the whole CTA.
 //
 // Per layer: the activations (M x K, BF16) and the transposed weights (N x K, BF16) sit in
 // shared memory in the canonical K-major, no-swizzle layout of the UMMA descriptors (core
@@ -179,26 +181,31 @@ __device__ __forceinline__ void tc_store_input(uint8_t* a_tile, int row, const f
 }
 
 // Shared memory of a tensor-core inference CTA.
+constexpr int kTcSub = 2;                     // sub-tiles per CTA
+constexpr int kTcThreads = kTcRows * kTcSub;  // 256 threads, 256 samples per tile
 struct TcSmem {
     uint8_t w[kTcWBytes];        // transposed weight images (B operands)
-    uint8_t a[kTcABytes];        // activation tile (A operand)
+    uint8_t a[kTcSub][kTcABytes];  // activation tiles (A operands), one per sub-tile
     float bias[64 * 3 + 48];     // b1, b2, b3, b4 (b4 zero-padded to 48)
     unsigned long long mbar;
     uint32_t tmem_slot;
     int failed;
 };
+__device__ __forceinline__ int tc_sub() { return (int)threadIdx.x / kTcRows; }  // this thread's sub-tile
+__device__ __forceinline__ int tc_row() { return (int)threadIdx.x % kTcRows; }  // its row (TMEM lane)
 
-// The whole network for the CTA's current 128-row tile (inputs already in s.a, fenced and
+// The whole network for the CTA's current tile (inputs already in s.a, fenced and
 // synchronised). Leaves each thread's 40 raw outputs in `raw`. Returns false when a wait
-// gave up (outputs invalid). All 128 threads call it. test_polls > 0 (a test hook) limits the
-// first wait of each layer to that many non-blocking polls, so it gives up while the layer's
-// MMA is still running; the bounded drain that follows still waits for that MMA to finish.
+// gave up (outputs invalid). All threads of the CTA call it; sub-tile b accumulates in TMEM
+// columns [64 b, 64 b + 64). test_polls > 0 (a test hook) limits the first wait of each
+// layer to that many non-blocking polls, so it gives up while the layer's MMA is still
+// running; the bounded drain that follows still waits for that MMA to finish.
 __device__ __forceinline__ bool tc_network(TcSmem& s, uint32_t tmem, uint32_t& phase, float raw[kGuideOut],
                                            int test_polls = 0) {
-    const int t = threadIdx.x, warp = t >> 5;
+    const int t = threadIdx.x, warp = t >> 5, sub = tc_sub(), row = tc_row();
     const uint32_t mbar = smem_u32(&s.mbar);
-    const uint32_t a_saddr = smem_u32(s.a), w_saddr = smem_u32(s.w);
-    const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t w_saddr = smem_u32(s.w);
+    const uint32_t tmem_row = tmem + 64u * sub + ((uint32_t)((warp & 3) * 32) << 16);
     const int kLimit = 1 << 22;
     for (int layer = 0; layer < 4; layer++) {
         if (t == 0) {
@@ -206,7 +213,15 @@ __device__ __forceinline__ bool tc_network(TcSmem& s, uint32_t tmem, uint32_t& p
             const int k = layer == 0 ? kGuideIn : kGuideHidden;
             const int n = layer == 3 ? 48 : 64;
             const int woff = layer == 0 ? kTcW1 : layer == 1 ? kTcW2 : layer == 2 ? kTcW3 : kTcW4;
-            tc_layer(tmem, a_saddr, w_saddr + woff, k, n, layer == 3 ? kTcLboW4 : kTcLboW, mbar);
+            const int lbo = layer == 3 ? kTcLboW4 : kTcLboW;
+            const uint32_t idesc = tc_idesc(kTcRows, n);
+            for (int b = 0; b < kTcSub; b++) {  // both sub-tiles, then one commit
+                const uint32_t a_saddr = smem_u32(s.a[b]);
+                for (int st = 0; st < k / 16; st++)
+                    tc_mma(tmem + 64u * b, tc_smem_desc(a_saddr + st * 2 * kTcLboA, kTcLboA, 128),
+                           tc_smem_desc(w_saddr + woff + st * 2 * lbo, lbo, 128), idesc, st > 0 ? 1u : 0u);
+            }
+            tc_commit(mbar);
         }
         bool done = false;
         if (test_polls > 0) {
@@ -223,7 +238,7 @@ __device__ __forceinline__ bool tc_network(TcSmem& s, uint32_t tmem, uint32_t& p
         phase ^= 1u;
         tc_fence_after();
         if (layer < 3) {
-            tc_epilogue_hidden(tmem_row, s.bias + 64 * layer, s.a, t);
+            tc_epilogue_hidden(tmem_row, s.bias + 64 * layer, s.a[sub], row);
             tc_fence_before();
             fence_async_smem();
             __syncthreads();
@@ -242,7 +257,8 @@ __device__ __forceinline__ bool tc_network(TcSmem& s, uint32_t tmem, uint32_t& p
     return true;
 }
 
-// CTA setup: weight images and biases into shared memory, mbarrier, 64 TMEM columns.
+// CTA setup: weight images and biases into shared memory, mbarrier, 64 TMEM columns per
+// sub-tile.
 __device__ __forceinline__ uint32_t tc_setup(TcSmem& s, const uint32_t* __restrict__ wpack_fwd,
                                              const uint32_t* __restrict__ wpack_tc) {
     copy_words16(wpack_tc, reinterpret_cast<uint32_t*>(s.w), kTcPackWords);
@@ -252,7 +268,7 @@ __device__ __forceinline__ uint32_t tc_setup(TcSmem& s, const uint32_t* __restri
         mbar_init(smem_u32(&s.mbar), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (threadIdx.x < 32) tc_alloc(smem_u32(&s.tmem_slot), 64);
+    if (threadIdx.x < 32) tc_alloc(smem_u32(&s.tmem_slot), 64 * kTcSub);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -264,7 +280,7 @@ __device__ __forceinline__ void tc_teardown(uint32_t tmem) {
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (threadIdx.x < 32) tc_dealloc(tmem, 64);
+    if (threadIdx.x < 32) tc_dealloc(tmem, 64 * kTcSub);
 }
 
 }  // namespace pt

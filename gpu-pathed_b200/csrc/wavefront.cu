@@ -923,26 +923,26 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2) k_guide_infer(FrameParams
     }
 }
 
-// Guide inference on the 5th-generation tensor cores: tiles of 128 queue slots, one thread
-// per slot; the network runs as tcgen05.mma into tensor memory (guide_tc.cuh). 128 registers
-// keep 4 CTAs (512 slots) resident per SM.
-__global__ void __launch_bounds__(kTcRows, 4) k_guide_infer_tc(FrameParams p, int depth) {
+// Guide inference on the 5th-generation tensor cores: tiles of 256 queue slots (two MMA
+// sub-tiles of 128), one thread per slot; the network runs as tcgen05.mma into tensor memory
+// (guide_tc.cuh). 128 registers keep 2 CTAs (512 slots) resident per SM.
+__global__ void __launch_bounds__(kTcThreads, 2) k_guide_infer_tc(FrameParams p, int depth) {
     extern __shared__ __align__(1024) uint8_t tsm[];
     TcSmem& s = *reinterpret_cast<TcSmem*>(tsm);
     const int count = p.counters->ray_count[depth];
-    const int tiles = (count + kTcRows - 1) / kTcRows;
+    const int tiles = (count + kTcThreads - 1) / kTcThreads;
     if ((int)blockIdx.x >= tiles) return;  // no work: skip the setup and the TMEM allocation
     const uint32_t tmem = tc_setup(s, p.gwpack, p.gwpack + kPackWords);
     uint32_t phase = 0;
     const PathQueue q = p.q[depth & 1];
     const int t = threadIdx.x;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int slot = tile * kTcRows + t;
+        const int slot = tile * kTcThreads + t;
         float x[kGuideIn];
         if (slot < count) guide_features(p, p.gframe, q.o[slot], q.d[slot], q.hit[slot], x);
         else
             for (int k = 0; k < kGuideIn; k++) x[k] = 0.f;
-        tc_store_input(s.a, t, x);
+        tc_store_input(s.a[tc_sub()], tc_row(), x);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -1122,7 +1122,7 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
             }
             if (p.guide_mode == 2 && d < p.max_depth - 1) {
                 if (!B && p.guide_tc)
-                    k_guide_infer_tc<<<p.num_sms * 4, kTcRows, sizeof(TcSmem), stream>>>(p, d);
+                    k_guide_infer_tc<<<p.num_sms * 2, kTcThreads, sizeof(TcSmem), stream>>>(p, d);
                 else
                     k_guide_infer<B><<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
                 mark(kStageGuide);
