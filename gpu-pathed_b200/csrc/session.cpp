@@ -667,7 +667,7 @@ int Session::set_launch(const pt_launch_config* c) {
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
         c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 4 || c->split_shade < 0 ||
-        c->split_shade > 2)
+        c->split_shade > 3)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
@@ -680,7 +680,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->sort_rays) shape_.sort_rays = c->sort_rays == 1 ? 1 : 0;
     if (c->refill_idle) shape_.refill_idle = c->refill_idle;
     if (c->speculate) shape_.speculate = speculate_bits(c->speculate);
-    if (c->split_shade) shape_.split_shade = c->split_shade == 1 ? 1 : 0;
+    if (c->split_shade) shape_.shade_kernel = c->split_shade == 1 ? kShadeClasses : c->split_shade == 2 ? kShadeAll128 : kShadeAll80;
     return PT_OK;
 }
 
@@ -695,7 +695,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->sort_rays = shape_.sort_rays ? 1 : 2;
     c->refill_idle = shape_.refill_idle;
     c->speculate = speculate_code(shape_.speculate);
-    c->split_shade = shape_.split_shade ? 1 : 2;
+    c->split_shade = shape_.shade_kernel == kShadeClasses ? 1 : shape_.shade_kernel == kShadeAll128 ? 2 : 3;
 }
 
 int Session::upload_materials() {
@@ -956,7 +956,7 @@ int Session::render_async(int spp) {
     p.renderer = renderer_;
     p.shape = shape_;
     p.shape.sort_materials = sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0);
-    p.class_mask = shape_.split_shade ? class_mask_ : 0;
+    p.class_mask = class_mask_;
     p.gframe = gframe_;  // scene bounds: guide encoding and ray-sort cells
     last_wave_paths_ = p.wave_pixels * spp;
     p.consistent_mis = consistent_mis_ || guiding_;
@@ -1241,7 +1241,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         shape_.sort_rays = c.rays;
         shape_.speculate = c.spec;
         wave_paths_ = c.wave;
-        shape_.split_shade = c.split;
+        shape_.shade_kernel = c.split;
         return PT_OK;
     };
     auto report = [&](const Cand& c) {
@@ -1252,7 +1252,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.sort_rays = c.rays ? 1 : 2;
         res.speculate = speculate_code(c.spec);
         res.wave_paths = c.wave;
-        res.split_shade = c.split ? 1 : 2;
+        res.split_shade = c.split == kShadeClasses ? 1 : c.split == kShadeAll128 ? 2 : 3;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1264,7 +1264,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 if (line.find(want) == std::string::npos) continue;
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
                        json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0),
-                       json_int(line, "wave_paths", wave_paths_), json_int(line, "split_shade", 1)};
+                       json_int(line, "wave_paths", wave_paths_), json_int(line, "shade_kernel", kShadeClasses)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1298,7 +1298,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
-              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.split_shade};
+              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.shade_kernel};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1331,10 +1331,14 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         c.sort = best.sort ? 0 : 1;
         if ((r = consider(c))) return r;
     }
-    if (best.sort && !guiding_) {  // the sorted shade stage as one kernel per class, or one for all
-        Cand c = best;
-        c.split = best.split ? 0 : 1;
-        if ((r = consider(c))) return r;
+    if (!guiding_) {  // the plain shade stage: per-class kernels (sorted frames), one kernel at 128 or 80 registers
+        const Cand base = best;
+        for (int k : {kShadeAll128, kShadeClasses, kShadeAll80})
+            if (k != base.split && (k != kShadeClasses || base.sort)) {
+                Cand c = base;
+                c.split = k;
+                if ((r = consider(c))) return r;
+            }
     }
     if (!batch && max_depth_ > 1) {
         Cand c = best;
@@ -1382,7 +1386,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         if (f) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
-                         "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"split_shade\": %d, "
+                         "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"shade_kernel\": %d, "
                          "\"ms\": %.4f, \"default_ms\": %.4f}\n",
                          key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, best.wave,
                          best.split, best_ms, res.default_ms);

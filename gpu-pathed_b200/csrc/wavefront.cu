@@ -56,11 +56,33 @@ __device__ __forceinline__ int warp_append(int* counter, bool want) {
     return want ? base + __popc(mask & lanemask_lt()) : -1;
 }
 
-// Persistent work fetch: one atomic per warp for 32 consecutive items.
-__device__ __forceinline__ int warp_fetch(int* cursor) {
+// Persistent work fetch: one atomic per warp for n (default 32) consecutive items.
+__device__ __forceinline__ int warp_fetch(int* cursor, int n = 32) {
     int base = 0;
-    if ((threadIdx.x & 31) == 0) base = atomicAdd(cursor, 32);
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(cursor, n);
     return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// Warp-aggregated append of up to N items per lane with one atomic per warp: slot[k] is the
+// slot of the lane's k-th item when want[k], -1 otherwise.
+template <int N>
+__device__ __forceinline__ void warp_append_n(int* counter, const bool (&want)[N], int (&slot)[N]) {
+    unsigned m[N];
+    int total = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        m[k] = __ballot_sync(0xffffffffu, want[k]);
+        total += __popc(m[k]);
+    }
+    int base = 0;
+    if (total > 0 && (threadIdx.x & 31) == 0) base = atomicAdd(counter, total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        slot[k] = want[k] ? base + __popc(m[k] & lt) : -1;
+        base += __popc(m[k]);
+    }
 }
 
 __device__ __forceinline__ int tag_path(int tag) { return tag & kTagPathMask; }
@@ -501,7 +523,9 @@ __host__ __device__ constexpr int shade_class_regs(int cls) { return cls == kMic
 // CLS: -1, every slot of the queue (in material-sorted order when sorting is on); >= 0, only
 // the slots the sort put in material class CLS (0 miss, type + 1 otherwise), with that
 // class's BSDF fixed at compile time, so each class kernel holds only its own registers.
-template <bool GUIDE, bool B, int CLS>
+// IPL items per lane per warp iteration: one fetch and one append atomic per warp serve
+// 32 x IPL items (the queue counters are single addresses every warp of the grid hits).
+template <bool GUIDE, bool B, int CLS, int IPL>
 __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long long wave_first, long long gfirst) {
     constexpr int kType = CLS > 0 ? CLS - 1 : -1;  // the material type of a class kernel
     int count = p.counters->ray_count[depth];
@@ -524,9 +548,14 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
         __syncthreads();
     }
     for (;;) {
-        const int base = warp_fetch(work);
+        const int base = warp_fetch(work, 32 * IPL);
         if (base >= count) break;
-        const int i = base + (threadIdx.x & 31);
+        bool cont_[IPL], shadow_[IPL];
+        float4 co_[IPL], cd_[IPL], cb_[IPL], so_[IPL], sd_[IPL], sc_[IPL];
+        uint2 crng_[IPL];
+#pragma unroll
+        for (int item = 0; item < IPL; item++) {
+        const int i = base + 32 * item + (threadIdx.x & 31);
         bool cont = false, shadow = false, record = false;
         float4 co, cd, cb, so, sd, sc4;
         uint2 crng;
@@ -699,23 +728,40 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
             const int r = warp_append(p.grec_count, record);
             if (record && r < p.grec_cap) p.grec[r] = rec;
         }
-        const int cslot = warp_append(&p.counters->ray_count[depth + 1], cont);
-        if (cont) {
-            qn.o[cslot] = co;
-            qn.d[cslot] = cd;
-            qn.beta[cslot] = cb;
-            qn.rng[cslot] = crng;
+        cont_[item] = cont;
+        shadow_[item] = shadow;
+        co_[item] = co;
+        cd_[item] = cd;
+        cb_[item] = cb;
+        crng_[item] = crng;
+        so_[item] = so;
+        sd_[item] = sd;
+        sc_[item] = sc4;
+        }
+        int cslot[IPL], sslot[IPL];
+        warp_append_n<IPL>(&p.counters->ray_count[depth + 1], cont_, cslot);
+#pragma unroll
+        for (int item = 0; item < IPL; item++) {
+            if (!cont_[item]) continue;
+            const int cs = cslot[item];
+            qn.o[cs] = co_[item];
+            qn.d[cs] = cd_[item];
+            qn.beta[cs] = cb_[item];
+            qn.rng[cs] = crng_[item];
             if (!B && rsort) {
-                const int key = ray_sort_key(p.gframe, co, cd);
-                qn.key[cslot] = key;
+                const int key = ray_sort_key(p.gframe, co_[item], cd_[item]);
+                qn.key[cs] = key;
                 atomicAdd(&rhist[key], 1);
             }
         }
-        const int sslot = warp_append(&p.counters->shadow_count[depth], shadow);
-        if (shadow) {
-            p.sq.o[sslot] = so;
-            p.sq.d[sslot] = sd;
-            p.sq.c[sslot] = sc4;
+        warp_append_n<IPL>(&p.counters->shadow_count[depth], shadow_, sslot);
+#pragma unroll
+        for (int item = 0; item < IPL; item++) {
+            if (!shadow_[item]) continue;
+            const int ss = sslot[item];
+            p.sq.o[ss] = so_[item];
+            p.sq.d[ss] = sd_[item];
+            p.sq.c[ss] = sc_[item];
         }
     }
     if (!B && rsort) {
@@ -730,14 +776,30 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
 template <bool GUIDE, bool B>
 __global__ void __launch_bounds__(GUIDE ? kShadeGuidedBlock : 512, GUIDE ? kShadeGuidedBlocksPerSm : 1)
     k_shade(FrameParams p, int depth, long long wave_first, long long gfirst) {
-    shade_body<GUIDE, B, -1>(p, depth, wave_first, gfirst);
+    shade_body<GUIDE, B, -1, 1>(p, depth, wave_first, gfirst);
+}
+
+// Items per lane of the plain shade kernels. 2 and 4 (one fetch and one append atomic per
+// 64 or 128 items) measured slower on every configuration: the extra live state costs more
+// warps than the contended queue counters do.
+constexpr int kShadeIpl = 1;
+// The plain shade stage over every slot of the queue (all materials) at a register budget
+// of REGS: 128 (16 warps per SM at 128-thread blocks) or 80 (24 warps, with spills), the
+// autotuner's choice per scene (the icosphere shaded 16% faster at 80, the spheres 7% slower).
+template <bool B, int REGS>
+__global__ void __maxnreg__(REGS) k_shade_all(FrameParams p, int depth, long long wave_first, long long gfirst) {
+    shade_body<false, B, -1, kShadeIpl>(p, depth, wave_first, gfirst);
+}
+__host__ __device__ constexpr int shade_resident(int regs, int block) {
+    return 65536 / (regs * block) < 2048 / block ? (65536 / (regs * block) > 0 ? 65536 / (regs * block) : 1)
+                                                 : 2048 / block;
 }
 
 // The shade stage over one material class of a sorted queue (plain frames).
 template <bool B, int CLS>
 __global__ void __maxnreg__(shade_class_regs(CLS)) k_shade_class(FrameParams p, int depth, long long wave_first,
                                                                 long long gfirst) {
-    shade_body<false, B, CLS>(p, depth, wave_first, gfirst);
+    shade_body<false, B, CLS, kShadeIpl>(p, depth, wave_first, gfirst);
 }
 
 template <int W, bool CNT, bool B, int Q>
@@ -1130,10 +1192,14 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
             if (p.guide_mode)
                 k_shade<true, B><<<p.num_sms * kShadeGuidedBlocksPerSm, kShadeGuidedBlock, 0, stream>>>(
                     p, d, wave_first, w.guided_first);
-            else if (p.shape.sort_materials && p.class_mask)
+            else if (p.shape.shade_kernel == kShadeClasses && p.shape.sort_materials && p.class_mask)
                 e = enqueue_class_shades<B>(p, d, wave_first, w.guided_first, stream);
+            else if (p.shape.shade_kernel == kShadeAll80)
+                k_shade_all<B, 80><<<p.num_sms * shade_resident(80, p.shape.block_shade), p.shape.block_shade, 0,
+                                     stream>>>(p, d, wave_first, w.guided_first);
             else
-                k_shade<false, B><<<p.num_sms * 4, p.shape.block_shade, 0, stream>>>(p, d, wave_first, w.guided_first);
+                k_shade_all<B, 128><<<p.num_sms * shade_resident(128, p.shape.block_shade), p.shape.block_shade, 0,
+                                      stream>>>(p, d, wave_first, w.guided_first);
             if (e != cudaSuccess) return e;
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {

@@ -84,8 +84,12 @@ struct LaunchShape {
     int sort_rays = 0;        // continuation rays extended in (origin cell, direction octant) order
     int refill_idle = 16;     // traversal stages: a warp fetches new rays once this many lanes are idle
     int speculate = 0;        // kSpeculate* bits: stages that park a lane's first leaf and descend on
-    int split_shade = 1;      // material-sorted plain frames: one shade kernel per material class
+    int shade_kernel = 1;     // plain frames' shade stage: kShadeAll128, kShadeClasses, kShadeAll80
 };
+
+constexpr int kShadeAll128 = 0;  // one kernel for all materials, 128 registers
+constexpr int kShadeClasses = 1; // material-sorted frames: one kernel per material class present
+constexpr int kShadeAll80 = 2;   // one kernel for all materials, 80 registers
 
 constexpr int kSpeculateExtend = 1;  // closest-hit stage
 constexpr int kSpeculateShadow = 2;  // shadow (any-hit) stage

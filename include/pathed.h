@@ -122,9 +122,11 @@ typedef struct pt_launch_config {
                               descending while other lanes of its warp search for one):
                               1 closest-hit and shadow stages, 2 off (default), 3 closest-hit
                               stage only, 4 shadow stage only */
-    int split_shade;       /* material-sorted frames without guiding: 1 one shade kernel per
-                              material class present, each compiled for its BSDF only (default),
-                              2 one kernel for all materials; images are the same either way */
+    int split_shade;       /* the shade stage of frames without guiding: 1 one kernel per material
+                              class present, each compiled for its BSDF only (material-sorted
+                              frames; default), 2 one kernel for all materials at 128 registers,
+                              3 the same at 80 registers (more resident warps, some spills);
+                              images are the same either way */
 } pt_launch_config;
 
 /* Result of pt_autotune. */
@@ -140,7 +142,8 @@ typedef struct pt_tune_result {
     int from_cache;
     int sort_rays;          /* 1 on, 2 off */
     int speculate;          /* as pt_launch_config.speculate: 1 both stages, 2 off, 3 closest hit, 4 shadow */
-    int split_shade;        /* as pt_launch_config.split_shade: 1 one shade kernel per material class, 2 one */
+    int split_shade;        /* as pt_launch_config.split_shade: 1 per-class kernels, 2 one kernel (128
+                               registers), 3 one kernel (80 registers) */
 } pt_tune_result;
 
 typedef struct pt_stats {
