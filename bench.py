@@ -316,7 +316,7 @@ def _count_frame(s, spp):
     return prof, st
 
 
-def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs, sm_mhz):
+def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs, sm_mhz, shape=None):
     """Roofline of the closest-hit stage (k_extend) on the bound its scene sets:
       issue  nodes + leaf entries fit in L1 (a few KB): warp instructions issued per second
              (ncu's instructions per query x queries per launch / live launch time) against
@@ -343,16 +343,18 @@ def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, 
             "avg_launch_ms": ext_ms, "queries_per_launch": queries_per_launch,
             "nodes_per_query": nodes / max(1, q_ext), "prims_per_query": prims / max(1, q_ext),
             "hbm_frac": bytes_gbs / hbm}
+    # instruction counts are measured per BVH shape: none for a shape without a capture
+    ipq = _ncu_per_query(f"{workload}@{shape}", "warp_inst_per_query", "k_extend_issue.txt") if shape else None
+    clk = sm_mhz or 1965.0
+    issue_peak = ISSUE_SLOTS_PER_CYCLE * clk * 1e6 / 1e9  # G warp instructions / s
+    issue_achieved = None if ipq is None else ipq * queries_per_launch / (ext_ms / 1e3) / 1e9
     if bound == "issue":
-        ipq = _ncu_per_query(workload, "warp_inst_per_query", "k_extend_issue.txt")
-        fpq = _ncu_per_query(workload, "fp32_flop_per_query", "k_extend_issue.txt")
-        clk = sm_mhz or 1965.0
-        peak = ISSUE_SLOTS_PER_CYCLE * clk * 1e6 / 1e9  # G warp instructions / s
-        achieved = None if ipq is None else ipq * queries_per_launch / (ext_ms / 1e3) / 1e9
-        roof.update({"achieved": achieved, "peak": peak, "unit": "G warp-inst/s",
-                     "frac": None if achieved is None else achieved / peak,
+        fpq = _ncu_per_query(f"{workload}@{shape}", "fp32_flop_per_query", "k_extend_issue.txt") if shape else None
+        roof.update({"achieved": issue_achieved, "peak": issue_peak, "unit": "G warp-inst/s",
+                     "frac": None if issue_achieved is None else issue_achieved / issue_peak,
                      "peak_source": f"4 x 148 issue slots per cycle at {clk:.0f} MHz (median SM clock, timed region)",
-                     "inst_source": "ncu smsp__inst_executed.sum per query (profiles/k_extend_issue.txt)"})
+                     "inst_source": f"ncu smsp__inst_executed.sum per query at shape {shape} "
+                                    "(profiles/k_extend_issue.txt)" if ipq else f"no capture at shape {shape}"})
         if fpq is not None:
             tflops = fpq * queries_per_launch / (ext_ms / 1e3) / 1e12
             fp_peak = 148 * 128 * 2 * clk * 1e6 / 1e12
@@ -365,6 +367,12 @@ def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, 
     else:
         roof.update({"achieved": bytes_gbs, "peak": hbm, "unit": "GB/s", "frac": bytes_gbs / hbm,
                      "peak_source": peak_kind + " hbm_gbs (burst copy)"})
+    if bound != "issue" and issue_achieved is not None:
+        # most node and leaf bytes of the mesh scenes hit L1: the issue rate beside the bytes
+        roof["issue_slots"] = {"achieved": issue_achieved, "peak": issue_peak, "unit": "G warp-inst/s",
+                               "frac": issue_achieved / issue_peak,
+                               "inst_source": f"ncu smsp__inst_executed.sum per query at shape {shape} "
+                                              "(profiles/k_extend_issue.txt)"}
     roof["stage_ms_per_step"] = {k: v / steps for k, v in stage_ms.items()}
     roof["stage_share"] = {k: v / max(1e-9, sum(stage_ms.values())) for k, v in stage_ms.items()}
     return roof
@@ -432,9 +440,10 @@ def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
            "ms_per_step": dev_ms / steps, "steps": steps, "warmup": warmup, "triangles": counts.num_triangles,
            "spheres": counts.num_spheres,
            "autotuned": {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays", "speculate",
-                                                "blocks_per_sm", "block", "wave_paths", "split_shade")},
+                                                "blocks_per_sm", "block", "wave_paths", "split_shade", "max_leaf")},
            "roofline": _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs,
-                                 None)}
+                                 None, extend_shape_key(counts.bvh_width, counts.bvh_max_leaf,
+                                                        tuned["speculate"]))}
     if with_reference:
         try:
             ref = _reference_cuda_config(cfg, rays / max(1, paths))
@@ -558,7 +567,8 @@ def run_ours(args):
     roof = None
     if rank == 0:
         roof = _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, args.steps, l2_gbs,
-                         clk.get("sm_mhz"))
+                         clk.get("sm_mhz"), extend_shape_key(counts.bvh_width, counts.bvh_max_leaf,
+                                                             s.get_launch()["speculate"]))
         roof["l2_probe"] = {"gbs": l2_gbs, "ms": l2_ms, "bytes": L2_PROBE_BYTES}
 
     cpu = None
@@ -609,7 +619,7 @@ def run_ours(args):
         if tuned is not None:
             line["config"]["autotuned"] = {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays",
                                                                "speculate", "blocks_per_sm", "block", "wave_paths",
-                                                               "split_shade", "best_ms", "default_ms")}
+                                                               "split_shade", "max_leaf", "best_ms", "default_ms")}
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:
@@ -843,6 +853,12 @@ def batch_time_to_relmse(budget_frames=16, ref_frames=128, draw=0x5EED + 4, n=48
             **out}
 
 
+def extend_shape_key(width, leaf, speculate_code):
+    """The closest-hit stage's shape as the instruction counts are keyed: BVH width, leaf
+    size and whether its speculation is on (speculate codes 1 and 3)."""
+    return f"w{width}_l{leaf}_s{1 if speculate_code in (1, 3) else 0}"
+
+
 def _ncu_per_query(workload, field, fname="k_extend_traffic.txt"):
     """A per-closest-hit-query figure that ncu measured on this workload (profiles/<fname>,
     one `<workload> <field>: value` line each), or None."""
@@ -873,13 +889,21 @@ def ncu_frames(args):
     spp = args.spp or wl["spp"]
     s = pathed.Session(w, h)
     s.load_config(args.config)
+    if args.tune_cache:  # the shape a benchmark run chose (read from its cache, no measuring)
+        s.autotune(spp, args.tune_cache)
+    if args.bvh:
+        s.set_bvh(args.bvh[0], args.bvh[1])
+    if args.speculate:
+        s.set_launch(speculate=args.speculate)
     if args.sort_rays:
         s.set_launch(sort_rays=1 if args.sort_rays == "on" else 2)
     s.set_profiling(stage_timing=True, work_counters=False)  # direct launches, counted per stage
     for _ in range(args.ncu_frames):
         s.render(spp)
         st = s.stats()
+        lc = s.get_launch()
         print(json.dumps({"workload": wl["name"], "resolution": [w, h], "spp": spp,
+                          "shape": extend_shape_key(s.counts().bvh_width, s.counts().bvh_max_leaf, lc["speculate"]),
                           "rays_extend": st["rays_extend"], "rays_shadow": st["rays_shadow"],
                           "extend_launches": s.profile()["stage_launches"]["extend"]}), flush=True)
     s.close()
@@ -948,6 +972,10 @@ def main():
                     help="profiling aid: load the configuration (at --res if given), render this many frames "
                          "with the default launch shape, print their closest-hit query counts and exit")
     ap.add_argument("--res", type=int, nargs=2, default=None, help="with --ncu-frames: width height")
+    ap.add_argument("--bvh", type=int, nargs=2, default=None, metavar=("WIDTH", "LEAF"),
+                    help="with --ncu-frames: BVH width and primitives per leaf")
+    ap.add_argument("--speculate", type=int, default=0,
+                    help="with --ncu-frames: pt_launch_config.speculate (1 both, 2 off, 3 closest hit, 4 shadow)")
     ap.add_argument("--ncu-train", type=int, default=0,
                     help="profiling aid: this many guide-gradient calls of 2^16 seeded samples on the mma.sync "
                          "training kernel, then as many on the tcgen05 kernel; prints their wall ms and exits")

@@ -1230,11 +1230,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     // paths of one frame: waves smaller than this split the frame
     const long long frame_paths = batch ? batch_paths_ : (long long)w_ * h_ * spp;
     struct Cand {
-        int width, sort, bps, block, rays, spec, wave, split;
+        int width, sort, bps, block, rays, spec, wave, split, leaf;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
-        if (c.width != bvh_width_ && (r = set_bvh(c.width, bvh_leaf_))) return r;
+        if ((c.width != bvh_width_ || c.leaf != bvh_leaf_) && (r = set_bvh(c.width, c.leaf))) return r;
         sort_mode_ = c.sort;
         shape_.blocks_per_sm = c.bps;
         shape_.block_extend = shape_.block_shadow = c.block;
@@ -1253,6 +1253,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.speculate = speculate_code(c.spec);
         res.wave_paths = c.wave;
         res.split_shade = c.split == kShadeClasses ? 1 : c.split == kShadeAll128 ? 2 : 3;
+        res.max_leaf = c.leaf;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1264,7 +1265,8 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 if (line.find(want) == std::string::npos) continue;
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
                        json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0),
-                       json_int(line, "wave_paths", wave_paths_), json_int(line, "shade_kernel", kShadeClasses)};
+                       json_int(line, "wave_paths", wave_paths_), json_int(line, "shade_kernel", kShadeClasses),
+                       json_int(line, "max_leaf", bvh_leaf_)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1298,7 +1300,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
-              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.shade_kernel};
+              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.shade_kernel, bvh_leaf_};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1326,6 +1328,15 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
             c.width = widths[i];
             if ((r = consider(c))) return r;
         }
+    if (!batch) {  // primitives per leaf (each a rebuild of the tree)
+        const int start_leaf = best.leaf;
+        for (int lf : {2, 4, 8})
+            if (lf != start_leaf) {
+                Cand c = best;
+                c.leaf = lf;
+                if ((r = consider(c))) return r;
+            }
+    }
     if (material_classes_ >= 2) {
         Cand c = best;
         c.sort = best.sort ? 0 : 1;
@@ -1387,9 +1398,9 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
                          "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"shade_kernel\": %d, "
-                         "\"ms\": %.4f, \"default_ms\": %.4f}\n",
+                         "\"max_leaf\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
                          key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, best.wave,
-                         best.split, best_ms, res.default_ms);
+                         best.split, best.leaf, best_ms, res.default_ms);
             std::fclose(f);
         }
     }

@@ -126,7 +126,7 @@ class GuideInfo(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("bvh_width", "sort_materials", "blocks_per_sm", "block", "wave_paths")] + \
                [("best_ms", C.c_float), ("default_ms", C.c_float), ("trials", C.c_int), ("from_cache", C.c_int),
-                ("sort_rays", C.c_int), ("speculate", C.c_int), ("split_shade", C.c_int)]
+                ("sort_rays", C.c_int), ("speculate", C.c_int), ("split_shade", C.c_int), ("max_leaf", C.c_int)]
 
 
 class BatchScene(C.Structure):
