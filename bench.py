@@ -343,18 +343,22 @@ def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, 
             "avg_launch_ms": ext_ms, "queries_per_launch": queries_per_launch,
             "nodes_per_query": nodes / max(1, q_ext), "prims_per_query": prims / max(1, q_ext),
             "hbm_frac": bytes_gbs / hbm}
-    # instruction counts are measured per BVH shape: none for a shape without a capture
-    ipq = _ncu_per_query(f"{workload}@{shape}", "warp_inst_per_query", "k_extend_issue.txt") if shape else None
+    # instruction counts are measured per BVH shape; a shape without a capture takes the
+    # nearest captured one, named in inst_source
+    ipq, ishape = _ncu_shape_per_query(workload, shape, "warp_inst_per_query")
+    inst_src = (None if ipq is None else f"ncu smsp__inst_executed.sum per query at shape {ishape}"
+                + ("" if ishape == shape else f" (nearest capture; this run's shape is {shape})")
+                + " (profiles/k_extend_issue.txt)")
     clk = sm_mhz or 1965.0
     issue_peak = ISSUE_SLOTS_PER_CYCLE * clk * 1e6 / 1e9  # G warp instructions / s
     issue_achieved = None if ipq is None else ipq * queries_per_launch / (ext_ms / 1e3) / 1e9
     if bound == "issue":
-        fpq = _ncu_per_query(f"{workload}@{shape}", "fp32_flop_per_query", "k_extend_issue.txt") if shape else None
+        fpq, _ = _ncu_shape_per_query(workload, shape, "fp32_flop_per_query")
         roof.update({"achieved": issue_achieved, "peak": issue_peak, "unit": "G warp-inst/s",
                      "frac": None if issue_achieved is None else issue_achieved / issue_peak,
                      "peak_source": f"4 x 148 issue slots per cycle at {clk:.0f} MHz (median SM clock, timed region)",
-                     "inst_source": f"ncu smsp__inst_executed.sum per query at shape {shape} "
-                                    "(profiles/k_extend_issue.txt)" if ipq else f"no capture at shape {shape}"})
+                     "inst_source": inst_src or f"no capture for this workload (shape {shape})",
+                     "inst_shape_exact": ishape == shape})
         if fpq is not None:
             tflops = fpq * queries_per_launch / (ext_ms / 1e3) / 1e12
             fp_peak = 148 * 128 * 2 * clk * 1e6 / 1e12
@@ -370,9 +374,8 @@ def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, 
     if bound != "issue" and issue_achieved is not None:
         # most node and leaf bytes of the mesh scenes hit L1: the issue rate beside the bytes
         roof["issue_slots"] = {"achieved": issue_achieved, "peak": issue_peak, "unit": "G warp-inst/s",
-                               "frac": issue_achieved / issue_peak,
-                               "inst_source": f"ncu smsp__inst_executed.sum per query at shape {shape} "
-                                              "(profiles/k_extend_issue.txt)"}
+                               "frac": issue_achieved / issue_peak, "inst_source": inst_src,
+                               "inst_shape_exact": ishape == shape}
     roof["stage_ms_per_step"] = {k: v / steps for k, v in stage_ms.items()}
     roof["stage_share"] = {k: v / max(1e-9, sum(stage_ms.values())) for k, v in stage_ms.items()}
     return roof
@@ -434,6 +437,7 @@ def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
     for _ in range(warmup):
         s.render(wl["spp"])
     dev_ms, rays, paths, stage_ms, stage_launches = _time_frames(s, wl["spp"], steps, flush)
+    shape = extend_shape_key(counts.bvh_width, counts.bvh_max_leaf, s.get_launch())
     s.close()
     out = {"workload": wl["name"], "resolution": [w, h], "spp": wl["spp"], "max_depth": wl["depth"],
            "value": rays / (dev_ms / 1e3) / 1e6, "unit": "Mrays/s", "mpaths_per_s": paths / (dev_ms / 1e3) / 1e6,
@@ -442,8 +446,7 @@ def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
            "autotuned": {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays", "speculate",
                                                 "blocks_per_sm", "block", "wave_paths", "split_shade", "max_leaf")},
            "roofline": _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs,
-                                 None, extend_shape_key(counts.bvh_width, counts.bvh_max_leaf,
-                                                        tuned["speculate"]))}
+                                 None, shape)}
     if with_reference:
         try:
             ref = _reference_cuda_config(cfg, rays / max(1, paths))
@@ -567,8 +570,7 @@ def run_ours(args):
     roof = None
     if rank == 0:
         roof = _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, args.steps, l2_gbs,
-                         clk.get("sm_mhz"), extend_shape_key(counts.bvh_width, counts.bvh_max_leaf,
-                                                             s.get_launch()["speculate"]))
+                         clk.get("sm_mhz"), extend_shape_key(counts.bvh_width, counts.bvh_max_leaf, s.get_launch()))
         roof["l2_probe"] = {"gbs": l2_gbs, "ms": l2_ms, "bytes": L2_PROBE_BYTES}
 
     cpu = None
@@ -853,10 +855,15 @@ def batch_time_to_relmse(budget_frames=16, ref_frames=128, draw=0x5EED + 4, n=48
             **out}
 
 
-def extend_shape_key(width, leaf, speculate_code):
-    """The closest-hit stage's shape as the instruction counts are keyed: BVH width, leaf
-    size and whether its speculation is on (speculate codes 1 and 3)."""
-    return f"w{width}_l{leaf}_s{1 if speculate_code in (1, 3) else 0}"
+def extend_shape_key(width, leaf, launch):
+    """The closest-hit stage's shape as the instruction counts are keyed: BVH width, largest
+    leaf, whether its speculation is on (speculate codes 1 and 3), its grid (blocks per SM x
+    threads per block) and the wave size (log2 of the paths per wave). The lane-refill
+    traversal's instructions per query depend on all of them: the grid and the wave set how
+    full the warps' lanes stay."""
+    sp = 1 if launch["speculate"] in (1, 3) else 0
+    q = max(0, int(launch["wave_paths"]).bit_length() - 1)
+    return f"w{width}_l{leaf}_s{sp}_b{launch['blocks_per_sm']}x{launch['block_extend']}_q{q}"
 
 
 def _ncu_per_query(workload, field, fname="k_extend_traffic.txt"):
@@ -872,6 +879,42 @@ def _ncu_per_query(workload, field, fname="k_extend_traffic.txt"):
     except OSError:
         pass
     return None
+
+
+def _ncu_shape_per_query(workload, shape, field):
+    """`field` of profiles/k_extend_issue.txt measured at `shape` on this workload, else at the
+    nearest captured shape: same BVH width first, then the same speculation, the closest leaf
+    size, the same grid and the closest wave size. Returns (value, captured shape) or
+    (None, None)."""
+    p = os.path.join(ROOT, "profiles", "k_extend_issue.txt")
+    found = {}
+    try:
+        with open(p) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and parts[1] == field + ":" and parts[0].startswith(workload + "@"):
+                    found[parts[0].split("@", 1)[1]] = float(parts[2])
+    except OSError:
+        return None, None
+    if not found or not shape:
+        return None, None
+    if shape in found:
+        return found[shape], shape
+
+    def parse(k):
+        f = k.split("_")
+        grid = f[3] if len(f) > 3 else ""
+        wave = int(f[4][1:]) if len(f) > 4 else 0
+        return int(f[0][1:]), int(f[1][1:]), int(f[2][1:]), grid, wave
+
+    tw, tl, ts, tg, tq = parse(shape)
+
+    def distance(k):
+        w, l, sp, g, q = parse(k)
+        return (w != tw, sp != ts, abs(l - tl), g != tg, abs(q - tq), k)
+
+    best = min(found, key=distance)
+    return found[best], best
 
 
 def _ncu_bytes_per_query(workload):
@@ -903,7 +946,7 @@ def ncu_frames(args):
         st = s.stats()
         lc = s.get_launch()
         print(json.dumps({"workload": wl["name"], "resolution": [w, h], "spp": spp,
-                          "shape": extend_shape_key(s.counts().bvh_width, s.counts().bvh_max_leaf, lc["speculate"]),
+                          "shape": extend_shape_key(s.counts().bvh_width, s.counts().bvh_max_leaf, lc),
                           "rays_extend": st["rays_extend"], "rays_shadow": st["rays_shadow"],
                           "extend_launches": s.profile()["stage_launches"]["extend"]}), flush=True)
     s.close()

@@ -156,15 +156,56 @@ __device__ __forceinline__ RayPre make_raypre(V o, V d) {
     return r;
 }
 
-// Slab test; returns the entry distance or +inf when the interval is empty.
-__device__ __forceinline__ float box_entry(const RayPre& r, float lx, float hx, float ly, float hy,
-                                           float lz, float hz, float tmin, float tlim) {
+// Slab test: the entry and exit distances of the box clipped to [tmin, tlim]; the box is
+// visited when tn <= tf * kBoxSlack.
+__device__ __forceinline__ void box_interval(const RayPre& r, float lx, float hx, float ly, float hy, float lz,
+                                             float hz, float tmin, float tlim, float& tn, float& tf) {
     const float t0x = fmaf(lx, r.ix, -r.ox), t1x = fmaf(hx, r.ix, -r.ox);
     const float t0y = fmaf(ly, r.iy, -r.oy), t1y = fmaf(hy, r.iy, -r.oy);
     const float t0z = fmaf(lz, r.iz, -r.oz), t1z = fmaf(hz, r.iz, -r.oz);
-    const float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), tmin));
-    const float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tlim));
+    tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), tmin));
+    tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tlim));
+}
+// Slab test; returns the entry distance or +inf when the interval is empty.
+__device__ __forceinline__ float box_entry(const RayPre& r, float lx, float hx, float ly, float hy,
+                                           float lz, float hz, float tmin, float tlim) {
+    float tn, tf;
+    box_interval(r, lx, hx, ly, hy, lz, hz, tmin, tlim, tn, tf);
     return (tn <= tf * kBoxSlack) ? tn : __int_as_float(0x7f800000);
+}
+
+// Children are ordered by an integer sort key: the entry distance, clamped at zero, with its
+// three low bits replaced by the child's slot (the slot breaks ties and travels with the
+// key), or kMissKey | slot for a child that was not hit. Keys of hit children are below
+// kMissKey, and for non-negative floats the bit patterns order like the values, so sorting the
+// keys orders the children by their distance bucket key_dist(tn) (tn with the three low bits
+// cleared: 8 ulp wide), nearest first.
+constexpr uint32_t kMissKey = 0x7f800000u;
+__device__ __forceinline__ float key_dist(float tn) { return __uint_as_float(__float_as_uint(fmaxf(tn, 0.f)) & ~7u); }
+__device__ __forceinline__ void key_order(uint32_t& a, uint32_t& b) {
+    const uint32_t lo = min(a, b);
+    b = max(a, b);
+    a = lo;
+}
+// Ascending sort of W keys by size-optimal sorting networks (1, 5 and 19 comparators; Knuth,
+// TAOCP vol. 3, 5.3.4).
+template <int W>
+__device__ __forceinline__ void sort_keys(uint32_t (&k)[W]) {
+    if constexpr (W == 2) {
+        key_order(k[0], k[1]);
+    } else if constexpr (W == 4) {
+        key_order(k[0], k[1]); key_order(k[2], k[3]);
+        key_order(k[0], k[2]); key_order(k[1], k[3]);
+        key_order(k[1], k[2]);
+    } else {
+        static_assert(W == 8, "BVH width 2, 4 or 8");
+        key_order(k[0], k[2]); key_order(k[1], k[3]); key_order(k[4], k[6]); key_order(k[5], k[7]);
+        key_order(k[0], k[4]); key_order(k[1], k[5]); key_order(k[2], k[6]); key_order(k[3], k[7]);
+        key_order(k[0], k[1]); key_order(k[2], k[3]); key_order(k[4], k[5]); key_order(k[6], k[7]);
+        key_order(k[2], k[4]); key_order(k[3], k[5]);
+        key_order(k[1], k[4]); key_order(k[3], k[6]);
+        key_order(k[1], k[2]); key_order(k[3], k[4]); key_order(k[5], k[6]);
+    }
 }
 
 // Closest-hit acceptance for one leaf entry (tie rules above). `tcur` is best.t or tmax.
@@ -285,8 +326,10 @@ struct TraceWork {
 // Next entry to process from the traversal stack, or kEmptyChild when it is empty.
 // Stack entry: x = node index, y = (remaining count << 24) | 3-bit child slots, nearest first;
 // the stack holds at most one entry per tree level. For closest-hit queries the popped child
-// is re-tested against the current hit distance; when it is culled, the siblings behind it
-// (sorted farther) are dropped with it.
+// is re-tested against the current hit distance. When it is culled, the siblings behind it are
+// dropped with it if its distance bucket already lies beyond the culling threshold: the
+// siblings' buckets are no nearer, so each of them would be culled by its own test. Otherwise
+// only the popped child is dropped and the next sibling is tested in turn.
 template <int W, bool ANY>
 __device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, bool quant, const RayPre& r, float tmin,
                                          float tmax, const Hit& best, int2* __restrict__ stk, int stride, int& sp) {
@@ -308,15 +351,16 @@ __device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, bool 
                 const uint32_t e = __float_as_uint(h.w);
                 const float sx = qscale(e), sy = qscale(e >> 8), sz = qscale(e >> 16);
                 const float tc = best.prim == kMissPrim ? tmax : best.t;
-                const float te = box_entry(
-                    r, __fmaf_rn((float)__ldg(b + 16 + 0 * W + sl), sx, h.x),
-                    __fmaf_rn((float)__ldg(b + 16 + 1 * W + sl), sx, h.x),
-                    __fmaf_rn((float)__ldg(b + 16 + 2 * W + sl), sy, h.y),
-                    __fmaf_rn((float)__ldg(b + 16 + 3 * W + sl), sy, h.y),
-                    __fmaf_rn((float)__ldg(b + 16 + 4 * W + sl), sz, h.z),
-                    __fmaf_rn((float)__ldg(b + 16 + 5 * W + sl), sz, h.z), tmin, tc * kBoxSlack);
-                if (te == __int_as_float(0x7f800000)) {
-                    if (cnt > 1) sp--;
+                float tn, tf;
+                box_interval(r, __fmaf_rn((float)__ldg(b + 16 + 0 * W + sl), sx, h.x),
+                             __fmaf_rn((float)__ldg(b + 16 + 1 * W + sl), sx, h.x),
+                             __fmaf_rn((float)__ldg(b + 16 + 2 * W + sl), sy, h.y),
+                             __fmaf_rn((float)__ldg(b + 16 + 3 * W + sl), sy, h.y),
+                             __fmaf_rn((float)__ldg(b + 16 + 4 * W + sl), sz, h.z),
+                             __fmaf_rn((float)__ldg(b + 16 + 5 * W + sl), sz, h.z), tmin, tc * kBoxSlack, tn, tf);
+                const float thr = tf * kBoxSlack;
+                if (!(tn <= thr)) {
+                    if (cnt > 1 && key_dist(tn) > fmaxf(thr, 0.f)) sp--;
                     continue;
                 }
             }
@@ -325,11 +369,13 @@ __device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, bool 
         const float* pf = reinterpret_cast<const float*>(nodes + (size_t)parent * kNF4);
         if (!ANY) {
             const float tc = best.prim == kMissPrim ? tmax : best.t;
-            const float te = box_entry(r, __ldg(pf + 0 * W + sl), __ldg(pf + 1 * W + sl), __ldg(pf + 2 * W + sl),
-                                       __ldg(pf + 3 * W + sl), __ldg(pf + 4 * W + sl), __ldg(pf + 5 * W + sl), tmin,
-                                       tc * kBoxSlack);
-            if (te == __int_as_float(0x7f800000)) {
-                if (cnt > 1) sp--;
+            float tn, tf;
+            box_interval(r, __ldg(pf + 0 * W + sl), __ldg(pf + 1 * W + sl), __ldg(pf + 2 * W + sl),
+                         __ldg(pf + 3 * W + sl), __ldg(pf + 4 * W + sl), __ldg(pf + 5 * W + sl), tmin, tc * kBoxSlack,
+                         tn, tf);
+            const float thr = tf * kBoxSlack;
+            if (!(tn <= thr)) {
+                if (cnt > 1 && key_dist(tn) > fmaxf(thr, 0.f)) sp--;
                 continue;
             }
         }
@@ -354,37 +400,26 @@ __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool
     if (CNT) work->nodes++;
     const float tcur = best.prim == kMissPrim ? tmax : best.t;
     const float tlim = tcur * kBoxSlack;
-    float key[W];
-    int slot[W];
+    // sort keys: nearest first for closest hit; for any hit, hit children first in slot order
+    uint32_t key[W];
     int nhit = 0;
 #pragma unroll
     for (int k = 0; k < W; k++) {
-        float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k], tmin, tlim);
-        if (nv.child[k] == kEmptyChild) te = __int_as_float(0x7f800000);
-        key[k] = te;
-        slot[k] = k;
-        nhit += te != __int_as_float(0x7f800000) ? 1 : 0;
+        const float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k], tmin, tlim);
+        const bool hit = te != __int_as_float(0x7f800000) && nv.child[k] != kEmptyChild;
+        if (ANY) key[k] = hit ? (uint32_t)k : kMissKey | (uint32_t)k;
+        else key[k] = hit ? (__float_as_uint(key_dist(te)) | (uint32_t)k) : kMissKey | (uint32_t)k;
+        nhit += hit ? 1 : 0;
     }
-    // odd-even transposition network: nearest first (closest hit) or hits first
-#pragma unroll
-    for (int pass = 0; pass < W; pass++) {
-#pragma unroll
-        for (int k = (pass & 1); k + 1 < W; k += 2) {
-            const bool swap = ANY ? (key[k] == __int_as_float(0x7f800000) && key[k + 1] != __int_as_float(0x7f800000))
-                                  : (key[k + 1] < key[k]);
-            if (swap) {
-                const float tk = key[k]; key[k] = key[k + 1]; key[k + 1] = tk;
-                const int ts = slot[k]; slot[k] = slot[k + 1]; slot[k + 1] = ts;
-            }
-        }
-    }
+    sort_keys<W>(key);
     int next = kEmptyChild;
     if (nhit > 0) {
         if (nhit > 1) {
+            // slots of the hit children after the nearest, nearest in the low bits (entries
+            // past nhit - 1 are never read)
             uint32_t list = 0;
 #pragma unroll
-            for (int k = W - 1; k >= 1; k--)
-                if (k < nhit) list = (list << 3) | (uint32_t)slot[k];
+            for (int k = W - 1; k >= 1; k--) list = (list << 3) | (key[k] & 7u);
             if (sp >= max_depth) {
                 overflow = 1;
                 alive = false;  // reported to the host; the query gives up
@@ -393,7 +428,7 @@ __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool
                 sp++;
             }
         }
-        const int sel = slot[0];
+        const int sel = (int)(key[0] & 7u);
 #pragma unroll
         for (int k = 0; k < W; k++)
             if (k == sel) next = nv.child[k];

@@ -85,6 +85,37 @@ __device__ __forceinline__ void warp_append_n(int* counter, const bool (&want)[N
     }
 }
 
+// Two warp-aggregated appends (counters ca and cb) whose atomics are both issued before
+// either result is read, so their round trips overlap.
+template <int N>
+__device__ __forceinline__ void warp_append_pair(int* ca, const bool (&wa)[N], int (&sa)[N], int* cb,
+                                                 const bool (&wb)[N], int (&sb)[N]) {
+    unsigned ma[N], mb[N];
+    int ta = 0, tb = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        ma[k] = __ballot_sync(0xffffffffu, wa[k]);
+        mb[k] = __ballot_sync(0xffffffffu, wb[k]);
+        ta += __popc(ma[k]);
+        tb += __popc(mb[k]);
+    }
+    int ba = 0, bb = 0;
+    if ((threadIdx.x & 31) == 0) {
+        if (ta > 0) ba = atomicAdd(ca, ta);
+        if (tb > 0) bb = atomicAdd(cb, tb);
+    }
+    ba = __shfl_sync(0xffffffffu, ba, 0);
+    bb = __shfl_sync(0xffffffffu, bb, 0);
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        sa[k] = wa[k] ? ba + __popc(ma[k] & lt) : -1;
+        sb[k] = wb[k] ? bb + __popc(mb[k] & lt) : -1;
+        ba += __popc(ma[k]);
+        bb += __popc(mb[k]);
+    }
+}
+
 __device__ __forceinline__ int tag_path(int tag) { return tag & kTagPathMask; }
 __device__ __forceinline__ int tag_scene(int tag) { return tag >> kTagPathBits; }
 
@@ -525,7 +556,12 @@ __host__ __device__ constexpr int shade_class_regs(int cls) { return cls == kMic
 // class's BSDF fixed at compile time, so each class kernel holds only its own registers.
 // IPL items per lane per warp iteration: one fetch and one append atomic per warp serve
 // 32 x IPL items (the queue counters are single addresses every warp of the grid hits).
-template <bool GUIDE, bool B, int CLS, int IPL>
+// AHEAD (kernels with registers to spare): the warp claims its next chunk while the current
+// one shades (lane 0's atomic is read at the top of the next iteration), loads a slot's
+// random state with its other records, and issues the continuation and shadow appends'
+// atomics together, so fewer global round trips are serialised per chunk. Under a tight
+// register budget the extra live values spill and the stage slows down.
+template <bool GUIDE, bool B, int CLS, int IPL, bool AHEAD = false>
 __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long long wave_first, long long gfirst) {
     constexpr int kType = CLS > 0 ? CLS - 1 : -1;  // the material type of a class kernel
     int count = p.counters->ray_count[depth];
@@ -547,9 +583,12 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
         for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x) rhist[j] = 0;
         __syncthreads();
     }
+    int claimed = 0;  // AHEAD: lane 0's claim of the warp's next chunk
+    if (AHEAD && (threadIdx.x & 31) == 0) claimed = atomicAdd(work, 32 * IPL);
     for (;;) {
-        const int base = warp_fetch(work, 32 * IPL);
+        const int base = AHEAD ? __shfl_sync(0xffffffffu, claimed, 0) : warp_fetch(work, 32 * IPL);
         if (base >= count) break;
+        if (AHEAD && (threadIdx.x & 31) == 0) claimed = atomicAdd(work, 32 * IPL);
         bool cont_[IPL], shadow_[IPL];
         float4 co_[IPL], cd_[IPL], cb_[IPL], so_[IPL], sd_[IPL], sc_[IPL];
         uint2 crng_[IPL];
@@ -566,6 +605,8 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
             const float4 d4 = q.d[slot];
             const float4 b4 = q.beta[slot];
             float4 h4 = q.hit[slot];
+            uint2 rng0 = make_uint2(0u, 0u);
+            if (AHEAD) rng0 = q.rng[slot];
             // a negative t: the BSDF-direct ray stopped closer (hitd), this is the continuation's hit
             const bool split = __float_as_int(h4.x) < 0;
             h4.x = fabsf(h4.x);
@@ -627,7 +668,8 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
                     const uint32_t pixel =
                         B ? (uint32_t)((gp - p.batch[sid].path_base) / p.batch[sid].spp) : (uint32_t)(gp / p.spp);
                     const uint64_t inc = pcg_inc(pixel);
-                    uint64_t st = ((uint64_t)q.rng[slot].y << 32) | q.rng[slot].x;
+                    if (!AHEAD) rng0 = q.rng[slot];
+                    uint64_t st = ((uint64_t)rng0.y << 32) | rng0.x;
                     const bool delta_mat = mtype == kMirror || mtype == kGlass;
                     const bool use_guide = guided && !delta_mat;
                     const float* mix = use_guide ? p.gmix + (size_t)slot * kGuideOut : nullptr;
@@ -739,7 +781,11 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
         sc_[item] = sc4;
         }
         int cslot[IPL], sslot[IPL];
-        warp_append_n<IPL>(&p.counters->ray_count[depth + 1], cont_, cslot);
+        if (AHEAD)
+            warp_append_pair<IPL>(&p.counters->ray_count[depth + 1], cont_, cslot, &p.counters->shadow_count[depth],
+                                  shadow_, sslot);
+        else
+            warp_append_n<IPL>(&p.counters->ray_count[depth + 1], cont_, cslot);
 #pragma unroll
         for (int item = 0; item < IPL; item++) {
             if (!cont_[item]) continue;
@@ -754,7 +800,7 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
                 atomicAdd(&rhist[key], 1);
             }
         }
-        warp_append_n<IPL>(&p.counters->shadow_count[depth], shadow_, sslot);
+        if (!AHEAD) warp_append_n<IPL>(&p.counters->shadow_count[depth], shadow_, sslot);
 #pragma unroll
         for (int item = 0; item < IPL; item++) {
             if (!shadow_[item]) continue;
@@ -788,7 +834,7 @@ constexpr int kShadeIpl = 1;
 // autotuner's choice per scene (the icosphere shaded 16% faster at 80, the spheres 7% slower).
 template <bool B, int REGS>
 __global__ void __maxnreg__(REGS) k_shade_all(FrameParams p, int depth, long long wave_first, long long gfirst) {
-    shade_body<false, B, -1, kShadeIpl>(p, depth, wave_first, gfirst);
+    shade_body<false, B, -1, kShadeIpl, REGS >= 128>(p, depth, wave_first, gfirst);
 }
 __host__ __device__ constexpr int shade_resident(int regs, int block) {
     return 65536 / (regs * block) < 2048 / block ? (65536 / (regs * block) > 0 ? 65536 / (regs * block) : 1)

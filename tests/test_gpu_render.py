@@ -160,6 +160,24 @@ def test_launch_shapes_do_not_change_images(sort, width):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("config", [2, 3])
+def test_leaf_sizes_do_not_change_images(config):
+    """the leaf sizes the autotuner picks from (2, 4, 8) change the tree, not the hits: with
+    the same launch shape the frames are bit-identical"""
+    s = pathed.Session(64, 64)
+    s.load_config(config, level=4)
+    imgs = []
+    for leaf in (2, 4, 8):
+        s.set_bvh(4, leaf)
+        assert s.counts().bvh_max_leaf <= leaf
+        s.reset()
+        s.render(2)
+        imgs.append(s.readback().copy())
+    s.close()
+    assert np.array_equal(imgs[0], imgs[1]) and np.array_equal(imgs[0], imgs[2])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", [(0, None), (1, None), (2, 4), (3, 4)], ids=lambda c: f"cfg{c[0]}")
 def test_ray_sorting_does_not_change_images(case):
     """sorting continuation rays by origin cell and octant reorders the closest-hit stage's
