@@ -280,30 +280,50 @@ def _reference_cuda(args, rays_per_path):
         return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
-def _time_frames(s, spp, steps, flush, barrier=None):
-    """Device time (CUDA events on the session's stream, summed) of `steps` frames with L2
-    flushed before each, the canonical rays and paths they traced, per-stage ms and launches."""
+def _time_frames(s, spp, steps, flush):
+    """Device time (CUDA events on the session's stream around each frame, summed) of `steps`
+    frames on the product path (graph replay, the shadow stages overlapped, no per-launch
+    events) with L2 flushed before each, and the canonical rays and paths they traced."""
+    import torch
+
+    s.set_profiling(stage_timing=False, work_counters=False)
+    dev_ms = 0.0
+    rays = paths = 0
+    for _ in range(steps):
+        flush.zero_()  # L2 flush between steps (outside the frame's events)
+        torch.cuda.synchronize()
+        dev_ms += s.render(spp)
+        st = s.stats()
+        rays += st["rays_extend"] + st["rays_shadow"]
+        paths += st["rays_camera"]
+    return dev_ms, rays, paths
+
+
+def _stage_frames(s, spp, steps, flush):
+    """Per-stage device time and launches of `steps` frames with an event after every launch,
+    all stages on one stream (a kernel's launch time is then its own, not shared with the
+    overlapped shadow stage), L2 flushed before each frame; the launch shape is restored."""
     import torch
 
     import pathed
 
-    dev_ms = 0.0
-    rays = paths = 0
+    overlap = s.get_launch()["overlap_shadow"]
+    s.set_launch(overlap_shadow=2)
+    s.set_profiling(stage_timing=True, work_counters=False)
+    s.render(spp)  # untimed: direct launches after the graph replays
     stage_ms = {k: 0.0 for k in pathed.STAGES}
     stage_launches = {k: 0 for k in pathed.STAGES}
     for _ in range(steps):
-        flush.zero_()  # L2 flush between steps (outside the frame's events)
+        flush.zero_()
         torch.cuda.synchronize()
-        ms = s.render(spp)
-        dev_ms += ms
-        st = s.stats()
-        rays += st["rays_extend"] + st["rays_shadow"]
-        paths += st["rays_camera"]
+        s.render(spp)
         p = s.profile()
         for k in pathed.STAGES:
             stage_ms[k] += p["stage_ms"][k]
             stage_launches[k] += p["stage_launches"][k]
-    return dev_ms, rays, paths, stage_ms, stage_launches
+    s.set_profiling(stage_timing=False, work_counters=False)
+    s.set_launch(overlap_shadow=overlap)
+    return stage_ms, stage_launches
 
 
 def _count_frame(s, spp):
@@ -376,6 +396,9 @@ def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, 
         roof["issue_slots"] = {"achieved": issue_achieved, "peak": issue_peak, "unit": "G warp-inst/s",
                                "frac": issue_achieved / issue_peak, "inst_source": inst_src,
                                "inst_shape_exact": ishape == shape}
+    roof["stage_timing"] = ("per-stage CUDA events of as many frames again, all stages on one stream, "
+                            "right after the timed frames (which overlap the shadow stage with the next "
+                            "depth's closest-hit stage on a second stream)")
     roof["stage_ms_per_step"] = {k: v / steps for k, v in stage_ms.items()}
     roof["stage_share"] = {k: v / max(1e-9, sum(stage_ms.values())) for k, v in stage_ms.items()}
     return roof
@@ -434,9 +457,11 @@ def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
     tuned = s.autotune(wl["spp"], tune_cache)
     counts = s.counts()
     prof_count, st_count = _count_frame(s, wl["spp"])
+    s.set_profiling(stage_timing=False, work_counters=False)  # warm-up on the timed path
     for _ in range(warmup):
         s.render(wl["spp"])
-    dev_ms, rays, paths, stage_ms, stage_launches = _time_frames(s, wl["spp"], steps, flush)
+    dev_ms, rays, paths = _time_frames(s, wl["spp"], steps, flush)
+    stage_ms, stage_launches = _stage_frames(s, wl["spp"], steps, flush)
     shape = extend_shape_key(counts.bvh_width, counts.bvh_max_leaf, s.get_launch())
     s.close()
     out = {"workload": wl["name"], "resolution": [w, h], "spp": wl["spp"], "max_depth": wl["depth"],
@@ -509,6 +534,7 @@ def run_ours(args):
 
     # one untimed frame with work counters for the algorithmic-bytes accounting
     prof_count, st_count = _count_frame(s, spp)
+    s.set_profiling(stage_timing=False, work_counters=False)  # warm-up on the timed path
     for _ in range(args.warmup):
         s.render(spp)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -523,9 +549,12 @@ def run_ours(args):
     clocks.wait_first()
     barrier()
     t_clk0 = time.time()
-    dev_ms, rays, paths, stage_ms, stage_launches = _time_frames(s, spp, args.steps, flush)
+    dev_ms, rays, paths = _time_frames(s, spp, args.steps, flush)
     barrier()
     clk = clocks.stop(t_clk0, time.time())
+    # per-stage times (the roofline's launch times and the stage breakdown): as many frames
+    # again with an event after every launch, on one stream
+    stage_ms, stage_launches = _stage_frames(s, spp, args.steps, flush)
     t_max, (rays_all, paths_all) = reduce_over_ranks(dev_ms, [rays, paths], world)
     value = rays_all / (t_max / 1e3) / 1e6
 

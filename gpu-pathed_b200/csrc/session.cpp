@@ -50,6 +50,14 @@ Session::~Session() {
         if (rb_done_) cudaEventDestroy(rb_done_);
         if (ev_begin_) cudaEventDestroy(ev_begin_);
         if (ev_end_) cudaEventDestroy(ev_end_);
+        if (side_stream_) {
+            cudaStreamSynchronize(side_stream_);
+            cudaStreamDestroy(side_stream_);
+        }
+        for (cudaEvent_t e : side_shaded_)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : side_shadowed_)
+            if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : mark_events_) cudaEventDestroy(e);
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         if (h_dyn_) cudaFreeHost(h_dyn_);
@@ -102,6 +110,17 @@ int Session::ensure_device() {
         return r;
     if ((r = check_cuda(cudaEventCreate(&ev_begin_), "cudaEventCreate"))) return r;
     if ((r = check_cuda(cudaEventCreate(&ev_end_), "cudaEventCreate"))) return r;
+    if ((r = check_cuda(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "cudaStreamCreate")))
+        return r;
+    side_shaded_.assign(kMaxDepthLimit, nullptr);
+    side_shadowed_.assign(kMaxDepthLimit, nullptr);
+    for (int d = 0; d < kMaxDepthLimit; d++) {
+        if ((r = check_cuda(cudaEventCreateWithFlags(&side_shaded_[d], cudaEventDisableTiming), "cudaEventCreate")))
+            return r;
+        if ((r = check_cuda(cudaEventCreateWithFlags(&side_shadowed_[d], cudaEventDisableTiming), "cudaEventCreate")))
+            return r;
+    }
+    side_ = SideStream{side_stream_, side_shaded_.data(), side_shadowed_.data()};
     if ((r = check_cuda(cudaMallocHost((void**)&h_stats_, sizeof(FrameStats)), "cudaMallocHost"))) return r;
     std::memset(h_stats_, 0, sizeof(FrameStats));
     if ((r = check_cuda(d_counters_.alloc(sizeof(WaveCounters)), "counters"))) return r;
@@ -667,7 +686,7 @@ int Session::set_launch(const pt_launch_config* c) {
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
         c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 4 || c->split_shade < 0 ||
-        c->split_shade > 3)
+        c->split_shade > 3 || c->overlap_shadow < 0 || c->overlap_shadow > 2)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
@@ -681,6 +700,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->refill_idle) shape_.refill_idle = c->refill_idle;
     if (c->speculate) shape_.speculate = speculate_bits(c->speculate);
     if (c->split_shade) shape_.shade_kernel = c->split_shade == 1 ? kShadeClasses : c->split_shade == 2 ? kShadeAll128 : kShadeAll80;
+    if (c->overlap_shadow) shape_.overlap_shadow = c->overlap_shadow == 1 ? 1 : 0;
     return PT_OK;
 }
 
@@ -696,6 +716,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->refill_idle = shape_.refill_idle;
     c->speculate = speculate_code(shape_.speculate);
     c->split_shade = shape_.shade_kernel == kShadeClasses ? 1 : shape_.shade_kernel == kShadeAll128 ? 2 : 3;
+    c->overlap_shadow = shape_.overlap_shadow ? 1 : 2;
 }
 
 int Session::upload_materials() {
@@ -1023,15 +1044,17 @@ int Session::render_async(int spp) {
     marks_active_ = false;
     if (stage_timing_) {
         const int waves = batch ? (int)batch_waves_.size() : (w_ * h_ + p.wave_pixels - 1) / p.wave_pixels;
-        const size_t need = (size_t)waves * (p.max_depth * 7 + 4) + 8;
+        const size_t need = (size_t)waves * (p.max_depth * 10 + 4) + 8;
         while (mark_events_.size() < need) {
             cudaEvent_t e;
             if ((r = check_cuda(cudaEventCreate(&e), "cudaEventCreate"))) return r;
             mark_events_.push_back(e);
         }
         mark_stage_.assign(mark_events_.size(), -1);
+        mark_begin_.assign(mark_events_.size(), -1);
         marks_.events = mark_events_.data();
         marks_.stage = mark_stage_.data();
+        marks_.begin = mark_begin_.data();
         marks_.capacity = (int)mark_events_.size();
         marks_.used = 0;
         mk = &marks_;
@@ -1088,8 +1111,8 @@ int Session::render_async(int spp) {
 // frame's timed region.
 cudaError_t Session::enqueue_frame_and_training(const FrameParams& p, StageMarks* marks) {
     cudaError_t e = p.num_scenes > 0
-                        ? enqueue_batch_frame(p, batch_waves_.data(), (int)batch_waves_.size(), stream_, marks)
-                        : enqueue_frame(p, stream_, marks);
+                        ? enqueue_batch_frame(p, batch_waves_.data(), (int)batch_waves_.size(), stream_, marks, &side_)
+                        : enqueue_frame(p, stream_, marks, &side_);
     if (e != cudaSuccess || !p.guide_mode) return e;
     for (int k = 0; k < p.gtrain_steps; k++) {
         e = guide_train_step(guide_view(), p.gring, p.gring_cap, p.gring_count, p.gtrain_batch, p.gtrain_lr, stream_);
@@ -1116,10 +1139,10 @@ int Session::finish_frame(float* ms) {
             stage_launches_[k] = 0;
         }
         for (int i = 1; i < marks_.used; i++) {
-            const int st = marks_.stage[i];
-            if (st < 0) continue;
+            const int st = marks_.stage[i], b = marks_.begin[i];
+            if (st < 0 || b < 0) continue;
             float dt = 0.f;
-            if ((r = check_cuda(cudaEventElapsedTime(&dt, marks_.events[i - 1], marks_.events[i]), "stage timing")))
+            if ((r = check_cuda(cudaEventElapsedTime(&dt, marks_.events[b], marks_.events[i]), "stage timing")))
                 return r;
             stage_ms_[st] += dt;
             stage_launches_[st]++;

@@ -172,6 +172,10 @@ private:
     bool in_flight_ = false;
     int inflight_spp_ = 0;
     cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
+    // side stream of the overlapped shadow stages, with a fork and a join event per depth
+    cudaStream_t side_stream_ = nullptr;
+    std::vector<cudaEvent_t> side_shaded_, side_shadowed_;
+    SideStream side_;
     // asynchronous readback: snapshot on stream_, device-to-host copy on copy_stream_
     cudaStream_t copy_stream_ = nullptr;
     cudaEvent_t rb_snap_ = nullptr, rb_done_ = nullptr;
@@ -187,7 +191,7 @@ private:
     int work_counters_ = 0;
     int renderer_ = 0;
     std::vector<cudaEvent_t> mark_events_;
-    std::vector<int> mark_stage_;
+    std::vector<int> mark_stage_, mark_begin_;
     StageMarks marks_{};
     bool marks_active_ = false;
     float stage_ms_[kNumStages] = {};

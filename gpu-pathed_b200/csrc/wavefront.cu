@@ -1152,14 +1152,20 @@ __global__ void k_accumulate(FrameParams p, int first_pixel, int npix, long long
     p.rgba8[pixel] = c;
 }
 
+// Records an event on its stream after each launch; a stage's time runs from the previous
+// event on the same stream (stage -1 marks a point with no launch before it: a wave's start,
+// or the end of a wait for the other stream).
 struct Marker {
     StageMarks* m;
     cudaStream_t s;
     cudaError_t err = cudaSuccess;
+    int last = -1;
     void operator()(int stage) {
         if (!m || err != cudaSuccess) return;
         if (m->used >= m->capacity) { err = cudaErrorInvalidValue; return; }
         m->stage[m->used] = stage;
+        m->begin[m->used] = last;
+        last = m->used;
         err = cudaEventRecord(m->events[m->used++], s);
     }
 };
@@ -1188,11 +1194,17 @@ cudaError_t enqueue_class_shades(const FrameParams& p, int d, long long wave_fir
 
 template <int W, bool CNT, bool B>
 cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
-                          StageMarks* marks) {
+                          StageMarks* marks, const SideStream* side) {
     const int grid_e = p.num_sms * p.shape.blocks_per_sm;
+    // shadow stage of depth d on the side stream: forked after the shade stage of d, joined
+    // before the shade stage of d + 1 (which adds to the same path radiance after it); the
+    // closest-hit stage of d + 1 runs beside it
+    const bool overlap = side && side->stream && p.shape.overlap_shadow && p.nee;
+    const cudaStream_t sstream = overlap ? side->stream : stream;
     const size_t smem_e = stack_bytes(p.stack_depth, p.shape.block_extend);
     const size_t smem_s = stack_bytes(p.stack_depth, p.shape.block_shadow);
     Marker mark{marks, stream};
+    Marker smark{marks, sstream};  // the side stream's shadow stages
     for (int wv = 0; wv < nwaves; wv++) {
         const WaveRange& w = waves[wv];
         const int n = w.npaths;
@@ -1235,6 +1247,10 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                     k_guide_infer<B><<<p.num_sms * 2, 32 * kInferWarps, kInferSmemBytes, stream>>>(p, d);
                 mark(kStageGuide);
             }
+            if (overlap && d > 0) {
+                if ((e = cudaStreamWaitEvent(stream, side->shadowed[d - 1], 0))) return e;
+                mark(-1);  // the shade stage's time starts after the wait
+            }
             if (p.guide_mode)
                 k_shade<true, B><<<p.num_sms * kShadeGuidedBlocksPerSm, kShadeGuidedBlock, 0, stream>>>(
                     p, d, wave_first, w.guided_first);
@@ -1249,16 +1265,26 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
             if (e != cudaSuccess) return e;
             mark(kStageShade);
             if (p.nee && d < p.max_depth - 1) {
+                if (overlap) {
+                    if ((e = cudaEventRecord(side->shaded[d], stream))) return e;
+                    if ((e = cudaStreamWaitEvent(sstream, side->shaded[d], 0))) return e;
+                    smark(-1);
+                }
                 if (p.sc.watertight)
-                    k_shadow<W, CNT, B, 2><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d, wave_first,
-                                                                                           w.guided_first);
+                    k_shadow<W, CNT, B, 2><<<grid_e, p.shape.block_shadow, smem_s, sstream>>>(p, d, wave_first,
+                                                                                            w.guided_first);
                 else if (W >= 4 && p.sc.node_q)
-                    k_shadow<W, CNT, B, (W >= 4 ? 1 : 0)><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(
+                    k_shadow<W, CNT, B, (W >= 4 ? 1 : 0)><<<grid_e, p.shape.block_shadow, smem_s, sstream>>>(
                         p, d, wave_first, w.guided_first);
                 else
-                    k_shadow<W, CNT, B, 0><<<grid_e, p.shape.block_shadow, smem_s, stream>>>(p, d, wave_first,
-                                                                                           w.guided_first);
-                mark(kStageShadow);
+                    k_shadow<W, CNT, B, 0><<<grid_e, p.shape.block_shadow, smem_s, sstream>>>(p, d, wave_first,
+                                                                                            w.guided_first);
+                if (overlap) {
+                    if ((e = cudaEventRecord(side->shadowed[d], sstream))) return e;
+                    smark(kStageShadow);
+                } else {
+                    mark(kStageShadow);
+                }
             }
         }
         k_accumulate<B><<<(w.npix + 127) / 128, 128, 0, stream>>>(p, w.first_pixel, w.npix, wave_first);
@@ -1270,6 +1296,7 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (mark.err != cudaSuccess) return mark.err;
+        if (smark.err != cudaSuccess) return smark.err;
     }
     return cudaSuccess;
 }
@@ -1347,7 +1374,7 @@ cudaError_t enqueue_normals_w(const FrameParams& p, cudaStream_t stream, StageMa
 
 // Single-scene frame: waves of whole pixels, p.wave_pixels each.
 template <int W, bool CNT>
-cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
+cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMarks* marks, const SideStream* side) {
     const int npixels = p.width * p.height;
     const int nwaves = (npixels + p.wave_pixels - 1) / p.wave_pixels;
     WaveRange local[64];
@@ -1362,7 +1389,7 @@ cudaError_t enqueue_frame_w(const FrameParams& p, cudaStream_t stream, StageMark
         const int npix = npixels - first < p.wave_pixels ? npixels - first : p.wave_pixels;
         waves[k] = WaveRange{first, npix, (long long)first * p.spp, npix * p.spp, 0, 0, npix * p.spp, 0};
     }
-    return enqueue_waves<W, CNT, false>(p, waves, nwaves, stream, marks);
+    return enqueue_waves<W, CNT, false>(p, waves, nwaves, stream, marks, side);
 }
 
 template <int W>
@@ -1472,7 +1499,7 @@ __global__ void k_hit_test(SceneDevice sc, CameraParams cam, int stack_depth, in
 
 }  // namespace
 
-cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks* marks) {
+cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks* marks, const SideStream* side) {
     if (p.max_depth < 0 || p.max_depth > kMaxDepthLimit) return cudaErrorInvalidValue;
     if (p.renderer == 1) {
         if (p.spp != 1) return cudaErrorInvalidValue;
@@ -1485,24 +1512,24 @@ cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks*
     }
     const bool cnt = p.count_work != 0;
     switch (p.sc.bvh_width) {
-        case 2: return cnt ? enqueue_frame_w<2, true>(p, stream, marks) : enqueue_frame_w<2, false>(p, stream, marks);
-        case 4: return cnt ? enqueue_frame_w<4, true>(p, stream, marks) : enqueue_frame_w<4, false>(p, stream, marks);
-        case 8: return cnt ? enqueue_frame_w<8, true>(p, stream, marks) : enqueue_frame_w<8, false>(p, stream, marks);
+        case 2: return cnt ? enqueue_frame_w<2, true>(p, stream, marks, side) : enqueue_frame_w<2, false>(p, stream, marks, side);
+        case 4: return cnt ? enqueue_frame_w<4, true>(p, stream, marks, side) : enqueue_frame_w<4, false>(p, stream, marks, side);
+        case 8: return cnt ? enqueue_frame_w<8, true>(p, stream, marks, side) : enqueue_frame_w<8, false>(p, stream, marks, side);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t enqueue_batch_frame(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
-                                StageMarks* marks) {
+                                StageMarks* marks, const SideStream* side) {
     if (p.max_depth < 0 || p.max_depth > kMaxDepthLimit || p.num_scenes <= 0) return cudaErrorInvalidValue;
     const bool cnt = p.count_work != 0;
     switch (p.sc.bvh_width) {
-        case 2: return cnt ? enqueue_waves<2, true, true>(p, waves, nwaves, stream, marks)
-                           : enqueue_waves<2, false, true>(p, waves, nwaves, stream, marks);
-        case 4: return cnt ? enqueue_waves<4, true, true>(p, waves, nwaves, stream, marks)
-                           : enqueue_waves<4, false, true>(p, waves, nwaves, stream, marks);
-        case 8: return cnt ? enqueue_waves<8, true, true>(p, waves, nwaves, stream, marks)
-                           : enqueue_waves<8, false, true>(p, waves, nwaves, stream, marks);
+        case 2: return cnt ? enqueue_waves<2, true, true>(p, waves, nwaves, stream, marks, side)
+                           : enqueue_waves<2, false, true>(p, waves, nwaves, stream, marks, side);
+        case 4: return cnt ? enqueue_waves<4, true, true>(p, waves, nwaves, stream, marks, side)
+                           : enqueue_waves<4, false, true>(p, waves, nwaves, stream, marks, side);
+        case 8: return cnt ? enqueue_waves<8, true, true>(p, waves, nwaves, stream, marks, side)
+                           : enqueue_waves<8, false, true>(p, waves, nwaves, stream, marks, side);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -72,7 +72,8 @@ struct StageMarks {
     cudaEvent_t* events = nullptr;  // pool
     int capacity = 0;
     int used = 0;
-    int* stage = nullptr;           // stage of the launch that ends at events[i] (-1: wave start)
+    int* stage = nullptr;           // stage of the launch that ends at events[i] (-1: no launch)
+    int* begin = nullptr;           // the event on the same stream before that launch (-1: none)
 };
 
 struct LaunchShape {
@@ -85,6 +86,15 @@ struct LaunchShape {
     int refill_idle = 16;     // traversal stages: a warp fetches new rays once this many lanes are idle
     int speculate = 0;        // kSpeculate* bits: stages that park a lane's first leaf and descend on
     int shade_kernel = 1;     // plain frames' shade stage: kShadeAll128, kShadeClasses, kShadeAll80
+    int overlap_shadow = 1;   // shadow stage of depth d on the side stream beside extend of d + 1
+};
+
+// The second stream of a frame whose shadow stages overlap the next depth's closest-hit stage,
+// with one fork and one join event per depth.
+struct SideStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t* shaded = nullptr;    // recorded on the main stream after the shade stage of depth d
+    cudaEvent_t* shadowed = nullptr;  // recorded on the side stream after the shadow stage of depth d
 };
 
 constexpr int kShadeAll128 = 0;  // one kernel for all materials, 128 registers
@@ -211,12 +221,14 @@ struct FrameParams {
 // Enqueue one batched frame (p.num_scenes > 0): the given waves over the scenes' global path
 // order, every stage one launch for all scenes of the wave.
 cudaError_t enqueue_batch_frame(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
-                                StageMarks* marks = nullptr);
+                                StageMarks* marks = nullptr, const SideStream* side = nullptr);
 
 // Enqueue one frame (all waves) on `stream`. Grid sizes do not depend on queue lengths,
 // so the sequence can be captured into a CUDA graph. With `marks`, an event is recorded
-// after every launch (per-stage timing; not capturable).
-cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks* marks = nullptr);
+// after every launch (per-stage timing; not capturable). With `side` and
+// p.shape.overlap_shadow (and no marks), each depth's shadow stage runs on the side stream.
+cudaError_t enqueue_frame(const FrameParams& p, cudaStream_t stream, StageMarks* marks = nullptr,
+                          const SideStream* side = nullptr);
 
 // Raise the dynamic shared-memory limit of the traversal kernels to `bytes`.
 cudaError_t configure_traversal_smem(size_t bytes);

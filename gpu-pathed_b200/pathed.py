@@ -109,7 +109,7 @@ class SceneExport(C.Structure):
 class LaunchConfig(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "wave_paths", "block_extend", "block_shade", "block_shadow", "blocks_per_sm", "sort_materials",
-        "use_graph", "sort_rays", "refill_idle", "speculate", "split_shade")]
+        "use_graph", "sort_rays", "refill_idle", "speculate", "split_shade", "overlap_shadow")]
 
 
 class Stats(C.Structure):

@@ -127,6 +127,10 @@ typedef struct pt_launch_config {
                               frames; default), 2 one kernel for all materials at 128 registers,
                               3 the same at 80 registers (more resident warps, some spills);
                               images are the same either way */
+    int overlap_shadow;    /* 1: the shadow stage of depth d runs on a second stream beside the
+                              closest-hit stage of depth d + 1, each filling the other's tail
+                              (default; the shade stage of depth d + 1 waits for both), 2: one
+                              stream; images are the same either way */
 } pt_launch_config;
 
 /* Result of pt_autotune. */

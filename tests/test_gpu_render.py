@@ -160,6 +160,33 @@ def test_launch_shapes_do_not_change_images(sort, width):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", [(0, None, 2), (1, None, 4), (3, 4, 2)], ids=lambda c: f"cfg{c[0]}")
+@pytest.mark.parametrize("graph", [1, 2])
+def test_overlapped_shadow_stage_does_not_change_images(case, graph):
+    """the shadow stage of depth d on a second stream beside the closest-hit stage of d + 1:
+    the shade stage of d + 1 waits for it, so every path's radiance takes its additions in the
+    same order and frames are bit-identical, graph-captured or launched directly, across
+    waves (a small queue splits the frame)"""
+    cfg, level, spp = case
+    imgs = []
+    for overlap, timing in ((2, False), (1, False), (1, True)):
+        s = pathed.Session(64, 48)
+        s.load_config(cfg, level=level) if level else s.load_config(cfg)
+        s.set_launch(overlap_shadow=overlap, use_graph=graph, wave_paths=4096)
+        s.set_profiling(stage_timing=timing)
+        assert s.get_launch()["overlap_shadow"] == overlap
+        for _ in range(2):
+            s.render(spp)
+        if timing:  # per-stage events on both streams
+            p = s.profile()
+            for k in ("extend", "shade", "shadow"):
+                assert p["stage_ms"][k] > 0 and p["stage_launches"][k] > 0, k
+        imgs.append(s.readback().copy())
+        s.close()
+    assert np.array_equal(imgs[0], imgs[1]) and np.array_equal(imgs[0], imgs[2])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("config", [2, 3])
 def test_leaf_sizes_do_not_change_images(config):
     """the leaf sizes the autotuner picks from (2, 4, 8) change the tree, not the hits: with
