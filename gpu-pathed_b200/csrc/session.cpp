@@ -58,6 +58,14 @@ Session::~Session() {
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : side_shadowed_)
             if (e) cudaEventDestroy(e);
+        for (cudaStream_t c : cls_streams_)
+            if (c) {
+                cudaStreamSynchronize(c);
+                cudaStreamDestroy(c);
+            }
+        for (cudaEvent_t e : cls_done_)
+            if (e) cudaEventDestroy(e);
+        if (cls_fork_) cudaEventDestroy(cls_fork_);
         for (cudaEvent_t e : mark_events_) cudaEventDestroy(e);
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         if (h_dyn_) cudaFreeHost(h_dyn_);
@@ -120,7 +128,17 @@ int Session::ensure_device() {
         if ((r = check_cuda(cudaEventCreateWithFlags(&side_shadowed_[d], cudaEventDisableTiming), "cudaEventCreate")))
             return r;
     }
-    side_ = SideStream{side_stream_, side_shaded_.data(), side_shadowed_.data()};
+    cls_streams_.assign(kMaterialClasses, nullptr);
+    cls_done_.assign(kMaterialClasses, nullptr);
+    for (int c = 0; c < kMaterialClasses; c++) {
+        if ((r = check_cuda(cudaStreamCreateWithFlags(&cls_streams_[c], cudaStreamNonBlocking), "cudaStreamCreate")))
+            return r;
+        if ((r = check_cuda(cudaEventCreateWithFlags(&cls_done_[c], cudaEventDisableTiming), "cudaEventCreate")))
+            return r;
+    }
+    if ((r = check_cuda(cudaEventCreateWithFlags(&cls_fork_, cudaEventDisableTiming), "cudaEventCreate"))) return r;
+    side_ = SideStream{side_stream_, side_shaded_.data(), side_shadowed_.data(), cls_streams_.data(), cls_fork_,
+                       cls_done_.data()};
     if ((r = check_cuda(cudaMallocHost((void**)&h_stats_, sizeof(FrameStats)), "cudaMallocHost"))) return r;
     std::memset(h_stats_, 0, sizeof(FrameStats));
     if ((r = check_cuda(d_counters_.alloc(sizeof(WaveCounters)), "counters"))) return r;

@@ -175,6 +175,9 @@ private:
     // side stream of the overlapped shadow stages, with a fork and a join event per depth
     cudaStream_t side_stream_ = nullptr;
     std::vector<cudaEvent_t> side_shaded_, side_shadowed_;
+    std::vector<cudaStream_t> cls_streams_;
+    std::vector<cudaEvent_t> cls_done_;
+    cudaEvent_t cls_fork_ = nullptr;
     SideStream side_;
     // asynchronous readback: snapshot on stream_, device-to-host copy on copy_stream_
     cudaStream_t copy_stream_ = nullptr;

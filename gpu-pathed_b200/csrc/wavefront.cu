@@ -1175,21 +1175,41 @@ struct Marker {
 // fewer registers than the kernel of all materials; each persistent grid is as many blocks
 // as the SMs keep resident at that register budget, and a class absent at a depth returns
 // before its first fetch.
+// With `par`, each class kernel runs on its own stream, forked from and joined back to
+// `stream`: the classes touch disjoint paths and append through atomics, so they may run
+// side by side, each filling the SMs the others' ramps and tails leave idle.
 template <bool B>
 cudaError_t enqueue_class_shades(const FrameParams& p, int d, long long wave_first, long long gfirst,
-                                 cudaStream_t stream) {
+                                 cudaStream_t stream, const SideStream* par) {
     const int bs = p.shape.block_shade;
     auto grid = [&](int cls) {
         const int per_sm = std::max(1, std::min(65536 / (shade_class_regs(cls) * bs), 2048 / bs));
         return p.num_sms * per_sm;
     };
-    if (p.class_mask & 1) k_shade_class<B, 0><<<grid(0), bs, 0, stream>>>(p, d, wave_first, gfirst);
-    if (p.class_mask & 2) k_shade_class<B, 1><<<grid(1), bs, 0, stream>>>(p, d, wave_first, gfirst);
-    if (p.class_mask & 4) k_shade_class<B, 2><<<grid(2), bs, 0, stream>>>(p, d, wave_first, gfirst);
-    if (p.class_mask & 8) k_shade_class<B, 3><<<grid(3), bs, 0, stream>>>(p, d, wave_first, gfirst);
-    if (p.class_mask & 16) k_shade_class<B, 4><<<grid(4), bs, 0, stream>>>(p, d, wave_first, gfirst);
-    if (p.class_mask & 64) k_shade_class<B, 6><<<grid(6), bs, 0, stream>>>(p, d, wave_first, gfirst);
-    return cudaGetLastError();
+    cudaError_t e;
+    if (par && (e = cudaEventRecord(par->cls_fork, stream))) return e;
+    cudaError_t we = cudaSuccess;
+    auto on = [&](int cls) -> cudaStream_t {
+        if (!par) return stream;
+        const cudaError_t w = cudaStreamWaitEvent(par->cls[cls], par->cls_fork, 0);
+        if (w != cudaSuccess) we = w;
+        return par->cls[cls];
+    };
+    if (p.class_mask & 1) k_shade_class<B, 0><<<grid(0), bs, 0, on(0)>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 2) k_shade_class<B, 1><<<grid(1), bs, 0, on(1)>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 4) k_shade_class<B, 2><<<grid(2), bs, 0, on(2)>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 8) k_shade_class<B, 3><<<grid(3), bs, 0, on(3)>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 16) k_shade_class<B, 4><<<grid(4), bs, 0, on(4)>>>(p, d, wave_first, gfirst);
+    if (p.class_mask & 64) k_shade_class<B, 6><<<grid(6), bs, 0, on(6)>>>(p, d, wave_first, gfirst);
+    if ((e = cudaGetLastError())) return e;
+    if (we != cudaSuccess) return we;
+    if (par)
+        for (int c = 0; c < kMaterialClasses; c++) {
+            if (!(p.class_mask & (1 << c))) continue;
+            if ((e = cudaEventRecord(par->cls_done[c], par->cls[c]))) return e;
+            if ((e = cudaStreamWaitEvent(stream, par->cls_done[c], 0))) return e;
+        }
+    return cudaSuccess;
 }
 
 template <int W, bool CNT, bool B>
@@ -1199,7 +1219,8 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
     // shadow stage of depth d on the side stream: forked after the shade stage of d, joined
     // before the shade stage of d + 1 (which adds to the same path radiance after it); the
     // closest-hit stage of d + 1 runs beside it
-    const bool overlap = side && side->stream && p.shape.overlap_shadow && p.nee;
+    const bool concurrent = side && side->stream && p.shape.overlap_shadow;
+    const bool overlap = concurrent && p.nee;
     const cudaStream_t sstream = overlap ? side->stream : stream;
     const size_t smem_e = stack_bytes(p.stack_depth, p.shape.block_extend);
     const size_t smem_s = stack_bytes(p.stack_depth, p.shape.block_shadow);
@@ -1255,7 +1276,8 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                 k_shade<true, B><<<p.num_sms * kShadeGuidedBlocksPerSm, kShadeGuidedBlock, 0, stream>>>(
                     p, d, wave_first, w.guided_first);
             else if (p.shape.shade_kernel == kShadeClasses && p.shape.sort_materials && p.class_mask)
-                e = enqueue_class_shades<B>(p, d, wave_first, w.guided_first, stream);
+                e = enqueue_class_shades<B>(p, d, wave_first, w.guided_first, stream,
+                                            concurrent && !marks && side->cls ? side : nullptr);
             else if (p.shape.shade_kernel == kShadeAll80)
                 k_shade_all<B, 80><<<p.num_sms * shade_resident(80, p.shape.block_shade), p.shape.block_shade, 0,
                                      stream>>>(p, d, wave_first, w.guided_first);

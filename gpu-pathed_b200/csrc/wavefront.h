@@ -89,12 +89,17 @@ struct LaunchShape {
     int overlap_shadow = 1;   // shadow stage of depth d on the side stream beside extend of d + 1
 };
 
-// The second stream of a frame whose shadow stages overlap the next depth's closest-hit stage,
-// with one fork and one join event per depth.
+// The side streams of a frame whose independent stages overlap (LaunchShape.overlap_shadow):
+// the shadow stage of depth d beside the closest-hit stage of depth d + 1, with one fork and
+// one join event per depth, and the per-class shade kernels of a depth side by side, each on
+// its own stream between a fork and a join event.
 struct SideStream {
     cudaStream_t stream = nullptr;
     cudaEvent_t* shaded = nullptr;    // recorded on the main stream after the shade stage of depth d
     cudaEvent_t* shadowed = nullptr;  // recorded on the side stream after the shadow stage of depth d
+    cudaStream_t* cls = nullptr;      // kMaterialClasses streams of the class shade kernels
+    cudaEvent_t cls_fork = nullptr;   // recorded on the main stream before them
+    cudaEvent_t* cls_done = nullptr;  // recorded on each class stream after its kernel
 };
 
 constexpr int kShadeAll128 = 0;  // one kernel for all materials, 128 registers
