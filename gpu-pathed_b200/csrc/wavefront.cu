@@ -116,6 +116,10 @@ __device__ __forceinline__ void warp_append_pair(int* ca, const bool (&wa)[N], i
     }
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* ptr) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
 __device__ __forceinline__ int tag_path(int tag) { return tag & kTagPathMask; }
 __device__ __forceinline__ int tag_scene(int tag) { return tag >> kTagPathBits; }
 
@@ -583,12 +587,28 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
         for (int j = threadIdx.x; j < kRayBuckets; j += blockDim.x) rhist[j] = 0;
         __syncthreads();
     }
-    int claimed = 0;  // AHEAD: lane 0's claim of the warp's next chunk
-    if (AHEAD && (threadIdx.x & 31) == 0) claimed = atomicAdd(work, 32 * IPL);
+    static_assert(!AHEAD || IPL == 1, "the claim-ahead loop shades one item per lane");
+    const int lane = threadIdx.x & 31;
+    auto slot_of = [&](int i) {
+        return CLS >= 0 ? p.sort_index[cls_first + i] : (p.shape.sort_materials ? p.sort_index[i] : i);
+    };
+    // AHEAD: the chunk after next is claimed while a chunk shades (lane 0's atomic result,
+    // read one chunk later), the next chunk's slots are loaded then too, and its queue records
+    // are prefetched into L2 before this chunk's results are written
+    int claimed = 0, cur_base = 0, next_base = 0, cur_slot = -1;
+    if (AHEAD) {
+        cur_base = warp_fetch(work);
+        next_base = warp_fetch(work);
+        if (cur_base + lane < count) cur_slot = slot_of(cur_base + lane);
+    }
     for (;;) {
-        const int base = AHEAD ? __shfl_sync(0xffffffffu, claimed, 0) : warp_fetch(work, 32 * IPL);
+        const int base = AHEAD ? cur_base : warp_fetch(work, 32 * IPL);
         if (base >= count) break;
-        if (AHEAD && (threadIdx.x & 31) == 0) claimed = atomicAdd(work, 32 * IPL);
+        int next_slot = -1;
+        if (AHEAD) {
+            if (lane == 0) claimed = atomicAdd(work, 32);
+            if (next_base + lane < count) next_slot = slot_of(next_base + lane);
+        }
         bool cont_[IPL], shadow_[IPL];
         float4 co_[IPL], cd_[IPL], cb_[IPL], so_[IPL], sd_[IPL], sc_[IPL];
         uint2 crng_[IPL];
@@ -600,7 +620,7 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
         uint2 crng;
         GuideRecord rec;
         if (i < count) {
-            const int slot = CLS >= 0 ? p.sort_index[cls_first + i] : (p.shape.sort_materials ? p.sort_index[i] : i);
+            const int slot = AHEAD ? cur_slot : slot_of(i);
             const float4 o4 = q.o[slot];
             const float4 d4 = q.d[slot];
             const float4 b4 = q.beta[slot];
@@ -780,6 +800,13 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
         sd_[item] = sd;
         sc_[item] = sc4;
         }
+        if (AHEAD && next_slot >= 0) {
+            prefetch_l2(q.o + next_slot);
+            prefetch_l2(q.d + next_slot);
+            prefetch_l2(q.beta + next_slot);
+            prefetch_l2(q.hit + next_slot);
+            prefetch_l2(q.rng + next_slot);
+        }
         int cslot[IPL], sslot[IPL];
         if (AHEAD)
             warp_append_pair<IPL>(&p.counters->ray_count[depth + 1], cont_, cslot, &p.counters->shadow_count[depth],
@@ -808,6 +835,11 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
             p.sq.o[ss] = so_[item];
             p.sq.d[ss] = sd_[item];
             p.sq.c[ss] = sc_[item];
+        }
+        if (AHEAD) {
+            cur_base = next_base;
+            next_base = __shfl_sync(0xffffffffu, claimed, 0);
+            cur_slot = next_slot;
         }
     }
     if (!B && rsort) {
