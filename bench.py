@@ -396,6 +396,20 @@ def _roofline(workload, counts, prof_count, st_count, stage_ms, stage_launches, 
         roof["issue_slots"] = {"achieved": issue_achieved, "peak": issue_peak, "unit": "G warp-inst/s",
                                "frac": issue_achieved / issue_peak, "inst_source": inst_src,
                                "inst_shape_exact": ishape == shape}
+    # the shade stage beside it, on HBM: the queue records it must move per frame (a lower bound
+    # of its DRAM traffic: gathers at material-sorted slots fetch whole 32-byte sectors)
+    items = st_count["rays_extend"]
+    cont = max(0, items - st_count["rays_camera"])
+    shade_bytes = items * (4 + 72) + cont * 72 + st_count["rays_shadow"] * 48
+    shade_ms = stage_ms["shade"] / max(1, steps)
+    if shade_ms > 0:
+        gbs = shade_bytes / (shade_ms / 1e3) / 1e9
+        roof["shade"] = {"kernel": "k_shade_all / k_shade_class (shade stage)", "bound": "hbm",
+                         "algorithmic_bytes_per_frame": shade_bytes, "ms_per_frame": shade_ms,
+                         "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "bytes": "per item 4 B sorted slot + 72 B queue record (origin, direction, "
+                                  "throughput, hit, random state) read; per continuation 72 B and per "
+                                  "shadow ray 48 B written"}
     roof["stage_timing"] = ("per-stage CUDA events of as many frames again, all stages on one stream, "
                             "right after the timed frames (which overlap the shadow stage with the next "
                             "depth's closest-hit stage on a second stream)")
