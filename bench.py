@@ -476,14 +476,15 @@ def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
         s.render(wl["spp"])
     dev_ms, rays, paths = _time_frames(s, wl["spp"], steps, flush)
     stage_ms, stage_launches = _stage_frames(s, wl["spp"], steps, flush)
-    shape = extend_shape_key(counts.bvh_width, counts.bvh_max_leaf, s.get_launch())
+    shape = extend_shape_key(counts.bvh_width, counts.bvh_max_leaf, s.get_launch(), tuned["bvh_builder"])
     s.close()
     out = {"workload": wl["name"], "resolution": [w, h], "spp": wl["spp"], "max_depth": wl["depth"],
            "value": rays / (dev_ms / 1e3) / 1e6, "unit": "Mrays/s", "mpaths_per_s": paths / (dev_ms / 1e3) / 1e6,
            "ms_per_step": dev_ms / steps, "steps": steps, "warmup": warmup, "triangles": counts.num_triangles,
            "spheres": counts.num_spheres,
            "autotuned": {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays", "speculate",
-                                                "blocks_per_sm", "block", "wave_paths", "split_shade", "max_leaf")},
+                                                "blocks_per_sm", "block", "wave_paths", "split_shade", "max_leaf",
+                                                "bvh_builder")},
            "roofline": _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs,
                                  None, shape)}
     if with_reference:
@@ -527,8 +528,8 @@ def run_ours(args):
         s.set_guiding(True)
         spp = 0
     else:
-        if args.gpu_bvh:  # BVH built on the device (LBVH collapsed to the wide format)
-            s.set_bvh_builder(True)
+        if args.gpu_bvh:  # BVH built on the device (LBVH or PLOC, collapsed to the wide format)
+            s.set_bvh_builder(2 if args.gpu_bvh == "ploc" else 1)
         s.load_config(args.config)
         if args.guided:  # learned guiding on the main workload (trained online during warm-up)
             s.set_guiding(True)
@@ -613,7 +614,9 @@ def run_ours(args):
     roof = None
     if rank == 0:
         roof = _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, args.steps, l2_gbs,
-                         clk.get("sm_mhz"), extend_shape_key(counts.bvh_width, counts.bvh_max_leaf, s.get_launch()))
+                         clk.get("sm_mhz"),
+                         extend_shape_key(counts.bvh_width, counts.bvh_max_leaf, s.get_launch(),
+                                          tuned["bvh_builder"] if tuned else {None: 0, "lbvh": 1, "ploc": 2}[args.gpu_bvh]))
         roof["l2_probe"] = {"gbs": l2_gbs, "ms": l2_ms, "bytes": L2_PROBE_BYTES}
 
     cpu = None
@@ -641,7 +644,7 @@ def run_ours(args):
             "config": ({"workload": wl["name"], "resolution": [w, h], "spp": spp, "max_depth": wl["depth"],
                         "nee": True, "triangles": counts.num_triangles, "spheres": counts.num_spheres,
                         "bvh_width": counts.bvh_width, "parallelism": f"replicas{world}",
-                        "guided": bool(args.guided), "bvh_builder": "gpu-lbvh" if args.gpu_bvh else "host-sah",
+                        "guided": bool(args.guided), "bvh_builder": f"gpu-{args.gpu_bvh}" if args.gpu_bvh else "host-sah",
                         "bvh_nodes": "quantized" if args.quantized_bvh else "float",
                         "sort_rays": s.get_launch()["sort_rays"] == 1,
                         "l2": "flushed between steps (256 MiB write)"} if not batch else
@@ -664,7 +667,10 @@ def run_ours(args):
         if tuned is not None:
             line["config"]["autotuned"] = {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays",
                                                                "speculate", "blocks_per_sm", "block", "wave_paths",
-                                                               "split_shade", "max_leaf", "best_ms", "default_ms")}
+                                                               "split_shade", "max_leaf", "bvh_builder", "best_ms",
+                                                               "default_ms")}
+            if tuned["bvh_builder"] == 2:
+                line["config"]["bvh_builder"] = "gpu-ploc (autotuned)"
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:
@@ -898,15 +904,17 @@ def batch_time_to_relmse(budget_frames=16, ref_frames=128, draw=0x5EED + 4, n=48
             **out}
 
 
-def extend_shape_key(width, leaf, launch):
+def extend_shape_key(width, leaf, launch, builder=0):
     """The closest-hit stage's shape as the instruction counts are keyed: BVH width, largest
     leaf, whether its speculation is on (speculate codes 1 and 3), its grid (blocks per SM x
-    threads per block) and the wave size (log2 of the paths per wave). The lane-refill
+    threads per block), the wave size (log2 of the paths per wave) and, for a tree built on
+    the GPU, its builder (suffix _lbvh or _ploc; none for the host's SAH tree). The lane-refill
     traversal's instructions per query depend on all of them: the grid and the wave set how
     full the warps' lanes stay."""
     sp = 1 if launch["speculate"] in (1, 3) else 0
     q = max(0, int(launch["wave_paths"]).bit_length() - 1)
-    return f"w{width}_l{leaf}_s{sp}_b{launch['blocks_per_sm']}x{launch['block_extend']}_q{q}"
+    tag = {1: "_lbvh", 2: "_ploc"}.get(int(builder or 0), "")
+    return f"w{width}_l{leaf}_s{sp}_b{launch['blocks_per_sm']}x{launch['block_extend']}_q{q}{tag}"
 
 
 def _ncu_per_query(workload, field, fname="k_extend_traffic.txt"):
@@ -926,8 +934,8 @@ def _ncu_per_query(workload, field, fname="k_extend_traffic.txt"):
 
 def _ncu_shape_per_query(workload, shape, field):
     """`field` of profiles/k_extend_issue.txt measured at `shape` on this workload, else at the
-    nearest captured shape: same BVH width first, then the same speculation, the closest leaf
-    size, the same grid and the closest wave size. Returns (value, captured shape) or
+    nearest captured shape: the same tree builder first, then the same BVH width, the same
+    speculation, the closest leaf size, the same grid and the closest wave size. Returns (value, captured shape) or
     (None, None)."""
     p = os.path.join(ROOT, "profiles", "k_extend_issue.txt")
     found = {}
@@ -948,13 +956,14 @@ def _ncu_shape_per_query(workload, shape, field):
         f = k.split("_")
         grid = f[3] if len(f) > 3 else ""
         wave = int(f[4][1:]) if len(f) > 4 else 0
-        return int(f[0][1:]), int(f[1][1:]), int(f[2][1:]), grid, wave
+        tree = f[5] if len(f) > 5 else "sah"
+        return int(f[0][1:]), int(f[1][1:]), int(f[2][1:]), grid, wave, tree
 
-    tw, tl, ts, tg, tq = parse(shape)
+    tw, tl, ts, tg, tq, tt = parse(shape)
 
     def distance(k):
-        w, l, sp, g, q = parse(k)
-        return (w != tw, sp != ts, abs(l - tl), g != tg, abs(q - tq), k)
+        w, l, sp, g, q, t = parse(k)
+        return (t != tt, w != tw, sp != ts, abs(l - tl), g != tg, abs(q - tq), k)
 
     best = min(found, key=distance)
     return found[best], best
@@ -975,8 +984,11 @@ def ncu_frames(args):
     spp = args.spp or wl["spp"]
     s = pathed.Session(w, h)
     s.load_config(args.config)
+    builder = {None: 0, "lbvh": 1, "ploc": 2}[args.gpu_bvh]
+    if builder:
+        s.set_bvh_builder(builder)
     if args.tune_cache:  # the shape a benchmark run chose (read from its cache, no measuring)
-        s.autotune(spp, args.tune_cache)
+        builder = s.autotune(spp, args.tune_cache)["bvh_builder"]
     if args.bvh:
         s.set_bvh(args.bvh[0], args.bvh[1])
     if args.speculate:
@@ -989,7 +1001,7 @@ def ncu_frames(args):
         st = s.stats()
         lc = s.get_launch()
         print(json.dumps({"workload": wl["name"], "resolution": [w, h], "spp": spp,
-                          "shape": extend_shape_key(s.counts().bvh_width, s.counts().bvh_max_leaf, lc),
+                          "shape": extend_shape_key(s.counts().bvh_width, s.counts().bvh_max_leaf, lc, builder),
                           "rays_extend": st["rays_extend"], "rays_shadow": st["rays_shadow"],
                           "extend_launches": s.profile()["stage_launches"]["extend"]}), flush=True)
     s.close()
@@ -1042,7 +1054,8 @@ def main():
     ap.add_argument("--guided", action="store_true", help="render the main workload with learned guiding")
     ap.add_argument("--guide-inference", choices=("mma", "tc"), default=None,
                     help="with --guided: guide inference on mma.sync or on tcgen05 (default: the library's)")
-    ap.add_argument("--gpu-bvh", action="store_true", help="build the BVH on the GPU instead of the host")
+    ap.add_argument("--gpu-bvh", nargs="?", const="lbvh", default=None, choices=["lbvh", "ploc"],
+                    help="build the BVH on the GPU instead of the host: a linear BVH (default) or PLOC")
     ap.add_argument("--quantized-bvh", action="store_true",
                     help="traverse quantized wide nodes (8-bit child planes) instead of float nodes")
     ap.add_argument("--no-autotune", action="store_true",

@@ -1,23 +1,31 @@
-// GPU BVH construction: a linear BVH (Morton order, Karras 2012 radix tree) collapsed to the
-// same W-wide node format, padded boxes and leaf-entry layout as the host's binned-SAH
-// builder (bvh_build.cpp), so every traversal kernel works on either tree unchanged and the
+// GPU BVH construction: a binary tree over the Morton-sorted primitives, either a linear BVH
+// (Karras 2012 radix tree) or agglomerative clustering (PLOC), collapsed to the same W-wide
+// node format, padded boxes and leaf-entry layout as the host's binned-SAH builder
+// (bvh_build.cpp), so every traversal kernel works on any of the trees unchanged and the
 // closest-hit results stay identical (the tie rule lives in the leaf test, the padding keeps
 // every child box conservative).
 //
 //   1. primitive boxes and centroids (triangles: vertex min/max; spheres: centre -/+ radius)
 //   2. scene and centroid bounds (warp reduction + atomics on order-preserving integers)
 //   3. 63-bit Morton codes of the centroids, sorted with their primitive ids (CUB radix sort)
-//   4. radix tree over the sorted codes (Karras, "Maximizing parallelism in the construction
-//      of BVHs, octrees, and k-d trees", HPG 2012): each internal node finds its range and
-//      split from the codes' common-prefix lengths
-//   5. bounds and primitive counts bottom-up (the second child to arrive at a node merges)
+//   4. LBVH: radix tree over the sorted codes (Karras, "Maximizing parallelism in the
+//      construction of BVHs, octrees, and k-d trees", HPG 2012): each internal node finds its
+//      range and split from the codes' common-prefix lengths;
+//   5. bounds and primitive counts bottom-up (the second child to arrive at a node merges).
+//   4'. PLOC instead (Meister and Bittner, "Parallel Locally-Ordered Clustering for Bounding
+//      Volume Hierarchy Construction", TVCG 2018): starting from one cluster per primitive in
+//      Morton order, each cluster finds the neighbour within kPlocRadius positions whose union
+//      box has the smallest surface area; mutual nearest neighbours merge into a new node, and
+//      the surviving clusters are compacted in order, until one is left. Leaves are then
+//      numbered in the tree's depth-first order, so every subtree's primitives are contiguous.
 //   6. top-down collapse, one launch per level: a wide node opens its largest-area children
 //      that hold more than max_leaf primitives until it has W children; children with at
 //      most max_leaf primitives become leaves (their primitives are contiguous in Morton order)
-//   7. leaf entries in Morton order
+//   7. leaf entries in Morton order (LBVH) or depth-first order (PLOC)
 #include "bvh_gpu.h"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <cfloat>
 #include <cmath>
@@ -217,7 +225,7 @@ __device__ __forceinline__ void pad_box(float4 lo, float4 hi, double abs_pad, fl
 struct CollapseArgs {
     const int* left;
     const int* right;
-    const int* first;  // internal nodes: range start
+    const int* first;  // every binary node: its first leaf entry
     NodeBox nb;
     int n;
     int max_leaf;
@@ -237,7 +245,7 @@ __global__ void k_lb_collapse(CollapseArgs a) {
     if (q >= a.qn) return;
     const int2 job = a.qin[q];
     auto count_of = [&](int id) { return __float_as_int(a.nb.lo[id].w); };
-    auto first_of = [&](int id) { return id >= a.n - 1 ? id - (a.n - 1) : a.first[id]; };
+    auto first_of = [&](int id) { return a.first[id]; };
     auto internal = [&](int id) { return id < a.n - 1; };
     int list[W];
     int cnt = 0;
@@ -320,19 +328,175 @@ cudaError_t grow(DevBuf& b, size_t count) {
     return b.alloc(count * sizeof(T));
 }
 
+// LBVH leaves are numbered in Morton order: leaf e starts at entry e.
+__global__ void k_lb_leaf_first(int n, int* first) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) first[n - 1 + e] = e;
+}
+
+// ---- PLOC ----
+constexpr int kPlocRadius = 16;
+
+// Half the surface area of the union of two boxes (ordering only). Symmetric in its
+// arguments, so both clusters of a pair compute the same value.
+__device__ __forceinline__ float ploc_union_area(float4 alo, float4 ahi, float4 blo, float4 bhi) {
+    const float dx = fmaxf(ahi.x, bhi.x) - fminf(alo.x, blo.x);
+    const float dy = fmaxf(ahi.y, bhi.y) - fminf(alo.y, blo.y);
+    const float dz = fmaxf(ahi.z, bhi.z) - fminf(alo.z, blo.z);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
+}
+
+// One cluster per primitive, in Morton order: binary leaf n - 1 + e and its box.
+__global__ void k_ploc_init(int n, NodeBox nb, int* cnode, float4* clo, float4* chi) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    cnode[e] = n - 1 + e;
+    clo[e] = nb.lo[n - 1 + e];
+    chi[e] = nb.hi[n - 1 + e];
+}
+
+// Each cluster's nearest neighbour among the kPlocRadius clusters on either side. Pairs are
+// ordered by (union area, lower index, higher index), a total order: scanning j upwards with
+// a strict comparison keeps the smaller index on equal areas, which is the same order, so the
+// pair that is smallest overall is always a mutual choice and every pass merges.
+__global__ void k_ploc_nn(const float4* __restrict__ clo, const float4* __restrict__ chi, int m, int* nn) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const float4 alo = clo[i], ahi = chi[i];
+    float best = INFINITY;
+    int bj = -1;
+    const int j0 = max(0, i - kPlocRadius), j1 = min(m - 1, i + kPlocRadius);
+    for (int j = j0; j <= j1; j++) {
+        if (j == i) continue;
+        const float a = ploc_union_area(alo, ahi, clo[j], chi[j]);
+        if (a < best) {
+            best = a;
+            bj = j;
+        }
+    }
+    nn[i] = bj;
+}
+
+// Mutual nearest neighbours i < j merge into a new internal node (ids n - 2 down to 0, so the
+// last merge, the root, is node 0) that takes position i; position j is dropped. A cluster has
+// one nearest neighbour, so it is in at most one pair, and the n - 1 merges of the whole build
+// use exactly the ids n - 2 .. 0.
+__global__ void k_ploc_merge(const int* __restrict__ nn, int m, const int* __restrict__ cnode,
+                             const float4* __restrict__ clo, const float4* __restrict__ chi, int* next_id, int* left,
+                             int* right, int* parent, NodeBox nb, int* keep, int* onode, float4* olo, float4* ohi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int j = nn[i];
+    if (j >= 0 && nn[j] == i) {
+        if (j < i) {
+            keep[i] = 0;
+            return;
+        }
+        const int id = atomicSub(next_id, 1) - 1;
+        const int a = cnode[i], b = cnode[j];
+        left[id] = a;
+        right[id] = b;
+        parent[a] = id;
+        parent[b] = id;
+        const float4 la = clo[i], ha = chi[i], lb = clo[j], hb = chi[j];
+        const int cnt = __float_as_int(nb.lo[a].w) + __float_as_int(nb.lo[b].w);
+        const float4 lo = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), __int_as_float(cnt));
+        const float4 hi = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.f);
+        nb.lo[id] = lo;
+        nb.hi[id] = hi;
+        keep[i] = 1;
+        onode[i] = id;
+        olo[i] = lo;
+        ohi[i] = hi;
+    } else {
+        keep[i] = 1;
+        onode[i] = cnode[i];
+        olo[i] = clo[i];
+        ohi[i] = chi[i];
+    }
+}
+
+// The kept clusters, in order, into the next pass's arrays; the new count into *m_out.
+__global__ void k_ploc_compact(const int* __restrict__ keep, const int* __restrict__ pos, int m,
+                               const int* __restrict__ onode, const float4* __restrict__ olo,
+                               const float4* __restrict__ ohi, int* cnode, float4* clo, float4* chi, int* m_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    if (i == m - 1) *m_out = pos[i] + keep[i];
+    if (!keep[i]) return;
+    const int k = pos[i];
+    cnode[k] = onode[i];
+    clo[k] = olo[i];
+    chi[k] = ohi[i];
+}
+
+// The climbs below follow parent links that the merges wrote; each step checks the link
+// (an internal node, a bounded number of steps) and raises *err instead of leaving the tree.
+constexpr int kPlocMaxClimb = 1 << 16;
+
+// Depth-first numbering of the leaves: a leaf's first entry is the primitive count of the
+// left subtrees beside its path to the root (node 0).
+__global__ void k_ploc_leaf_first(int n, const int* left, const int* parent, NodeBox nb, int* first, int* err) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    int node = n - 1 + e, pos = 0;
+    for (int step = 0; node != 0; step++) {
+        const int p = parent[node];
+        if (p < 0 || p >= n - 1 || step >= kPlocMaxClimb) {
+            atomicOr(err, 1);
+            return;
+        }
+        if (left[p] != node) pos += __float_as_int(nb.lo[left[p]].w);
+        node = p;
+    }
+    first[n - 1 + e] = pos;
+}
+
+// An internal node's first entry is its leftmost leaf's: each leaf climbs while it is a left
+// child.
+__global__ void k_ploc_node_first(int n, const int* left, const int* parent, int* first, int* err) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    int node = n - 1 + e;
+    const int pos = first[node];
+    for (int step = 0; node != 0; step++) {
+        const int p = parent[node];
+        if (p < 0 || p >= n - 1 || step >= kPlocMaxClimb) {
+            atomicOr(err, 1);
+            return;
+        }
+        if (left[p] != node) break;
+        first[p] = pos;
+        node = p;
+    }
+}
+
+// Primitive ids in leaf-entry order: dfs_ids[first of leaf e] = sorted id e.
+__global__ void k_ploc_order(int n, const int* sids, const int* first, int* dfs_ids, int* err) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int f = first[n - 1 + e];
+    if (f < 0 || f >= n) {
+        atomicOr(err, 1);
+        return;
+    }
+    dfs_ids[f] = sids[e];
+}
+
 }  // namespace
 
 cudaError_t gpu_build_bvh(const float4* tri_p, int nt, const float4* sph, int ns, int width, int max_leaf,
                           GpuBvhScratch& sc, DevBuf& nodes_out, DevBuf& prims_out, GpuBvhInfo& info,
-                          cudaStream_t st) {
+                          cudaStream_t st, int algorithm) {
     const int n = nt + ns;
     if (n <= 0 || n >= (1 << 27) || max_leaf < 1 || max_leaf > kMaxLeafPrims ||
-        (width != 2 && width != 4 && width != 8))
+        (width != 2 && width != 4 && width != 8) || (algorithm != kGpuBvhLbvh && algorithm != kGpuBvhPloc))
         return cudaErrorInvalidValue;
+    const bool ploc = algorithm == kGpuBvhPloc;
     cudaError_t e;
     if ((e = grow<float4>(sc.box_lo, n)) || (e = grow<float4>(sc.box_hi, n)) || (e = grow<float4>(sc.cen, n)) ||
         (e = grow<unsigned>(sc.bounds, 16)) || (e = grow<unsigned long long>(sc.keys, 2 * (size_t)n)) ||
-        (e = grow<int>(sc.ids, 2 * (size_t)n)) || (e = grow<int>(sc.tree, 6 * (size_t)n + 4)) ||
+        (e = grow<int>(sc.ids, 3 * (size_t)n)) || (e = grow<int>(sc.tree, 7 * (size_t)n + 4)) ||
         (e = grow<float4>(sc.nbox, 4 * (size_t)n)) || (e = grow<int>(sc.visits, n)) ||
         (e = grow<int2>(sc.queue, 2 * (size_t)n + 2)) || (e = grow<int>(sc.counters, 8)))
         return e;
@@ -358,14 +522,64 @@ cudaError_t gpu_build_bvh(const float4* tri_p, int nt, const float4* sph, int ns
     int* left = sc.tree.as<int>();  // n - 1 internal nodes
     int* right = left + n;
     int* parent = right + n;        // 2n - 1 binary nodes
-    int* first = parent + 2 * n;    // internal nodes: range start and end
-    int* last = first + n;
+    int* first = parent + 2 * n;    // 2n - 1 binary nodes: first leaf entry
+    int* last = first + 2 * n;      // internal nodes: range end (LBVH)
     const NodeBox nb{sc.nbox.as<float4>(), sc.nbox.as<float4>() + 2 * (size_t)n};
-    if (n > 1) k_lb_tree<<<(n - 1 + 255) / 256, 256, 0, st>>>(skeys, n, left, right, parent, first, last);
     k_lb_leaf_boxes<<<gb, 256, 0, st>>>(sids, sc.box_lo.as<float4>(), sc.box_hi.as<float4>(), n, nb);
-    if ((e = cudaMemsetAsync(sc.visits.p, 0, (size_t)n * sizeof(int), st))) return e;
-    k_lb_refit<<<gb, 256, 0, st>>>(n, left, right, parent, nb, sc.visits.as<int>());
-    k_lb_prims<<<gb, 256, 0, st>>>(sids, n, in, prims_out.as<float4>());
+    const int* entry_ids = sids;  // primitive of each leaf entry
+    if (!ploc) {
+        if (n > 1) k_lb_tree<<<(n - 1 + 255) / 256, 256, 0, st>>>(skeys, n, left, right, parent, first, last);
+        k_lb_leaf_first<<<gb, 256, 0, st>>>(n, first);
+        if ((e = cudaMemsetAsync(sc.visits.p, 0, (size_t)n * sizeof(int), st))) return e;
+        k_lb_refit<<<gb, 256, 0, st>>>(n, left, right, parent, nb, sc.visits.as<int>());
+    } else {
+        if ((e = grow<float4>(sc.cbox, 6 * (size_t)n)) || (e = grow<int>(sc.cint, 7 * (size_t)n + 8))) return e;
+        float4* clo[2] = {sc.cbox.as<float4>(), sc.cbox.as<float4>() + n};
+        float4* chi[2] = {clo[1] + n, clo[1] + 2 * (size_t)n};
+        float4* olo = chi[1] + n;
+        float4* ohi = olo + n;
+        int* cnode[2] = {sc.cint.as<int>(), sc.cint.as<int>() + n};
+        int* nn = cnode[1] + n;
+        int* keep = nn + n;
+        int* pos = keep + n;
+        int* onode = pos + n;
+        int* ctr = onode + n;  // [0] next internal id, [1] next cluster count, [2] tree error
+        size_t stmp = 0;
+        if ((e = cub::DeviceScan::ExclusiveSum(nullptr, stmp, keep, pos, n, st))) return e;
+        if ((e = sc.scan_tmp.alloc(stmp + 16))) return e;
+        k_ploc_init<<<gb, 256, 0, st>>>(n, nb, cnode[0], clo[0], chi[0]);
+        if ((e = cudaMemsetAsync(parent, 0xFF, 2 * (size_t)n * sizeof(int), st))) return e;  // -1: none
+        if ((e = cudaMemsetAsync(first, 0xFF, 2 * (size_t)n * sizeof(int), st))) return e;
+        const int ctr0[3] = {n - 1, 0, 0};
+        if ((e = cudaMemcpyAsync(ctr, ctr0, sizeof(ctr0), cudaMemcpyHostToDevice, st))) return e;
+        int m = n, cur = 0, passes = 0;
+        while (m > 1) {
+            if (++passes > 4096) return cudaErrorInvalidValue;  // every pass merges at least one pair
+            const int g = (m + 255) / 256;
+            k_ploc_nn<<<g, 256, 0, st>>>(clo[cur], chi[cur], m, nn);
+            k_ploc_merge<<<g, 256, 0, st>>>(nn, m, cnode[cur], clo[cur], chi[cur], ctr, left, right, parent, nb, keep,
+                                            onode, olo, ohi);
+            if ((e = cub::DeviceScan::ExclusiveSum(sc.scan_tmp.p, stmp, keep, pos, m, st))) return e;
+            k_ploc_compact<<<g, 256, 0, st>>>(keep, pos, m, onode, olo, ohi, cnode[cur ^ 1], clo[cur ^ 1],
+                                              chi[cur ^ 1], ctr + 1);
+            int m2 = 0;
+            if ((e = cudaMemcpyAsync(&m2, ctr + 1, sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
+            if ((e = cudaStreamSynchronize(st))) return e;
+            if (m2 >= m || m2 < 1) return cudaErrorInvalidValue;
+            m = m2;
+            cur ^= 1;
+        }
+        k_ploc_leaf_first<<<gb, 256, 0, st>>>(n, left, parent, nb, first, ctr + 2);
+        k_ploc_node_first<<<gb, 256, 0, st>>>(n, left, parent, first, ctr + 2);
+        int* dfs_ids = ids + 2 * (size_t)n;
+        k_ploc_order<<<gb, 256, 0, st>>>(n, sids, first, dfs_ids, ctr + 2);
+        int terr = 0;
+        if ((e = cudaMemcpyAsync(&terr, ctr + 2, sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
+        if ((e = cudaStreamSynchronize(st))) return e;
+        if (terr) return cudaErrorInvalidValue;
+        entry_ids = dfs_ids;
+    }
+    k_lb_prims<<<gb, 256, 0, st>>>(entry_ids, n, in, prims_out.as<float4>());
     // abs_pad = 1e-3 x the scene diagonal, as the host builder
     unsigned hb[6];
     if ((e = cudaMemcpyAsync(hb, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st))) return e;

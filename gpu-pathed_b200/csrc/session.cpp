@@ -505,7 +505,8 @@ int Session::set_bvh(int width, int max_leaf) {
 
 int Session::set_bvh_builder(int gpu) {
     if (in_flight_) return fail(PT_ERR_STATE, "a frame is in flight");
-    const bool g = gpu != 0;
+    if (gpu < 0 || gpu > 2) return fail(PT_ERR_ARG, "builder must be 0 (host SAH), 1 (GPU LBVH) or 2 (GPU PLOC)");
+    const int g = gpu == 1 ? kGpuBvhLbvh : gpu == 2 ? kGpuBvhPloc : 0;
     if (g == bvh_gpu_) return PT_OK;
     bvh_gpu_ = g;
     if (have_scene_ && !batch_mode()) return set_bvh(bvh_width_, bvh_leaf_);  // rebuild with the new builder
@@ -756,7 +757,7 @@ int Session::upload_scene() {
                 tp[(size_t)i * 12 + v * 4 + k] = scene_.tri_p[(size_t)i * 9 + v * 3 + k];
                 tn[(size_t)i * 12 + v * 4 + k] = scene_.tri_n[(size_t)i * 9 + v * 3 + k];
             }
-    const bool gpu_tree = bvh_gpu_ && !batch_mode();
+    const bool gpu_tree = bvh_gpu_ != 0 && !batch_mode();
     if (!gpu_tree) {
         if ((r = check_cuda(upload(d_nodes_, bvh_.nodes, stream_), "upload BVH nodes"))) return r;
         if ((r = check_cuda(upload(d_prims_, bvh_.prims, stream_), "upload BVH primitives"))) return r;
@@ -779,7 +780,7 @@ int Session::upload_scene() {
         cudaEventRecord(e0, stream_);
         GpuBvhInfo info;
         const cudaError_t be = gpu_build_bvh(d_tri_p_.as<float4>(), nt, d_sph_.as<float4>(), scene_.num_sph(),
-                                             bvh_width_, bvh_leaf_, gbvh_, d_nodes_, d_prims_, info, stream_);
+                                             bvh_width_, bvh_leaf_, gbvh_, d_nodes_, d_prims_, info, stream_, bvh_gpu_);
         cudaEventRecord(e1, stream_);
         cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -1271,11 +1272,14 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     // paths of one frame: waves smaller than this split the frame
     const long long frame_paths = batch ? batch_paths_ : (long long)w_ * h_ * spp;
     struct Cand {
-        int width, sort, bps, block, rays, spec, wave, split, leaf;
+        int width, sort, bps, block, rays, spec, wave, split, leaf, builder;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
-        if ((c.width != bvh_width_ || c.leaf != bvh_leaf_) && (r = set_bvh(c.width, c.leaf))) return r;
+        if (c.width != bvh_width_ || c.leaf != bvh_leaf_ || c.builder != bvh_gpu_) {
+            bvh_gpu_ = c.builder;
+            if ((r = set_bvh(c.width, c.leaf))) return r;
+        }
         sort_mode_ = c.sort;
         shape_.blocks_per_sm = c.bps;
         shape_.block_extend = shape_.block_shadow = c.block;
@@ -1295,6 +1299,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.wave_paths = c.wave;
         res.split_shade = c.split == kShadeClasses ? 1 : c.split == kShadeAll128 ? 2 : 3;
         res.max_leaf = c.leaf;
+        res.bvh_builder = c.builder == kGpuBvhPloc ? 2 : c.builder == kGpuBvhLbvh ? 1 : 0;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1307,7 +1312,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
                        json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0),
                        json_int(line, "wave_paths", wave_paths_), json_int(line, "shade_kernel", kShadeClasses),
-                       json_int(line, "max_leaf", bvh_leaf_)};
+                       json_int(line, "max_leaf", bvh_leaf_), batch ? bvh_gpu_ : json_int(line, "builder", bvh_gpu_)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1341,7 +1346,8 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     };
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
-              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.shade_kernel, bvh_leaf_};
+              shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.shade_kernel, bvh_leaf_,
+              bvh_gpu_};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1369,6 +1375,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
             c.width = widths[i];
             if ((r = consider(c))) return r;
         }
+    if (!batch) {  // the tree's builder: the host's binned SAH or the device's PLOC clustering
+        Cand c = best;
+        c.builder = best.builder == kGpuBvhPloc ? 0 : kGpuBvhPloc;
+        if ((r = consider(c))) return r;
+    }
     if (!batch) {  // primitives per leaf (each a rebuild of the tree)
         const int start_leaf = best.leaf;
         for (int lf : {2, 4, 8})
@@ -1439,9 +1450,9 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
                          "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"shade_kernel\": %d, "
-                         "\"max_leaf\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
+                         "\"max_leaf\": %d, \"builder\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
                          key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, best.wave,
-                         best.split, best.leaf, best_ms, res.default_ms);
+                         best.split, best.leaf, best.builder, best_ms, res.default_ms);
             std::fclose(f);
         }
     }

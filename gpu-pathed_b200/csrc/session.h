@@ -229,7 +229,7 @@ private:
     uint64_t guide_seed_ = 0x9e11deULL;
     GuideFrame gframe_{};
     int ensure_guide();
-    bool bvh_gpu_ = false;
+    int bvh_gpu_ = 0;  // 0 host SAH, kGpuBvhLbvh, kGpuBvhPloc
     GpuBvhScratch gbvh_;
     int guide_nets_ = 1;
     int guide_ring_cap_ = 1 << 21;

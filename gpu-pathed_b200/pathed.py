@@ -126,7 +126,8 @@ class GuideInfo(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("bvh_width", "sort_materials", "blocks_per_sm", "block", "wave_paths")] + \
                [("best_ms", C.c_float), ("default_ms", C.c_float), ("trials", C.c_int), ("from_cache", C.c_int),
-                ("sort_rays", C.c_int), ("speculate", C.c_int), ("split_shade", C.c_int), ("max_leaf", C.c_int)]
+                ("sort_rays", C.c_int), ("speculate", C.c_int), ("split_shade", C.c_int), ("max_leaf", C.c_int),
+                ("bvh_builder", C.c_int)]
 
 
 class BatchScene(C.Structure):
@@ -567,9 +568,10 @@ class Session:
         out, self._pending_out = getattr(self, "_pending_out", None), None
         return out
 
-    def set_bvh_builder(self, gpu: bool):
-        """Build the BVH on the GPU (LBVH collapsed to the wide format) or on the host (SAH)."""
-        self._check(lib.pt_set_bvh_builder(self._h, int(bool(gpu))))
+    def set_bvh_builder(self, gpu):
+        """Build the BVH on the host (SAH; False or 0) or on the GPU, collapsed to the wide
+        format: True or 1 a linear BVH (Karras radix tree), 2 PLOC clustering."""
+        self._check(lib.pt_set_bvh_builder(self._h, int(gpu)))
 
     def set_bvh_quantized(self, on: bool):
         """Traverse quantized wide nodes (widths 4 and 8) instead of float nodes."""

@@ -149,6 +149,7 @@ typedef struct pt_tune_result {
     int split_shade;        /* as pt_launch_config.split_shade: 1 per-class kernels, 2 one kernel (128
                                registers), 3 one kernel (80 registers) */
     int max_leaf;           /* primitives per BVH leaf (2, 4 or 8; as pt_set_bvh) */
+    int bvh_builder;        /* as pt_set_bvh_builder: 0 host binned SAH, 2 GPU PLOC (single scenes) */
 } pt_tune_result;
 
 typedef struct pt_stats {
@@ -332,9 +333,9 @@ int pt_set_launch(pt_session* s, const pt_launch_config* cfg);
 int pt_get_launch(const pt_session* s, pt_launch_config* out);
 /* Autotuner (no counterpart in the reference, whose only tuning is SppOptimizer's spp
  * budget, src/spp_optimizer.cpp:8-29): times frames of `spp` samples on the loaded scene over
- * BVH width, material sorting, ray sorting, speculative traversal, persistent-grid size and block
- * size (coordinate descent),
- * applies the fastest and restarts accumulation. With cache_path, results are stored as one
+ * BVH width, the tree's builder (host SAH or GPU PLOC; single scenes) and leaf size, material
+ * sorting, the shade kernel, ray sorting, speculative traversal, persistent-grid size, block
+ * size and wave size (coordinate descent), applies the fastest and restarts accumulation. With cache_path, results are stored as one
  * JSON object per line keyed by scene size, material classes, resolution, spp, depth and
  * NEE, and a cached key is applied without measuring. */
 int pt_autotune(pt_session* s, int spp, const char* cache_path, pt_tune_result* out);
@@ -448,12 +449,15 @@ int pt_batch_get_info(const pt_session* s, int scene, pt_batch_info* out);
 /* Running mean (pass_only = 0) or last frame's pass of one scene: width * height * 3 floats. */
 int pt_batch_readback(pt_session* s, int scene, float* rgb, size_t n, int pass_only);
 
-/* BVH construction on the GPU (gpu = 1): primitive boxes, 63-bit Morton codes, radix sort,
- * a Karras radix tree, bottom-up bounds and a top-down collapse to the same wide-node format,
- * run when the scene is next uploaded (the first render or query after a load or edit).
- * gpu = 0 (default) selects the host's binned-SAH builder. Closest hits are identical with
- * either tree. No counterpart in the reference, whose CUDA backend scans every primitive
- * (src/world.cu:5-41). Batches always use the host builder. */
+/* BVH construction on the GPU: primitive boxes, 63-bit Morton codes and a radix sort, then a
+ * binary tree, either (gpu = 1) a Karras radix tree with bottom-up bounds, or (gpu = 2)
+ * locally-ordered agglomerative clustering (PLOC: mutual nearest neighbours by union surface
+ * area within 16 positions in Morton order, merged pass by pass), and a top-down collapse to
+ * the same wide-node format, run when the scene is next uploaded (the first render or query
+ * after a load or edit). gpu = 0 (default) selects the host's binned-SAH builder. Closest hits
+ * are identical with any tree. No counterpart in the reference, whose CUDA backend scans
+ * every primitive (src/world.cu:5-41). Batches always use the host builder. Other values:
+ * PT_ERR_ARG. */
 int pt_set_bvh_builder(pt_session* s, int gpu);
 
 /* quantized = 1: traversal reads quantized copies of the wide nodes (widths 4 and 8: 64 and

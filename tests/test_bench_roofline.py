@@ -19,6 +19,8 @@ def test_shape_key():
     assert bench.extend_shape_key(8, 3, _launch(1, 16, 256, 1 << 24)) == "w8_l3_s1_b16x256_q24"
     assert bench.extend_shape_key(4, 8, _launch(3)).startswith("w4_l8_s1_")
     assert bench.extend_shape_key(2, 1, _launch(4)).startswith("w2_l1_s0_")  # shadow-only speculation
+    assert bench.extend_shape_key(4, 2, _launch(2), 2) == "w4_l2_s0_b8x128_q25_ploc"
+    assert bench.extend_shape_key(4, 2, _launch(2), 1) == "w4_l2_s0_b8x128_q25_lbvh"
 
 
 def test_instruction_counts_by_shape(tmp_path, monkeypatch):
@@ -32,6 +34,7 @@ def test_instruction_counts_by_shape(tmp_path, monkeypatch):
         "scene-a@w8_l2_s1_b8x128_q25 warp_inst_per_query: 70.0\n"
         "scene-a@w4_l2_s0_b8x128_q25 warp_inst_per_query: 120.0\n"
         "scene-a@w4_l2_s1_b8x128_q25 fp32_flop_per_query: 300.0\n"
+        "scene-a@w4_l2_s1_b8x128_q25_ploc warp_inst_per_query: 60.0\n"
         "scene-b@w4_l2_s0_b8x128_q25 warp_inst_per_query: 50.0\n")
     monkeypatch.setattr(bench, "ROOT", str(tmp_path))
     f = bench._ncu_shape_per_query
@@ -47,6 +50,10 @@ def test_instruction_counts_by_shape(tmp_path, monkeypatch):
     assert f("scene-a", "w8_l4_s1_b8x128_q25", k) == (70.0, "w8_l2_s1_b8x128_q25")
     assert f("scene-a", "w4_l4_s0_b8x128_q25", k) == (120.0, "w4_l2_s0_b8x128_q25")
     assert f("scene-a", "w4_l8_s1_b8x128_q25", "fp32_flop_per_query") == (300.0, "w4_l2_s1_b8x128_q25")
+    # a tree built by another builder is matched first by its builder
+    assert f("scene-a", "w4_l2_s1_b8x128_q25_ploc", k) == (60.0, "w4_l2_s1_b8x128_q25_ploc")
+    assert f("scene-a", "w8_l4_s0_b16x256_q24_ploc", k) == (60.0, "w4_l2_s1_b8x128_q25_ploc")
+    assert f("scene-a", "w4_l2_s1_b8x128_q25_lbvh", k) == (100.0, "w4_l2_s1_b8x128_q25")
     # a workload or field without a capture gives nothing
     assert f("scene-c", "w4_l2_s0_b8x128_q25", k) == (None, None)
     assert f("scene-b", "w4_l2_s0_b8x128_q25", "fp32_flop_per_query") == (None, None)
