@@ -769,10 +769,12 @@ def guided_time_to_relmse(budget_spp=256, ref_spp=2048, res=1024):
     ref = slit_reference(ref_spp, res)
     t_plain, target = plain_to_budget(ref, budget_spp, res)
     crossed, spp, steps = guided_to_target(ref, t_plain, target, res)
-    # the configuration as written: guide fraction 0.5, Adam lr 1e-3, one 2^18-sample step per frame
-    aw_crossed, aw_spp, aw_steps = guided_to_target(ref, t_plain, target, res, fraction=0.5, steps=1, lr=1e-3,
+    # the configuration's hyperparameters as written: guide fraction 0.5, Adam lr 1e-3, 2^18
+    # samples per Adam step; the steps per frame, which it leaves open, on the automatic schedule
+    aw_crossed, aw_spp, aw_steps = guided_to_target(ref, t_plain, target, res, fraction=0.5, steps=0, lr=1e-3,
                                                     batch=1 << 18)
-    as_written = {"fraction": 0.5, "lr": 1e-3, "samples_per_step": 1 << 18, "steps_per_frame": 1,
+    as_written = {"fraction": 0.5, "lr": 1e-3, "samples_per_step": 1 << 18,
+                  "steps_per_frame": "automatic: 16 for the first 512 steps, 4 up to 1024, then 2",
                   "guided_ms": aw_crossed, "guided_spp": aw_spp, "guide_steps": aw_steps,
                   "speedup": (t_plain / aw_crossed) if aw_crossed else None}
     return {"workload": f"slit-room {res}x{res} depth 10 (2002 + 1310720 triangles, env through a 0.05 slit)",

@@ -1382,7 +1382,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     }
     if (!batch) {  // primitives per leaf (each a rebuild of the tree)
         const int start_leaf = best.leaf;
-        for (int lf : {2, 4, 8})
+        for (int lf : {2, 4, 8, 16})
             if (lf != start_leaf) {
                 Cand c = best;
                 c.leaf = lf;

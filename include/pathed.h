@@ -148,7 +148,7 @@ typedef struct pt_tune_result {
     int speculate;          /* as pt_launch_config.speculate: 1 both stages, 2 off, 3 closest hit, 4 shadow */
     int split_shade;        /* as pt_launch_config.split_shade: 1 per-class kernels, 2 one kernel (128
                                registers), 3 one kernel (80 registers) */
-    int max_leaf;           /* primitives per BVH leaf (2, 4 or 8; as pt_set_bvh) */
+    int max_leaf;           /* primitives per BVH leaf (2, 4, 8 or 16; as pt_set_bvh) */
     int bvh_builder;        /* as pt_set_bvh_builder: 0 host binned SAH, 2 GPU PLOC (single scenes) */
 } pt_tune_result;
 

@@ -188,20 +188,23 @@ def test_overlapped_shadow_stage_does_not_change_images(case, graph):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("config", [2, 3])
-def test_leaf_sizes_do_not_change_images(config):
-    """the leaf sizes the autotuner picks from (2, 4, 8) change the tree, not the hits: with
-    the same launch shape the frames are bit-identical"""
+@pytest.mark.parametrize("builder", [0, 2], ids=["sah", "ploc"])
+def test_leaf_sizes_do_not_change_images(config, builder):
+    """the trees the autotuner picks from (host SAH or device PLOC, leaves of 2, 4, 8 or 16)
+    change the visiting order, not the hits: with the same launch shape the frames are
+    bit-identical"""
     s = pathed.Session(64, 64)
+    s.set_bvh_builder(builder)
     s.load_config(config, level=4)
     imgs = []
-    for leaf in (2, 4, 8):
+    for leaf in (2, 4, 8, 16):
         s.set_bvh(4, leaf)
         assert s.counts().bvh_max_leaf <= leaf
         s.reset()
         s.render(2)
         imgs.append(s.readback().copy())
     s.close()
-    assert np.array_equal(imgs[0], imgs[1]) and np.array_equal(imgs[0], imgs[2])
+    assert all(np.array_equal(imgs[0], im) for im in imgs[1:])
 
 
 @pytest.mark.gpu
