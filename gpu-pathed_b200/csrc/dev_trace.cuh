@@ -385,14 +385,14 @@ __device__ __forceinline__ int stack_pop(const float4* __restrict__ nodes, bool 
 }
 
 // One internal-node visit of a live query (`cur` >= 0): test the node's children, push the
-// farther hits (nearest first for closest hit, hits first for any hit), descend into the
-// first, or pop the stack when none was hit. The query ends (`alive` false) when the stack
+// farther hits (nearest first for closest hit; for any hit, nearest first with `near`, else in
+// the node's order), descend into the first, or pop the stack when none was hit. The query ends (`alive` false) when the stack
 // runs empty, or gives up with `overflow` set when it would exceed `max_depth` entries.
 template <int W, bool ANY, bool CNT>
 __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool quant, const RayPre& r, float tmin,
                                           float tmax, int2* __restrict__ stk, int stride, int max_depth,
                                           const Hit& best, int& cur, int& sp, bool& alive, int& overflow,
-                                          TraceWork* work) {
+                                          TraceWork* work, bool near = false) {
     constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
     NodeView<W> nv;
     if (quant) load_qnode<W>(nodes + (size_t)cur * (qnode_bytes(W) / 16), nv);
@@ -400,14 +400,15 @@ __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool
     if (CNT) work->nodes++;
     const float tcur = best.prim == kMissPrim ? tmax : best.t;
     const float tlim = tcur * kBoxSlack;
-    // sort keys: nearest first for closest hit; for any hit, hit children first in slot order
+    // sort keys: nearest first for closest hit (and any hit with `near`); otherwise hit
+    // children first in slot order
     uint32_t key[W];
     int nhit = 0;
 #pragma unroll
     for (int k = 0; k < W; k++) {
         const float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k], tmin, tlim);
         const bool hit = te != __int_as_float(0x7f800000) && nv.child[k] != kEmptyChild;
-        if (ANY) key[k] = hit ? (uint32_t)k : kMissKey | (uint32_t)k;
+        if (ANY && !near) key[k] = hit ? (uint32_t)k : kMissKey | (uint32_t)k;
         else key[k] = hit ? (__float_as_uint(key_dist(te)) | (uint32_t)k) : kMissKey | (uint32_t)k;
         nhit += hit ? 1 : 0;
     }
@@ -484,12 +485,12 @@ __device__ __forceinline__ void traverse_round(const float4* __restrict__ nodes,
                                                bool quant, bool spec, const RayPre& r, float tmin, float tmax,
                                                int2* __restrict__ stk, int stride, int max_depth, Hit& best,
                                                int& cur, int& pend, int& sp, bool& alive, bool& hit_any,
-                                               int& overflow, TraceWork* work, bool wt = false) {
+                                               int& overflow, TraceWork* work, bool wt = false, bool near = false) {
     // ---- phase 1: internal nodes, while some live lane has found no leaf
     while (__any_sync(0xffffffffu, alive && cur >= 0 && pend == kEmptyChild)) {
         if (alive && cur >= 0) {
             node_step<W, ANY, CNT>(nodes, quant, r, tmin, tmax, stk, stride, max_depth, best, cur, sp, alive, overflow,
-                                   work);
+                                   work, near);
             if (spec) {
                 if (!alive && !overflow && pend != kEmptyChild) {
                     alive = true;  // the stack ran empty: only the parked leaf is left

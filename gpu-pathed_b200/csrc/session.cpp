@@ -705,7 +705,8 @@ int Session::set_launch(const pt_launch_config* c) {
         return fail(PT_ERR_ARG, "invalid wave size or blocks per SM");
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
         c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 4 || c->split_shade < 0 ||
-        c->split_shade > 3 || c->overlap_shadow < 0 || c->overlap_shadow > 2)
+        c->split_shade > 3 || c->overlap_shadow < 0 || c->overlap_shadow > 2 || c->shadow_order < 0 ||
+        c->shadow_order > 2)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
@@ -720,6 +721,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->speculate) shape_.speculate = speculate_bits(c->speculate);
     if (c->split_shade) shape_.shade_kernel = c->split_shade == 1 ? kShadeClasses : c->split_shade == 2 ? kShadeAll128 : kShadeAll80;
     if (c->overlap_shadow) shape_.overlap_shadow = c->overlap_shadow == 1 ? 1 : 0;
+    if (c->shadow_order) shape_.shadow_near = c->shadow_order == 1 ? 1 : 0;
     return PT_OK;
 }
 
@@ -736,6 +738,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->speculate = speculate_code(shape_.speculate);
     c->split_shade = shape_.shade_kernel == kShadeClasses ? 1 : shape_.shade_kernel == kShadeAll128 ? 2 : 3;
     c->overlap_shadow = shape_.overlap_shadow ? 1 : 2;
+    c->shadow_order = shape_.shadow_near ? 1 : 2;
 }
 
 int Session::upload_materials() {
@@ -1272,7 +1275,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     // paths of one frame: waves smaller than this split the frame
     const long long frame_paths = batch ? batch_paths_ : (long long)w_ * h_ * spp;
     struct Cand {
-        int width, sort, bps, block, rays, spec, wave, split, leaf, builder;
+        int width, sort, bps, block, rays, spec, wave, split, leaf, builder, near;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
@@ -1287,6 +1290,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         shape_.speculate = c.spec;
         wave_paths_ = c.wave;
         shape_.shade_kernel = c.split;
+        shape_.shadow_near = c.near;
         return PT_OK;
     };
     auto report = [&](const Cand& c) {
@@ -1300,6 +1304,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.split_shade = c.split == kShadeClasses ? 1 : c.split == kShadeAll128 ? 2 : 3;
         res.max_leaf = c.leaf;
         res.bvh_builder = c.builder == kGpuBvhPloc ? 2 : c.builder == kGpuBvhLbvh ? 1 : 0;
+        res.shadow_order = c.near ? 1 : 2;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1312,7 +1317,8 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 Cand c{json_int(line, "bvh_width", 4), json_int(line, "sort", 0), json_int(line, "blocks_per_sm", 16),
                        json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0),
                        json_int(line, "wave_paths", wave_paths_), json_int(line, "shade_kernel", kShadeClasses),
-                       json_int(line, "max_leaf", bvh_leaf_), batch ? bvh_gpu_ : json_int(line, "builder", bvh_gpu_)};
+                       json_int(line, "max_leaf", bvh_leaf_), batch ? bvh_gpu_ : json_int(line, "builder", bvh_gpu_),
+                       json_int(line, "shadow_near", shape_.shadow_near)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1347,7 +1353,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
               shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.shade_kernel, bvh_leaf_,
-              bvh_gpu_};
+              bvh_gpu_, shape_.shadow_near};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1417,6 +1423,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                 if ((r = consider(c))) return r;
             }
     }
+    if (nee_ && max_depth_ > 1) {  // the shadow stage's child order: nearest first or the node's order
+        Cand c = best;
+        c.near = best.near ? 0 : 1;
+        if ((r = consider(c))) return r;
+    }
     for (int bps : {8, 24}) {
         Cand c = best;
         c.bps = bps;
@@ -1450,9 +1461,10 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
                          "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"shade_kernel\": %d, "
-                         "\"max_leaf\": %d, \"builder\": %d, \"ms\": %.4f, \"default_ms\": %.4f}\n",
+                         "\"max_leaf\": %d, \"builder\": %d, \"shadow_near\": %d, \"ms\": %.4f, "
+                         "\"default_ms\": %.4f}\n",
                          key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, best.wave,
-                         best.split, best.leaf, best.builder, best_ms, res.default_ms);
+                         best.split, best.leaf, best.builder, best.near, best_ms, res.default_ms);
             std::fclose(f);
         }
     }

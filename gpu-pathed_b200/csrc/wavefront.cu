@@ -887,6 +887,7 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
     const int lane = threadIdx.x & 31;
     const int refill_idle = p.shape.refill_idle;
     const bool spec = (p.shape.speculate & kSpeculateShadow) != 0;
+    const bool near = p.shape.shadow_near != 0;  // children nearest first
     const bool quant = W >= 4 && Q == 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.stats->rays_shadow, (unsigned long long)count);
     int2* const st = stk + threadIdx.x;
@@ -930,7 +931,7 @@ __global__ void k_shadow(FrameParams p, int depth, long long wave_first, long lo
         if (!__any_sync(0xffffffffu, alive)) break;
         const SceneDevice& sc = B ? scb : p.sc;
         traverse_round<W, true, CNT>(sc.nodes, sc.prims, quant, spec, r, kShadowTMin, tmax, st, stride, p.stack_depth,
-                                     h, cur, pend, sp, alive, occ, of, &work, Q == 2);
+                                     h, cur, pend, sp, alive, occ, of, &work, Q == 2, near);
         if (slot >= 0 && !alive) {  // the query ended: occluded, or the stack ran empty
             const int i = slot;
             slot = -1;

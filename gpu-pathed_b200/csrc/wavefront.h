@@ -87,6 +87,7 @@ struct LaunchShape {
     int speculate = 0;        // kSpeculate* bits: stages that park a lane's first leaf and descend on
     int shade_kernel = 1;     // plain frames' shade stage: kShadeAll128, kShadeClasses, kShadeAll80
     int overlap_shadow = 1;   // shadow stage of depth d on the side stream beside extend of d + 1
+    int shadow_near = 0;      // shadow stage: a node's hit children visited nearest first (else in order)
 };
 
 // The side streams of a frame whose independent stages overlap (LaunchShape.overlap_shadow):

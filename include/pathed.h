@@ -131,6 +131,8 @@ typedef struct pt_launch_config {
                               closest-hit stage of depth d + 1, each filling the other's tail
                               (default; the shade stage of depth d + 1 waits for both), 2: one
                               stream; images are the same either way */
+    int shadow_order;      /* shadow stage: 1 a node's hit children are visited nearest first, 2 in
+                              the node's order (default); the same occlusion results either way */
 } pt_launch_config;
 
 /* Result of pt_autotune. */
@@ -150,6 +152,7 @@ typedef struct pt_tune_result {
                                registers), 3 one kernel (80 registers) */
     int max_leaf;           /* primitives per BVH leaf (2, 4, 8 or 16; as pt_set_bvh) */
     int bvh_builder;        /* as pt_set_bvh_builder: 0 host binned SAH, 2 GPU PLOC (single scenes) */
+    int shadow_order;       /* as pt_launch_config.shadow_order: 1 nearest first, 2 the node's order */
 } pt_tune_result;
 
 typedef struct pt_stats {
@@ -334,8 +337,9 @@ int pt_get_launch(const pt_session* s, pt_launch_config* out);
 /* Autotuner (no counterpart in the reference, whose only tuning is SppOptimizer's spp
  * budget, src/spp_optimizer.cpp:8-29): times frames of `spp` samples on the loaded scene over
  * BVH width, the tree's builder (host SAH or GPU PLOC; single scenes) and leaf size, material
- * sorting, the shade kernel, ray sorting, speculative traversal, persistent-grid size, block
- * size and wave size (coordinate descent), applies the fastest and restarts accumulation. With cache_path, results are stored as one
+ * sorting, the shade kernel, ray sorting, speculative traversal, the shadow stage's child
+ * order, persistent-grid size, block size and wave size (coordinate descent), applies the
+ * fastest and restarts accumulation. With cache_path, results are stored as one
  * JSON object per line keyed by scene size, material classes, resolution, spp, depth and
  * NEE, and a cached key is applied without measuring. */
 int pt_autotune(pt_session* s, int spp, const char* cache_path, pt_tune_result* out);

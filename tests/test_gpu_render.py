@@ -187,6 +187,23 @@ def test_overlapped_shadow_stage_does_not_change_images(case, graph):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", [(1, None), (3, 4)], ids=lambda c: f"cfg{c[0]}")
+def test_shadow_child_order_does_not_change_images(case):
+    """the shadow stage visiting a node's hit children nearest first or in the node's order
+    finds the same occluders, so frames are bit-identical"""
+    imgs = []
+    for order in (2, 1):
+        s = pathed.Session(64, 48)
+        s.load_config(case[0], level=case[1])
+        s.set_launch(shadow_order=order)
+        assert s.get_launch()["shadow_order"] == order
+        s.render(4)
+        imgs.append(s.readback().copy())
+        s.close()
+    assert np.array_equal(imgs[0], imgs[1])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("config", [2, 3])
 @pytest.mark.parametrize("builder", [0, 2], ids=["sah", "ploc"])
 def test_leaf_sizes_do_not_change_images(config, builder):
