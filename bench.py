@@ -484,7 +484,7 @@ def _per_config(cfg, steps, warmup, flush, l2_gbs, tune_cache, with_reference):
            "spheres": counts.num_spheres,
            "autotuned": {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays", "speculate",
                                                 "blocks_per_sm", "block", "wave_paths", "split_shade", "max_leaf",
-                                                "bvh_builder", "shadow_order")},
+                                                "bvh_builder", "shadow_order", "fuse_camera")},
            "roofline": _roofline(wl["name"], counts, prof_count, st_count, stage_ms, stage_launches, steps, l2_gbs,
                                  None, shape)}
     if with_reference:
@@ -668,7 +668,7 @@ def run_ours(args):
             line["config"]["autotuned"] = {k: tuned[k] for k in ("bvh_width", "sort_materials", "sort_rays",
                                                                "speculate", "blocks_per_sm", "block", "wave_paths",
                                                                "split_shade", "max_leaf", "bvh_builder",
-                                                               "shadow_order", "best_ms", "default_ms")}
+                                                               "shadow_order", "fuse_camera", "best_ms", "default_ms")}
             if tuned["bvh_builder"] == 2:
                 line["config"]["bvh_builder"] = "gpu-ploc (autotuned)"
         print(json.dumps(line), flush=True)

@@ -706,7 +706,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->sort_materials < 0 || c->sort_materials > 3 || c->use_graph < 0 || c->use_graph > 2 ||
         c->sort_rays < 0 || c->sort_rays > 2 || c->speculate < 0 || c->speculate > 4 || c->split_shade < 0 ||
         c->split_shade > 3 || c->overlap_shadow < 0 || c->overlap_shadow > 2 || c->shadow_order < 0 ||
-        c->shadow_order > 2)
+        c->shadow_order > 2 || c->fuse_camera < 0 || c->fuse_camera > 2)
         return fail(PT_ERR_ARG, "invalid sort or graph mode");
     if (c->refill_idle < 0 || c->refill_idle > 32) return fail(PT_ERR_ARG, "refill_idle must be in [1, 32]");
     if (c->wave_paths) wave_paths_ = c->wave_paths;
@@ -722,6 +722,7 @@ int Session::set_launch(const pt_launch_config* c) {
     if (c->split_shade) shape_.shade_kernel = c->split_shade == 1 ? kShadeClasses : c->split_shade == 2 ? kShadeAll128 : kShadeAll80;
     if (c->overlap_shadow) shape_.overlap_shadow = c->overlap_shadow == 1 ? 1 : 0;
     if (c->shadow_order) shape_.shadow_near = c->shadow_order == 1 ? 1 : 0;
+    if (c->fuse_camera) shape_.fuse_camera = c->fuse_camera == 1 ? 1 : 0;
     return PT_OK;
 }
 
@@ -739,6 +740,7 @@ void Session::get_launch(pt_launch_config* c) const {
     c->split_shade = shape_.shade_kernel == kShadeClasses ? 1 : shape_.shade_kernel == kShadeAll128 ? 2 : 3;
     c->overlap_shadow = shape_.overlap_shadow ? 1 : 2;
     c->shadow_order = shape_.shadow_near ? 1 : 2;
+    c->fuse_camera = shape_.fuse_camera ? 1 : 2;
 }
 
 int Session::upload_materials() {
@@ -1275,7 +1277,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     // paths of one frame: waves smaller than this split the frame
     const long long frame_paths = batch ? batch_paths_ : (long long)w_ * h_ * spp;
     struct Cand {
-        int width, sort, bps, block, rays, spec, wave, split, leaf, builder, near;
+        int width, sort, bps, block, rays, spec, wave, split, leaf, builder, near, fuse;
     };
     auto apply = [&](const Cand& c) -> int {
         int r;
@@ -1291,6 +1293,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         wave_paths_ = c.wave;
         shape_.shade_kernel = c.split;
         shape_.shadow_near = c.near;
+        shape_.fuse_camera = c.fuse;
         return PT_OK;
     };
     auto report = [&](const Cand& c) {
@@ -1305,6 +1308,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         res.max_leaf = c.leaf;
         res.bvh_builder = c.builder == kGpuBvhPloc ? 2 : c.builder == kGpuBvhLbvh ? 1 : 0;
         res.shadow_order = c.near ? 1 : 2;
+        res.fuse_camera = c.fuse ? 1 : 2;
     };
     if (cache_path) {
         FILE* f = std::fopen(cache_path, "r");
@@ -1318,7 +1322,8 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
                        json_int(line, "block", 128), json_int(line, "sort_rays", 0), json_int(line, "speculate", 0),
                        json_int(line, "wave_paths", wave_paths_), json_int(line, "shade_kernel", kShadeClasses),
                        json_int(line, "max_leaf", bvh_leaf_), batch ? bvh_gpu_ : json_int(line, "builder", bvh_gpu_),
-                       json_int(line, "shadow_near", shape_.shadow_near)};
+                       json_int(line, "shadow_near", shape_.shadow_near),
+                       json_int(line, "fuse_camera", shape_.fuse_camera)};
                 std::fclose(f);
                 int r;
                 if ((r = apply(c))) return r;
@@ -1353,7 +1358,7 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
     const int prims = scene_.num_tri() + scene_.num_sph();
     Cand best{bvh_width_, sort_mode_ >= 0 ? sort_mode_ : (material_classes_ >= 2 ? 1 : 0), shape_.blocks_per_sm,
               shape_.block_extend, shape_.sort_rays, shape_.speculate, wave_paths_, shape_.shade_kernel, bvh_leaf_,
-              bvh_gpu_, shape_.shadow_near};
+              bvh_gpu_, shape_.shadow_near, shape_.fuse_camera};
     float best_ms;
     int r;
     if ((r = measure(best, best_ms))) return r;
@@ -1428,6 +1433,11 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
         c.near = best.near ? 0 : 1;
         if ((r = consider(c))) return r;
     }
+    if (!guiding_) {  // camera rays computed where used (the 128-register shade kernel) or queued
+        Cand c = best;
+        c.fuse = best.fuse ? 0 : 1;
+        if ((r = consider(c))) return r;
+    }
     for (int bps : {8, 24}) {
         Cand c = best;
         c.bps = bps;
@@ -1461,10 +1471,10 @@ int Session::autotune(int spp, const char* cache_path, pt_tune_result* out) {
             std::fprintf(f,
                          "{\"key\": \"%s\", \"bvh_width\": %d, \"sort\": %d, \"blocks_per_sm\": %d, \"block\": %d, "
                          "\"sort_rays\": %d, \"speculate\": %d, \"wave_paths\": %d, \"shade_kernel\": %d, "
-                         "\"max_leaf\": %d, \"builder\": %d, \"shadow_near\": %d, \"ms\": %.4f, "
-                         "\"default_ms\": %.4f}\n",
+                         "\"max_leaf\": %d, \"builder\": %d, \"shadow_near\": %d, \"fuse_camera\": %d, "
+                         "\"ms\": %.4f, \"default_ms\": %.4f}\n",
                          key.c_str(), best.width, best.sort, best.bps, best.block, best.rays, best.spec, best.wave,
-                         best.split, best.leaf, best.builder, best.near, best_ms, res.default_ms);
+                         best.split, best.leaf, best.builder, best.near, best.fuse, best_ms, res.default_ms);
             std::fclose(f);
         }
     }

@@ -146,54 +146,90 @@ __device__ __forceinline__ SceneDevice batch_scene_view(const FrameParams& p, in
     return sc;
 }
 
+// The camera ray of path i of the wave (Camera::generateRay with the sample's two jitter
+// draws, camera.h:40-61), its queue tag and the path's random state after the draws. The
+// closest-hit, guide-inference and shade stages of depth 0 each compute it from the path
+// index instead of reading it from the queue: the same operations on the same inputs, so
+// every stage sees the same ray, and no camera stage writes 56 bytes per path for them.
+template <bool B>
+__device__ __forceinline__ void camera_path(const FrameParams& p, long long wave_first, int i, V& o, V& d,
+                                            int& tag, uint64_t& st) {
+    const long long gp = wave_first + i;
+    long long local = gp;
+    int sid = 0, spp = p.spp, width = p.width;
+    const CameraParams* cp = &p.dyn->cam;
+    uint64_t sd = p.dyn->seed, sb = p.dyn->sample_base;
+    if (B) {
+        sid = batch_find(p.batch_path_base, p.num_scenes, gp);
+        const BatchScene& b = p.batch[sid];
+        local = gp - b.path_base;
+        spp = b.spp;
+        width = b.width;
+        cp = &b.cam;
+        sd = b.seed;
+        sb = b.sample_base;
+    }
+    const int pixel = (int)(local / spp);
+    const int s = (int)(local - (long long)pixel * spp);
+    const int row = pixel / width;
+    const int col = pixel - row * width;
+    const uint64_t inc = pcg_inc((uint32_t)pixel);
+    st = pcg_seed(sd, sb + (uint64_t)s, (uint32_t)pixel);
+    const float xi1 = pcg_uniform(st, inc);
+    const float xi2 = pcg_uniform(st, inc);
+    camera_ray(*cp, row, col, xi1, xi2, o, d);
+    tag = i | (sid << kTagPathBits);
+}
+
+// The origin and direction records of queue slot `slot` at `depth` (depth 0 of a wave whose
+// camera rays are not queued: the camera ray of path `slot`, with no MIS pdf).
+template <bool B>
+__device__ __forceinline__ void queue_ray(const FrameParams& p, const PathQueue& q, int depth, long long wave_first,
+                                          int slot, float4& o4, float4& d4) {
+    if (depth == 0 && p.cam_fused) {
+        V o, d;
+        int tag;
+        uint64_t st;
+        camera_path<B>(p, wave_first, slot, o, d, tag, st);
+        o4 = make_float4(o.x, o.y, o.z, __int_as_float(tag));
+        d4 = make_float4(d.x, d.y, d.z, 0.f);
+    } else {
+        o4 = q.o[slot];
+        d4 = q.d[slot];
+    }
+}
+
+// The depth-0 queue of a wave: its camera rays, unit throughput, random states, and zero
+// radiance per path. Used when the shade kernel of the frame reads the queue at depth 0.
 template <bool B>
 __global__ void k_camera(FrameParams p, long long wave_first, int n) {
     const PathQueue q = p.q[0];
-    __shared__ CameraParams cam;
-    __shared__ uint64_t seed, sample_base;
-    if (!B) {
-        if (threadIdx.x == 0) {
-            cam = p.dyn->cam;
-            seed = p.dyn->seed;
-            sample_base = p.dyn->sample_base;
-        }
-        __syncthreads();
-    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const long long gp = wave_first + i;
-        long long local = gp;
-        int sid = 0, spp = p.spp, width = p.width;
-        const CameraParams* cp = &cam;
-        uint64_t sd = 0, sb = 0;
-        if (B) {
-            sid = batch_find(p.batch_path_base, p.num_scenes, gp);
-            const BatchScene& b = p.batch[sid];
-            local = gp - b.path_base;
-            spp = b.spp;
-            width = b.width;
-            cp = &b.cam;
-            sd = b.seed;
-            sb = b.sample_base;
-        } else {
-            sd = seed;
-            sb = sample_base;
-        }
-        const int pixel = (int)(local / spp);
-        const int s = (int)(local - (long long)pixel * spp);
-        const int row = pixel / width;
-        const int col = pixel - row * width;
-        const uint64_t inc = pcg_inc((uint32_t)pixel);
-        uint64_t st = pcg_seed(sd, sb + (uint64_t)s, (uint32_t)pixel);
-        const float xi1 = pcg_uniform(st, inc);
-        const float xi2 = pcg_uniform(st, inc);
         V o, d;
-        camera_ray(*cp, row, col, xi1, xi2, o, d);
-        q.o[i] = make_float4(o.x, o.y, o.z, __int_as_float(i | (sid << kTagPathBits)));
+        int tag;
+        uint64_t st;
+        camera_path<B>(p, wave_first, i, o, d, tag, st);
+        q.o[i] = make_float4(o.x, o.y, o.z, __int_as_float(tag));
         q.d[i] = make_float4(d.x, d.y, d.z, 0.f);
         q.beta[i] = make_float4(1.f, 1.f, 1.f, __int_as_float(1));  // camera ray: no MIS
         q.rng[i] = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
         p.L[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        p.counters->ray_count[0] = n;
+        atomicAdd(&p.stats->rays_camera, (unsigned long long)n);
+    }
+}
+
+// A wave's start when the frame's shade kernel computes its depth-0 rays itself (the kernel
+// of all materials at 128 registers, plain frames: p.cam_fused): the closest-hit and shade
+// stages of depth 0 take each camera ray from camera_path, so no queue records are written;
+// the shade stage of depth 0 writes each path's first radiance. Without any depth, the paths'
+// radiance is zero.
+__global__ void k_wave_start(FrameParams p, int n) {
+    if (p.max_depth == 0)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            p.L[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         p.counters->ray_count[0] = n;
         atomicAdd(&p.stats->rays_camera, (unsigned long long)n);
@@ -287,7 +323,7 @@ __global__ void __launch_bounds__(kRaySortBlock) k_ray_scatter(FrameParams p, in
 // queries ended. With kSpeculateExtend set, traverse_round parks each lane's first leaf and
 // keeps descending while another lane of the warp still searches for one.
 template <int W, bool CNT, bool B, int Q>
-__global__ void k_extend(FrameParams p, int depth) {
+__global__ void k_extend(FrameParams p, int depth, long long wave_first) {
     extern __shared__ int2 stk[];
     __shared__ int s_class[8];  // the block's hits per material class
     const int count = p.counters->ray_count[depth];
@@ -331,7 +367,8 @@ __global__ void k_extend(FrameParams p, int depth) {
                 const int k = base + __popc(~busy & lanemask_lt());
                 if (slot < 0 && k < count) {
                     slot = sorted ? p.ray_index[k] : k;
-                    const float4 o = q.o[slot], d = q.d[slot];
+                    float4 o, d;
+                    queue_ray<B>(p, q, depth, wave_first, slot, o, d);
                     r = make_raypre(mkv(o), mkv(d));
                     int last = p.max_depth - 1;
                     if (B) {
@@ -621,12 +658,24 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
         GuideRecord rec;
         if (i < count) {
             const int slot = AHEAD ? cur_slot : slot_of(i);
-            const float4 o4 = q.o[slot];
-            const float4 d4 = q.d[slot];
-            const float4 b4 = q.beta[slot];
+            float4 o4, d4, b4;
             float4 h4 = q.hit[slot];
             uint2 rng0 = make_uint2(0u, 0u);
-            if (AHEAD) rng0 = q.rng[slot];
+            if (AHEAD && depth == 0) {  // camera ray of path `slot` (p.cam_fused): unit throughput, no MIS
+                V o, d;
+                int tg;
+                uint64_t st0;
+                camera_path<B>(p, wave_first, slot, o, d, tg, st0);
+                o4 = make_float4(o.x, o.y, o.z, __int_as_float(tg));
+                d4 = make_float4(d.x, d.y, d.z, 0.f);
+                b4 = make_float4(1.f, 1.f, 1.f, __int_as_float(1));
+                rng0 = make_uint2((uint32_t)st0, (uint32_t)(st0 >> 32));
+            } else {
+                o4 = q.o[slot];
+                d4 = q.d[slot];
+                b4 = q.beta[slot];
+                if (AHEAD) rng0 = q.rng[slot];
+            }
             // a negative t: the BSDF-direct ray stopped closer (hitd), this is the continuation's hit
             const bool split = __float_as_int(h4.x) < 0;
             h4.x = fabsf(h4.x);
@@ -778,7 +827,9 @@ __device__ __forceinline__ void shade_body(const FrameParams& p, int depth, long
                     }
                 }
             }
-            if (!is_zero(Ladd)) {
+            if (AHEAD && depth == 0) {  // the path's first radiance (p.cam_fused: no earlier stage wrote it)
+                p.L[path] = make_float4(Ladd.x, Ladd.y, Ladd.z, 0.f);
+            } else if (!is_zero(Ladd)) {
                 float4 l = p.L[path];
                 l.x += Ladd.x;
                 l.y += Ladd.y;
@@ -1246,8 +1297,13 @@ cudaError_t enqueue_class_shades(const FrameParams& p, int d, long long wave_fir
 }
 
 template <int W, bool CNT, bool B>
-cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwaves, cudaStream_t stream,
+cudaError_t enqueue_waves(const FrameParams& p_in, const WaveRange* waves, int nwaves, cudaStream_t stream,
                           StageMarks* marks, const SideStream* side) {
+    // depth-0 rays are computed where they are used when every depth-0 stage can do so: plain
+    // frames whose shade stage is the kernel of all materials at 128 registers
+    FrameParams p = p_in;
+    const bool classes = p.shape.shade_kernel == kShadeClasses && p.shape.sort_materials && p.class_mask;
+    p.cam_fused = p.shape.fuse_camera && !p.guide_mode && !classes && p.shape.shade_kernel != kShadeAll80 ? 1 : 0;
     const int grid_e = p.num_sms * p.shape.blocks_per_sm;
     // shadow stage of depth d on the side stream: forked after the shade stage of d, joined
     // before the shade stage of d + 1 (which adds to the same path radiance after it); the
@@ -1274,7 +1330,8 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
             if ((e = cudaMemsetAsync(p.grec_count, 0, sizeof(int), stream))) return e;
         }
         mark(-1);
-        k_camera<B><<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
+        if (p.cam_fused) k_wave_start<<<p.max_depth == 0 ? (n + 255) / 256 : 1, 256, 0, stream>>>(p, n);
+        else k_camera<B><<<(n + 255) / 256, 256, 0, stream>>>(p, wave_first, n);
         mark(kStageCamera);
         for (int d = 0; d < p.max_depth; d++) {
             if (sort_rays && d > 0) {  // keys and counts come from the previous shade launch
@@ -1282,12 +1339,12 @@ cudaError_t enqueue_waves(const FrameParams& p, const WaveRange* waves, int nwav
                 mark(kStageSort);
             }
             if (p.sc.watertight) {
-                k_extend<W, CNT, B, 2><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+                k_extend<W, CNT, B, 2><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d, wave_first);
             } else if constexpr (W >= 4) {
-                if (p.sc.node_q) k_extend<W, CNT, B, 1><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
-                else k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+                if (p.sc.node_q) k_extend<W, CNT, B, 1><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d, wave_first);
+                else k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d, wave_first);
             } else {
-                k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d);
+                k_extend<W, CNT, B, 0><<<grid_e, p.shape.block_extend, smem_e, stream>>>(p, d, wave_first);
             }
             mark(kStageExtend);
             if (p.shape.sort_materials) {

@@ -88,6 +88,7 @@ struct LaunchShape {
     int shade_kernel = 1;     // plain frames' shade stage: kShadeAll128, kShadeClasses, kShadeAll80
     int overlap_shadow = 1;   // shadow stage of depth d on the side stream beside extend of d + 1
     int shadow_near = 0;      // shadow stage: a node's hit children visited nearest first (else in order)
+    int fuse_camera = 1;      // depth-0 rays computed where used when the shade kernel allows (cam_fused)
 };
 
 // The side streams of a frame whose independent stages overlap (LaunchShape.overlap_shadow):
@@ -196,6 +197,7 @@ struct FrameParams {
     LaunchShape shape;
     // ---- learned path guiding (guide.cuh) ----
     int guide_mode;          // 0 off, 1 collect training data only, 2 guided sampling + collect
+    int cam_fused;           // set per wave: depth-0 rays computed where used, not queued (see k_wave_start)
     float gfrac;             // probability of sampling the guide at a non-delta vertex
     int consistent_mis;      // NEE weights use the BSDF's true sampling density (microfacet)
     int guide_tc;            // guide inference on tcgen05 / tensor memory (single-scene frames)

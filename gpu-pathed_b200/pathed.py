@@ -109,7 +109,8 @@ class SceneExport(C.Structure):
 class LaunchConfig(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "wave_paths", "block_extend", "block_shade", "block_shadow", "blocks_per_sm", "sort_materials",
-        "use_graph", "sort_rays", "refill_idle", "speculate", "split_shade", "overlap_shadow", "shadow_order")]
+        "use_graph", "sort_rays", "refill_idle", "speculate", "split_shade", "overlap_shadow", "shadow_order",
+        "fuse_camera")]
 
 
 class Stats(C.Structure):
@@ -127,7 +128,7 @@ class TuneResult(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("bvh_width", "sort_materials", "blocks_per_sm", "block", "wave_paths")] + \
                [("best_ms", C.c_float), ("default_ms", C.c_float), ("trials", C.c_int), ("from_cache", C.c_int),
                 ("sort_rays", C.c_int), ("speculate", C.c_int), ("split_shade", C.c_int), ("max_leaf", C.c_int),
-                ("bvh_builder", C.c_int), ("shadow_order", C.c_int)]
+                ("bvh_builder", C.c_int), ("shadow_order", C.c_int), ("fuse_camera", C.c_int)]
 
 
 class BatchScene(C.Structure):

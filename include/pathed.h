@@ -133,6 +133,10 @@ typedef struct pt_launch_config {
                               stream; images are the same either way */
     int shadow_order;      /* shadow stage: 1 a node's hit children are visited nearest first, 2 in
                               the node's order (default); the same occlusion results either way */
+    int fuse_camera;       /* 1 (default): in plain frames whose shade stage is the one kernel at 128
+                              registers, the closest-hit and shade stages of depth 0 compute each
+                              camera ray from its path index instead of reading it from a queue
+                              that a camera stage wrote; 2: always queued; the same images */
 } pt_launch_config;
 
 /* Result of pt_autotune. */
@@ -153,6 +157,7 @@ typedef struct pt_tune_result {
     int max_leaf;           /* primitives per BVH leaf (2, 4, 8 or 16; as pt_set_bvh) */
     int bvh_builder;        /* as pt_set_bvh_builder: 0 host binned SAH, 2 GPU PLOC (single scenes) */
     int shadow_order;       /* as pt_launch_config.shadow_order: 1 nearest first, 2 the node's order */
+    int fuse_camera;        /* as pt_launch_config.fuse_camera */
 } pt_tune_result;
 
 typedef struct pt_stats {

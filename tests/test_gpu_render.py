@@ -187,6 +187,32 @@ def test_overlapped_shadow_stage_does_not_change_images(case, graph):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", [(0, None), (1, None), (3, 4), ("batch", None)], ids=lambda c: f"cfg{c[0]}")
+def test_fused_camera_rays_do_not_change_images(case):
+    """camera rays computed from the path index in the depth-0 closest-hit and shade stages
+    (no camera queue) give the frames of the queued camera rays, bit for bit, across waves"""
+    imgs = []
+    for fuse in (2, 1):
+        s = pathed.Session(64, 48)
+        if case[0] == "batch":
+            s.load_batch(pathed.batch_generate(0x5EED + 4, 6))
+        else:
+            s.load_config(case[0], level=case[1])
+        s.set_launch(split_shade=2, fuse_camera=fuse, wave_paths=20000)
+        assert s.get_launch()["fuse_camera"] == fuse
+        s.set_seed(3)
+        for _ in range(2):
+            s.render(0 if case[0] == "batch" else 4)
+        if case[0] == "batch":
+            imgs.append([s.batch_readback(k).copy() for k in range(6)])
+        else:
+            imgs.append([s.readback().copy()])
+        s.close()
+    for a, b in zip(imgs[0], imgs[1]):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", [(1, None), (3, 4)], ids=lambda c: f"cfg{c[0]}")
 def test_shadow_child_order_does_not_change_images(case):
     """the shadow stage visiting a node's hit children nearest first or in the node's order
