@@ -428,6 +428,7 @@ __global__ void k_extend(FrameParams p, int depth, long long wave_first) {
     if (CNT) flush_work(work, &p.stats->extend_nodes, &p.stats->extend_prims);
 }
 
+constexpr int kSortItems = 4;  // queue entries per thread and chunk of the material sort
 __global__ void k_sort(FrameParams p, int depth) {
     const int count = p.counters->ray_count[depth];
     const PathQueue q = p.q[depth & 1];
@@ -438,33 +439,47 @@ __global__ void k_sort(FrameParams p, int depth) {
         off[c] = acc;
         acc += p.counters->sort_count[depth][c];
     }
-    // Slots are reserved per block: warps add their class counts into shared counters, then
-    // one global atomic per class and block reserves the block's range (the grid is capped at
-    // a few blocks per SM and strides over the queue).
+    // Slots are reserved per block and chunk of kSortItems x blockDim.x entries: warps add
+    // their class counts into shared counters, then one global atomic per class and chunk
+    // reserves the chunk's range (the grid is capped at a few blocks per SM and strides over
+    // the queue). Several entries per thread share each chunk's barriers and atomics.
     __shared__ int s_cnt[8], s_base[8];
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x; base < count; base += stride) {
+    const int stride = gridDim.x * blockDim.x * kSortItems;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    for (int base = blockIdx.x * blockDim.x * kSortItems; base < count; base += stride) {
         if (threadIdx.x < 8) s_cnt[threadIdx.x] = 0;
         __syncthreads();
-        const int i = base + threadIdx.x;
-        const bool valid = i < count;
-        const int key = valid ? q.key[i] : 7;
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
-        const int lane = threadIdx.x & 31;
-        const int leader = __ffs(peers) - 1;
-        int b = 0;
-        if (valid && lane == leader) b = atomicAdd(&s_cnt[key], __popc(peers));
+        int key[kSortItems], b[kSortItems], leader[kSortItems];
+        unsigned peers[kSortItems];
+#pragma unroll
+        for (int j = 0; j < kSortItems; j++) {
+            const int i = base + j * blockDim.x + threadIdx.x;
+            key[j] = i < count ? q.key[i] : 7;  // 7: no entry (no class uses it)
+        }
+#pragma unroll
+        for (int j = 0; j < kSortItems; j++) {
+            const int i = base + j * blockDim.x + threadIdx.x;
+            peers[j] = __match_any_sync(0xffffffffu, key[j]);
+            leader[j] = __ffs(peers[j]) - 1;
+            b[j] = 0;
+            if (i < count && lane == leader[j]) b[j] = atomicAdd(&s_cnt[key[j]], __popc(peers[j]));
+        }
         __syncthreads();
         if (threadIdx.x < kMaterialClasses && s_cnt[threadIdx.x] > 0)
             s_base[threadIdx.x] = atomicAdd(&p.counters->sort_fill[depth][threadIdx.x], s_cnt[threadIdx.x]);
         __syncthreads();
-        b = __shfl_sync(0xffffffffu, b, leader);
-        if (valid) {
-            int ko = 0;
 #pragma unroll
-            for (int c = 0; c < kMaterialClasses; c++)
-                if (c == key) ko = off[c] + s_base[c];
-            p.sort_index[ko + b + __popc(peers & lanemask_lt())] = i;
+        for (int j = 0; j < kSortItems; j++) {
+            const int i = base + j * blockDim.x + threadIdx.x;
+            const int bj = __shfl_sync(0xffffffffu, b[j], leader[j]);
+            if (i < count) {
+                int ko = 0;
+#pragma unroll
+                for (int c = 0; c < kMaterialClasses; c++)
+                    if (c == key[j]) ko = off[c] + s_base[c];
+                p.sort_index[ko + bj + __popc(peers[j] & lt)] = i;
+            }
         }
         __syncthreads();  // s_cnt / s_base are reused by the next chunk
     }
@@ -1348,7 +1363,8 @@ cudaError_t enqueue_waves(const FrameParams& p_in, const WaveRange* waves, int n
             }
             mark(kStageExtend);
             if (p.shape.sort_materials) {
-                k_sort<<<std::min((n + 255) / 256, p.num_sms * 8), 256, 0, stream>>>(p, d);
+                k_sort<<<std::min((n + 256 * kSortItems - 1) / (256 * kSortItems), p.num_sms * 8), 256, 0, stream>>>(
+                    p, d);
                 mark(kStageSort);
             }
             if (p.guide_mode == 2 && d < p.max_depth - 1) {
