@@ -1222,11 +1222,23 @@ __global__ void k_accumulate(FrameParams p, int first_pixel, int npix, long long
     }
     float r = 0.f, g = 0.f, b = 0.f;
     const float inv_spp = (float)spp;
-    for (int s = 0; s < spp; s++) {  // passRadiances += Li / spp (path_tracer.cu:258-262)
-        const float4 l = p.L[path0 + s];
-        r += l.x / inv_spp;
-        g += l.y / inv_spp;
-        b += l.z / inv_spp;
+    if ((spp & (spp - 1)) == 0) {
+        // a power-of-two spp: x / spp and x * (1 / spp) are the same correctly rounded value
+        // (the reciprocal is exact), without a division per sample
+        const float rs = 1.f / inv_spp;
+        for (int s = 0; s < spp; s++) {  // passRadiances += Li / spp (path_tracer.cu:258-262)
+            const float4 l = p.L[path0 + s];
+            r += l.x * rs;
+            g += l.y * rs;
+            b += l.z * rs;
+        }
+    } else {
+        for (int s = 0; s < spp; s++) {
+            const float4 l = p.L[path0 + s];
+            r += l.x / inv_spp;
+            g += l.y / inv_spp;
+            b += l.z / inv_spp;
+        }
     }
     p.pass_rgb[3 * (size_t)pixel + 0] = r;
     p.pass_rgb[3 * (size_t)pixel + 1] = g;
