@@ -149,6 +149,18 @@ def test_launch_config_host_state():
         assert s.get_launch()["speculate"] == code
     with pytest.raises(pathed.PathedError):
         s.set_launch(speculate=5)
+    # concurrent shadow stage and fused camera rays on by default, node-order shadow traversal
+    assert cfg["overlap_shadow"] == 1 and cfg["fuse_camera"] == 1 and cfg["shadow_order"] == 2
+    for field in ("overlap_shadow", "shadow_order", "fuse_camera", "split_shade"):
+        start = s.get_launch()[field]
+        for code in (1, 2):
+            s.set_launch(**{field: code})
+            assert s.get_launch()[field] == code
+        s.set_launch(**{field: start})
+        for bad in (-1, 5):
+            with pytest.raises(pathed.PathedError) as e:
+                s.set_launch(**{field: bad})
+            assert e.value.code == pathed.PT_ERR_ARG
     s.close()
 
 
