@@ -288,6 +288,54 @@ __device__ __forceinline__ void load_node(const float4* __restrict__ p, NodeView
     }
 }
 
+// A float node (W = 4 or 8) read in the ray's octant order: per axis the near planes (the
+// lower bounds where the ray's direction component is positive, the upper ones where it is
+// negative) into lo_*, the far planes into hi_*. For a box with lower <= upper bound, the near
+// plane's slab distance is the smaller one (fmaf is monotone in its first operand for a fixed
+// nonzero factor), so the slab test needs no min/max per axis and gives the same entry and exit
+// distances bit for bit. The choice of plane is an address offset per load.
+template <int W>
+__device__ __forceinline__ void load_node_oct(const float4* __restrict__ p, const RayPre& r, NodeView<W>& nv) {
+    static_assert(W == 4 || W == 8, "octant loads need whole float4 planes");
+    constexpr int A = W / 4;  // float4s per plane
+    const int sx = __float_as_int(r.ix) < 0 ? A : 0;
+    const int sy = __float_as_int(r.iy) < 0 ? A : 0;
+    const int sz = __float_as_int(r.iz) < 0 ? A : 0;
+    float4 raw[7 * A];
+#pragma unroll
+    for (int a = 0; a < A; a++) {
+        raw[0 * A + a] = __ldg(p + 0 * A + sx + a);
+        raw[1 * A + a] = __ldg(p + 1 * A - sx + a);
+        raw[2 * A + a] = __ldg(p + 2 * A + sy + a);
+        raw[3 * A + a] = __ldg(p + 3 * A - sy + a);
+        raw[4 * A + a] = __ldg(p + 4 * A + sz + a);
+        raw[5 * A + a] = __ldg(p + 5 * A - sz + a);
+        raw[6 * A + a] = __ldg(p + 6 * A + a);
+    }
+    const float* f = reinterpret_cast<const float*>(raw);
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        nv.lo_x[k] = f[0 * W + k];
+        nv.hi_x[k] = f[1 * W + k];
+        nv.lo_y[k] = f[2 * W + k];
+        nv.hi_y[k] = f[3 * W + k];
+        nv.lo_z[k] = f[4 * W + k];
+        nv.hi_z[k] = f[5 * W + k];
+        nv.child[k] = __float_as_int(f[6 * W + k]);
+    }
+}
+
+// Slab test on near and far planes (load_node_oct): the entry distance, or +inf when empty.
+__device__ __forceinline__ float box_entry_nf(const RayPre& r, float nx, float fx, float ny, float fy, float nz,
+                                              float fz, float tmin, float tlim) {
+    const float tnx = fmaf(nx, r.ix, -r.ox), tfx = fmaf(fx, r.ix, -r.ox);
+    const float tny = fmaf(ny, r.iy, -r.oy), tfy = fmaf(fy, r.iy, -r.oy);
+    const float tnz = fmaf(nz, r.iz, -r.oz), tfz = fmaf(fz, r.iz, -r.oz);
+    const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+    const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tlim));
+    return (tn <= tf * kBoxSlack) ? tn : __int_as_float(0x7f800000);
+}
+
 // Scale of a quantized node's axis: the FP32 power of two with biased exponent e.
 __device__ __forceinline__ float qscale(uint32_t e) { return __uint_as_float((e & 0xFFu) << 23); }
 
@@ -395,7 +443,9 @@ __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool
                                           TraceWork* work, bool near = false) {
     constexpr int kNF4 = sizeof(BvhNode<W>) / 16;
     NodeView<W> nv;
+    constexpr bool kOct = W >= 4 && !ANY;  // closest hit: float nodes read in octant order (near, far planes)
     if (quant) load_qnode<W>(nodes + (size_t)cur * (qnode_bytes(W) / 16), nv);
+    else if constexpr (kOct) load_node_oct<W>(nodes + (size_t)cur * kNF4, r, nv);
     else load_node<W>(nodes + (size_t)cur * kNF4, nv);
     if (CNT) work->nodes++;
     const float tcur = best.prim == kMissPrim ? tmax : best.t;
@@ -406,7 +456,10 @@ __device__ __forceinline__ void node_step(const float4* __restrict__ nodes, bool
     int nhit = 0;
 #pragma unroll
     for (int k = 0; k < W; k++) {
-        const float te = box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k], tmin, tlim);
+        const float te =
+            kOct && !quant
+                ? box_entry_nf(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k], tmin, tlim)
+                : box_entry(r, nv.lo_x[k], nv.hi_x[k], nv.lo_y[k], nv.hi_y[k], nv.lo_z[k], nv.hi_z[k], tmin, tlim);
         const bool hit = te != __int_as_float(0x7f800000) && nv.child[k] != kEmptyChild;
         if (ANY && !near) key[k] = hit ? (uint32_t)k : kMissKey | (uint32_t)k;
         else key[k] = hit ? (__float_as_uint(key_dist(te)) | (uint32_t)k) : kMissKey | (uint32_t)k;
