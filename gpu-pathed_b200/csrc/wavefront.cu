@@ -147,10 +147,10 @@ __device__ __forceinline__ SceneDevice batch_scene_view(const FrameParams& p, in
 }
 
 // The camera ray of path i of the wave (Camera::generateRay with the sample's two jitter
-// draws, camera.h:40-61), its queue tag and the path's random state after the draws. The
-// closest-hit, guide-inference and shade stages of depth 0 each compute it from the path
-// index instead of reading it from the queue: the same operations on the same inputs, so
-// every stage sees the same ray, and no camera stage writes 56 bytes per path for them.
+// draws, camera.h:40-61), its queue tag and the path's random state after the draws. k_camera
+// queues it; in frames that do not queue camera rays (p.cam_fused) the closest-hit and shade
+// stages of depth 0 each compute it from the path index instead: the same operations on the
+// same inputs, so both stages see the same ray, and no camera stage writes 56 bytes per path.
 template <bool B>
 __device__ __forceinline__ void camera_path(const FrameParams& p, long long wave_first, int i, V& o, V& d,
                                             int& tag, uint64_t& st) {
